@@ -1,0 +1,132 @@
+// fsm_internal.h -- descriptors shared by the host planner and the sm_100a kernels.
+//
+// Layout in HBM (per event, all in the reference cell order
+// is = (DIM_Y*DIM_ETA)*ix + DIM_ETA*iy + ieta):
+//   2D: nodes[is]  float4 (F, F_x*DX, F_y*DY, F_xy*DX*DY): the bicubic node data
+//       of F = e/(2 pi), 16 B/cell, read by the stream kernel through a shared-
+//       memory footprint of each output tile.
+//   3D: efield[is] float e (fm^-4) and the caller's nB[is] float, read through L1.
+//   T[10][DIM], J[4][DIM]: moments written by the stream kernels, read by the
+//   Landau kernel.  Outputs e,P,Pi,u[4],pi[10],nB,V[4] are [comp][DIM] floats.
+#pragma once
+#include <stdint.h>
+
+#ifndef __CUDACC__
+struct float2_h { float x, y; };
+struct float4_h { float x, y, z, w; };
+#define FSM_FLOAT2 float2_h
+#define FSM_FLOAT4 float4_h
+#else
+#define FSM_FLOAT2 float2
+#define FSM_FLOAT4 float4
+#endif
+
+namespace fsm {
+
+constexpr int kTileX = 16;   // 2D output tile: x extent (slow index)
+constexpr int kTileY = 16;   // 2D output tile: y extent (fast index)
+constexpr int kThreads2D = kTileX * kTileY;
+constexpr int kThreads3D = 256;
+constexpr int kThreadsLandau = 128;
+constexpr int kPhiChunk = 16;  // FP32 partial sums are folded into Kahan totals every 16 phi_p
+
+// Natural-spline axis data for the 2D prep kernels (host computed, double):
+// h[i] = x[i+1]-x[i] of the float grid coordinates, and the elimination
+// factors f[k] / modified diagonals dg[k] of the tridiagonal system for the
+// interior second derivatives (k = 0..n-3).
+struct SplineAxis {
+  const double* h;
+  const double* f;
+  const double* dg;
+  int n;
+};
+
+struct Ev2D {
+  int NX, NY, NPHI, NR;
+  float DX, DY, DTAU, TAU;
+  float xmin, ymin, xmax_i, ymax_i;  // grid origin and spline domain (src/FreeStream.cpp:113,142-146)
+  float inv_dx, inv_dy;
+  float d_phip;
+  int Rx, Ry;        // footprint halo in cells
+  int use_smem;      // footprint fits the block's shared memory
+  int tiles_y;       // tiles along y
+  const FSM_FLOAT2* cs;  // [NPHI] (cos phi_p, sin phi_p), float as the reference computes them
+  // prep
+  const float* e_gev;    // input
+  SplineAxis ax, ay;
+  double* zx;            // scratch [DIM]
+  double* zy;            // scratch [DIM]
+  FSM_FLOAT4* nodes;     // [DIM]
+  // outputs of the stream kernel
+  float* T;              // [10][DIM]
+};
+
+// Per-(ieta, irap) quantities of the 3D path, computed on the host with the
+// reference's float arithmetic (src/FreeStream.cpp:174-201, LandauMatch.cpp:36-55).
+struct RapEta {
+  float D;      // TAU*cosh(rap-eta_new) - TAU0*cosh(rap-eta): transverse shift length
+  float efrac;  // fractional part of the shifted eta index
+  int efl;      // floor of the shifted eta index (sample valid iff 1 <= efl < NE-1)
+  float A;      // 1/cosh(d),  d = rap - eta                (rows 1,2)
+  float B;      // 1/cosh(d)^2                             (rows 4,5,7)
+  float C;      // tanh(d)/(TAU cosh d)                     (rows 6,8)
+  float Dt;     // tanh(d)/TAU                              (row 3)
+  float E;      // tanh(d)^2/TAU^2                          (row 9)
+};
+
+struct Ev3D {
+  int NX, NY, NE, NR, NPHI;
+  int r_lo, r_hi;  // live rapidity nodes [r_lo, r_hi)
+  int baryon;
+  float DX, DY;
+  float xmin, ymin;
+  float inv_dx, inv_dy;
+  float norm, normB, d_phip, DRAP;
+  const FSM_FLOAT2* cs;   // [NPHI]
+  const RapEta* re;       // [NE*NR]
+  const float* rapf;      // [NE*NR] energy rapidity weight  cosh^2 d exp(-d^2/2 sigma^2)
+  const float* rapfB;     // [NE*NR] baryon weight on the uniform rapidity grid
+  const float* jac;       // [NR] tan-map Jacobian (src/LandauMatch.cpp:92-93)
+  const float* e_gev;     // input
+  float* efield;          // converted energy density (fm^-4)
+  const float* nB;        // input baryon density
+  float* T;               // [10][DIM]
+  float* J;               // [4][DIM]
+  long long cell_begin;   // first global cell index of this event in the 3D work list
+};
+
+struct EvLandau {
+  int DIM;
+  int is3d;
+  int baryon;
+  int eos;
+  int viscous;
+  float TAU;
+  const float* T;
+  const float* J;
+  float *e, *P, *Pi, *u, *pi, *nB, *V;
+  long long cell_begin;   // first global cell index of this event in the Landau work list
+};
+
+// Work-list entries: a block of spline lines / cells of one event.
+struct LineBlock {
+  int ev, begin;
+};
+struct CellBlock {
+  int ev, begin;
+};
+
+// One 2D output tile of one event.
+struct Tile2D {
+  int ev, x0, y0, pad;
+};
+
+// Counters reset before each launch sequence.
+struct Counters {
+  int tile2d;
+  int block3d;
+  int fallback;
+  int pad;
+};
+
+}  // namespace fsm

@@ -1,0 +1,324 @@
+// fsm_plan.cpp -- parameters, status strings and per-event planning (host).
+//
+// Compiled with the host compiler and -ffp-contract=off: every float table
+// entry below repeats the reference's own expression with its float/double
+// mixing, so the kernels see the same shift lengths, node angles and index
+// floors the reference computes (a one-ulp difference in a shift can move a
+// sample across the in-grid test at src/FreeStream.cpp:213).
+#include "fsm_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace fsm {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int output_components(bool baryon) { return baryon ? 36 : 27; }
+
+static inline float tanmap_w(int irap, int NR) {  // src/FreeStream.cpp:174
+  return (float)(-.9975 + (float)irap * (1.995 / (float)(NR - 1)));
+}
+
+fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
+                      std::string* why) {
+  EventPlan& E = *out;
+  E = EventPlan();
+  fsm_params p = in;
+  auto fail = [&](fsm_status s, const char* msg) {
+    if (why) *why = msg;
+    return s;
+  };
+  if (p.DIM_X < 4 || p.DIM_Y < 4)
+    return fail(FSM_ERR_INVALID_ARG, "DIM_X and DIM_Y must be >= 4 (bicubic spline minimum)");
+  if (p.DIM_ETA < 1 || p.DIM_RAP < 1 || p.DIM_PHIP < 1)
+    return fail(FSM_ERR_INVALID_ARG, "DIM_ETA, DIM_RAP and DIM_PHIP must be >= 1");
+  if (!(p.DX > 0) || !(p.DY > 0)) return fail(FSM_ERR_INVALID_ARG, "DX and DY must be > 0");
+  if (!(p.DTAU >= 0)) return fail(FSM_ERR_INVALID_ARG, "DTAU must be >= 0");
+  E.is3d = p.DIM_ETA > 1;
+  if (E.is3d) {
+    if (p.DIM_RAP < 2)
+      return fail(FSM_ERR_UNSUPPORTED,
+                  "3D needs DIM_RAP >= 2 (the reference's tan-map node is NaN for DIM_RAP = 1)");
+    if (!(p.DETA > 0) || !(p.TAU0 > 0))
+      return fail(FSM_ERR_INVALID_ARG, "3D needs DETA > 0 and TAU0 > 0");
+  }
+  E.baryon = p.BARYON != 0;
+  if (E.baryon && !E.is3d)
+    return fail(FSM_ERR_UNSUPPORTED, "BARYON with DIM_ETA = 1 is not implemented on the GPU path");
+  long long dim = (long long)p.DIM_X * p.DIM_Y * p.DIM_ETA;
+  if (dim > (1ll << 30)) return fail(FSM_ERR_TOO_LARGE, "grid too large");
+  p.DIM = (int)dim;
+  p.TAU = p.TAU0 + p.DTAU;  // src/FreestreamMilne.cpp:177-178
+
+  const float hbarc = 0.197326938;
+  if (p.E_DEP_FS == 1) {  // src/FreeStream.cpp:389-417 on the converted profile
+    if (!host_e_gev)
+      return fail(FSM_ERR_UNSUPPORTED, "E_DEP_FS=1 needs the profile on the host (fsm_run_event)");
+    float numerator = 0.0, denominator = 0.0;
+    float rescale = 1.0, lower_tolerance = 1.0e-7;
+    for (int i = 0; i < p.DIM; i++) {
+      float eps = host_e_gev[i] * rescale / (float)hbarc + lower_tolerance;
+      numerator += (eps * eps);
+      denominator += eps;
+    }
+    float e_T = numerator / (denominator + 1.0e-7);
+    e_T = e_T * hbarc;
+    float tau_fs = p.TAU_R * std::pow((e_T / p.E_R), p.ALPHA);
+    p.DTAU = tau_fs;
+    p.TAU = p.TAU0 + p.DTAU;
+  }
+  if (!(p.TAU > 0)) return fail(FSM_ERR_INVALID_ARG, "TAU0 + DTAU must be > 0");
+  {  // phi_p arc-length rule, src/FreestreamMilne.cpp:329-332
+    float min_dx_dy = std::min(p.DX, p.DY);
+    int nphip = int(std::ceil((2.0 * M_PI * p.DTAU) / min_dx_dy));
+    p.DIM_PHIP = std::max(p.DIM_PHIP, nphip);
+  }
+  if (p.DIM_PHIP > 16384) return fail(FSM_ERR_TOO_LARGE, "DIM_PHIP above 16384");
+  E.p = p;
+  E.DIM = p.DIM;
+  const int NX = p.DIM_X, NY = p.DIM_Y, NE = p.DIM_ETA, NR = p.DIM_RAP, NP = p.DIM_PHIP;
+
+  // grid origin (src/FreeStream.cpp:113-115) and spline domain (:142-146)
+  E.xmin = (-1.0) * ((float)(NX - 1) / 2.0) * p.DX;
+  E.ymin = (-1.0) * ((float)(NY - 1) / 2.0) * p.DY;
+  E.etamin = (-1.0) * ((float)(NE - 1) / 2.0) * p.DETA;
+  E.xmax_i = (float)(NX - 1) * p.DX + E.xmin;
+  E.ymax_i = (float)(NY - 1) * p.DY + E.ymin;
+  E.d_phip = (2.0 * M_PI) / float(NP);  // src/LandauMatch.cpp:74
+
+  // phi_p nodes (src/FreeStream.cpp:179, cos/sin of a float)
+  E.cs.resize(NP);
+  for (int k = 0; k < NP; ++k) {
+    float phip = float(k) * (2.0 * M_PI) / float(NP);
+    E.cs[k].x = std::cos(phip);
+    E.cs[k].y = std::sin(phip);
+  }
+
+  if (!E.is3d) {
+    // natural-spline axes on the float grid coordinates (src/FreeStream.cpp:129-140)
+    auto axis = [](int n, float d, float lo, std::vector<double>& h, std::vector<double>& f,
+                   std::vector<double>& dg) {
+      std::vector<double> xv(n);
+      for (int i = 0; i < n; ++i) {
+        float xf = (float)i * d + lo;
+        xv[i] = xf;
+      }
+      h.resize(n - 1);
+      for (int i = 0; i + 1 < n; ++i) h[i] = xv[i + 1] - xv[i];
+      int m = n - 2;
+      f.assign(std::max(m, 1), 0.0);
+      dg.assign(std::max(m, 1), 0.0);
+      for (int k = 0; k < m; ++k) dg[k] = 2.0 * (h[k] + h[k + 1]);
+      for (int k = 1; k < m; ++k) {
+        f[k] = h[k] / dg[k - 1];
+        dg[k] -= f[k] * h[k];
+      }
+    };
+    axis(NX, p.DX, E.xmin, E.hx, E.fx, E.dgx);
+    axis(NY, p.DY, E.ymin, E.hy, E.fy, E.dgy);
+    E.Rx = (int)std::ceil(p.DTAU / p.DX) + 2;
+    E.Ry = (int)std::ceil(p.DTAU / p.DY) + 2;
+    E.samples = (double)p.DIM * NP;
+    E.ref_samples = (double)p.DIM * NR * NP;
+    return FSM_OK;
+  }
+
+  // ---------------------------------------------------------------- 3D tables
+  const float TAU = p.TAU, TAU0 = p.TAU0, DETA = p.DETA;
+  {
+    float SIGMA = p.SIGMA;
+    float n = std::sqrt(M_PI / 2.0) * SIGMA * (1.0 + std::exp(2.0 * SIGMA * SIGMA));
+    E.norm = 1.0 / (2.0 * M_PI * n);  // src/FreeStream.cpp:302-303
+    float SIGMA_B = p.SIGMA_B;
+    float nb = std::sqrt(2.0 * M_PI) * SIGMA_B * std::exp(SIGMA_B * SIGMA_B / 2.0);
+    E.normB = 1.0 / (2.0 * M_PI * nb);  // src/FreeStream.cpp:365-366
+  }
+  E.jac.resize(NR);
+  for (int irap = 0; irap < NR; ++irap) {  // src/LandauMatch.cpp:92-93
+    float w = tanmap_w(irap, NR);
+    E.jac[irap] = (M_PI / 2.0) / std::cos((M_PI / 2.0) * w) / std::cos((M_PI / 2.0) * w) *
+                  (1.995 / float(NR - 1));
+  }
+  E.re.resize((size_t)NE * NR);
+  E.rapf.resize((size_t)NE * NR);
+  E.rapfB.resize((size_t)NE * NR);
+  const float rapmin = (-1.0) * ((float)(NR - 1) / 2.0) * p.DRAP;
+  const float SIGMA = p.SIGMA, SIGMA_B = p.SIGMA_B;
+  std::vector<int> live_cnt(NR, 0);
+  for (int ieta = 0; ieta < NE; ++ieta) {
+    float eta = (float)ieta * DETA + E.etamin;
+    for (int irap = 0; irap < NR; ++irap) {
+      float w = tanmap_w(irap, NR);
+      float rap = eta + std::tan((M_PI / 2.0) * w);
+      // streaming step (src/FreeStream.cpp:192-201)
+      float eta_new = std::asinh((TAU / TAU0) * std::sinh(eta - rap)) + rap;
+      float D = (TAU * std::cosh(rap - eta_new) - TAU0 * std::cosh(rap - eta));
+      float ieta_new = (eta_new - E.etamin) / DETA;
+      float fl = std::floor(ieta_new);
+      RapEta r;
+      r.D = D;
+      if (std::isfinite(ieta_new) && fl > -1.0e6f && fl < 1.0e6f) {
+        r.efl = (int)fl;
+        r.efrac = ieta_new - fl;
+      } else {
+        r.efl = -1;
+        r.efrac = 0.0f;
+      }
+      // hypertrig factors (src/LandauMatch.cpp:46-55) with d = rap - eta
+      float d = rap - eta;
+      float ch = std::cosh(d), th = std::tanh(d);
+      r.A = 1.0f / ch;
+      r.B = 1.0f / (ch * ch);
+      r.C = (1.0 / TAU) * ((double)th / (double)ch);
+      r.Dt = (1.0 / TAU) * std::tanh(rap - eta);
+      r.E = (1.0 / (TAU * TAU)) * std::tanh(rap - eta) * std::tanh(rap - eta);
+      E.re[(size_t)ieta * NR + irap] = r;
+      // rapidity weights of the initial densities (src/FreeStream.cpp:345, 381-382)
+      float de = eta - rap;
+      E.rapf[(size_t)ieta * NR + irap] =
+          std::cosh(de) * std::cosh(de) * std::exp((-1.0) * de * de / (2.0 * SIGMA * SIGMA));
+      float rapu = (float)irap * p.DRAP + rapmin;
+      float du = eta - rapu;
+      E.rapfB[(size_t)ieta * NR + irap] =
+          std::cosh(du) * std::exp((-1.0) * du * du / (SIGMA_B * SIGMA_B));
+      bool live = (r.efl >= 1 && r.efl < NE - 1) && std::isfinite(D) &&
+                  std::fabs(D) <= (float)(NX + NY) * std::max(p.DX, p.DY);
+      if (live) live_cnt[irap] += 1;
+    }
+  }
+  E.r_lo = NR;
+  E.r_hi = 0;
+  double live_pairs = 0;
+  for (int irap = 0; irap < NR; ++irap)
+    if (live_cnt[irap] > 0) {
+      E.r_lo = std::min(E.r_lo, irap);
+      E.r_hi = std::max(E.r_hi, irap + 1);
+    }
+  if (E.r_lo >= E.r_hi) E.r_lo = E.r_hi = 0;
+  for (int irap = E.r_lo; irap < E.r_hi; ++irap)
+    for (int ieta = 0; ieta < NE; ++ieta) {
+      const RapEta& r = E.re[(size_t)ieta * NR + irap];
+      if (r.efl >= 1 && r.efl < NE - 1 && std::isfinite(r.D)) live_pairs += 1;
+    }
+  E.samples = live_pairs * (double)NX * NY * NP;
+  E.ref_samples = (double)p.DIM * NR * NP;
+  return FSM_OK;
+}
+
+}  // namespace fsm
+
+// ------------------------------------------------------------------ C ABI
+using namespace fsm;
+
+extern "C" const char* fsm_status_str(fsm_status s) {
+  switch (s) {
+    case FSM_OK: return "ok";
+    case FSM_ERR_INVALID_ARG: return "invalid argument";
+    case FSM_ERR_SIZE_MISMATCH: return "input size does not match the grid";
+    case FSM_ERR_INVALID_IC: return "not a valid initial condition";
+    case FSM_ERR_UNSUPPORTED: return "unsupported parameter combination";
+    case FSM_ERR_CUDA: return "CUDA error";
+    case FSM_ERR_NO_DEVICE: return "no CUDA device";
+    case FSM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case FSM_ERR_FILE: return "file not found";
+    case FSM_ERR_BUSY: return "busy";
+    case FSM_ERR_TIMEOUT: return "timed out";
+    case FSM_ERR_PENDING: return "pending";
+    case FSM_ERR_TOO_LARGE: return "request too large";
+    case FSM_ERR_CANCELLED: return "cancelled";
+  }
+  return "unknown status";
+}
+
+extern "C" const char* fsm_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" void fsm_params_default(fsm_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  // src/FreestreamMilne.cpp:149-171
+  p->OUTPUTFORMAT = 2;
+  p->BARYON = 0;
+  p->IC_ENERGY = 5;
+  p->IC_BARYON = 1;
+  p->ETA_WIDTH = 0.5;
+  p->ETA_FLAT = 0.5;
+  p->SIGMA = 1.0;
+  p->SIGMA_B = 1.0;
+  p->DIM_X = 101;
+  p->DIM_Y = 101;
+  p->DIM_ETA = 1;
+  p->DIM_RAP = 1;
+  p->DIM_PHIP = 51;
+  p->DX = 0.1;
+  p->DY = 0.1;
+  p->DETA = 0.1;
+  p->DRAP = 0.2;
+  p->DTAU = 0.5;
+  p->TAU0 = 0.1;
+  p->EOS_TYPE = 1;
+  p->E_FREEZE = 1.7;
+  p->VISCOUS_MATCHING = 1;
+  p->E_DEP_FS = 0;
+  p->E_R = 1.0;
+  p->TAU_R = 1.0;
+  p->ALPHA = 0.0;
+  fsm_params_derive(p);
+}
+
+extern "C" void fsm_params_derive(fsm_params* p) {
+  if (!p) return;
+  p->DIM = p->DIM_X * p->DIM_Y * p->DIM_ETA;
+  p->TAU = p->TAU0 + p->DTAU;
+}
+
+// Positional parse with the reference's own format strings (src/FileIO.cpp:279-334).
+extern "C" fsm_status fsm_params_read_file(const char* path, fsm_params* p) {
+  if (!path || !p) return FSM_ERR_INVALID_ARG;
+  FILE* fileIn = std::fopen(path, "r");
+  if (!fileIn) {
+    set_last_error(std::string("cannot open parameter file ") + path);
+    return FSM_ERR_FILE;
+  }
+  char dummyChar[255];
+  int dummyInt = 0;
+  float dummyFloat = 0;
+  auto rdi = [&](int* dst) {
+    if (std::fscanf(fileIn, "%254s\t%d\n", dummyChar, &dummyInt) == 2) *dst = dummyInt;
+  };
+  auto rdf = [&](float* dst) {
+    if (std::fscanf(fileIn, "%254s\t%f\n", dummyChar, &dummyFloat) == 2) *dst = dummyFloat;
+  };
+  rdi(&p->OUTPUTFORMAT);
+  rdi(&p->BARYON);
+  rdi(&p->IC_ENERGY);
+  rdi(&p->IC_BARYON);
+  rdf(&p->ETA_WIDTH);
+  rdf(&p->ETA_FLAT);
+  rdf(&p->SIGMA);
+  rdf(&p->SIGMA_B);
+  rdi(&p->DIM_X);
+  rdi(&p->DIM_Y);
+  rdi(&p->DIM_ETA);
+  rdi(&p->DIM_RAP);
+  rdi(&p->DIM_PHIP);
+  rdf(&p->DX);
+  rdf(&p->DY);
+  rdf(&p->DETA);
+  rdf(&p->DRAP);
+  rdf(&p->DTAU);
+  rdf(&p->TAU0);
+  rdi(&p->EOS_TYPE);
+  rdf(&p->E_FREEZE);
+  rdi(&p->VISCOUS_MATCHING);
+  rdi(&p->E_DEP_FS);
+  rdf(&p->E_R);
+  rdf(&p->TAU_R);
+  rdf(&p->ALPHA);
+  std::fclose(fileIn);
+  fsm_params_derive(p);
+  return FSM_OK;
+}

@@ -1,0 +1,45 @@
+// fsm_plan.h -- host-side event planning: effective parameters and the small
+// per-event tables the kernels read.  Implemented in fsm_plan.cpp, which is
+// compiled by the host compiler with FMA contraction disabled so that every
+// table entry is rounded exactly as the reference computes it.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/fsm.h"
+#include "fsm_internal.h"
+
+namespace fsm {
+
+struct EventPlan {
+  fsm_params p;  // effective parameters (E_DEP_FS and phi_p rule applied, DIM/TAU set)
+  bool is3d = false;
+  bool baryon = false;
+  int DIM = 0;
+  float xmin = 0, ymin = 0, etamin = 0, xmax_i = 0, ymax_i = 0, d_phip = 0;
+  std::vector<FSM_FLOAT2> cs;  // (cos, sin) of phi_p
+  // 2D spline axes
+  std::vector<double> hx, fx, dgx, hy, fy, dgy;
+  int Rx = 0, Ry = 0;
+  // 3D tables
+  std::vector<RapEta> re;
+  std::vector<float> rapf, rapfB, jac;
+  int r_lo = 0, r_hi = 0;
+  float norm = 0, normB = 0;
+  double samples = 0;  // cell x momentum samples the stream kernel evaluates
+  double ref_samples = 0;  // DIM * DIM_RAP * DIM_PHIP, the reference's count
+};
+
+// Validates `in`, applies the energy-dependent free-streaming time (needs the
+// host profile; pass NULL to reject E_DEP_FS=1) and the phi_p arc-length rule,
+// and fills the tables.  Returns FSM_OK or an error with a message in *why.
+fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
+                      std::string* why);
+
+// Output components of one event in the slab order used by batches:
+// T(10) e P Pi u(4) pi(10) [J(4) nB V(4)].
+int output_components(bool baryon);
+
+void set_last_error(const std::string& msg);
+
+}  // namespace fsm

@@ -1,0 +1,852 @@
+// fsm_runtime.cu -- contexts, batches, launches and the C ABI of libfsm.so.
+//
+// A batch is the unit of execution: n events (2D and/or 3D, any sizes) planned
+// on the host, laid out in one device allocation (tables, scratch, descriptor
+// arrays, work lists and optionally input/output slabs), and run as a fixed
+// sequence of six launches on one stream:
+//   memset(counters) -> prep2d_lines -> prep2d_pack -> prep3d -> stream2d
+//   -> stream3d -> landau
+// The sequence is captured into a CUDA graph on the first fsm_batch_launch and
+// replayed afterwards.  The single-event entry points run a cached one-event
+// batch, so a repeated call with the same shape allocates nothing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fsm.h"
+#include "fsm_internal.h"
+#include "fsm_plan.h"
+
+namespace fsm {
+__global__ void fsm_prep2d_lines_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_pack_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
+__global__ void fsm_stream3d_kernel(const Ev3D*, const CellBlock*, int, int, Counters*);
+__global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
+}  // namespace fsm
+
+using namespace fsm;
+
+#define FSM_CUDA_TRY(call)                                                        \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+      return (e_ == cudaErrorMemoryAllocation) ? FSM_ERR_OUT_OF_MEMORY : FSM_ERR_CUDA; \
+    }                                                                             \
+  } while (0)
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+struct TimingSet {
+  cudaEvent_t ev[4];
+  double samples;
+};
+
+}  // namespace
+
+struct fsm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool timing = false;
+  int num_sms = 0;
+  int smem_optin = 0;
+  fsm_timing acc{};
+  std::vector<TimingSet> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::mutex mu;
+  // cached one-event batches
+  fsm_batch* single_host = nullptr;
+  fsm_batch* single_dev = nullptr;
+};
+
+struct fsm_batch {
+  fsm_ctx* ctx = nullptr;
+  std::vector<EventPlan> plans;
+  bool own_io = true;
+  // device allocation
+  char* d_mem = nullptr;
+  size_t bytes = 0;
+  // staging for descriptor uploads (pinned)
+  char* h_stage = nullptr;
+  size_t stage_bytes = 0;
+  size_t desc_off = 0, desc_bytes = 0;
+  // per-event device views
+  std::vector<float*> d_in_e, d_in_nB;
+  std::vector<fsm_outputs> d_out;
+  std::vector<size_t> in_off, out_off;  // element offsets inside the slabs
+  size_t in_slab_off = 0, in_slab_bytes = 0, out_slab_off = 0, out_slab_bytes = 0;
+  std::vector<float*> d_T, d_J;         // moment buffers the Landau kernel reads
+  // host copies of descriptors
+  std::vector<Ev2D> ev2;
+  std::vector<Ev3D> ev3;
+  std::vector<EvLandau> evl;
+  std::vector<int> ev2_of, ev3_of;      // event -> index in ev2/ev3 (or -1)
+  // device descriptor arrays and work lists
+  Ev2D* d_ev2 = nullptr;
+  Ev3D* d_ev3 = nullptr;
+  EvLandau* d_evl = nullptr;
+  Tile2D* d_tiles = nullptr;
+  LineBlock *d_lines = nullptr, *d_packs = nullptr;
+  CellBlock *d_prep3 = nullptr, *d_b3 = nullptr, *d_bl = nullptr;
+  Counters* d_ctr = nullptr;
+  int* d_err = nullptr;
+  int ntiles = 0, nlines = 0, npacks = 0, nprep3 = 0, nb3 = 0, nbl = 0;
+  int cs_cap2 = 0, cs_cap3 = 0;
+  size_t smem2 = 0, smem3 = 0;
+  int grid2 = 0, grid3 = 0;
+  double samples = 0;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+struct Layout {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off = align_up(off + bytes);
+    return o;
+  }
+};
+
+bool has_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n > 0;
+}
+
+void batch_free(fsm_batch* b) {
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_mem) cudaFree(b->d_mem);
+  if (b->h_stage) cudaFreeHost(b->h_stage);
+  delete b;
+}
+
+// Builds descriptors and uploads everything.  ext_in / ext_out (one event)
+// select external device buffers instead of owned slabs.
+fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
+                       const float* const* ext_in_e, const float* const* ext_in_nB,
+                       const fsm_outputs* ext_out, fsm_batch** out) {
+  if (n <= 0 || !params) return FSM_ERR_INVALID_ARG;
+  std::unique_ptr<fsm_batch, void (*)(fsm_batch*)> b(new fsm_batch(), batch_free);
+  b->ctx = ctx;
+  b->own_io = (ext_in_e == nullptr);
+  b->plans.resize(n);
+  for (int i = 0; i < n; ++i) {
+    std::string why;
+    fsm_status s = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why);
+    if (s != FSM_OK) {
+      set_last_error("event " + std::to_string(i) + ": " + why);
+      return s;
+    }
+  }
+  // ---- layout
+  Layout L;
+  struct EvOffs {
+    size_t cs, hx, fx, dgx, hy, fy, dgy, re, rapf, rapfB, jac;
+    size_t zx, zy, nodes, efield, T, J, in_e, in_nB, out;
+  };
+  std::vector<EvOffs> eo(n);
+  int n2 = 0, n3 = 0;
+  b->ev2_of.assign(n, -1);
+  b->ev3_of.assign(n, -1);
+  b->in_off.assign(n, 0);
+  b->out_off.assign(n, 0);
+  size_t in_elems = 0, out_elems = 0;
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    b->in_off[i] = in_elems;
+    in_elems += (size_t)P.DIM * (P.baryon ? 2 : 1);
+    b->out_off[i] = out_elems;
+    out_elems += (size_t)P.DIM * output_components(P.baryon);
+    if (P.is3d) b->ev3_of[i] = n3++;
+    else b->ev2_of[i] = n2++;
+  }
+  // tables
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    EvOffs& o = eo[i];
+    o.cs = L.take(P.cs.size() * sizeof(FSM_FLOAT2));
+    if (!P.is3d) {
+      o.hx = L.take(P.hx.size() * 8);
+      o.fx = L.take(P.fx.size() * 8);
+      o.dgx = L.take(P.dgx.size() * 8);
+      o.hy = L.take(P.hy.size() * 8);
+      o.fy = L.take(P.fy.size() * 8);
+      o.dgy = L.take(P.dgy.size() * 8);
+    } else {
+      o.re = L.take(P.re.size() * sizeof(RapEta));
+      o.rapf = L.take(P.rapf.size() * 4);
+      o.rapfB = L.take(P.rapfB.size() * 4);
+      o.jac = L.take(P.jac.size() * 4);
+    }
+  }
+  // work lists (host side first, to know their sizes)
+  std::vector<Tile2D> tiles;
+  std::vector<LineBlock> lines, packs;
+  std::vector<CellBlock> prep3, b3, bl;
+  {
+    std::vector<int> order2;
+    for (int i = 0; i < n; ++i)
+      if (!b->plans[i].is3d) order2.push_back(i);
+    std::stable_sort(order2.begin(), order2.end(), [&](int a, int c) {
+      return b->plans[a].p.DIM_PHIP > b->plans[c].p.DIM_PHIP;
+    });
+    for (int i : order2) {
+      const EventPlan& P = b->plans[i];
+      int tx = (P.p.DIM_X + kTileX - 1) / kTileX, ty = (P.p.DIM_Y + kTileY - 1) / kTileY;
+      for (int a = 0; a < tx; ++a)
+        for (int c = 0; c < ty; ++c) tiles.push_back(Tile2D{b->ev2_of[i], a * kTileX, c * kTileY, 0});
+    }
+    for (int i = 0; i < n; ++i) {
+      const EventPlan& P = b->plans[i];
+      if (P.is3d) continue;
+      int nl = P.p.DIM_X + P.p.DIM_Y;
+      for (int s = 0; s < nl; s += 128) lines.push_back(LineBlock{b->ev2_of[i], s});
+      for (int s = 0; s < P.p.DIM_Y; s += 128) packs.push_back(LineBlock{b->ev2_of[i], s});
+    }
+    std::vector<int> order3;
+    for (int i = 0; i < n; ++i)
+      if (b->plans[i].is3d) order3.push_back(i);
+    std::stable_sort(order3.begin(), order3.end(), [&](int a, int c) {
+      const EventPlan &A = b->plans[a], &C = b->plans[c];
+      return A.samples / std::max(1, A.DIM) > C.samples / std::max(1, C.DIM);
+    });
+    for (int i : order3) {
+      const EventPlan& P = b->plans[i];
+      for (int s = 0; s < P.DIM; s += kThreads3D) b3.push_back(CellBlock{b->ev3_of[i], s});
+    }
+    for (int i = 0; i < n; ++i) {
+      const EventPlan& P = b->plans[i];
+      if (P.is3d)
+        for (int s = 0; s < P.DIM; s += 256) prep3.push_back(CellBlock{b->ev3_of[i], s});
+      for (int s = 0; s < P.DIM; s += kThreadsLandau) bl.push_back(CellBlock{i, s});
+    }
+  }
+  // descriptors + work lists
+  size_t o_ev2 = L.take(std::max(n2, 1) * sizeof(Ev2D));
+  size_t o_ev3 = L.take(std::max(n3, 1) * sizeof(Ev3D));
+  size_t o_evl = L.take(n * sizeof(EvLandau));
+  size_t o_tiles = L.take(std::max<size_t>(tiles.size(), 1) * sizeof(Tile2D));
+  size_t o_lines = L.take(std::max<size_t>(lines.size(), 1) * sizeof(LineBlock));
+  size_t o_packs = L.take(std::max<size_t>(packs.size(), 1) * sizeof(LineBlock));
+  size_t o_prep3 = L.take(std::max<size_t>(prep3.size(), 1) * sizeof(CellBlock));
+  size_t o_b3 = L.take(std::max<size_t>(b3.size(), 1) * sizeof(CellBlock));
+  size_t o_bl = L.take(bl.size() * sizeof(CellBlock));
+  size_t o_ctr = L.take(sizeof(Counters));
+  size_t o_err = L.take(sizeof(int) * 4);
+  const size_t upload_bytes = L.off;  // everything above comes from the host
+  // scratch and moments
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    EvOffs& o = eo[i];
+    if (!P.is3d) {
+      o.zx = L.take((size_t)P.DIM * 8);
+      o.zy = L.take((size_t)P.DIM * 8);
+      o.nodes = L.take((size_t)P.DIM * 16);
+    } else {
+      o.efield = L.take((size_t)P.DIM * 4);
+    }
+    if (!b->own_io) {
+      o.T = L.take((size_t)P.DIM * 10 * 4);
+      o.J = P.baryon ? L.take((size_t)P.DIM * 4 * 4) : 0;
+    }
+  }
+  if (b->own_io) {
+    b->in_slab_off = L.take(in_elems * 4);
+    b->in_slab_bytes = in_elems * 4;
+    b->out_slab_off = L.take(out_elems * 4);
+    b->out_slab_bytes = out_elems * 4;
+  }
+  b->bytes = L.off;
+  cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
+  if (ce != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
+                   cudaGetErrorString(ce));
+    return FSM_ERR_OUT_OF_MEMORY;
+  }
+  char* D = b->d_mem;
+  b->stage_bytes = upload_bytes;
+  FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
+  char* H = b->h_stage;
+  std::memset(H, 0, upload_bytes);
+  b->desc_off = o_ev2;
+  b->desc_bytes = o_tiles - o_ev2;
+  // ---- fill tables
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    EvOffs& o = eo[i];
+    std::memcpy(H + o.cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
+    if (!P.is3d) {
+      std::memcpy(H + o.hx, P.hx.data(), P.hx.size() * 8);
+      std::memcpy(H + o.fx, P.fx.data(), P.fx.size() * 8);
+      std::memcpy(H + o.dgx, P.dgx.data(), P.dgx.size() * 8);
+      std::memcpy(H + o.hy, P.hy.data(), P.hy.size() * 8);
+      std::memcpy(H + o.fy, P.fy.data(), P.fy.size() * 8);
+      std::memcpy(H + o.dgy, P.dgy.data(), P.dgy.size() * 8);
+    } else {
+      std::memcpy(H + o.re, P.re.data(), P.re.size() * sizeof(RapEta));
+      std::memcpy(H + o.rapf, P.rapf.data(), P.rapf.size() * 4);
+      std::memcpy(H + o.rapfB, P.rapfB.data(), P.rapfB.size() * 4);
+      std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
+    }
+  }
+  // ---- per-event io views
+  b->d_in_e.assign(n, nullptr);
+  b->d_in_nB.assign(n, nullptr);
+  b->d_out.assign(n, fsm_outputs{});
+  b->d_T.assign(n, nullptr);
+  b->d_J.assign(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    const size_t DIM = P.DIM;
+    if (b->own_io) {
+      float* in = reinterpret_cast<float*>(D + b->in_slab_off) + b->in_off[i];
+      b->d_in_e[i] = in;
+      b->d_in_nB[i] = P.baryon ? in + DIM : nullptr;
+      float* o = reinterpret_cast<float*>(D + b->out_slab_off) + b->out_off[i];
+      fsm_outputs v{};
+      v.T = o;
+      v.e = o + 10 * DIM;
+      v.P = o + 11 * DIM;
+      v.Pi = o + 12 * DIM;
+      v.u = o + 13 * DIM;
+      v.pi = o + 17 * DIM;
+      if (P.baryon) {
+        v.J = o + 27 * DIM;
+        v.nB = o + 31 * DIM;
+        v.V = o + 32 * DIM;
+      }
+      b->d_out[i] = v;
+      b->d_T[i] = v.T;
+      b->d_J[i] = v.J;
+    } else {
+      b->d_in_e[i] = const_cast<float*>(ext_in_e[i]);
+      b->d_in_nB[i] = ext_in_nB ? const_cast<float*>(ext_in_nB[i]) : nullptr;
+      b->d_out[i] = ext_out[i];
+      b->d_T[i] = ext_out[i].T ? ext_out[i].T : reinterpret_cast<float*>(D + eo[i].T);
+      b->d_J[i] = P.baryon ? (ext_out[i].J ? ext_out[i].J : reinterpret_cast<float*>(D + eo[i].J))
+                           : nullptr;
+    }
+  }
+  // ---- descriptors
+  b->ev2.assign(n2, Ev2D{});
+  b->ev3.assign(n3, Ev3D{});
+  b->evl.assign(n, EvLandau{});
+  int max_np2 = 0, max_np3 = 0;
+  size_t max_fp = 0;
+  const size_t smem_budget = 96 * 1024;  // footprint bytes staged per CTA (2 CTAs/SM)
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    const EvOffs& o = eo[i];
+    const fsm_params& p = P.p;
+    if (!P.is3d) {
+      Ev2D& e = b->ev2[b->ev2_of[i]];
+      e.NX = p.DIM_X;
+      e.NY = p.DIM_Y;
+      e.NPHI = p.DIM_PHIP;
+      e.NR = p.DIM_RAP;
+      e.DX = p.DX;
+      e.DY = p.DY;
+      e.DTAU = p.DTAU;
+      e.TAU = p.TAU;
+      e.xmin = P.xmin;
+      e.ymin = P.ymin;
+      e.xmax_i = P.xmax_i;
+      e.ymax_i = P.ymax_i;
+      e.inv_dx = 1.0f / p.DX;
+      e.inv_dy = 1.0f / p.DY;
+      e.d_phip = P.d_phip;
+      e.Rx = P.Rx;
+      e.Ry = P.Ry;
+      size_t fpw = std::min(p.DIM_Y, kTileY + 2 * P.Ry + 1);
+      size_t fph = std::min(p.DIM_X, kTileX + 2 * P.Rx + 1);
+      size_t fp = fpw * fph * 16;
+      e.use_smem = fp <= smem_budget ? 1 : 0;
+      if (e.use_smem) max_fp = std::max(max_fp, fp);
+      e.tiles_y = (p.DIM_Y + kTileY - 1) / kTileY;
+      e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o.cs);
+      e.e_gev = b->d_in_e[i];
+      e.ax = SplineAxis{reinterpret_cast<const double*>(D + o.hx),
+                        reinterpret_cast<const double*>(D + o.fx),
+                        reinterpret_cast<const double*>(D + o.dgx), p.DIM_X};
+      e.ay = SplineAxis{reinterpret_cast<const double*>(D + o.hy),
+                        reinterpret_cast<const double*>(D + o.fy),
+                        reinterpret_cast<const double*>(D + o.dgy), p.DIM_Y};
+      e.zx = reinterpret_cast<double*>(D + o.zx);
+      e.zy = reinterpret_cast<double*>(D + o.zy);
+      e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o.nodes);
+      e.T = b->d_T[i];
+      max_np2 = std::max(max_np2, p.DIM_PHIP);
+    } else {
+      Ev3D& e = b->ev3[b->ev3_of[i]];
+      e.NX = p.DIM_X;
+      e.NY = p.DIM_Y;
+      e.NE = p.DIM_ETA;
+      e.NR = p.DIM_RAP;
+      e.NPHI = p.DIM_PHIP;
+      e.r_lo = P.r_lo;
+      e.r_hi = P.r_hi;
+      e.baryon = P.baryon ? 1 : 0;
+      e.DX = p.DX;
+      e.DY = p.DY;
+      e.xmin = P.xmin;
+      e.ymin = P.ymin;
+      e.inv_dx = 1.0f / p.DX;
+      e.inv_dy = 1.0f / p.DY;
+      e.norm = P.norm;
+      e.normB = P.normB;
+      e.d_phip = P.d_phip;
+      e.DRAP = p.DRAP;
+      e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o.cs);
+      e.re = reinterpret_cast<const RapEta*>(D + o.re);
+      e.rapf = reinterpret_cast<const float*>(D + o.rapf);
+      e.rapfB = reinterpret_cast<const float*>(D + o.rapfB);
+      e.jac = reinterpret_cast<const float*>(D + o.jac);
+      e.e_gev = b->d_in_e[i];
+      e.efield = reinterpret_cast<float*>(D + o.efield);
+      e.nB = b->d_in_nB[i];
+      e.T = b->d_T[i];
+      e.J = b->d_J[i];
+      max_np3 = std::max(max_np3, p.DIM_PHIP);
+    }
+    EvLandau& l = b->evl[i];
+    l.DIM = P.DIM;
+    l.is3d = P.is3d ? 1 : 0;
+    l.baryon = P.baryon ? 1 : 0;
+    l.eos = p.EOS_TYPE;
+    l.viscous = p.VISCOUS_MATCHING;
+    l.TAU = p.TAU;
+    l.T = b->d_T[i];
+    l.J = b->d_J[i];
+    const fsm_outputs& v = b->d_out[i];
+    l.e = v.e;
+    l.P = v.P;
+    l.Pi = v.Pi;
+    l.u = v.u;
+    l.pi = v.pi;
+    l.nB = v.nB;
+    l.V = v.V;
+    b->samples += P.samples;
+  }
+  b->cs_cap2 = (max_np2 + 1) & ~1;
+  b->cs_cap3 = (max_np3 + 1) & ~1;
+  b->smem2 = (size_t)b->cs_cap2 * 8 + max_fp;
+  b->smem3 = (size_t)b->cs_cap3 * 8;
+  std::memcpy(H + o_ev2, b->ev2.data(), n2 * sizeof(Ev2D));
+  std::memcpy(H + o_ev3, b->ev3.data(), n3 * sizeof(Ev3D));
+  std::memcpy(H + o_evl, b->evl.data(), n * sizeof(EvLandau));
+  std::memcpy(H + o_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
+  std::memcpy(H + o_lines, lines.data(), lines.size() * sizeof(LineBlock));
+  std::memcpy(H + o_packs, packs.data(), packs.size() * sizeof(LineBlock));
+  std::memcpy(H + o_prep3, prep3.data(), prep3.size() * sizeof(CellBlock));
+  std::memcpy(H + o_b3, b3.data(), b3.size() * sizeof(CellBlock));
+  std::memcpy(H + o_bl, bl.data(), bl.size() * sizeof(CellBlock));
+  b->d_ev2 = reinterpret_cast<Ev2D*>(D + o_ev2);
+  b->d_ev3 = reinterpret_cast<Ev3D*>(D + o_ev3);
+  b->d_evl = reinterpret_cast<EvLandau*>(D + o_evl);
+  b->d_tiles = reinterpret_cast<Tile2D*>(D + o_tiles);
+  b->d_lines = reinterpret_cast<LineBlock*>(D + o_lines);
+  b->d_packs = reinterpret_cast<LineBlock*>(D + o_packs);
+  b->d_prep3 = reinterpret_cast<CellBlock*>(D + o_prep3);
+  b->d_b3 = reinterpret_cast<CellBlock*>(D + o_b3);
+  b->d_bl = reinterpret_cast<CellBlock*>(D + o_bl);
+  b->d_ctr = reinterpret_cast<Counters*>(D + o_ctr);
+  b->d_err = reinterpret_cast<int*>(D + o_err);
+  b->ntiles = (int)tiles.size();
+  b->nlines = (int)lines.size();
+  b->npacks = (int)packs.size();
+  b->nprep3 = (int)prep3.size();
+  b->nb3 = (int)b3.size();
+  b->nbl = (int)bl.size();
+  FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
+  // ---- launch geometry
+  if (b->ntiles) {
+    FSM_CUDA_TRY(cudaFuncSetAttribute(fsm_stream2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)std::max<size_t>(b->smem2, 1)));
+    int occ = 0;
+    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream2d_kernel, kThreads2D,
+                                                               b->smem2));
+    b->grid2 = std::max(1, std::min(b->ntiles, ctx->num_sms * std::max(occ, 1)));
+  }
+  if (b->nb3) {
+    FSM_CUDA_TRY(cudaFuncSetAttribute(fsm_stream3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)std::max<size_t>(b->smem3, 1)));
+    int occ = 0;
+    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_kernel, kThreads3D,
+                                                               b->smem3));
+    b->grid3 = std::max(1, std::min(b->nb3, ctx->num_sms * std::max(occ, 1)));
+  }
+  FSM_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int) * 4));
+  *out = b.release();
+  return FSM_OK;
+}
+
+cudaEvent_t pool_event(fsm_ctx* ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// The six-launch sequence.  With `timing`, CUDA events bracket the prep,
+// stream and Landau groups on the launching stream.
+fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
+  fsm_ctx* ctx = b->ctx;
+  TimingSet ts{};
+  if (timing) {
+    for (int k = 0; k < 4; ++k) ts.ev[k] = pool_event(ctx);
+    ts.samples = b->samples;
+    cudaEventRecord(ts.ev[0], s);
+  }
+  FSM_CUDA_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(Counters), s));
+  if (b->nlines) fsm_prep2d_lines_kernel<<<b->nlines, 128, 0, s>>>(b->d_ev2, b->d_lines);
+  if (b->npacks) fsm_prep2d_pack_kernel<<<b->npacks, 128, 0, s>>>(b->d_ev2, b->d_packs);
+  if (b->nprep3) fsm_prep3d_kernel<<<b->nprep3, 256, 0, s>>>(b->d_ev3, b->d_prep3);
+  if (timing) cudaEventRecord(ts.ev[1], s);
+  if (b->ntiles)
+    fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
+                                                               b->cs_cap2, b->d_ctr, b->d_err);
+  if (b->nb3)
+    fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_b3, b->nb3,
+                                                               b->cs_cap3, b->d_ctr);
+  if (timing) cudaEventRecord(ts.ev[2], s);
+  if (b->nbl) fsm_landau_kernel<<<b->nbl, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl, b->d_ctr);
+  if (timing) {
+    cudaEventRecord(ts.ev[3], s);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->pending.push_back(ts);
+  }
+  FSM_CUDA_TRY(cudaGetLastError());
+  return FSM_OK;
+}
+
+fsm_status launch(fsm_batch* b, cudaStream_t s) {
+  fsm_ctx* ctx = b->ctx;
+  if (ctx->timing) return enqueue(b, s, true);
+  if (!b->graph || b->graph_stream != s) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    FSM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    fsm_status st = enqueue(b, s, false);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (st != FSM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (ce != cudaSuccess) {
+      set_last_error(std::string("graph capture: ") + cudaGetErrorString(ce));
+      return FSM_ERR_CUDA;
+    }
+    ce = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      set_last_error(std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      b->graph = nullptr;
+      return FSM_ERR_CUDA;
+    }
+    b->graph_stream = s;
+  }
+  FSM_CUDA_TRY(cudaGraphLaunch(b->graph, s));
+  return FSM_OK;
+}
+
+fsm_status check_kernel_errors(fsm_batch* b) {
+  int err[4] = {0, 0, 0, 0};
+  FSM_CUDA_TRY(cudaMemcpy(err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+  if (err[0]) {
+    set_last_error("stream kernel: " + std::to_string(err[0]) +
+                   " samples fell outside the staged footprint");
+    return FSM_ERR_CUDA;
+  }
+  return FSM_OK;
+}
+
+bool same_params(const fsm_params& a, const fsm_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+fsm_status fill_info(const EventPlan& P, fsm_run_info* info) {
+  if (!info) return FSM_OK;
+  info->dim_phip = P.p.DIM_PHIP;
+  info->dtau = P.p.DTAU;
+  info->tau = P.p.TAU;
+  info->live_rap_lo = P.r_lo;
+  info->live_rap_hi = P.r_hi;
+  info->samples = P.samples;
+  return FSM_OK;
+}
+
+cudaStream_t pick_stream(fsm_ctx* ctx, void* stream) {
+  return stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" fsm_status fsm_ctx_create(fsm_ctx** out, const fsm_ctx_opts* opts) {
+  if (!out) return FSM_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!has_device()) {
+    set_last_error("no CUDA device visible; the library has no CPU fallback");
+    return FSM_ERR_NO_DEVICE;
+  }
+  std::unique_ptr<fsm_ctx> c(new fsm_ctx());
+  if (opts) {
+    c->device = opts->device;
+    c->timing = opts->enable_timing != 0;
+  }
+  FSM_CUDA_TRY(cudaSetDevice(c->device));
+  FSM_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+  FSM_CUDA_TRY(cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  FSM_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  *out = c.release();
+  return FSM_OK;
+}
+
+extern "C" void fsm_ctx_destroy(fsm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  batch_free(ctx->single_host);
+  batch_free(ctx->single_dev);
+  for (auto& t : ctx->pending)
+    for (int k = 0; k < 4; ++k) cudaEventDestroy(t.ev[k]);
+  for (auto e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" fsm_status fsm_ctx_timing(fsm_ctx* ctx, fsm_timing* t, int reset) {
+  if (!ctx) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  for (auto& ts : ctx->pending) {
+    FSM_CUDA_TRY(cudaEventSynchronize(ts.ev[3]));
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ts.ev[0], ts.ev[1]);
+    cudaEventElapsedTime(&b, ts.ev[1], ts.ev[2]);
+    cudaEventElapsedTime(&c, ts.ev[2], ts.ev[3]);
+    ctx->acc.prep_ms += a;
+    ctx->acc.stream_ms += b;
+    ctx->acc.landau_ms += c;
+    ctx->acc.prep_launches += 1;
+    ctx->acc.stream_launches += 1;
+    ctx->acc.landau_launches += 1;
+    ctx->acc.stream_samples += ts.samples;
+    for (int k = 0; k < 4; ++k) ctx->event_pool.push_back(ts.ev[k]);
+  }
+  ctx->pending.clear();
+  if (t) *t = ctx->acc;
+  if (reset) ctx->acc = fsm_timing{};
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
+                                    const float* nB, const fsm_outputs* host_out,
+                                    fsm_run_info* info) {
+  if (!ctx || !p || !e_gev || !host_out) return FSM_ERR_INVALID_ARG;
+  if (p->BARYON && !nB) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  EventPlan P;
+  std::string why;
+  fsm_status s = plan_event(*p, e_gev, &P, &why);
+  if (s != FSM_OK) {
+    set_last_error(why);
+    return s;
+  }
+  fsm_batch* b = ctx->single_host;
+  if (!b || !same_params(b->plans[0].p, P.p)) {
+    batch_free(ctx->single_host);
+    ctx->single_host = nullptr;
+    const float* he[1] = {e_gev};
+    s = batch_build(ctx, 1, p, he, nullptr, nullptr, nullptr, &ctx->single_host);
+    if (s != FSM_OK) return s;
+    b = ctx->single_host;
+  }
+  cudaStream_t st = ctx->stream;
+  const size_t DIM = P.DIM;
+  FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_e[0], e_gev, DIM * 4, cudaMemcpyHostToDevice, st));
+  if (P.baryon) FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_nB[0], nB, DIM * 4, cudaMemcpyHostToDevice, st));
+  s = launch(b, st);
+  if (s != FSM_OK) return s;
+  const fsm_outputs& d = b->d_out[0];
+  auto dl = [&](float* h, const float* dv, size_t comps) -> fsm_status {
+    if (h && dv) FSM_CUDA_TRY(cudaMemcpyAsync(h, dv, comps * DIM * 4, cudaMemcpyDeviceToHost, st));
+    return FSM_OK;
+  };
+  if ((s = dl(host_out->T, d.T, 10)) != FSM_OK) return s;
+  if ((s = dl(host_out->e, d.e, 1)) != FSM_OK) return s;
+  if ((s = dl(host_out->P, d.P, 1)) != FSM_OK) return s;
+  if ((s = dl(host_out->Pi, d.Pi, 1)) != FSM_OK) return s;
+  if ((s = dl(host_out->u, d.u, 4)) != FSM_OK) return s;
+  if ((s = dl(host_out->pi, d.pi, 10)) != FSM_OK) return s;
+  if (P.baryon) {
+    if ((s = dl(host_out->J, d.J, 4)) != FSM_OK) return s;
+    if ((s = dl(host_out->nB, d.nB, 1)) != FSM_OK) return s;
+    if ((s = dl(host_out->V, d.V, 4)) != FSM_OK) return s;
+  }
+  FSM_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((s = check_kernel_errors(b)) != FSM_OK) return s;
+  return fill_info(b->plans[0], info);
+}
+
+extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* d_e_gev,
+                                           const float* d_nB, const fsm_outputs* dev_out,
+                                           void* stream, fsm_run_info* info) {
+  if (!ctx || !p || !d_e_gev || !dev_out) return FSM_ERR_INVALID_ARG;
+  if (p->BARYON && !d_nB) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  EventPlan P;
+  std::string why;
+  fsm_status s = plan_event(*p, nullptr, &P, &why);
+  if (s != FSM_OK) {
+    set_last_error(why);
+    return s;
+  }
+  cudaStream_t st = pick_stream(ctx, stream);
+  fsm_batch* b = ctx->single_dev;
+  const bool same_io = b && b->d_in_e[0] == d_e_gev && b->d_in_nB[0] == d_nB &&
+                       std::memcmp(&b->d_out[0], dev_out, sizeof(fsm_outputs)) == 0;
+  if (!b || !same_params(b->plans[0].p, P.p) || !same_io) {
+    if (b) cudaStreamSynchronize(b->graph_stream ? b->graph_stream : st);
+    batch_free(ctx->single_dev);
+    ctx->single_dev = nullptr;
+    const float* ie[1] = {d_e_gev};
+    const float* inb[1] = {d_nB};
+    s = batch_build(ctx, 1, p, nullptr, ie, inb, dev_out, &ctx->single_dev);
+    if (s != FSM_OK) return s;
+    b = ctx->single_dev;
+  }
+  s = launch(b, st);
+  if (s != FSM_OK) return s;
+  return fill_info(b->plans[0], info);
+}
+
+extern "C" fsm_status fsm_batch_create(fsm_ctx* ctx, int n, const fsm_params* params,
+                                       fsm_batch** out) {
+  if (!ctx || !params || !out || n <= 0) return FSM_ERR_INVALID_ARG;
+  *out = nullptr;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  return batch_build(ctx, n, params, nullptr, nullptr, nullptr, nullptr, out);
+}
+
+extern "C" void fsm_batch_destroy(fsm_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  cudaDeviceSynchronize();
+  batch_free(b);
+}
+
+extern "C" fsm_status fsm_batch_views(fsm_batch* b, int ev, float** d_e, float** d_nB,
+                                      fsm_outputs* dev_out) {
+  if (!b || ev < 0 || ev >= (int)b->plans.size()) return FSM_ERR_INVALID_ARG;
+  if (d_e) *d_e = b->d_in_e[ev];
+  if (d_nB) *d_nB = b->d_in_nB[ev];
+  if (dev_out) *dev_out = b->d_out[ev];
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_launch(fsm_batch* b, void* stream) {
+  if (!b) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  return launch(b, pick_stream(b->ctx, stream));
+}
+
+extern "C" fsm_status fsm_batch_run_host(fsm_batch* b, const float* const* e_gev,
+                                         const float* const* nB, const fsm_outputs* host_out,
+                                         void* stream) {
+  if (!b || !e_gev) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = pick_stream(b->ctx, stream);
+  const int n = (int)b->plans.size();
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = b->plans[i];
+    if (!e_gev[i]) return FSM_ERR_INVALID_ARG;
+    FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_e[i], e_gev[i], (size_t)P.DIM * 4, cudaMemcpyHostToDevice, st));
+    if (P.baryon) {
+      if (!nB || !nB[i]) return FSM_ERR_INVALID_ARG;
+      FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_nB[i], nB[i], (size_t)P.DIM * 4, cudaMemcpyHostToDevice, st));
+    }
+  }
+  fsm_status s = launch(b, st);
+  if (s != FSM_OK) return s;
+  if (host_out) {
+    for (int i = 0; i < n; ++i) {
+      const size_t DIM = b->plans[i].DIM;
+      const fsm_outputs& d = b->d_out[i];
+      const fsm_outputs& h = host_out[i];
+      auto dl = [&](float* hp, const float* dp, size_t comps) -> fsm_status {
+        if (hp && dp) FSM_CUDA_TRY(cudaMemcpyAsync(hp, dp, comps * DIM * 4, cudaMemcpyDeviceToHost, st));
+        return FSM_OK;
+      };
+      if ((s = dl(h.T, d.T, 10)) || (s = dl(h.e, d.e, 1)) || (s = dl(h.P, d.P, 1)) ||
+          (s = dl(h.Pi, d.Pi, 1)) || (s = dl(h.u, d.u, 4)) || (s = dl(h.pi, d.pi, 10)) ||
+          (s = dl(h.J, d.J, 4)) || (s = dl(h.nB, d.nB, 1)) || (s = dl(h.V, d.V, 4)))
+        return s;
+    }
+  }
+  FSM_CUDA_TRY(cudaStreamSynchronize(st));
+  return check_kernel_errors(b);
+}
+
+extern "C" fsm_status fsm_batch_info(fsm_batch* b, int ev, fsm_run_info* info) {
+  if (!b || ev < 0 || ev >= (int)b->plans.size()) return FSM_ERR_INVALID_ARG;
+  return fill_info(b->plans[ev], info);
+}
+
+extern "C" double fsm_batch_samples(fsm_batch* b) { return b ? b->samples : 0.0; }
+
+extern "C" fsm_status fsm_batch_slabs(fsm_batch* b, size_t* in_bytes, size_t* out_bytes) {
+  if (!b || !b->own_io) return FSM_ERR_INVALID_ARG;
+  if (in_bytes) *in_bytes = b->in_slab_bytes;
+  if (out_bytes) *out_bytes = b->out_slab_bytes;
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_elem,
+                                              size_t* out_elem) {
+  if (!b || !b->own_io || ev < 0 || ev >= (int)b->plans.size()) return FSM_ERR_INVALID_ARG;
+  if (in_elem) *in_elem = b->in_off[ev];
+  if (out_elem) *out_elem = b->out_off[ev];
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_upload(fsm_batch* b, const void* host_in, void* stream) {
+  if (!b || !b->own_io || !host_in) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaMemcpyAsync(b->d_mem + b->in_slab_off, host_in, b->in_slab_bytes,
+                               cudaMemcpyHostToDevice, pick_stream(b->ctx, stream)));
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream) {
+  if (!b || !b->own_io || !host_out) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaMemcpyAsync(host_out, b->d_mem + b->out_slab_off, b->out_slab_bytes,
+                               cudaMemcpyDeviceToHost, pick_stream(b->ctx, stream)));
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_check(fsm_batch* b) {
+  if (!b) return FSM_ERR_INVALID_ARG;
+  return check_kernel_errors(b);
+}

@@ -1,0 +1,303 @@
+"""ctypes binding of libfsm.so, the C ABI declared in include/fsm.h.
+
+This module is a thin Python mirror of the C entry points for tests and the
+benchmark; the product is the C ABI itself (and the C++ FREESTREAMMILNE
+compatibility class built on it).  Loading fails loudly when the library has
+not been built: there is no Python or CPU fallback for the compute path.
+"""
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libfsm.so"
+
+FSM_OK = 0
+STATUS = {0: "FSM_OK", 1: "FSM_ERR_INVALID_ARG", 2: "FSM_ERR_SIZE_MISMATCH", 3: "FSM_ERR_INVALID_IC",
+          4: "FSM_ERR_UNSUPPORTED", 5: "FSM_ERR_CUDA", 6: "FSM_ERR_NO_DEVICE",
+          7: "FSM_ERR_OUT_OF_MEMORY", 8: "FSM_ERR_FILE", 9: "FSM_ERR_BUSY", 10: "FSM_ERR_TIMEOUT",
+          11: "FSM_ERR_PENDING", 12: "FSM_ERR_TOO_LARGE", 13: "FSM_ERR_CANCELLED"}
+
+# Field order of fsm_params == struct parameters (reference src/Parameter.h:2-33)
+PARAM_FIELDS = [
+    ("OUTPUTFORMAT", ctypes.c_int), ("BARYON", ctypes.c_int), ("IC_ENERGY", ctypes.c_int),
+    ("IC_BARYON", ctypes.c_int), ("ETA_WIDTH", ctypes.c_float), ("ETA_FLAT", ctypes.c_float),
+    ("SIGMA", ctypes.c_float), ("SIGMA_B", ctypes.c_float), ("DIM_X", ctypes.c_int),
+    ("DIM_Y", ctypes.c_int), ("DIM_ETA", ctypes.c_int), ("DIM_RAP", ctypes.c_int),
+    ("DIM_PHIP", ctypes.c_int), ("DX", ctypes.c_float), ("DY", ctypes.c_float),
+    ("DETA", ctypes.c_float), ("DRAP", ctypes.c_float), ("DTAU", ctypes.c_float),
+    ("TAU0", ctypes.c_float), ("EOS_TYPE", ctypes.c_int), ("E_FREEZE", ctypes.c_float),
+    ("VISCOUS_MATCHING", ctypes.c_int), ("E_DEP_FS", ctypes.c_int), ("E_R", ctypes.c_float),
+    ("TAU_R", ctypes.c_float), ("ALPHA", ctypes.c_float), ("DIM", ctypes.c_int),
+    ("TAU", ctypes.c_float),
+]
+
+
+class Params(ctypes.Structure):
+    _fields_ = PARAM_FIELDS
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in PARAM_FIELDS}
+
+
+_FP = ctypes.POINTER(ctypes.c_float)
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [("T", ctypes.c_void_p), ("J", ctypes.c_void_p), ("e", ctypes.c_void_p),
+                ("P", ctypes.c_void_p), ("Pi", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("pi", ctypes.c_void_p), ("nB", ctypes.c_void_p), ("V", ctypes.c_void_p)]
+
+
+class RunInfo(ctypes.Structure):
+    _fields_ = [("dim_phip", ctypes.c_int), ("dtau", ctypes.c_float), ("tau", ctypes.c_float),
+                ("live_rap_lo", ctypes.c_int), ("live_rap_hi", ctypes.c_int),
+                ("samples", ctypes.c_double)]
+
+
+class CtxOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("enable_timing", ctypes.c_int)]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [("prep_ms", ctypes.c_double), ("stream_ms", ctypes.c_double),
+                ("landau_ms", ctypes.c_double), ("prep_launches", ctypes.c_longlong),
+                ("stream_launches", ctypes.c_longlong), ("landau_launches", ctypes.c_longlong),
+                ("stream_samples", ctypes.c_double)]
+
+
+# Every symbol include/fsm.h declares, with (restype, argtypes).
+_VP = ctypes.c_void_p
+_ST = ctypes.c_int
+SIGNATURES = {
+    "fsm_status_str": (ctypes.c_char_p, [ctypes.c_int]),
+    "fsm_last_error": (ctypes.c_char_p, []),
+    "fsm_params_default": (None, [ctypes.POINTER(Params)]),
+    "fsm_params_read_file": (_ST, [ctypes.c_char_p, ctypes.POINTER(Params)]),
+    "fsm_params_derive": (None, [ctypes.POINTER(Params)]),
+    "fsm_ctx_create": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(CtxOpts)]),
+    "fsm_ctx_destroy": (None, [_VP]),
+    "fsm_ctx_timing": (_ST, [_VP, ctypes.POINTER(Timing), ctypes.c_int]),
+    "fsm_run_event": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP, ctypes.POINTER(Outputs),
+                            ctypes.POINTER(RunInfo)]),
+    "fsm_run_event_device": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP,
+                                   ctypes.POINTER(Outputs), _VP, ctypes.POINTER(RunInfo)]),
+    "fsm_batch_create": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(_VP)]),
+    "fsm_batch_destroy": (None, [_VP]),
+    "fsm_batch_views": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+                              ctypes.POINTER(Outputs)]),
+    "fsm_batch_launch": (_ST, [_VP, _VP]),
+    "fsm_batch_run_host": (_ST, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+                                 ctypes.POINTER(Outputs), _VP]),
+    "fsm_batch_info": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(RunInfo)]),
+    "fsm_batch_samples": (ctypes.c_double, [_VP]),
+    "fsm_batch_slabs": (_ST, [_VP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    "fsm_batch_event_offsets": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                                      ctypes.POINTER(ctypes.c_size_t)]),
+    "fsm_batch_upload": (_ST, [_VP, _VP, _VP]),
+    "fsm_batch_download": (_ST, [_VP, _VP, _VP]),
+    "fsm_batch_check": (_ST, [_VP]),
+    "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is not built (run `make -C freestream-milne_b200`); "
+                               "the compute path has no fallback")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class FsmError(RuntimeError):
+    def __init__(self, status, where):
+        msg = lib().fsm_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({msg})")
+        self.status = status
+
+
+def check(status, where):
+    if status != FSM_OK:
+        raise FsmError(status, where)
+
+
+def default_params(**kw):
+    p = Params()
+    lib().fsm_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    lib().fsm_params_derive(ctypes.byref(p))
+    return p
+
+
+def read_params_file(path, base=None):
+    p = base if base is not None else default_params()
+    check(lib().fsm_params_read_file(str(path).encode(), ctypes.byref(p)), "fsm_params_read_file")
+    return p
+
+
+OUT_COMPS = dict(T=10, J=4, e=1, P=1, Pi=1, u=4, pi=10, nB=1, V=4)
+SLAB_ORDER = ["T", "e", "P", "Pi", "u", "pi"]
+SLAB_ORDER_BARYON = SLAB_ORDER + ["J", "nB", "V"]
+
+
+def probe_fp32_tflops(device=0):
+    v = ctypes.c_double()
+    check(lib().fsm_probe_fp32_tflops(device, ctypes.byref(v)), "fsm_probe_fp32_tflops")
+    return v.value
+
+
+class Context:
+    def __init__(self, device=0, timing=False):
+        self.h = ctypes.c_void_p()
+        opts = CtxOpts(device, int(timing))
+        check(lib().fsm_ctx_create(ctypes.byref(self.h), ctypes.byref(opts)), "fsm_ctx_create")
+
+    def close(self):
+        if self.h:
+            lib().fsm_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def timing(self, reset=False):
+        t = Timing()
+        check(lib().fsm_ctx_timing(self.h, ctypes.byref(t), int(reset)), "fsm_ctx_timing")
+        return {k: getattr(t, k) for k, _ in Timing._fields_}
+
+    def run_event(self, params, e_gev, nB=None, outputs=None):
+        """Plain per-event path with host buffers; returns {name: ndarray}."""
+        e_gev = np.ascontiguousarray(e_gev, dtype=np.float32).ravel()
+        dim = params.DIM_X * params.DIM_Y * params.DIM_ETA
+        if e_gev.size != dim:
+            raise ValueError(f"input has {e_gev.size} cells, grid has {dim}")
+        baryon = bool(params.BARYON)
+        names = outputs or (list(OUT_COMPS) if baryon else [k for k in OUT_COMPS if k not in ("J", "nB", "V")])
+        arrs = {}
+        o = Outputs()
+        for k in names:
+            a = np.zeros((OUT_COMPS[k], dim) if OUT_COMPS[k] > 1 else (dim,), dtype=np.float32)
+            arrs[k] = a
+            setattr(o, k, a.ctypes.data)
+        nb_ptr = None
+        if baryon:
+            nB = np.ascontiguousarray(nB, dtype=np.float32).ravel()
+            nb_ptr = nB.ctypes.data
+        info = RunInfo()
+        check(lib().fsm_run_event(self.h, ctypes.byref(params), e_gev.ctypes.data, nb_ptr,
+                                  ctypes.byref(o), ctypes.byref(info)), "fsm_run_event")
+        arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
+        return arrs
+
+    def run_event_device(self, params, d_e, d_nB, dev_out, stream=None):
+        """Device path; d_e/d_nB/dev_out values are raw device pointers (ints)."""
+        o = Outputs(**{k: v for k, v in dev_out.items()})
+        info = RunInfo()
+        check(lib().fsm_run_event_device(self.h, ctypes.byref(params), d_e, d_nB, ctypes.byref(o),
+                                         stream, ctypes.byref(info)), "fsm_run_event_device")
+        return {k: getattr(info, k) for k, _ in RunInfo._fields_}
+
+
+class Batch:
+    def __init__(self, ctx, params_list):
+        self.ctx = ctx
+        n = len(params_list)
+        arr = (Params * n)(*params_list)
+        self.params = list(params_list)
+        self.h = ctypes.c_void_p()
+        check(lib().fsm_batch_create(ctx.h, n, arr, ctypes.byref(self.h)), "fsm_batch_create")
+        self.n = n
+        ib, ob = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib().fsm_batch_slabs(self.h, ctypes.byref(ib), ctypes.byref(ob)), "fsm_batch_slabs")
+        self.in_bytes, self.out_bytes = ib.value, ob.value
+
+    def close(self):
+        if self.h:
+            lib().fsm_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def offsets(self, ev):
+        a, b = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib().fsm_batch_event_offsets(self.h, ev, ctypes.byref(a), ctypes.byref(b)),
+              "fsm_batch_event_offsets")
+        return a.value, b.value
+
+    def info(self, ev):
+        info = RunInfo()
+        check(lib().fsm_batch_info(self.h, ev, ctypes.byref(info)), "fsm_batch_info")
+        return {k: getattr(info, k) for k, _ in RunInfo._fields_}
+
+    def samples(self):
+        return lib().fsm_batch_samples(self.h)
+
+    def upload(self, host_ptr, stream=None):
+        check(lib().fsm_batch_upload(self.h, host_ptr, stream), "fsm_batch_upload")
+
+    def download(self, host_ptr, stream=None):
+        check(lib().fsm_batch_download(self.h, host_ptr, stream), "fsm_batch_download")
+
+    def launch(self, stream=None):
+        check(lib().fsm_batch_launch(self.h, stream), "fsm_batch_launch")
+
+    def check_errors(self):
+        check(lib().fsm_batch_check(self.h), "fsm_batch_check")
+
+    def pack_inputs(self, inputs):
+        """inputs: list of (e_gev, nB or None) -> float32 host slab."""
+        slab = np.zeros(self.in_bytes // 4, dtype=np.float32)
+        for ev, (e, nb) in enumerate(inputs):
+            off, _ = self.offsets(ev)
+            e = np.ascontiguousarray(e, dtype=np.float32).ravel()
+            slab[off:off + e.size] = e
+            if self.params[ev].BARYON:
+                slab[off + e.size:off + 2 * e.size] = np.ascontiguousarray(nb, np.float32).ravel()
+        return slab
+
+    def unpack_outputs(self, slab, ev):
+        """Per-event dict of output arrays from a downloaded output slab."""
+        p = self.params[ev]
+        dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        _, off = self.offsets(ev)
+        res = {}
+        order = SLAB_ORDER_BARYON if p.BARYON else SLAB_ORDER
+        for k in order:
+            c = OUT_COMPS[k]
+            a = slab[off:off + c * dim]
+            res[k] = a.reshape(c, dim) if c > 1 else a
+            off += c * dim
+        return res
+
+    def run_host(self, inputs):
+        """Upload, launch, download, synchronise; returns per-event output dicts."""
+        import torch  # pinned staging only
+        ins = torch.from_numpy(self.pack_inputs(inputs)).pin_memory()
+        outs = torch.empty(self.out_bytes // 4, dtype=torch.float32).pin_memory()
+        self.upload(ins.data_ptr())
+        self.launch()
+        self.download(outs.data_ptr())
+        self.check_errors()  # synchronises
+        o = outs.numpy()
+        return [{k: v.copy() for k, v in self.unpack_outputs(o, ev).items()} for ev in range(self.n)]

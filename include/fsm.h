@@ -1,0 +1,200 @@
+/* fsm.h -- C ABI of the B200 free-streaming + Landau-matching library (libfsm.so).
+ *
+ * This is the drop-in boundary for the hot path of freestream-milne's
+ * FREESTREAMMILNE class (reference src/FreestreamMilne.cpp:28-136).  Every entry
+ * point takes plain pointers and sizes; CUDA streams are passed as `void*`
+ * (a cudaStream_t, NULL = the context's own stream).  Device work runs on one
+ * GPU with hand-written sm_100a kernels; there is no CPU fallback: every
+ * compute entry point returns FSM_ERR_NO_DEVICE when no GPU is present.
+ *
+ * Array conventions (identical to the reference):
+ *   cell index  is = (DIM_Y*DIM_ETA)*ix + DIM_ETA*iy + ieta
+ *               (src/FreeStream.cpp:23-25, FileIO.cpp:132)
+ *   tensors are component-major: T[c*DIM + is], components in the order
+ *   tt tx ty tn xx xy xn yy yn nn (src/LandauMatch.cpp:46-55), vectors t x y n.
+ *   Units: inputs e in GeV/fm^3 as initialize_from_vector takes them
+ *   (src/FreestreamMilne.cpp:43-46); nB as the IC_BARYON=3 file gives it
+ *   (src/FileIO.cpp:227-258, no conversion); float outputs are in the
+ *   reference's internal units (fm^-4, fm^-3) -- the compat class applies the
+ *   hbar*c factor of src/FreestreamMilne.cpp:700-716 when filling its vectors.
+ */
+#ifndef FSM_H_
+#define FSM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes replace the reference's printf+return / exit() paths. */
+typedef enum fsm_status {
+  FSM_OK = 0,
+  FSM_ERR_INVALID_ARG = 1,   /* NULL pointer, non-positive size, malformed params   */
+  FSM_ERR_SIZE_MISMATCH = 2, /* input length != DIM: reference exit(-1), FreestreamMilne.cpp:259-264 */
+  FSM_ERR_INVALID_IC = 3,    /* unknown IC_ENERGY/IC_BARYON: FreestreamMilne.cpp:277-281,302-306 */
+  FSM_ERR_UNSUPPORTED = 4,   /* parameter combination outside the implemented path  */
+  FSM_ERR_CUDA = 5,          /* a CUDA runtime call failed (see fsm_last_error)     */
+  FSM_ERR_NO_DEVICE = 6,     /* no CUDA device: there is no CPU fallback            */
+  FSM_ERR_OUT_OF_MEMORY = 7, /* device allocation failed                            */
+  FSM_ERR_FILE = 8,          /* params/IC file missing: FileIO.cpp:150-154,272-275  */
+  FSM_ERR_BUSY = 9,          /* server: request does not fit the HBM budget now     */
+  FSM_ERR_TIMEOUT = 10,      /* a bounded wait ran out                              */
+  FSM_ERR_PENDING = 11,      /* server: request admitted, result not ready yet      */
+  FSM_ERR_TOO_LARGE = 12,    /* request can never fit (budget / fixed limits)       */
+  FSM_ERR_CANCELLED = 13     /* server stopped before the request ran               */
+} fsm_status;
+
+const char* fsm_status_str(fsm_status s);
+/* Human-readable detail of the last error raised on the calling thread. */
+const char* fsm_last_error(void);
+
+/* Parameters: same fields, order and meaning as `struct parameters`
+ * (src/Parameter.h:2-33).  DIM and TAU are derived (FreestreamMilne.cpp:177-178). */
+typedef struct fsm_params {
+  int OUTPUTFORMAT;
+  int BARYON;
+  int IC_ENERGY;
+  int IC_BARYON;
+  float ETA_WIDTH;
+  float ETA_FLAT;
+  float SIGMA;
+  float SIGMA_B;
+  int DIM_X;
+  int DIM_Y;
+  int DIM_ETA;
+  int DIM_RAP;
+  int DIM_PHIP;
+  float DX;
+  float DY;
+  float DETA;
+  float DRAP;
+  float DTAU;
+  float TAU0;
+  int EOS_TYPE;
+  float E_FREEZE;
+  int VISCOUS_MATCHING;
+  int E_DEP_FS;
+  float E_R;
+  float TAU_R;
+  float ALPHA;
+  int DIM;
+  float TAU;
+} fsm_params;
+
+/* Defaults of src/FreestreamMilne.cpp:149-171 (E_R, TAU_R, ALPHA: 1, 1, 0). */
+void fsm_params_default(fsm_params* p);
+/* Positional parse of a freestream_input file (src/FileIO.cpp:260-339): 26
+ * "KEY<ws>value" lines in fixed order, the key text is ignored.  A missing
+ * file returns FSM_ERR_FILE and leaves *p untouched (the reference prints and
+ * keeps its defaults, FileIO.cpp:272-275). */
+fsm_status fsm_params_read_file(const char* path, fsm_params* p);
+/* Fills DIM and TAU (FreestreamMilne.cpp:177-178). */
+void fsm_params_derive(fsm_params* p);
+
+/* ------------------------------------------------------------------ context */
+typedef struct fsm_ctx fsm_ctx;
+
+typedef struct fsm_ctx_opts {
+  int device;          /* CUDA device ordinal                                    */
+  int enable_timing;   /* record CUDA events around every kernel (fsm_ctx_timing) */
+} fsm_ctx_opts;
+
+fsm_status fsm_ctx_create(fsm_ctx** ctx, const fsm_ctx_opts* opts /* NULL = defaults */);
+void fsm_ctx_destroy(fsm_ctx* ctx);
+
+/* Accumulated device time per kernel family since the last reset, measured
+ * with CUDA events on the launching stream (enable_timing must be set). */
+typedef struct fsm_timing {
+  double prep_ms;      /* input conversion + spline node construction          */
+  double stream_ms;    /* fused free-streaming + moment quadrature             */
+  double landau_ms;    /* Landau matching + EoS + viscous/baryon decomposition */
+  long long prep_launches, stream_launches, landau_launches;
+  double stream_samples; /* cell x momentum samples processed by stream launches */
+} fsm_timing;
+fsm_status fsm_ctx_timing(fsm_ctx* ctx, fsm_timing* t, int reset);
+
+/* --------------------------------------------------------------- outputs */
+/* Output views; host pointers for fsm_run_event, device pointers for the
+ * *_device entry points.  Any pointer may be NULL to skip that output. */
+typedef struct fsm_outputs {
+  float* T;   /* 10*DIM  T^{mu nu}                                            */
+  float* J;   /* 4*DIM   J^mu (BARYON)                                        */
+  float* e;   /* DIM     energy density                                       */
+  float* P;   /* DIM     pressure                                             */
+  float* Pi;  /* DIM     bulk pressure                                        */
+  float* u;   /* 4*DIM   flow velocity u^mu                                   */
+  float* pi;  /* 10*DIM  shear stress pi^{mu nu}                              */
+  float* nB;  /* DIM     baryon density (BARYON)                              */
+  float* V;   /* 4*DIM   baryon diffusion V^mu (BARYON)                        */
+} fsm_outputs;
+
+/* Effective run values (after E_DEP_FS and the phi_p rule of
+ * src/FreestreamMilne.cpp:316-332); n_fallback counts cells where Landau
+ * matching found no acceptable eigenvector (LandauMatch.cpp:283-291). */
+typedef struct fsm_run_info {
+  int dim_phip;
+  float dtau;
+  float tau;   /* tau_LandauMatch (FreestreamMilne.cpp:326) */
+  int live_rap_lo, live_rap_hi; /* 3D: rapidity nodes that can reach the grid */
+  double samples;               /* cell x momentum samples evaluated            */
+} fsm_run_info;
+
+/* ------------------------------------------------------------ plain path */
+/* One event, host buffers in and out (replaces run_freestream_milne's
+ * compute, src/FreestreamMilne.cpp:251-506).  Synchronous. */
+fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
+                         const float* nB, const fsm_outputs* host_out, fsm_run_info* info);
+
+/* One event on device-resident buffers, enqueued on `stream`; returns without
+ * synchronising.  E_DEP_FS=1 needs a host-visible profile and is rejected here
+ * (use fsm_run_event). */
+fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* d_e_gev,
+                                const float* d_nB, const fsm_outputs* dev_out, void* stream,
+                                fsm_run_info* info);
+
+/* --------------------------------------------------------------- batches */
+/* Many 2D/3D events of uneven size in one persistent launch per kernel family,
+ * captured into a CUDA graph on first launch.  The batch owns device input
+ * and output slabs; per-event views come from fsm_batch_views. */
+typedef struct fsm_batch fsm_batch;
+
+fsm_status fsm_batch_create(fsm_ctx* ctx, int n_events, const fsm_params* params,
+                            fsm_batch** batch);
+void fsm_batch_destroy(fsm_batch* b);
+/* Device views of event `ev`: input slots (d_e, d_nB) and outputs. */
+fsm_status fsm_batch_views(fsm_batch* b, int ev, float** d_e, float** d_nB,
+                           fsm_outputs* dev_out);
+/* Enqueue the whole batch on `stream` (graph replay after the first call). */
+fsm_status fsm_batch_launch(fsm_batch* b, void* stream);
+/* Host round trip: copy every event's input from host, launch, copy the
+ * outputs named in host_out[ev] back, synchronise.  nB may be NULL. */
+fsm_status fsm_batch_run_host(fsm_batch* b, const float* const* e_gev, const float* const* nB,
+                              const fsm_outputs* host_out, void* stream);
+fsm_status fsm_batch_info(fsm_batch* b, int ev, fsm_run_info* info);
+/* Slab interface: the batch keeps every event's inputs in one contiguous
+ * device slab (per event: e[DIM] then nB[DIM] when BARYON) and every event's
+ * outputs in another (per event: T(10) e P Pi u(4) pi(10), then J(4) nB V(4)
+ * when BARYON; each component DIM floats).  Offsets are in floats. */
+fsm_status fsm_batch_slabs(fsm_batch* b, size_t* in_bytes, size_t* out_bytes);
+fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_elem, size_t* out_elem);
+/* One host->device copy of the whole input slab / device->host copy of the
+ * whole output slab, enqueued on `stream` (pinned host memory makes them async). */
+fsm_status fsm_batch_upload(fsm_batch* b, const void* host_in, void* stream);
+fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream);
+/* Synchronous check of the kernels' internal error counters after a launch. */
+fsm_status fsm_batch_check(fsm_batch* b);
+/* Total cell x momentum samples of one launch of the batch. */
+double fsm_batch_samples(fsm_batch* b);
+
+/* ------------------------------------------------------------ diagnostics */
+/* Measured FP32 FMA throughput of `device` in TFLOP/s (a short FMA-chain
+ * kernel timed with CUDA events): the peak the stream kernels' roofline
+ * fraction is quoted against. */
+fsm_status fsm_probe_fp32_tflops(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSM_H_ */

@@ -1,0 +1,168 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE.  Compiles the freestream-milne
+// reference's own, unmodified sources (the single translation unit rooted at
+// src/FreestreamMilne.cpp) against the project's GSL-API stand-in
+// (gslshim/gsl/*.h) and exposes its hot path to the tests through a C ABI.
+//
+// Built by oracle/Makefile into oracle/_ref/ only where the reference sources
+// are present; never part of the product.  GSL itself is absent on this
+// machine, so results are "the reference's loops with the project's spline and
+// eigensolver", which pins everything except GSL's internals.
+#include "FreestreamMilne.cpp"  // reference: src/FreestreamMilne.cpp (via -I <reference>/src)
+
+#include <unistd.h>
+
+#include <cstring>
+
+#include "fsm_oracle.h"
+
+static_assert(sizeof(oracle_params) == sizeof(parameters), "parameter layout must match");
+
+// Runs the pipeline of src/FreestreamMilne.cpp:251-506 on the given inputs by
+// calling the reference's own functions in the reference's order.
+extern "C" int ref_run(const oracle_params* pin, const float* e_gev, const float* nB_in,
+                       oracle_out* out) {
+  parameters params;
+  std::memcpy(&params, pin, sizeof(params));
+  params.DIM = params.DIM_X * params.DIM_Y * params.DIM_ETA;
+  params.TAU = params.TAU0 + params.DTAU;
+  const int DIM = params.DIM;
+  float hbarc = 0.197326938;
+  float lower_tolerance = 1.0e-7;
+  float rescale = 1.0;
+
+  float* initialEnergyDensity = (float*)calloc(params.DIM, sizeof(float));
+  for (int i = 0; i < DIM; i++)
+    initialEnergyDensity[i] = e_gev[i] * rescale / (float)hbarc + lower_tolerance;
+  float* initialChargeDensity = NULL;
+  if (params.BARYON) {
+    initialChargeDensity = (float*)calloc(params.DIM, sizeof(float));
+    for (int i = 0; i < DIM; i++) initialChargeDensity[i] = nB_in[i];
+  }
+  if (params.E_DEP_FS == 1) {
+    float tau_fs = getEnergyDependentTau(initialEnergyDensity, params);
+    params.DTAU = tau_fs;
+    params.TAU = params.TAU0 + params.DTAU;
+  }
+  float min_dx_dy = min(params.DX, params.DY);
+  int nphip = int(ceil((2.0 * M_PI * params.DTAU) / min_dx_dy));
+  params.DIM_PHIP = max(params.DIM_PHIP, nphip);
+  out->dim_phip = params.DIM_PHIP;
+  out->dtau = params.DTAU;
+  out->tau = params.TAU;
+
+  float** density = NULL;
+  density = calloc2dArrayf(density, params.DIM, params.DIM_RAP);
+  float** chargeDensity = NULL;
+  if (params.BARYON) chargeDensity = calloc2dArrayf(chargeDensity, params.DIM, params.DIM_RAP);
+  convertInitialDensity(initialEnergyDensity, density, params);
+  free(initialEnergyDensity);
+  if (params.BARYON) convertInitialChargeDensity(initialChargeDensity, chargeDensity, params);
+  if (params.BARYON) free(initialChargeDensity);
+
+  float*** shiftedDensity = NULL;
+  shiftedDensity = calloc3dArrayf(shiftedDensity, params.DIM, params.DIM_RAP, params.DIM_PHIP);
+  float*** shiftedChargeDensity = NULL;
+  if (params.BARYON)
+    shiftedChargeDensity =
+        calloc3dArrayf(shiftedChargeDensity, params.DIM, params.DIM_RAP, params.DIM_PHIP);
+  freeStream(density, shiftedDensity, params);
+  free2dArrayf(density, params.DIM);
+  if (params.BARYON) freeStream(chargeDensity, shiftedChargeDensity, params);
+  if (params.BARYON) free2dArrayf(chargeDensity, params.DIM);
+
+  float** stressTensor = NULL;
+  stressTensor = calloc2dArrayf(stressTensor, 10, params.DIM);
+  float** baryonCurrent = NULL;
+  if (params.BARYON) baryonCurrent = calloc2dArrayf(baryonCurrent, 4, params.DIM);
+  float**** hypertrigTable = NULL;
+  hypertrigTable =
+      calloc4dArrayf(hypertrigTable, 10, params.DIM_RAP, params.DIM_PHIP, params.DIM_ETA);
+  calculateHypertrigTable(hypertrigTable, params);
+  calculateStressTensor(stressTensor, shiftedDensity, hypertrigTable, params);
+  free3dArrayf(shiftedDensity, params.DIM, params.DIM_RAP);
+  if (params.BARYON) {
+    calculateBaryonCurrent(baryonCurrent, shiftedChargeDensity, hypertrigTable, params);
+    free3dArrayf(shiftedChargeDensity, params.DIM, params.DIM_RAP);
+  }
+  free4dArrayf(hypertrigTable, 10, params.DIM_RAP, params.DIM_PHIP);
+
+  float* energyDensity = (float*)calloc(params.DIM, sizeof(float));
+  float* baryonDensity = NULL;
+  if (params.BARYON) baryonDensity = (float*)calloc(params.DIM, sizeof(float));
+  float** flowVelocity = NULL;
+  flowVelocity = calloc2dArrayf(flowVelocity, 4, params.DIM);
+  float* pressure = (float*)calloc(params.DIM, sizeof(float));
+  float* bulkPressure = (float*)calloc(params.DIM, sizeof(float));
+  float** shearTensor = NULL;
+  shearTensor = calloc2dArrayf(shearTensor, 10, params.DIM);
+  float** baryonDiffusion = NULL;
+  if (params.BARYON) baryonDiffusion = calloc2dArrayf(baryonDiffusion, 4, params.DIM);
+
+  solveEigenSystem(stressTensor, energyDensity, flowVelocity, params);
+  if (params.BARYON) {
+    calculateBaryonDensity(baryonDensity, baryonCurrent, flowVelocity, params);
+    calculateBaryonDiffusion(baryonDiffusion, baryonCurrent, baryonDensity, flowVelocity, params);
+  }
+  calculatePressure(energyDensity, baryonDensity, pressure, params);
+  if (params.VISCOUS_MATCHING) {
+    calculateBulkPressure(stressTensor, energyDensity, pressure, bulkPressure, params);
+    calculateShearViscTensor(stressTensor, energyDensity, flowVelocity, pressure, bulkPressure,
+                             shearTensor, params);
+  }
+
+  int nfb = 0;
+  for (int is = 0; is < DIM; ++is) {
+    if (out->T)
+      for (int v = 0; v < 10; ++v) out->T[(size_t)v * DIM + is] = stressTensor[v][is];
+    if (out->J && params.BARYON)
+      for (int v = 0; v < 4; ++v) out->J[(size_t)v * DIM + is] = baryonCurrent[v][is];
+    if (out->e) out->e[is] = energyDensity[is];
+    if (out->P) out->P[is] = pressure[is];
+    if (out->Pi) out->Pi[is] = bulkPressure[is];
+    if (out->u)
+      for (int v = 0; v < 4; ++v) out->u[(size_t)v * DIM + is] = flowVelocity[v][is];
+    if (out->pi)
+      for (int v = 0; v < 10; ++v) out->pi[(size_t)v * DIM + is] = shearTensor[v][is];
+    if (out->nB && params.BARYON) out->nB[is] = baryonDensity[is];
+    if (out->V && params.BARYON)
+      for (int v = 0; v < 4; ++v) out->V[(size_t)v * DIM + is] = baryonDiffusion[v][is];
+    if (energyDensity[is] == 1.0e-3f && flowVelocity[0][is] == 1.0f && flowVelocity[1][is] == 0.0f &&
+        flowVelocity[2][is] == 0.0f && flowVelocity[3][is] == 0.0f)
+      ++nfb;
+  }
+  out->n_fallback = nfb;
+
+  free2dArrayf(stressTensor, 10);
+  free(energyDensity);
+  free2dArrayf(flowVelocity, 4);
+  free(pressure);
+  free(bulkPressure);
+  free2dArrayf(shearTensor, 10);
+  if (params.BARYON) {
+    free2dArrayf(baryonCurrent, 4);
+    free(baryonDensity);
+    free2dArrayf(baryonDiffusion, 4);
+  }
+  return 0;
+}
+
+// Runs the reference's public entry point end to end (FREESTREAMMILNE, i.e.
+// src/FreestreamMilne.cpp:97-136,139-741) inside `workdir`, which must hold a
+// `freestream_input` file and an `output/` directory.  out17 receives the 17
+// output_to_vectors arrays (each n doubles) in the reference's argument order.
+extern "C" int ref_run_full(const char* workdir, const float* e_gev, int n, double* out17) {
+  char old[4096];
+  if (!getcwd(old, sizeof(old))) return 1;
+  if (chdir(workdir) != 0) return 2;
+  FREESTREAMMILNE fs;
+  std::vector<float> v(e_gev, e_gev + n);
+  fs.initialize_from_vector(v);
+  int rc = fs.run_freestream_milne();
+  std::vector<double> o[17];
+  fs.output_to_vectors(o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8], o[9], o[10], o[11],
+                       o[12], o[13], o[14], o[15], o[16]);
+  for (int k = 0; k < 17; ++k)
+    for (int i = 0; i < n && i < (int)o[k].size(); ++i) out17[(size_t)k * n + i] = o[k][i];
+  if (chdir(old) != 0) return 3;
+  return rc;
+}

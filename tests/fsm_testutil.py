@@ -1,0 +1,107 @@
+"""Shared helpers for the parity tests: fixtures, parameter conversion and the
+tolerance checks (each tolerance is stated where it is checked)."""
+import ctypes
+import pathlib
+
+import numpy as np
+
+import oracle_py as O
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+
+# Parity tolerances against the reference's float path (and the FP64 oracle):
+#   T^{mu nu}, J^mu : 1e-5, relative to the cell's T^{tau tau} (J^tau for J)
+#   e               : 1e-4 relative
+#   u^mu            : 1e-4, relative to u^tau
+#   Pi, pi^{mu nu}  : 1e-4, relative to the cell's e + P
+#   n_B, V^mu       : 1e-4, relative to the cell's |J^tau|
+# evaluated in cells with e > 1e-6 * max e.  Components with eta indices are
+# scaled by tau per eta index so that all components share the units of
+# T^{tau tau} (u^eta -> tau u^eta, T^{tau eta} -> tau T^{tau eta}, ...).
+TOL_T = 1e-5
+TOL_E = 1e-4
+TOL_U = 1e-4
+TOL_VISC = 1e-4
+TOL_B = 1e-4
+ETA_POW_T = np.array([0, 0, 0, 1, 0, 0, 1, 0, 1, 2])  # eta indices per T / pi component
+ETA_POW_V = np.array([0, 0, 0, 1])
+
+
+def golden_names():
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("full_"))
+
+
+def load_golden(name):
+    z = np.load(GOLDEN / f"{name}.npz")
+    ints = [k for k, t in O.PARAM_FIELDS if t is ctypes.c_int]
+    flts = [k for k, t in O.PARAM_FIELDS if t is ctypes.c_float]
+    d = {}
+    for k, v in zip(ints, z["params_int"]):
+        d[k] = int(v)
+    for k, v in zip(flts, z["params_float"]):
+        d[k] = float(v)
+    out = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
+    nB = z["nB_in"] if "nB_in" in z.files else None
+    meta = z["meta"]
+    return d, z["e_gev"], nB, out, meta
+
+
+def oracle_params(d):
+    p = O.Params(**d)
+    return p
+
+
+def fsm_params(d):
+    import fsm_b200 as F
+    p = F.Params(**d)
+    F.lib().fsm_params_derive(ctypes.byref(p))
+    return p
+
+
+def mask_of(ref):
+    e = np.asarray(ref["e"], dtype=np.float64)
+    return e > 1e-6 * e.max()
+
+
+def scale_eta(a, pow_, tau):
+    a = np.asarray(a, dtype=np.float64)
+    return a * (float(tau) ** pow_)[:, None]
+
+
+def compare(got, ref, tau, what=("T", "e", "u", "Pi", "pi"), baryon=False, tolT=TOL_T):
+    """Returns {name: worst scaled error} and raises AssertionError on failure."""
+    m = mask_of(ref)
+    errs = {}
+    Tref = np.asarray(ref["T"], np.float64)
+    ttt = Tref[0][m]
+    if "T" in what:
+        d = np.abs(scale_eta(got["T"], ETA_POW_T, tau) - scale_eta(Tref, ETA_POW_T, tau))[:, m]
+        errs["T"] = float(np.max(d / ttt))
+    if "e" in what:
+        e_r = np.asarray(ref["e"], np.float64)[m]
+        errs["e"] = float(np.max(np.abs(np.asarray(got["e"], np.float64)[m] - e_r) / e_r))
+    if "u" in what:
+        ur = scale_eta(ref["u"], ETA_POW_V, tau)[:, m]
+        ug = scale_eta(got["u"], ETA_POW_V, tau)[:, m]
+        errs["u"] = float(np.max(np.abs(ug - ur) / ur[0]))
+    ep = (np.asarray(ref["e"], np.float64) + np.asarray(ref["P"], np.float64))[m]
+    if "Pi" in what:
+        errs["Pi"] = float(np.max(np.abs(np.asarray(got["Pi"], np.float64)[m] -
+                                         np.asarray(ref["Pi"], np.float64)[m]) / ep))
+    if "pi" in what:
+        d = np.abs(scale_eta(got["pi"], ETA_POW_T, tau) - scale_eta(ref["pi"], ETA_POW_T, tau))[:, m]
+        errs["pi"] = float(np.max(d / ep))
+    if baryon:
+        Jr = np.asarray(ref["J"], np.float64)
+        jt = np.abs(Jr[0][m])
+        jm = jt > 1e-6 * jt.max()
+        dJ = np.abs(scale_eta(got["J"], ETA_POW_V, tau) - scale_eta(Jr, ETA_POW_V, tau))[:, m]
+        errs["J"] = float(np.max(dJ[:, jm] / jt[jm]))
+        dn = np.abs(np.asarray(got["nB"], np.float64)[m] - np.asarray(ref["nB"], np.float64)[m])
+        errs["nB"] = float(np.max(dn[jm] / jt[jm]))
+        dV = np.abs(scale_eta(got["V"], ETA_POW_V, tau) - scale_eta(ref["V"], ETA_POW_V, tau))[:, m]
+        errs["V"] = float(np.max(dV[:, jm] / jt[jm]))
+    limits = dict(T=tolT, e=TOL_E, u=TOL_U, Pi=TOL_VISC, pi=TOL_VISC, J=tolT, nB=TOL_B, V=TOL_B)
+    bad = {k: v for k, v in errs.items() if not v <= limits[k]}
+    assert not bad, f"tolerance exceeded: {bad} (all: {errs})"
+    return errs

@@ -1,0 +1,112 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the reference's
+float results (golden fixtures made from the reference sources), the oracle's
+float restatement and its FP64 run.  Tolerances are defined in fsm_testutil."""
+import numpy as np
+import pytest
+
+import fsm_b200 as F
+import oracle_py as O
+import workloads as W
+from fsm_testutil import (compare, fsm_params, golden_names, load_golden, oracle_params)
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle(p_fsm, e, nB=None, fp64=False):
+    po = O.Params(**p_fsm.as_dict())
+    return O.run(po, e, nB=nB, fp64=fp64)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_gpu_matches_reference_fixture(ctx, name):
+    d, e, nB, ref, meta = load_golden(name)
+    p = fsm_params(d)
+    got = ctx.run_event(p, e, nB)
+    assert got["info"]["dim_phip"] == int(meta[0])
+    assert got["info"]["tau"] == pytest.approx(float(meta[2]))
+    errs = compare(got, ref, meta[2], baryon=bool(d["BARYON"]))
+    # the FP64 run of the same algorithm bounds the error of both float paths
+    ref64 = O.run(oracle_params(d), e, nB=nB, fp64=True)
+    errs64 = compare(got, ref64, meta[2], baryon=bool(d["BARYON"]))
+    print(name, "vs reference float:", errs, "vs FP64:", errs64)
+
+
+def test_gpu_gaussian_full_grid(ctx):
+    """The plain 2D configuration at full size (101^2, DIM_PHIP=51)."""
+    p, e, _ = W.gaussian2d()
+    got = ctx.run_event(p, e)
+    ref = _oracle(p, e)
+    compare(got, ref, ref["tau"])
+    ref64 = _oracle(p, e, fp64=True)
+    compare(got, ref64, ref["tau"])
+
+
+def test_gpu_lumpy_full_grid(ctx):
+    """The lumpy 2D configuration at full size (261^2, DIM_PHIP=200, WB EoS)."""
+    p, e, _ = W.lumpy2d(seed=1)
+    got = ctx.run_event(p, e)
+    ref = _oracle(p, e)
+    errs = compare(got, ref, ref["tau"])
+    errs64 = compare(got, _oracle(p, e, fp64=True), ref["tau"])
+    print("lumpy2d vs float", errs, "vs FP64", errs64)
+
+
+def test_gpu_3d_baryon_reduced(ctx):
+    """3D + baryon path on a reduced grid the oracle runs in seconds."""
+    p, e, nB = W.baryon3d(seed=5, side=41, neta=21, nrap=21, nphip=40)
+    got = ctx.run_event(p, e, nB)
+    ref = _oracle(p, e, nB)
+    compare(got, ref, ref["tau"], baryon=True)
+
+
+def test_batch_equals_single_events(ctx):
+    """Every event of a mixed 2D/3D batch equals its single-event result bit for bit."""
+    evs = []
+    for name in golden_names():
+        d, e, nB, _, _ = load_golden(name)
+        evs.append((fsm_params(d), e, nB))
+    b = F.Batch(ctx, [p for p, _, _ in evs])
+    outs = b.run_host([(e, nB) for _, e, nB in evs])
+    for (p, e, nB), o in zip(evs, outs):
+        s = ctx.run_event(p, e, nB)
+        for k in o:
+            assert np.array_equal(o[k], s[k]), k
+    # a second launch (graph replay) gives the same results
+    outs2 = b.run_host([(e, nB) for _, e, nB in evs])
+    for o, o2 in zip(outs, outs2):
+        for k in o:
+            assert np.array_equal(o[k], o2[k])
+    b.close()
+
+
+def test_device_entry_point(ctx):
+    import torch
+    p, e, _ = W.lumpy2d(seed=9, side=101, dx=0.08, nphip=64, dtau=0.7)
+    dim = e.size
+    d_e = torch.from_numpy(e).cuda()
+    outs = {k: torch.zeros((F.OUT_COMPS[k] * dim,), dtype=torch.float32, device="cuda")
+            for k in ("T", "e", "P", "Pi", "u", "pi")}
+    stream = torch.cuda.current_stream().cuda_stream
+    ctx.run_event_device(p, d_e.data_ptr(), None, {k: v.data_ptr() for k, v in outs.items()},
+                         stream=stream)
+    torch.cuda.synchronize()
+    host = ctx.run_event(p, e)
+    for k, v in outs.items():
+        assert np.array_equal(v.cpu().numpy().reshape(host[k].shape), host[k]), k
+
+
+def test_energy_dependent_tau(ctx):
+    d, e, nB, ref, meta = load_golden("edepfs2d_45")
+    got = ctx.run_event(fsm_params(d), e)
+    assert got["info"]["dtau"] == pytest.approx(float(meta[1]), rel=0, abs=0)
+    compare(got, ref, meta[2])
+
+
+def test_invalid_inputs_are_rejected(ctx):
+    p = F.default_params(DIM_X=3)
+    with pytest.raises(F.FsmError):
+        ctx.run_event(p, np.zeros(3 * 101, np.float32))
+    p = F.default_params(DIM_ETA=5, DIM_RAP=1, DETA=0.2)
+    with pytest.raises(F.FsmError) as ei:
+        ctx.run_event(p, np.zeros(101 * 101 * 5, np.float32))
+    assert ei.value.status == 4

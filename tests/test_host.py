@@ -1,0 +1,152 @@
+"""CPU tests of the host side: the C-ABI library loads and exports every entry
+point include/fsm.h declares, parameter handling mirrors the reference, the
+library refuses to compute without a GPU, and the Landau-matching algorithm
+(compiled for the CPU from the same header the kernel uses) agrees with the
+oracle's reference-faithful solver."""
+import ctypes
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+import fsm_b200 as F
+import oracle_py as O
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def header_functions():
+    text = (ROOT / "include" / "fsm.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fsm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = F.lib()
+    names = header_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in include/fsm.h but not exported"
+        assert n in F.SIGNATURES, f"{n} missing from the ctypes binding"
+
+
+def test_param_struct_layout_matches_reference_order():
+    assert [f for f, _ in F.PARAM_FIELDS] == [f for f, _ in O.PARAM_FIELDS]
+    assert ctypes.sizeof(F.Params) == ctypes.sizeof(O.Params) == 28 * 4
+
+
+def test_params_default_match_reference():
+    p = F.default_params()
+    for k, v in O.DEFAULTS.items():
+        if k in ("DIM", "TAU"):
+            continue
+        assert getattr(p, k) == pytest.approx(v), k
+    assert p.DIM == 101 * 101 and p.TAU == pytest.approx(0.6)
+
+
+def test_params_positional_file(tmp_path):
+    # keys are ignored: only the position of each value matters (src/FileIO.cpp:279-334)
+    vals = ["2", "1", "5", "3", "0.7", "2.5", "0.9", "1.1", "31", "29", "7", "5", "33", "0.12",
+            "0.13", "0.2", "0.25", "0.75", "0.3", "2", "1.9", "0", "0", "3.0", "0.8", "0.5"]
+    text = "".join(f"KEY{i}\t{v}\n" for i, v in enumerate(vals))
+    f = tmp_path / "freestream_input"
+    f.write_text(text)
+    p = F.read_params_file(f)
+    assert (p.OUTPUTFORMAT, p.BARYON, p.IC_ENERGY, p.IC_BARYON) == (2, 1, 5, 3)
+    assert (p.DIM_X, p.DIM_Y, p.DIM_ETA, p.DIM_RAP, p.DIM_PHIP) == (31, 29, 7, 5, 33)
+    assert p.DX == pytest.approx(0.12) and p.DTAU == pytest.approx(0.75)
+    assert p.EOS_TYPE == 2 and p.VISCOUS_MATCHING == 0 and p.ALPHA == pytest.approx(0.5)
+    assert p.DIM == 31 * 29 * 7 and p.TAU == pytest.approx(0.3 + 0.75)
+
+
+def test_params_missing_file_reports_file_error(tmp_path):
+    p = F.default_params()
+    st = F.lib().fsm_params_read_file(str(tmp_path / "nope").encode(), ctypes.byref(p))
+    assert st == 8  # FSM_ERR_FILE, defaults untouched
+    assert p.DIM_X == 101
+
+
+def test_status_strings():
+    for code in F.STATUS:
+        assert F.lib().fsm_status_str(code)
+
+
+def test_no_cpu_fallback_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    st = F.lib().fsm_ctx_create(ctypes.byref(h), None)
+    assert st == 6  # FSM_ERR_NO_DEVICE: the library never computes on the CPU
+
+
+def _host_landau():
+    L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
+    L.fsm_hosttest_landau_cell.argtypes = ([ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 +
+                                           [ctypes.c_float, ctypes.c_void_p])
+    return L
+
+
+def _boosted_fluid(rng, is3d, tau):
+    e = 10 ** rng.uniform(-3, 2)
+    P = e * rng.uniform(0, 1, 3) * (1 if rng.random() < 0.8 else 0.01)
+    rap = rng.normal(0, 1.5 if rng.random() < 0.5 else 3.0, 3)
+    if not is3d:
+        rap[2] = 0
+    v = np.tanh(rap) / np.sqrt(3)
+    gam = 1 / np.sqrt(1 - np.sum(v ** 2))
+    L = np.eye(4)
+    L[0, 0] = gam
+    L[0, 1:] = gam * v
+    L[1:, 0] = gam * v
+    L[1:, 1:] += (gam - 1) * np.outer(v, v) / max(np.sum(v ** 2), 1e-300)
+    Tr = np.diag([e, P[0], P[1], P[2] if is3d else 0.0])
+    if not is3d:
+        L[3, :] = 0
+        L[:, 3] = 0
+        L[3, 3] = 1
+    Tm = L @ Tr @ L.T
+    S = np.diag([1, 1, 1, 1 / tau])
+    Tm = S @ Tm @ S
+    if not is3d:
+        Tm[3, :] = 0
+        Tm[:, 3] = 0
+    iu = [(0, 0), (0, 1), (0, 2), (0, 3), (1, 1), (1, 2), (1, 3), (2, 2), (2, 3), (3, 3)]
+    return np.array([Tm[a, b] for a, b in iu], np.float32)
+
+
+def test_landau_algorithm_matches_oracle_on_boosted_fluids():
+    """RQI + partial-pivoting solver (the kernel's algorithm) vs the oracle's
+    Francis-QR solver with the reference's selection rules."""
+    L = _host_landau()
+    rng = np.random.default_rng(5)
+    tau = 1.3
+    worst_e = worst_u = 0.0
+    for k in range(6000):
+        is3d = k % 2
+        T10 = _boosted_fluid(rng, is3d, tau)
+        ok1, e1, u1 = O.landau_cell(T10, tau)
+        out = np.zeros(24, np.float32)
+        J = np.zeros(4, np.float32)
+        ok2 = L.fsm_hosttest_landau_cell(T10.ctypes.data, J.ctypes.data, is3d, 0, 1, 1,
+                                         ctypes.c_float(tau), out.ctypes.data)
+        assert ok1 == ok2, (T10, is3d)
+        if ok1:
+            worst_e = max(worst_e, abs(out[0] - e1) / e1)
+            worst_u = max(worst_u, float(np.max(np.abs(out[3:7] - u1)) / u1[0]))
+    assert worst_e < 1e-6 and worst_u < 1e-6
+
+
+def test_landau_fallback_for_empty_and_null_cells():
+    L = _host_landau()
+    out = np.zeros(24, np.float32)
+    J = np.zeros(4, np.float32)
+    for T10 in (np.zeros(10, np.float32),
+                # null dust along x: no timelike eigenvector
+                np.array([1, 1, 0, 0, 1, 0, 0, 0, 0, 0], np.float32)):
+        ok = L.fsm_hosttest_landau_cell(T10.ctypes.data, J.ctypes.data, 0, 0, 1, 1,
+                                        ctypes.c_float(1.0), out.ctypes.data)
+        ok_o, e_o, u_o = O.landau_cell(T10, 1.0)
+        assert ok == ok_o == 0
+        assert out[0] == np.float32(1e-3) and tuple(out[3:7]) == (1, 0, 0, 0)
