@@ -42,7 +42,7 @@ WORKLOAD = ("uneven_batch: 512 seeded lumpy 2D events, side {101,151,201,261,301
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--events", type=int, default=512)

@@ -137,6 +137,21 @@ void batch_free(fsm_batch* b) {
   delete b;
 }
 
+// The dynamic shared-memory limit of a kernel is a process-wide attribute, so
+// it only ever grows: a batch built later with a smaller footprint must not
+// shrink the limit under a batch (or captured graph) built earlier.
+fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> g(mu);
+  (void)device;
+  if ((int)bytes > *slot) {
+    FSM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    *slot = (int)bytes;
+  }
+  return FSM_OK;
+}
+int g_smem2[64] = {0}, g_smem3[64] = {0};
+
 // Builds descriptors and uploads everything.  ext_in / ext_out (one event)
 // select external device buffers instead of owned slabs.
 fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
@@ -478,16 +493,18 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
   // ---- launch geometry
   if (b->ntiles) {
-    FSM_CUDA_TRY(cudaFuncSetAttribute(fsm_stream2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)std::max<size_t>(b->smem2, 1)));
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_stream2d_kernel, ctx->device, b->smem2,
+                                    &g_smem2[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream2d_kernel, kThreads2D,
                                                                b->smem2));
     b->grid2 = std::max(1, std::min(b->ntiles, ctx->num_sms * std::max(occ, 1)));
   }
   if (b->nb3) {
-    FSM_CUDA_TRY(cudaFuncSetAttribute(fsm_stream3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)std::max<size_t>(b->smem3, 1)));
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_kernel, ctx->device, b->smem3,
+                                    &g_smem3[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_kernel, kThreads3D,
                                                                b->smem3));

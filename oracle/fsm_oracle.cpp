@@ -8,12 +8,20 @@
 // interleaving the components per cell keeps every component's order, so the
 // float sums are unchanged) and no momentum-resolved array is stored.
 //
-// Template parameter R: float reproduces the reference's float/double mixing
-// operation by operation; double runs the same algorithm in FP64.
+// Template parameters: R is the value type (interpolation, weights, sums,
+// Landau matching) and FG selects float geometry.  <float, *> reproduces the
+// reference's float/double mixing operation by operation; <double, false> runs
+// the whole algorithm in FP64; <double, true> keeps the reference's float
+// geometry (sample angles, shifted positions, index floors and therefore the
+// set of in-grid samples) and does every value computation in FP64 -- the
+// precision oracle for the float paths, which would otherwise be dominated by
+// samples that land exactly on the grid boundary and flip in or out with the
+// rounding of their position.
 #include "fsm_oracle.h"
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -161,8 +169,9 @@ R pressure_of(R e, int eos) {
   return (R)0.0;  // EOS_TYPE 3 placeholder (src/EquationOfState.cpp:72-79)
 }
 
-template <class R>
+template <class R, bool FG>
 int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle_out* out) {
+  using G = typename std::conditional<FG, float, R>::type;  // geometry type
   oracle_params p = pin;
   if (p.DIM_X < 4 || p.DIM_Y < 4 || p.DIM_ETA < 1 || p.DIM_RAP < 1 || p.DIM_PHIP < 1) return 1;
   if (p.DIM_ETA > 1 && (p.DIM_ETA < 3 || p.DIM_RAP < 2)) return 1;
@@ -183,16 +192,17 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
   }
 
   // energy-dependent free-streaming time (src/FreeStream.cpp:389-417)
-  if (p.E_DEP_FS == 1) {
-    R num = 0.0, den = 0.0;
+  if (p.E_DEP_FS == 1) {  // the free-streaming time is geometry: G arithmetic
+    G num = 0.0, den = 0.0;
     for (int i = 0; i < DIM; ++i) {
-      R eps = e0[i];
+      G eps = (sizeof(G) == 4) ? (G)(e_gev[i] * 1.0f / kHbarcF + 1.0e-7f)
+                               : (G)((double)e_gev[i] / 0.197326938 + 1.0e-7);
       num += (eps * eps);
       den += eps;
     }
-    R e_T = (R)(num / (den + 1.0e-7));
-    e_T = e_T * (sizeof(R) == 4 ? (R)kHbarcF : (R)0.197326938);
-    R tau_fs = (R)p.TAU_R * std::pow((e_T / (R)p.E_R), (R)p.ALPHA);
+    G e_T = (G)(num / (den + 1.0e-7));
+    e_T = e_T * (sizeof(G) == 4 ? (G)kHbarcF : (G)0.197326938);
+    G tau_fs = (G)p.TAU_R * std::pow((e_T / (G)p.E_R), (G)p.ALPHA);
     p.DTAU = (float)tau_fs;
     p.TAU = p.TAU0 + p.DTAU;
   }
@@ -206,7 +216,7 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
   out->dtau = p.DTAU;
   out->tau = p.TAU;
 
-  const Grid<R> g = make_grid<R>(p);
+  const Grid<G> g = make_grid<G>(p);
   const int NX = g.DIM_X, NY = g.DIM_Y, NE = g.DIM_ETA, NR = g.DIM_RAP, NP = g.DIM_PHIP;
   const bool is3d = NE > 1;
 
@@ -219,11 +229,11 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
     R n = (R)(std::sqrt(M_PI / 2.0) * SIGMA * (1.0 + std::exp(2.0 * SIGMA * SIGMA)));
     norm_factor = (R)(1.0 / (2.0 * M_PI * n));
     for (int ieta = 0; ieta < NE; ++ieta) {
-      R eta = (R)ieta * g.DETA + g.etamin;
+      G eta = (G)ieta * g.DETA + g.etamin;
       for (int irap = 0; irap < NR; ++irap) {
-        R w = tanmap_w<R>(irap, NR);
-        R rap = (R)(eta + std::tan((M_PI / 2.0) * w));
-        R d = eta - rap;
+        G w = tanmap_w<G>(irap, NR);
+        G rap = (G)(eta + std::tan((M_PI / 2.0) * w));
+        R d = (R)(eta - rap);
         R rf = (R)(std::cosh(d) * std::cosh(d) *
                    std::exp((-1.0) * d * d / (2.0 * SIGMA * SIGMA)));
         rapf[(size_t)ieta * NR + irap] = rf;
@@ -243,13 +253,13 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
     R SIGMA_B = p.SIGMA_B;
     R n = (R)(std::sqrt(2.0 * M_PI) * SIGMA_B * std::exp(SIGMA_B * SIGMA_B / 2.0));
     normB = (R)(1.0 / (2.0 * M_PI * n));
-    R rapmin = (R)((-1.0) * ((R)(NR - 1) / 2.0) * g.DRAP);
+    G rapmin = (G)((-1.0) * ((G)(NR - 1) / 2.0) * g.DRAP);
     rapfB.resize((size_t)NE * NR);
     for (int ieta = 0; ieta < NE; ++ieta) {
-      R eta = (R)ieta * g.DETA + g.etamin;
+      G eta = (G)ieta * g.DETA + g.etamin;
       for (int irap = 0; irap < NR; ++irap) {
-        R rap = (R)irap * g.DRAP + rapmin;
-        R d = eta - rap;
+        G rap = (G)irap * g.DRAP + rapmin;
+        R d = (R)(eta - rap);
         rapfB[(size_t)ieta * NR + irap] =
             (R)(std::cosh(d) * std::exp((-1.0) * d * d / (SIGMA_B * SIGMA_B)));
       }
@@ -274,8 +284,8 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
     for (int ix = 0; ix < NX; ++ix)
       for (int iy = 0; iy < NY; ++iy) {
         int is = NY * ix + iy;
-        xv[ix] = (R)((R)ix * g.DX + g.xmin);
-        yv[iy] = (R)((R)iy * g.DY + g.ymin);
+        xv[ix] = (G)((G)ix * g.DX + g.xmin);
+        yv[iy] = (G)((G)iy * g.DY + g.ymin);
         zv[(size_t)NX * iy + ix] = Gval(is, 0);
         if (baryon) zb[(size_t)NX * iy + ix] = Jval(is, 0);
       }
@@ -294,41 +304,36 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
   };
   for (int irap = 0; irap < NR; ++irap)
     for (int iphip = 0; iphip < NP; ++iphip) {
-      R phip = phip_of<R>(iphip, NP);
+      const R phip = (R)phip_of<G>(iphip, NP);
       for (int ieta = 0; ieta < NE; ++ieta) {
-        R eta = (R)ieta * g.DETA + g.etamin;
+        G eta = (G)ieta * g.DETA + g.etamin;
         if (NE == 1) eta = 0.0;
-        R w = tanmap_w<R>(irap, NR);
-        R rap = (R)(eta + std::tan((M_PI / 2.0) * w));
+        G w = tanmap_w<G>(irap, NR);
+        G rap = (G)(eta + std::tan((M_PI / 2.0) * w));
         if (NE == 1) rap = 0.0;
-        R TAU = g.TAU;
+        const R d = (R)(rap - eta);
+        const R TAU = (R)g.TAU;
         TI(0, irap, iphip, ieta) = 1.0;
-        TI(1, irap, iphip, ieta) = std::cos(phip) / std::cosh(rap - eta);
-        TI(2, irap, iphip, ieta) = std::sin(phip) / std::cosh(rap - eta);
-        TI(3, irap, iphip, ieta) = (R)((1.0 / TAU) * std::tanh(rap - eta));
-        TI(4, irap, iphip, ieta) =
-            (std::cos(phip) * std::cos(phip)) / (std::cosh(rap - eta) * std::cosh(rap - eta));
-        TI(5, irap, iphip, ieta) =
-            (std::cos(phip) * std::sin(phip)) / (std::cosh(rap - eta) * std::cosh(rap - eta));
-        TI(6, irap, iphip, ieta) =
-            (R)((1.0 / TAU) * (std::cos(phip) * std::tanh(rap - eta)) / std::cosh(rap - eta));
-        TI(7, irap, iphip, ieta) =
-            (std::sin(phip) * std::sin(phip)) / (std::cosh(rap - eta) * std::cosh(rap - eta));
-        TI(8, irap, iphip, ieta) =
-            (R)((1.0 / TAU) * (std::sin(phip) * std::tanh(rap - eta)) / std::cosh(rap - eta));
-        TI(9, irap, iphip, ieta) =
-            (R)((1.0 / (TAU * TAU)) * std::tanh(rap - eta) * std::tanh(rap - eta));
+        TI(1, irap, iphip, ieta) = std::cos(phip) / std::cosh(d);
+        TI(2, irap, iphip, ieta) = std::sin(phip) / std::cosh(d);
+        TI(3, irap, iphip, ieta) = (R)((1.0 / TAU) * std::tanh(d));
+        TI(4, irap, iphip, ieta) = (std::cos(phip) * std::cos(phip)) / (std::cosh(d) * std::cosh(d));
+        TI(5, irap, iphip, ieta) = (std::cos(phip) * std::sin(phip)) / (std::cosh(d) * std::cosh(d));
+        TI(6, irap, iphip, ieta) = (R)((1.0 / TAU) * (std::cos(phip) * std::tanh(d)) / std::cosh(d));
+        TI(7, irap, iphip, ieta) = (std::sin(phip) * std::sin(phip)) / (std::cosh(d) * std::cosh(d));
+        TI(8, irap, iphip, ieta) = (R)((1.0 / TAU) * (std::sin(phip) * std::tanh(d)) / std::cosh(d));
+        TI(9, irap, iphip, ieta) = (R)((1.0 / (TAU * TAU)) * std::tanh(d) * std::tanh(d));
       }
     }
   std::vector<R> jac(NR);  // (src/LandauMatch.cpp:92-93)
   for (int irap = 0; irap < NR; ++irap) {
-    R w = tanmap_w<R>(irap, NR);
+    R w = (R)tanmap_w<G>(irap, NR);
     jac[irap] = (R)((M_PI / 2.0) / std::cos((M_PI / 2.0) * w) / std::cos((M_PI / 2.0) * w) *
                     (1.995 / R(NR - 1)));
   }
-  std::vector<R> cphi(NP), sphi(NP);
+  std::vector<G> cphi(NP), sphi(NP);
   for (int iphip = 0; iphip < NP; ++iphip) {
-    R phip = phip_of<R>(iphip, NP);
+    G phip = phip_of<G>(iphip, NP);
     cphi[iphip] = std::cos(phip);
     sphi[iphip] = std::sin(phip);
   }
@@ -341,22 +346,22 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
     int ix = is / (NY * NE);
     int iy = (is - (NY * NE * ix)) / NE;
     int ieta = is - (NY * NE * ix) - (NE * iy);
-    R x = (R)ix * g.DX + g.xmin;
-    R y = (R)iy * g.DY + g.ymin;
-    R eta = (R)ieta * g.DETA + g.etamin;
+    G x = (G)ix * g.DX + g.xmin;
+    G y = (G)iy * g.DY + g.ymin;
+    G eta = (G)ieta * g.DETA + g.etamin;
     R T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     R J[4] = {0, 0, 0, 0};
     for (int irap = 0; irap < NR; ++irap) {
-      R w = tanmap_w<R>(irap, NR);
-      R rap = (R)(eta + std::tan((M_PI / 2.0) * w));
+      G w = tanmap_w<G>(irap, NR);
+      G rap = (G)(eta + std::tan((M_PI / 2.0) * w));
       // (src/FreeStream.cpp:192-194) pieces independent of phi_p
-      R eta_new3 = 0, D3 = 0;
+      G eta_new3 = 0, D3 = 0;
       if (is3d) {
         eta_new3 = std::asinh((g.TAU / g.TAU0) * std::sinh(eta - rap)) + rap;
         D3 = (g.TAU * std::cosh(rap - eta_new3) - g.TAU0 * std::cosh(rap - eta));
       }
       for (int iphip = 0; iphip < NP; ++iphip) {
-        R eta_new, x_new, y_new;
+        G eta_new, x_new, y_new;
         if (NE == 1) {
           eta_new = 0.0;
           x_new = x - cphi[iphip] * g.DTAU;
@@ -366,13 +371,13 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
           x_new = x - cphi[iphip] * D3;
           y_new = y - sphi[iphip] * D3;
         }
-        R ix_new = (x_new - g.xmin) / g.DX;
-        R iy_new = (y_new - g.ymin) / g.DY;
-        R ieta_new;
+        G ix_new = (x_new - g.xmin) / g.DX;
+        G iy_new = (y_new - g.ymin) / g.DY;
+        G ieta_new;
         if (NE > 1) ieta_new = (eta_new - g.etamin) / g.DETA;
         else ieta_new = 0;
-        R ix_f = std::floor(ix_new), iy_f = std::floor(iy_new), ie_f = std::floor(ieta_new);
-        R xf = ix_new - ix_f, yf = iy_new - iy_f, ef = ieta_new - ie_f;
+        G ix_f = std::floor(ix_new), iy_f = std::floor(iy_new), ie_f = std::floor(ieta_new);
+        R xf = (R)(ix_new - ix_f), yf = (R)(iy_new - iy_f), ef = (R)(ieta_new - ie_f);
         if (!((ix_f >= 1) && (ix_f < NX - 1) && (iy_f >= 1) && (iy_f < NY - 1))) continue;
         R interp = 0.0, interpB = 0.0;
         bool have = false;
@@ -419,24 +424,24 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
       }
     }
     for (int v = 0; v < 10; ++v) {  // (src/LandauMatch.cpp:104-105)
-      if (NE == 1) T[v] = T[v] * d_phip / g.TAU;
+      if (NE == 1) T[v] = T[v] * d_phip / (R)g.TAU;
       else T[v] = T[v] * d_phip;
     }
     if (baryon)
       for (int v = 0; v < 4; ++v) J[v] = J[v] * g.DRAP * d_phip;  // (LandauMatch.cpp:140)
 
     R e, u[4];
-    int ok = landau_cell<R>(T, g.TAU, &e, u);
+    int ok = landau_cell<R>(T, (R)g.TAU, &e, u);
     if (!ok) ++n_fallback;
     R nBc = 0, V[4] = {0, 0, 0, 0};
     if (baryon) {  // (src/LandauMatch.cpp:370-392)
-      nBc = (u[0] * J[0]) - (u[1] * J[1]) - (u[2] * J[2]) - (g.TAU * g.TAU * u[3] * J[3]);
+      nBc = (u[0] * J[0]) - (u[1] * J[1]) - (u[2] * J[2]) - ((R)g.TAU * (R)g.TAU * u[3] * J[3]);
       for (int v = 0; v < 4; ++v) V[v] = J[v] - (nBc * u[v]);
     }
     R P = pressure_of<R>(e, p.EOS_TYPE);
     R Pi = 0, pi[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (p.VISCOUS_MATCHING) {  // (src/LandauMatch.cpp:332-367)
-      R TAU = g.TAU;
+      R TAU = (R)g.TAU;
       R a = T[0] - T[4] - T[7] - TAU * TAU * T[9];
       Pi = (R)((-1.0 / 3.0) * (a - e) - P);
       R b = e + P + Pi;
@@ -480,8 +485,9 @@ extern "C" int oracle_run(const oracle_params* p, int fp64, const float* e_gev, 
 #else
   (void)nthreads;
 #endif
-  if (fp64) return run<double>(*p, e_gev, nB, out);
-  return run<float>(*p, e_gev, nB, out);
+  if (fp64 == 1) return run<double, false>(*p, e_gev, nB, out);
+  if (fp64 == 2) return run<double, true>(*p, e_gev, nB, out);
+  return run<float, true>(*p, e_gev, nB, out);
 }
 
 extern "C" void oracle_spline_derivs(const double* x, const double* y, int n, double* d) {

@@ -8,7 +8,10 @@
  *   fp64 = 0  mirrors the reference's float/double mixing operation by
  *             operation (float arrays, float transcendentals where the
  *             reference calls them on floats, double GSL stand-ins);
- *   fp64 = 1  runs the same algorithm entirely in double: the error oracle.
+ *   fp64 = 1  runs the same algorithm entirely in double;
+ *   fp64 = 2  keeps the reference's float geometry (sample angles, shifted
+ *             positions, index floors: the same set of in-grid samples) and
+ *             computes every value in double -- the precision oracle.
  */
 #ifndef FSM_ORACLE_H_
 #define FSM_ORACLE_H_

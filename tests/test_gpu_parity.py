@@ -24,9 +24,9 @@ def test_gpu_matches_reference_fixture(ctx, name):
     got = ctx.run_event(p, e, nB)
     assert got["info"]["dim_phip"] == int(meta[0])
     assert got["info"]["tau"] == pytest.approx(float(meta[2]))
-    errs = compare(got, ref, meta[2], baryon=bool(d["BARYON"]))
-    # the FP64 run of the same algorithm bounds the error of both float paths
-    ref64 = O.run(oracle_params(d), e, nB=nB, fp64=True)
+    errs = compare(got, ref, meta[2], baryon=bool(d["BARYON"]), e_normwise=True)
+    # the FP64 precision oracle (the reference's sample set, FP64 values)
+    ref64 = O.run(oracle_params(d), e, nB=nB, fp64=2)
     errs64 = compare(got, ref64, meta[2], baryon=bool(d["BARYON"]))
     print(name, "vs reference float:", errs, "vs FP64:", errs64)
 
@@ -36,8 +36,8 @@ def test_gpu_gaussian_full_grid(ctx):
     p, e, _ = W.gaussian2d()
     got = ctx.run_event(p, e)
     ref = _oracle(p, e)
-    compare(got, ref, ref["tau"])
-    ref64 = _oracle(p, e, fp64=True)
+    compare(got, ref, ref["tau"], e_normwise=True)
+    ref64 = _oracle(p, e, fp64=2)
     compare(got, ref64, ref["tau"])
 
 
@@ -46,8 +46,8 @@ def test_gpu_lumpy_full_grid(ctx):
     p, e, _ = W.lumpy2d(seed=1)
     got = ctx.run_event(p, e)
     ref = _oracle(p, e)
-    errs = compare(got, ref, ref["tau"])
-    errs64 = compare(got, _oracle(p, e, fp64=True), ref["tau"])
+    errs = compare(got, ref, ref["tau"], e_normwise=True)
+    errs64 = compare(got, _oracle(p, e, fp64=2), ref["tau"])
     print("lumpy2d vs float", errs, "vs FP64", errs64)
 
 
@@ -56,7 +56,8 @@ def test_gpu_3d_baryon_reduced(ctx):
     p, e, nB = W.baryon3d(seed=5, side=41, neta=21, nrap=21, nphip=40)
     got = ctx.run_event(p, e, nB)
     ref = _oracle(p, e, nB)
-    compare(got, ref, ref["tau"], baryon=True)
+    compare(got, ref, ref["tau"], baryon=True, e_normwise=True)
+    compare(got, _oracle(p, e, nB, fp64=2), ref["tau"], baryon=True)
 
 
 def test_batch_equals_single_events(ctx):
@@ -99,7 +100,7 @@ def test_energy_dependent_tau(ctx):
     d, e, nB, ref, meta = load_golden("edepfs2d_45")
     got = ctx.run_event(fsm_params(d), e)
     assert got["info"]["dtau"] == pytest.approx(float(meta[1]), rel=0, abs=0)
-    compare(got, ref, meta[2])
+    compare(got, ref, meta[2], e_normwise=True)
 
 
 def test_invalid_inputs_are_rejected(ctx):
