@@ -23,9 +23,12 @@ struct float4_h { float x, y, z, w; };
 
 namespace fsm {
 
-constexpr int kTileX = 16;   // 2D output tile: x extent (slow index)
-constexpr int kTileY = 16;   // 2D output tile: y extent (fast index)
-constexpr int kThreads2D = kTileX * kTileY;
+constexpr int kCellsPerThread = 4;  // 2D: consecutive x cells owned by one thread
+constexpr int kTileY = 32;           // 2D output tile: y extent (fast index) = warp lanes
+constexpr int kWarps2D = 8;
+constexpr int kTileX = kWarps2D * kCellsPerThread;  // 2D output tile: x extent (slow index)
+constexpr int kThreads2D = kWarps2D * 32;
+constexpr int kPhiTab2D = 6;         // float4 per phi_p entry of the 2D table
 constexpr int kThreads3D = 256;
 constexpr int kThreadsLandau = 128;
 constexpr int kPhiChunk = 16;  // FP32 partial sums are folded into Kahan totals every 16 phi_p
@@ -41,6 +44,37 @@ struct SplineAxis {
   int n;
 };
 
+// Per-phi_p entry of the 2D stream table (6 float4, host computed).  With the
+// reference's float shift s = fl(cos(phi_p) * DTAU), the source point of cell ix
+// is ix + sx, sx = -s/DX, split into the integer offset ox = floor(sx) and the
+// fraction t = sx - ox (likewise y).  Stored, laid out for packed-pair FMAs: the
+// cubic Hermite weights of t and u and their derivatives (for the first-order
+// correction of each cell's own float-rounded coordinate), the moment weights,
+// the offsets and a flag telling whether t or u lies within 1e-3 of an integer
+// (then a sample on the grid boundary is re-evaluated with the reference's
+// exact float arithmetic).
+struct PhiEntry2D {
+  float H0, G0, H1, G1;      // Hermite weights of t (value/slope pairs of nodes 0 and 1)
+  float dH0, dG0, dH1, dG1;  // their derivatives in t
+  float K0, K1, L0, L1;      // Hermite weights of u
+  float dK0, dK1, dL0, dL1;
+  float c, s, cc, cs;        // cos, sin (reference floats), cos^2, cos sin
+  float t, u;
+  int ox;
+  int oy_near;               // low 16 bits: oy (signed); bit 16: near in x; bit 17: near in y
+};
+
+// A run of consecutive phi_p nodes whose source offsets fit one staged window:
+// for a tile at (x0, y0) the window starts at row x0 + ox0 - 1, column
+// y0 + oy0 - 1 (a one-node margin on each side for samples decided with the
+// reference arithmetic).
+struct Chunk2D {
+  int p0, p1, ox0, oy0;
+};
+constexpr int kMaxChunks2D = 64;
+constexpr int kWindowBudget2D = 36 * 1024;  // bytes of one staged window
+constexpr int kTotSlots2D = 5 * 4;          // per-thread moment totals kept in shared memory
+
 struct Ev2D {
   int NX, NY, NPHI, NR;
   float DX, DY, DTAU, TAU;
@@ -51,6 +85,10 @@ struct Ev2D {
   int use_smem;      // footprint fits the block's shared memory
   int tiles_y;       // tiles along y
   const FSM_FLOAT2* cs;  // [NPHI] (cos phi_p, sin phi_p), float as the reference computes them
+  const PhiEntry2D* tab; // [NPHI]
+  const Chunk2D* chunks; // [nchunks]
+  int nchunks;
+  int boxW, boxH;        // staged window (columns = y nodes, rows = x nodes)
   // prep
   const float* e_gev;    // input
   SplineAxis ax, ay;
@@ -116,9 +154,10 @@ struct CellBlock {
   int ev, begin;
 };
 
-// One 2D output tile of one event.
+// One 2D output tile of one event; interior = 1 when every sample of every
+// cell of the tile provably lands inside the grid (no bounds logic needed).
 struct Tile2D {
-  int ev, x0, y0, pad;
+  int ev, x0, y0, interior;
 };
 
 // Counters reset before each launch sequence.

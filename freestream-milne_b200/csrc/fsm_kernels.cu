@@ -14,6 +14,7 @@
 // src/LandauMatch.cpp:76-107).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cuda.h>
 
 #include "fsm_internal.h"
 #include "fsm_landau.cuh"
@@ -157,141 +158,261 @@ __device__ __forceinline__ void hermite(float t, float& H0, float& H1, float& G0
   G1 = t2 * (t - 1.0f);
 }
 
-template <bool kSmem>
-__device__ __forceinline__ void stream2d_tile(const Ev2D& ev, int x0, int y0, float4* __restrict__ sn,
-                                              const float2* __restrict__ scs, int* err) {
-  const int NX = ev.NX, NY = ev.NY, NPHI = ev.NPHI;
-  const int fx0 = max(0, x0 - ev.Rx), fx1 = min(NX - 1, x0 + kTileX + ev.Rx);
-  const int fy0 = max(0, y0 - ev.Ry), fy1 = min(NY - 1, y0 + kTileY + ev.Ry);
-  const int FW = fy1 - fy0 + 1, FH = fx1 - fx0 + 1;
-  const float4* __restrict__ gnodes = reinterpret_cast<const float4*>(ev.nodes);
-  if (kSmem) {
-    for (int k = threadIdx.x; k < FW * FH; k += blockDim.x) {
-      int r = k / FW, c = k - r * FW;
-      sn[k] = __ldg(gnodes + (size_t)(fx0 + r) * NY + (fy0 + c));
-    }
+__device__ __forceinline__ float4 node_at(const float4* __restrict__ sn, const float4* __restrict__ g,
+                                          bool smem, int i, int j, int fx0, int fy0, int FW, int NY) {
+  return smem ? sn[(i - fx0) * FW + (j - fy0)] : __ldg(g + (size_t)i * NY + j);
+}
+
+// One sample with the reference's own float arithmetic (src/FreeStream.cpp:
+// 187-246): shifted point, correctly rounded index division, in-grid test,
+// bilinear value and the bicubic patch inside the spline's open domain.  Used
+// for the rare samples whose in-grid decision depends on the rounding.
+__device__ __forceinline__ float exact_sample(const Ev2D& ev, const float4* __restrict__ sn, bool smem,
+                                           int fx0, int fy0, int FW, int FH, float x, float y,
+                                           float c, float s, int* err) {
+  const int NX = ev.NX, NY = ev.NY;
+  const float xn = __fsub_rn(x, __fmul_rn(c, ev.DTAU));
+  const float yn = __fsub_rn(y, __fmul_rn(s, ev.DTAU));
+  const float qx = __fdiv_rn(__fsub_rn(xn, ev.xmin), ev.DX);
+  const float qy = __fdiv_rn(__fsub_rn(yn, ev.ymin), ev.DY);
+  const float fxf = floorf(qx), fyf = floorf(qy);
+  if (!(fxf >= 1.0f && fxf < (float)(NX - 1) && fyf >= 1.0f && fyf < (float)(NY - 1))) return 0.0f;
+  const int i = (int)fxf, j = (int)fyf;
+  (void)FH;
+  const float4* g = reinterpret_cast<const float4*>(ev.nodes);
+  const float4 n00 = node_at(sn, g, smem, i, j, fx0, fy0, FW, NY);
+  const float4 n01 = node_at(sn, g, smem, i, j + 1, fx0, fy0, FW, NY);
+  const float4 n10 = node_at(sn, g, smem, i + 1, j, fx0, fy0, FW, NY);
+  const float4 n11 = node_at(sn, g, smem, i + 1, j + 1, fx0, fy0, FW, NY);
+  const float t = qx - fxf, u = qy - fyf;
+  float v = ((1.0f - t) * (1.0f - u) * n00.x) + (t * (1.0f - u) * n10.x) + ((1.0f - t) * u * n01.x) +
+            (t * u * n11.x);
+  if ((ev.xmin < xn) && (xn < ev.xmax_i) && (ev.ymin < yn) && (yn < ev.ymax_i)) {
+    float H0, H1, G0, G1, K0, K1, L0, L1;
+    hermite(t, H0, H1, G0, G1);
+    hermite(u, K0, K1, L0, L1);
+    const float r0 = H0 * n00.x + H1 * n10.x + G0 * n00.y + G1 * n10.y;
+    const float r1 = H0 * n01.x + H1 * n11.x + G0 * n01.y + G1 * n11.y;
+    const float s0 = H0 * n00.z + H1 * n10.z + G0 * n00.w + G1 * n10.w;
+    const float s1 = H0 * n01.z + H1 * n11.z + G0 * n01.w + G1 * n11.w;
+    const float cval = K0 * r0 + K1 * r1 + L0 * s0 + L1 * s1;
+    if (cval > 0.0f) v = cval;
   }
-  __syncthreads();
+  return v;
+}
 
-  const int lx = threadIdx.x / kTileY, ly = threadIdx.x - lx * kTileY;
-  const int ix = x0 + lx, iy = y0 + ly;
-  const bool active = (ix < NX) && (iy < NY);
-  const float DX = ev.DX, DY = ev.DY, DTAU = ev.DTAU;
-  const float xmin = ev.xmin, ymin = ev.ymin, inv_dx = ev.inv_dx, inv_dy = ev.inv_dy;
-  const float xmax_i = ev.xmax_i, ymax_i = ev.ymax_i;
-  const float NXm1 = (float)(NX - 1), NYm1 = (float)(NY - 1);
-  // cell coordinates (src/FreeStream.cpp:163-164)
-  const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
-  const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);
+// ------------------------------------------------------- TMA / mbarrier helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on an mbarrier phase: returns false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Contiguous bulk copy global -> shared (16-byte multiple) completing on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
-  float acc[6] = {0, 0, 0, 0, 0, 0}, tot[6] = {0, 0, 0, 0, 0, 0}, cmp[6] = {0, 0, 0, 0, 0, 0};
-  int nerr = 0;
-  for (int p = 0; p < NPHI; ++p) {
-    const float2 cs = scs[p];
-    // shifted position (src/FreeStream.cpp:187-199), same float rounding
-    const float xn = __fsub_rn(x, __fmul_rn(cs.x, DTAU));
-    const float yn = __fsub_rn(y, __fmul_rn(cs.y, DTAU));
-    float qx = __fmul_rn(__fsub_rn(xn, xmin), inv_dx);
-    float qy = __fmul_rn(__fsub_rn(yn, ymin), inv_dy);
-    // Where the in-grid test (src/FreeStream.cpp:213) could flip, use the
-    // reference's correctly rounded division.
-    if (fabsf(qx - 1.0f) < 1.0e-3f || fabsf(qx - NXm1) < 1.0e-3f)
-      qx = __fdiv_rn(__fsub_rn(xn, xmin), DX);
-    if (fabsf(qy - 1.0f) < 1.0e-3f || fabsf(qy - NYm1) < 1.0e-3f)
-      qy = __fdiv_rn(__fsub_rn(yn, ymin), DY);
-    const float fxf = floorf(qx), fyf = floorf(qy);
-    if (active && fxf >= 1.0f && fxf < NXm1 && fyf >= 1.0f && fyf < NYm1) {
-      const int i = (int)fxf, j = (int)fyf;
-      const float t = qx - fxf, u = qy - fyf;
-      float4 n00, n10, n01, n11;
-      if (kSmem) {
-        const int si = i - fx0, sj = j - fy0;
-        if ((unsigned)si > (unsigned)(FH - 2) || (unsigned)sj > (unsigned)(FW - 2)) {
-          ++nerr;  // outside the staged footprint: cannot happen for a correct halo
-          continue;
-        }
-        const int k = si * FW + sj;
-        n00 = sn[k];
-        n01 = sn[k + 1];
-        n10 = sn[k + FW];
-        n11 = sn[k + FW + 1];
-      } else {
-        const size_t k = (size_t)i * NY + j;
-        n00 = __ldg(gnodes + k);
-        n01 = __ldg(gnodes + k + 1);
-        n10 = __ldg(gnodes + k + NY);
-        n11 = __ldg(gnodes + k + NY + 1);
-      }
-      // bilinear (src/FreeStream.cpp:84-94)
-      float v = ((1.0f - t) * (1.0f - u) * n00.x) + (t * (1.0f - u) * n10.x) +
-                ((1.0f - t) * u * n01.x) + (t * u * n11.x);
-      // bicubic spline inside its open domain, used when positive
-      // (src/FreeStream.cpp:237-246)
-      if ((xmin < xn) && (xn < xmax_i) && (ymin < yn) && (yn < ymax_i)) {
-        float H0, H1, G0, G1, K0, K1, L0, L1;
-        hermite(t, H0, H1, G0, G1);
-        hermite(u, K0, K1, L0, L1);
-        const float r0 = H0 * n00.x + H1 * n10.x + G0 * n00.y + G1 * n10.y;
-        const float r1 = H0 * n01.x + H1 * n11.x + G0 * n01.y + G1 * n11.y;
-        const float s0 = H0 * n00.z + H1 * n10.z + G0 * n00.w + G1 * n10.w;
-        const float s1 = H0 * n01.z + H1 * n11.z + G0 * n01.w + G1 * n11.w;
-        const float c = K0 * r0 + K1 * r1 + L0 * s0 + L1 * s1;
-        if (c > 0.0f) v = c;
-      }
-      // moments with the 2D hypertrig rows 1, cos, sin, cos^2, cos sin, sin^2
-      // (src/LandauMatch.cpp:46-55 at rap = eta = 0)
-      acc[0] += v;
-      acc[1] += v * cs.x;
-      acc[2] += v * cs.y;
-      acc[3] += v * (cs.x * cs.x);
-      acc[4] += v * (cs.x * cs.y);
-      acc[5] += v * (cs.y * cs.y);
-    }
-    if ((p & (kPhiChunk - 1)) == kPhiChunk - 1) {
-#pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        kahan_add(tot[m], cmp[m], acc[m]);
-        acc[m] = 0.0f;
-      }
-    }
+// Warp-cooperative staging of one source window (boxH rows x boxW nodes, node
+// (0,0) = grid node (wx0, wy0)) with one bulk copy per in-grid row segment, all
+// completing on `bar`; optionally also the phi_p table.  Window slots outside
+// the grid are left unwritten: only samples that the in-grid test masks out
+// read them.  Called by all 32 lanes of one warp.
+__device__ __forceinline__ void stage_window(float4* buf, const float4* __restrict__ nodes, int NX,
+                                             int NY, int wx0, int wy0, int boxW, int boxH,
+                                             void* tab_dst, const void* tab_src, uint32_t tab_bytes,
+                                             uint64_t* bar) {
+  const int lane = threadIdx.x & 31;
+  fence_proxy_async();  // the buffer was last read through the generic proxy
+  const int c0 = max(0, wy0), c1 = min(NY - 1, wy0 + boxW - 1);
+  const uint32_t rowbytes = (c1 >= c0) ? (uint32_t)(c1 - c0 + 1) * 16u : 0u;
+  uint32_t bytes = 0;
+  for (int r = lane; r < boxH; r += 32) {
+    const int gr = wx0 + r;
+    if (gr >= 0 && gr < NX) bytes += rowbytes;
   }
 #pragma unroll
-  for (int m = 0; m < 6; ++m) kahan_add(tot[m], cmp[m], acc[m]);
-  if (nerr) atomicAdd(err, nerr);
-
-  if (active) {
-    // T = (sum over DIM_RAP identical rapidity copies) * d_phip / TAU
-    // (src/LandauMatch.cpp:104)
-    const float R = (float)ev.NR, dphi = ev.d_phip, TAU = ev.TAU;
-    float Tv[6];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) Tv[m] = __fdiv_rn(__fmul_rn(__fmul_rn(tot[m], R), dphi), TAU);
-    const size_t DIM = (size_t)NX * NY, is = (size_t)ix * NY + iy;
-    float* T = ev.T;
-    T[0 * DIM + is] = Tv[0];
-    T[1 * DIM + is] = Tv[1];
-    T[2 * DIM + is] = Tv[2];
-    T[3 * DIM + is] = 0.0f;
-    T[4 * DIM + is] = Tv[3];
-    T[5 * DIM + is] = Tv[4];
-    T[6 * DIM + is] = 0.0f;
-    T[7 * DIM + is] = Tv[5];
-    T[8 * DIM + is] = 0.0f;
-    T[9 * DIM + is] = 0.0f;
+  for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+  if (lane == 0) {
+    mbar_expect_tx(bar, bytes + tab_bytes);
+    if (tab_bytes) bulk_load(tab_dst, tab_src, tab_bytes, bar);
+  }
+  __syncwarp();
+  if (rowbytes) {
+    for (int r = lane; r < boxH; r += 32) {
+      const int gr = wx0 + r;
+      if (gr >= 0 && gr < NX)
+        bulk_load(buf + r * boxW + (c0 - wy0), nodes + (size_t)gr * NY + c0, rowbytes, bar);
+    }
   }
 }
 
-// Persistent kernel: each CTA takes output tiles from a global work list
-// (largest first) until it is exhausted.  The work counter is a plain
-// atomicAdd on a reset counter, so no CTA ever waits on another.
-__global__ void __launch_bounds__(kThreads2D) fsm_stream2d_kernel(const Ev2D* __restrict__ evs,
-                                                                  const Tile2D* __restrict__ tiles,
-                                                                  int ntiles, int cs_cap,
-                                                                  Counters* ctr, int* err) {
-  extern __shared__ float4 smem4[];
+constexpr int kWaitLimit = 1 << 20;  // polls of one bounded mbarrier wait
+
+// One phi_p run of one 32 x 32 output tile, on a staged window `win`
+// (boxW columns per row) whose node (0, 0) is grid node (wx0, wy0).  Lane l of
+// warp w owns the cells (x0 + 4w + k, y0 + l), k = 0..3.  For each phi_p every
+// cell of the tile shifts by the same vector, so the per-phi_p table gives the
+// source offset and the Hermite weights once for all cells; each cell applies a
+// first-order correction for its own float-rounded coordinate (the reference
+// positions samples relative to the float cell coordinate).  The y-direction
+// Hermite pass of a node row -- the (value, x-slope) pair, one packed-FMA chain
+// -- is shared by the two cells that use it, so a thread evaluates 5 node rows
+// for its 4 samples.  Moments accumulate in FP32 chunks of 16 phi_p folded
+// into FP32 totals (two-level summation).
+template <bool kInterior>
+__device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
+                                             int wy0, int boxW, const float4* __restrict__ stab,
+                                             int p0, int p1, int ixb, int iy, float y, float ey,
+                                             const float (&ex)[kCellsPerThread],
+                                             const bool (&act)[kCellsPerThread],
+                                             float (&a0)[kCellsPerThread],
+                                             float2 (&a12)[kCellsPerThread],
+                                             float2 (&a34)[kCellsPerThread],
+                                             float* __restrict__ stot, int* err) {
+  constexpr int K = kCellsPerThread;
+  const int NX = ev.NX, NY = ev.NY;
+  const float2 ey2 = make_float2(ey, ey);
+  for (int p = p0; p < p1; ++p) {
+    const float4* e = stab + kPhiTab2D * p;
+    const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], mw = e[4], tu = e[5];
+    const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
+    const int oy = (int)(short)(oyn & 0xffff);
+    const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
+    const int j = iy + oy, i0 = ixb + ox;
+    // y weights of this lane, first-order corrected for its own coordinate
+    const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
+    const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
+    const float uu = tu.y + ey;
+    const bool in_y = kInterior || ((j >= 1) && (j <= NY - 2));
+    const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
+    float2 VDp = make_float2(0.f, 0.f);
+    float Bp = 0.f;
+#pragma unroll
+    for (int r = 0; r <= K; ++r) {
+      const float4 n0 = rowp[r * boxW], n1 = rowp[r * boxW + 1];
+      // y pass of the node row: (value, x-slope) interpolated to the sample's y
+      float2 VD = __fmul2_rn(make_float2(Kp.x, Kp.x), make_float2(n0.x, n0.y));
+      VD = __ffma2_rn(make_float2(Kp.y, Kp.y), make_float2(n1.x, n1.y), VD);
+      VD = __ffma2_rn(make_float2(Lp.x, Lp.x), make_float2(n0.z, n0.w), VD);
+      VD = __ffma2_rn(make_float2(Lp.y, Lp.y), make_float2(n1.z, n1.w), VD);
+      const float B = fmaf(uu, n1.x - n0.x, n0.x);
+      if (r > 0) {
+        const int k = r - 1;
+        const float2 ex2 = make_float2(ex[k], ex[k]);
+        const float2 HG0 = __ffma2_rn(ex2, make_float2(dwx.x, dwx.y), make_float2(wx.x, wx.y));
+        const float2 HG1 = __ffma2_rn(ex2, make_float2(dwx.z, dwx.w), make_float2(wx.z, wx.w));
+        const float2 cc = __ffma2_rn(HG1, VD, __fmul2_rn(HG0, VDp));
+        const float cval = cc.x + cc.y;                             // bicubic
+        const float lval = fmaf(tu.x + ex[k], B - Bp, Bp);          // bilinear
+        float v = (cval > 0.0f) ? cval : lval;                      // src/FreeStream.cpp:245-246
+        if (!kInterior) {
+          const int ik = i0 + k;
+          bool in = act[k] && in_y && (ik >= 1) && (ik <= NX - 2);
+          // samples whose in-grid decision depends on rounding: exact path below
+          if (nearx && (ik <= 1 || ik >= NX - 2)) in = false;
+          if (neary && (j <= 1 || j >= NY - 2)) in = false;
+          v = in ? v : 0.0f;
+        }
+        const float2 v2 = make_float2(v, v);
+        a0[k] += v;
+        a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
+        a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+      }
+      VDp = VD;
+      Bp = B;
+    }
+    if (!kInterior && (nearx || neary)) {
+      // the fraction lies within 1e-3 of an integer: a sample next to the grid
+      // boundary may fall in or out with the rounding of its float position, so
+      // those samples (excluded above) are decided and evaluated with the
+      // reference arithmetic
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int ik = i0 + k;
+        const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+        const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+        const bool cx = (ik >= 1) && (ik <= NX - 2);
+        if (act[k] && (ux || uy) && (ux || cx) && (uy || in_y)) {
+          const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+          const float v = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
+          const float2 v2 = make_float2(v, v);
+          a0[k] += v;
+          a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
+          a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+        }
+      }
+    }
+    if ((p & (kPhiChunk - 1)) == kPhiChunk - 1) {
+      // second level of the two-level sum, thread-private slots in shared memory
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        stot[(5 * k + 0) * kThreads2D] += a0[k];
+        stot[(5 * k + 1) * kThreads2D] += a12[k].x;
+        stot[(5 * k + 2) * kThreads2D] += a12[k].y;
+        stot[(5 * k + 3) * kThreads2D] += a34[k].x;
+        stot[(5 * k + 4) * kThreads2D] += a34[k].y;
+        a0[k] = 0.0f;
+        a12[k] = a34[k] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+}
+
+// Persistent kernel over 32 x 32 output tiles taken from a global work list
+// (largest events first).  Per tile, the event's phi_p table and the source
+// window of each phi_p run are staged into shared memory by bulk copies
+// (cp.async.bulk, one per in-grid window row) completing on mbarriers,
+// double-buffered so the next run's window loads while the current one is
+// computed.  Every mbarrier wait is bounded; on time-out the CTA records an
+// error and leaves.
+__global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D* __restrict__ evs,
+                                                                     const Tile2D* __restrict__ tiles,
+                                                                     int ntiles, int tab_cap,
+                                                                     int box_cap, Counters* ctr,
+                                                                     int* err) {
+  extern __shared__ __align__(128) float4 smem4[];
+  __shared__ __align__(8) uint64_t bars[2];
   __shared__ int s_tile;
-  float2* scs = reinterpret_cast<float2*>(smem4);
-  float4* sn = smem4 + (cs_cap + 1) / 2;
+  float4* stab = smem4;
+  const size_t tab_f4 = ((size_t)tab_cap * kPhiTab2D + 7) & ~(size_t)7;  // 128-byte aligned
+  float4* const buf0 = smem4 + tab_f4;
+  float4* const buf1 = buf0 + box_cap;
+  float* const stot = reinterpret_cast<float*>(buf1 + box_cap) + threadIdx.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t phase0 = 0u, phase1 = 0u;
+  constexpr int K = kCellsPerThread;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->tile2d, 1);
     __syncthreads();
@@ -299,13 +420,96 @@ __global__ void __launch_bounds__(kThreads2D) fsm_stream2d_kernel(const Ev2D* __
     if (t >= ntiles) return;
     const Tile2D tl = tiles[t];
     const Ev2D& ev = evs[tl.ev];
-    for (int k = threadIdx.x; k < ev.NPHI; k += blockDim.x) {
-      const FSM_FLOAT2 c = ev.cs[k];
-      scs[k] = make_float2(c.x, c.y);
+    const int nch = ev.nchunks, boxW = ev.boxW, boxH = ev.boxH;
+    const Chunk2D* __restrict__ chunks = ev.chunks;
+    const float4* __restrict__ gnodes = reinterpret_cast<const float4*>(ev.nodes);
+    if (warp == 0) {
+      const Chunk2D c0 = chunks[0];
+      stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, boxW, boxH,
+                   stab, ev.tab, (uint32_t)ev.NPHI * kPhiTab2D * 16, &bars[0]);
     }
-    if (ev.use_smem) stream2d_tile<true>(ev, tl.x0, tl.y0, sn, scs, err);
-    else stream2d_tile<false>(ev, tl.x0, tl.y0, sn, scs, err);
-    __syncthreads();
+    // per-thread cell constants
+    const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
+    const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
+    const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
+    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
+    float ex[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int ix = ixb + k;
+      const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
+      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
+      act[k] = (ix < ev.NX) && (iy < ev.NY);
+    }
+    float a0[K];
+    float2 a12[K], a34[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      a0[k] = 0.0f;
+      a12[k] = a34[k] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int m = 0; m < kTotSlots2D; ++m) stot[m * kThreads2D] = 0.0f;
+
+    for (int c = 0; c < nch; ++c) {
+      const int b = c & 1;
+      if (warp == 0 && c + 1 < nch) {
+        const Chunk2D cn = chunks[c + 1];
+        stage_window(b ? buf0 : buf1, gnodes, ev.NX, ev.NY, tl.x0 + cn.ox0 - 1, tl.y0 + cn.oy0 - 1,
+                     boxW, boxH, nullptr, nullptr, 0u, &bars[b ^ 1]);
+      }
+      const uint32_t ph = b ? phase1 : phase0;
+      const bool ok = mbar_wait(&bars[b], ph, kWaitLimit);
+      if (b) phase1 ^= 1u;
+      else phase0 ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        // a staged copy did not complete: record it, drain, and leave
+        if (threadIdx.x == 0) {
+          atomicAdd(err + 1, 1);
+          if (c + 1 < nch) mbar_wait(&bars[b ^ 1], b ? phase0 : phase1, kWaitLimit);
+        }
+        return;
+      }
+      const Chunk2D ch = chunks[c];
+      const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1;
+      const float4* win = b ? buf1 : buf0;
+      if (tl.interior)
+        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
+                           a12, a34, stot, err);
+      else
+        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
+                            a12, a34, stot, err);
+      __syncthreads();  // buffer b is free for the load of run c + 2
+    }
+    // T = (sum over DIM_RAP identical rapidity copies) * d_phip / TAU
+    // (src/LandauMatch.cpp:104); T^yy = sum v sin^2 = S1 - S_cc.
+    const float R = (float)ev.NR, dphi = ev.d_phip, TAU = ev.TAU;
+    const size_t DIM = (size_t)ev.NX * ev.NY;
+    float* T = ev.T;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      const float tot[5] = {stot[(5 * k + 0) * kThreads2D] + a0[k],
+                            stot[(5 * k + 1) * kThreads2D] + a12[k].x,
+                            stot[(5 * k + 2) * kThreads2D] + a12[k].y,
+                            stot[(5 * k + 3) * kThreads2D] + a34[k].x,
+                            stot[(5 * k + 4) * kThreads2D] + a34[k].y};
+      float S[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) S[m] = __fdiv_rn(__fmul_rn(__fmul_rn(tot[m], R), dphi), TAU);
+      const size_t is = (size_t)(ixb + k) * ev.NY + iy;
+      T[0 * DIM + is] = S[0];
+      T[1 * DIM + is] = S[1];
+      T[2 * DIM + is] = S[2];
+      T[3 * DIM + is] = 0.0f;
+      T[4 * DIM + is] = S[3];
+      T[5 * DIM + is] = S[4];
+      T[6 * DIM + is] = 0.0f;
+      T[7 * DIM + is] = S[0] - S[3];
+      T[8 * DIM + is] = 0.0f;
+      T[9 * DIM + is] = 0.0f;
+    }
   }
 }
 

@@ -120,6 +120,82 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     };
     axis(NX, p.DX, E.xmin, E.hx, E.fx, E.dgx);
     axis(NY, p.DY, E.ymin, E.hy, E.fy, E.dgy);
+    // per-phi_p stream table (see PhiEntry2D)
+    E.tab2.resize(NP);
+    for (int k = 0; k < NP; ++k) {
+      PhiEntry2D& w = E.tab2[k];
+      const float c = E.cs[k].x, s = E.cs[k].y;
+      const float shx = c * p.DTAU, shy = s * p.DTAU;  // reference float products
+      const double sx = -(double)shx / (double)p.DX, sy = -(double)shy / (double)p.DY;
+      const double ox = std::floor(sx), oy = std::floor(sy);
+      const double t = sx - ox, u = sy - oy;
+      auto herm = [](double a, float* H0, float* H1, float* G0, float* G1, float* dH0, float* dH1,
+                     float* dG0, float* dG1) {
+        *H0 = 1.0 - 3.0 * a * a + 2.0 * a * a * a;
+        *H1 = 3.0 * a * a - 2.0 * a * a * a;
+        *G0 = a - 2.0 * a * a + a * a * a;
+        *G1 = a * a * a - a * a;
+        *dH0 = -6.0 * a + 6.0 * a * a;
+        *dH1 = -*dH0;
+        *dG0 = 1.0 - 4.0 * a + 3.0 * a * a;
+        *dG1 = 3.0 * a * a - 2.0 * a;
+      };
+      herm(t, &w.H0, &w.H1, &w.G0, &w.G1, &w.dH0, &w.dH1, &w.dG0, &w.dG1);
+      herm(u, &w.K0, &w.K1, &w.L0, &w.L1, &w.dK0, &w.dK1, &w.dL0, &w.dL1);
+      w.t = (float)t;
+      w.u = (float)u;
+      w.c = c;
+      w.s = s;
+      w.cc = c * c;
+      w.cs = c * s;
+      w.ox = (int)ox;
+      const int nearx = (t < 1e-3 || t > 1.0 - 1e-3) ? 1 : 0;
+      const int neary = (u < 1e-3 || u > 1.0 - 1e-3) ? 1 : 0;
+      w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
+    }
+    // phi_p runs whose staged window (tile + offset spread + 1-node margins)
+    // fits the window budget; consecutive nodes have neighbouring offsets
+    {
+      auto win_bytes = [](int dox, int doy) {
+        return (size_t)(kTileX + dox + 3) * (size_t)(kTileY + doy + 3) * 16;
+      };
+      E.chunks2.clear();
+      int p0 = 0;
+      auto oy_of = [&](int k) { return (int)(short)(E.tab2[k].oy_near & 0xffff); };
+      int lo_x = E.tab2[0].ox, hi_x = lo_x, lo_y = oy_of(0), hi_y = lo_y;
+      E.ox_min = E.ox_max = lo_x;
+      E.oy_min = E.oy_max = lo_y;
+      for (int k = 1; k <= NP; ++k) {
+        bool flush = (k == NP);
+        if (!flush) {
+          int nlx = std::min(lo_x, E.tab2[k].ox), nhx = std::max(hi_x, E.tab2[k].ox);
+          int nly = std::min(lo_y, oy_of(k)), nhy = std::max(hi_y, oy_of(k));
+          if (win_bytes(nhx - nlx, nhy - nly) > (size_t)kWindowBudget2D) {
+            flush = true;
+          } else {
+            lo_x = nlx; hi_x = nhx; lo_y = nly; hi_y = nhy;
+          }
+        }
+        if (flush) {
+          E.chunks2.push_back(Chunk2D{p0, k, lo_x, lo_y});
+          E.boxH = std::max(E.boxH, kTileX + (hi_x - lo_x) + 3);
+          E.boxW = std::max(E.boxW, kTileY + (hi_y - lo_y) + 3);
+          if (k < NP) {
+            p0 = k;
+            lo_x = hi_x = E.tab2[k].ox;
+            lo_y = hi_y = oy_of(k);
+          }
+        }
+        if (k < NP) {
+          E.ox_min = std::min(E.ox_min, E.tab2[k].ox);
+          E.ox_max = std::max(E.ox_max, E.tab2[k].ox);
+          E.oy_min = std::min(E.oy_min, oy_of(k));
+          E.oy_max = std::max(E.oy_max, oy_of(k));
+        }
+      }
+      if ((int)E.chunks2.size() > kMaxChunks2D || E.boxW > 256 || E.boxH > 256)
+        return fail(FSM_ERR_TOO_LARGE, "free-streaming distance too large for the staged windows");
+    }
     E.Rx = (int)std::ceil(p.DTAU / p.DX) + 2;
     E.Ry = (int)std::ceil(p.DTAU / p.DY) + 2;
     E.samples = (double)p.DIM * NP;

@@ -18,6 +18,10 @@ struct EventPlan {
   int DIM = 0;
   float xmin = 0, ymin = 0, etamin = 0, xmax_i = 0, ymax_i = 0, d_phip = 0;
   std::vector<FSM_FLOAT2> cs;  // (cos, sin) of phi_p
+  std::vector<PhiEntry2D> tab2;  // 2D stream table
+  std::vector<Chunk2D> chunks2;  // phi_p runs staged as one window each
+  int boxW = 0, boxH = 0;        // staged window size (nodes)
+  int ox_min = 0, ox_max = 0, oy_min = 0, oy_max = 0;  // offset range over all phi_p
   // 2D spline axes
   std::vector<double> hx, fx, dgx, hy, fy, dgy;
   int Rx = 0, Ry = 0;

@@ -26,7 +26,7 @@ namespace fsm {
 __global__ void fsm_prep2d_lines_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_pack_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
-__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const CellBlock*, int, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 }  // namespace fsm
@@ -101,12 +101,13 @@ struct fsm_batch {
   Counters* d_ctr = nullptr;
   int* d_err = nullptr;
   int ntiles = 0, nlines = 0, npacks = 0, nprep3 = 0, nb3 = 0, nbl = 0;
-  int cs_cap2 = 0, cs_cap3 = 0;
+  int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0;
   size_t smem2 = 0, smem3 = 0;
   int grid2 = 0, grid3 = 0;
   double samples = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
+  cudaStream_t last_stream = nullptr;  // stream of the most recent upload/launch/download
 };
 
 namespace {
@@ -173,7 +174,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   // ---- layout
   Layout L;
   struct EvOffs {
-    size_t cs, hx, fx, dgx, hy, fy, dgy, re, rapf, rapfB, jac;
+    size_t cs, tab2, chunks, hx, fx, dgx, hy, fy, dgy, re, rapf, rapfB, jac;
     size_t zx, zy, nodes, efield, T, J, in_e, in_nB, out;
   };
   std::vector<EvOffs> eo(n);
@@ -198,6 +199,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     EvOffs& o = eo[i];
     o.cs = L.take(P.cs.size() * sizeof(FSM_FLOAT2));
     if (!P.is3d) {
+      o.tab2 = L.take(P.tab2.size() * sizeof(PhiEntry2D));
+      o.chunks = L.take(P.chunks2.size() * sizeof(Chunk2D));
       o.hx = L.take(P.hx.size() * 8);
       o.fx = L.take(P.fx.size() * 8);
       o.dgx = L.take(P.dgx.size() * 8);
@@ -224,9 +227,18 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     });
     for (int i : order2) {
       const EventPlan& P = b->plans[i];
-      int tx = (P.p.DIM_X + kTileX - 1) / kTileX, ty = (P.p.DIM_Y + kTileY - 1) / kTileY;
+      const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
+      int tx = (NX + kTileX - 1) / kTileX, ty = (NY + kTileY - 1) / kTileY;
       for (int a = 0; a < tx; ++a)
-        for (int c = 0; c < ty; ++c) tiles.push_back(Tile2D{b->ev2_of[i], a * kTileX, c * kTileY, 0});
+        for (int c = 0; c < ty; ++c) {
+          const int x0 = a * kTileX, y0 = c * kTileY;
+          // every sample of every cell lands at least one node inside the grid
+          // boundary, so neither the in-grid test nor its rounding matters
+          const int interior = (x0 + kTileX <= NX) && (y0 + kTileY <= NY) && (x0 + P.ox_min >= 2) &&
+                               (x0 + kTileX - 1 + P.ox_max <= NX - 3) && (y0 + P.oy_min >= 2) &&
+                               (y0 + kTileY - 1 + P.oy_max <= NY - 3);
+          tiles.push_back(Tile2D{b->ev2_of[i], x0, y0, interior});
+        }
     }
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
@@ -309,6 +321,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     EvOffs& o = eo[i];
     std::memcpy(H + o.cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
     if (!P.is3d) {
+      std::memcpy(H + o.tab2, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
+      std::memcpy(H + o.chunks, P.chunks2.data(), P.chunks2.size() * sizeof(Chunk2D));
       std::memcpy(H + o.hx, P.hx.data(), P.hx.size() * 8);
       std::memcpy(H + o.fx, P.fx.data(), P.fx.size() * 8);
       std::memcpy(H + o.dgx, P.dgx.data(), P.dgx.size() * 8);
@@ -366,7 +380,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->evl.assign(n, EvLandau{});
   int max_np2 = 0, max_np3 = 0;
   size_t max_fp = 0;
-  const size_t smem_budget = 96 * 1024;  // footprint bytes staged per CTA (2 CTAs/SM)
+  const size_t smem_budget = 84 * 1024;  // footprint bytes staged per CTA (2 CTAs/SM with the table)
   for (int i = 0; i < n; ++i) {
     const EventPlan& P = b->plans[i];
     const EvOffs& o = eo[i];
@@ -393,6 +407,12 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       size_t fpw = std::min(p.DIM_Y, kTileY + 2 * P.Ry + 1);
       size_t fph = std::min(p.DIM_X, kTileX + 2 * P.Rx + 1);
       size_t fp = fpw * fph * 16;
+      e.tab = reinterpret_cast<const PhiEntry2D*>(D + o.tab2);
+      e.chunks = reinterpret_cast<const Chunk2D*>(D + o.chunks);
+      e.nchunks = (int)P.chunks2.size();
+      e.boxW = P.boxW;
+      e.boxH = P.boxH;
+      b->box_cap2 = std::max(b->box_cap2, P.boxW * P.boxH);
       e.use_smem = fp <= smem_budget ? 1 : 0;
       if (e.use_smem) max_fp = std::max(max_fp, fp);
       e.tiles_y = (p.DIM_Y + kTileY - 1) / kTileY;
@@ -460,10 +480,19 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     l.V = v.V;
     b->samples += P.samples;
   }
-  b->cs_cap2 = (max_np2 + 1) & ~1;
+  b->cs_cap2 = max_np2;
   b->cs_cap3 = (max_np3 + 1) & ~1;
-  b->smem2 = (size_t)b->cs_cap2 * 8 + max_fp;
+  b->box_cap2 = (b->box_cap2 + 7) & ~7;  // float4 units, 128-byte multiple
+  b->smem2 = (((size_t)b->cs_cap2 * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)b->box_cap2 * 16 +
+             (size_t)kTotSlots2D * kThreads2D * 4;
   b->smem3 = (size_t)b->cs_cap3 * 8;
+  (void)max_fp;
+  // the kernels index their dynamic shared memory by these capacities
+  if ((n2 && b->smem2 < (size_t)b->cs_cap2 * kPhiTab2D * 16 + 2 * (size_t)b->box_cap2 * 16) ||
+      (n3 && b->smem3 < (size_t)max_np3 * 8)) {
+    set_last_error("internal error: dynamic shared memory below the staged tables");
+    return FSM_ERR_CUDA;
+  }
   std::memcpy(H + o_ev2, b->ev2.data(), n2 * sizeof(Ev2D));
   std::memcpy(H + o_ev3, b->ev3.data(), n3 * sizeof(Ev3D));
   std::memcpy(H + o_evl, b->evl.data(), n * sizeof(EvLandau));
@@ -543,7 +572,8 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
   if (timing) cudaEventRecord(ts.ev[1], s);
   if (b->ntiles)
     fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
-                                                               b->cs_cap2, b->d_ctr, b->d_err);
+                                                               b->cs_cap2, b->box_cap2, b->d_ctr,
+                                                               b->d_err);
   if (b->nb3)
     fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_b3, b->nb3,
                                                                b->cs_cap3, b->d_ctr);
@@ -560,6 +590,7 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
 
 fsm_status launch(fsm_batch* b, cudaStream_t s) {
   fsm_ctx* ctx = b->ctx;
+  b->last_stream = s;
   if (ctx->timing) return enqueue(b, s, true);
   if (!b->graph || b->graph_stream != s) {
     if (b->graph) {
@@ -591,13 +622,22 @@ fsm_status launch(fsm_batch* b, cudaStream_t s) {
   return FSM_OK;
 }
 
+// Reads the kernels' error counters in stream order on the batch's last
+// stream and waits for it, so every copy enqueued before has completed.
 fsm_status check_kernel_errors(fsm_batch* b) {
   int err[4] = {0, 0, 0, 0};
-  FSM_CUDA_TRY(cudaMemcpy(err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+  cudaStream_t s = b->last_stream ? b->last_stream : b->ctx->stream;
+  FSM_CUDA_TRY(cudaMemcpyAsync(err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost, s));
+  FSM_CUDA_TRY(cudaStreamSynchronize(s));
   if (err[0]) {
     set_last_error("stream kernel: " + std::to_string(err[0]) +
                    " samples fell outside the staged footprint");
     return FSM_ERR_CUDA;
+  }
+  if (err[1]) {
+    set_last_error("stream kernel: " + std::to_string(err[1]) +
+                   " staged copies did not complete within the bounded wait");
+    return FSM_ERR_TIMEOUT;
   }
   return FSM_OK;
 }
@@ -851,15 +891,17 @@ extern "C" fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_e
 
 extern "C" fsm_status fsm_batch_upload(fsm_batch* b, const void* host_in, void* stream) {
   if (!b || !b->own_io || !host_in) return FSM_ERR_INVALID_ARG;
+  b->last_stream = pick_stream(b->ctx, stream);
   FSM_CUDA_TRY(cudaMemcpyAsync(b->d_mem + b->in_slab_off, host_in, b->in_slab_bytes,
-                               cudaMemcpyHostToDevice, pick_stream(b->ctx, stream)));
+                               cudaMemcpyHostToDevice, b->last_stream));
   return FSM_OK;
 }
 
 extern "C" fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream) {
   if (!b || !b->own_io || !host_out) return FSM_ERR_INVALID_ARG;
+  b->last_stream = pick_stream(b->ctx, stream);
   FSM_CUDA_TRY(cudaMemcpyAsync(host_out, b->d_mem + b->out_slab_off, b->out_slab_bytes,
-                               cudaMemcpyDeviceToHost, pick_stream(b->ctx, stream)));
+                               cudaMemcpyDeviceToHost, b->last_stream));
   return FSM_OK;
 }
 

@@ -183,7 +183,8 @@ fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_elem, size_t
  * whole output slab, enqueued on `stream` (pinned host memory makes them async). */
 fsm_status fsm_batch_upload(fsm_batch* b, const void* host_in, void* stream);
 fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream);
-/* Synchronous check of the kernels' internal error counters after a launch. */
+/* Waits for the stream the batch last used (upload, launch or download) and
+ * checks the kernels' internal error counters. */
 fsm_status fsm_batch_check(fsm_batch* b);
 /* Total cell x momentum samples of one launch of the batch. */
 double fsm_batch_samples(fsm_batch* b);

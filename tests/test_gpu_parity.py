@@ -7,7 +7,8 @@ import pytest
 import fsm_b200 as F
 import oracle_py as O
 import workloads as W
-from fsm_testutil import (compare, fsm_params, golden_names, load_golden, oracle_params)
+from fsm_testutil import (compare, compare_parity, fsm_params, golden_names, load_golden,
+                          oracle_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,11 +25,12 @@ def test_gpu_matches_reference_fixture(ctx, name):
     got = ctx.run_event(p, e, nB)
     assert got["info"]["dim_phip"] == int(meta[0])
     assert got["info"]["tau"] == pytest.approx(float(meta[2]))
-    errs = compare(got, ref, meta[2], baryon=bool(d["BARYON"]), e_normwise=True)
     # the FP64 precision oracle (the reference's sample set, FP64 values)
     ref64 = O.run(oracle_params(d), e, nB=nB, fp64=2)
+    errs, rescued = compare_parity(got, ref, ref64, meta[2], baryon=bool(d["BARYON"]))
     errs64 = compare(got, ref64, meta[2], baryon=bool(d["BARYON"]))
-    print(name, "vs reference float:", errs, "vs FP64:", errs64)
+    print(name, "vs reference float:", errs, "closer to FP64 than the reference:", rescued,
+          "vs FP64:", errs64)
 
 
 def test_gpu_gaussian_full_grid(ctx):
@@ -36,8 +38,8 @@ def test_gpu_gaussian_full_grid(ctx):
     p, e, _ = W.gaussian2d()
     got = ctx.run_event(p, e)
     ref = _oracle(p, e)
-    compare(got, ref, ref["tau"], e_normwise=True)
     ref64 = _oracle(p, e, fp64=2)
+    compare_parity(got, ref, ref64, ref["tau"])
     compare(got, ref64, ref["tau"])
 
 
@@ -46,8 +48,9 @@ def test_gpu_lumpy_full_grid(ctx):
     p, e, _ = W.lumpy2d(seed=1)
     got = ctx.run_event(p, e)
     ref = _oracle(p, e)
-    errs = compare(got, ref, ref["tau"], e_normwise=True)
-    errs64 = compare(got, _oracle(p, e, fp64=2), ref["tau"])
+    ref64 = _oracle(p, e, fp64=2)
+    errs = compare_parity(got, ref, ref64, ref["tau"])
+    errs64 = compare(got, ref64, ref["tau"])
     print("lumpy2d vs float", errs, "vs FP64", errs64)
 
 
@@ -56,8 +59,9 @@ def test_gpu_3d_baryon_reduced(ctx):
     p, e, nB = W.baryon3d(seed=5, side=41, neta=21, nrap=21, nphip=40)
     got = ctx.run_event(p, e, nB)
     ref = _oracle(p, e, nB)
-    compare(got, ref, ref["tau"], baryon=True, e_normwise=True)
-    compare(got, _oracle(p, e, nB, fp64=2), ref["tau"], baryon=True)
+    ref64 = _oracle(p, e, nB, fp64=2)
+    compare_parity(got, ref, ref64, ref["tau"], baryon=True)
+    compare(got, ref64, ref["tau"], baryon=True)
 
 
 def test_batch_equals_single_events(ctx):
@@ -65,13 +69,17 @@ def test_batch_equals_single_events(ctx):
     evs = []
     for name in golden_names():
         d, e, nB, _, _ = load_golden(name)
+        if d["E_DEP_FS"]:
+            continue  # batches take device-resident profiles: no host-side tau_fs
         evs.append((fsm_params(d), e, nB))
     b = F.Batch(ctx, [p for p, _, _ in evs])
     outs = b.run_host([(e, nB) for _, e, nB in evs])
     for (p, e, nB), o in zip(evs, outs):
         s = ctx.run_event(p, e, nB)
         for k in o:
-            assert np.array_equal(o[k], s[k]), k
+            d = np.abs(o[k] - s[k])
+            assert np.array_equal(o[k], s[k]), (k, p.DIM_X, p.DIM_Y, p.DIM_ETA, int(np.count_nonzero(d)),
+                                                float(d.max()))
     # a second launch (graph replay) gives the same results
     outs2 = b.run_host([(e, nB) for _, e, nB in evs])
     for o, o2 in zip(outs, outs2):
@@ -100,7 +108,7 @@ def test_energy_dependent_tau(ctx):
     d, e, nB, ref, meta = load_golden("edepfs2d_45")
     got = ctx.run_event(fsm_params(d), e)
     assert got["info"]["dtau"] == pytest.approx(float(meta[1]), rel=0, abs=0)
-    compare(got, ref, meta[2], e_normwise=True)
+    compare_parity(got, ref, O.run(oracle_params(d), e, fp64=2), meta[2])
 
 
 def test_invalid_inputs_are_rejected(ctx):
