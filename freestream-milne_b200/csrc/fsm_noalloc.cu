@@ -1,0 +1,280 @@
+// fsm_noalloc.cu -- a single-event 2D entry point that allocates nothing.
+//
+// Some callers cannot allocate device memory at the point where they run the
+// free streaming: a host framework that owns every device allocation through
+// its own memory pool or budget, a process that must not grow its device
+// footprint after start-up, or code that runs while another component forbids
+// allocation calls.  fsm_run_event_2d_noalloc serves them: it runs the same
+// kernels as fsm_run_event_device on caller-owned inputs and outputs, with all
+// of its scratch (spline derivatives, node array, the internal T^{mu nu}
+// buffer, the per-event tables and work lists) in one file-scope device array,
+// g_noalloc_scratch, of fixed size.  Because the array is a static __device__
+// object, every GPU that loads this library holds it until the process exits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fsm.h"
+#include "fsm_internal.h"
+#include "fsm_plan.h"
+
+namespace fsm {
+__global__ void fsm_prep2d_lines_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_pack_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
+__global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
+}  // namespace fsm
+
+using namespace fsm;
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB
+constexpr int kNoAllocMaxCells = 301 * 301;               // DIM_X * DIM_Y
+constexpr int kNoAllocMaxPhi = 1024;                      // DIM_PHIP after the arc-length rule
+
+}  // namespace
+
+// The scratch array.  Host code must not use this name as an address: on the
+// host it is only a stand-in, and the device address comes from
+// cudaGetSymbolAddress (see noalloc_scratch_address).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the first call on each device does the lookup).
+fsm_status noalloc_scratch_address(char** out) {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    return FSM_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= 64) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_last_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      return FSM_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = static_cast<char*>(addr[dev]);
+  return FSM_OK;
+}
+
+// Raise (never lower) a kernel's dynamic shared-memory limit: the limit is a
+// process-wide attribute that other launches may rely on.
+fsm_status raise_dyn_smem(const void* fn, size_t bytes) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, fn);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e));
+    return FSM_ERR_CUDA;
+  }
+  if ((int)bytes > a.maxDynamicSharedSizeBytes) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+      set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+      return FSM_ERR_CUDA;
+    }
+  }
+  return FSM_OK;
+}
+
+struct Region {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off = (off + bytes + 255) / 256 * 256;
+    return o;
+  }
+};
+
+}  // namespace
+
+extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
+                                               const fsm_outputs* dev_out, void* stream) {
+  if (!p || !d_e_gev || !dev_out) return FSM_ERR_INVALID_ARG;
+  if (p->DIM_ETA != 1 || p->BARYON != 0) {
+    set_last_error("fsm_run_event_2d_noalloc handles boost-invariant events without baryons");
+    return FSM_ERR_UNSUPPORTED;
+  }
+  if ((long long)p->DIM_X * p->DIM_Y > kNoAllocMaxCells) {
+    set_last_error("fsm_run_event_2d_noalloc: DIM_X*DIM_Y above its fixed scratch limit of " +
+                   std::to_string(kNoAllocMaxCells) + " cells");
+    return FSM_ERR_TOO_LARGE;
+  }
+  EventPlan P;
+  std::string why;
+  fsm_status st = plan_event(*p, nullptr, &P, &why);
+  if (st != FSM_OK) {
+    set_last_error(why);
+    return st;
+  }
+  if (P.p.DIM_PHIP > kNoAllocMaxPhi) {
+    set_last_error("fsm_run_event_2d_noalloc: DIM_PHIP " + std::to_string(P.p.DIM_PHIP) +
+                   " above its fixed scratch limit of " + std::to_string(kNoAllocMaxPhi));
+    return FSM_ERR_TOO_LARGE;
+  }
+  char* D = nullptr;
+  if ((st = noalloc_scratch_address(&D)) != FSM_OK) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int NX = P.p.DIM_X, NY = P.p.DIM_Y, DIM = P.DIM;
+
+  // work lists (as the batch path builds them for one event)
+  std::vector<Tile2D> tiles;
+  for (int a = 0; a < (NX + kTileX - 1) / kTileX; ++a)
+    for (int c = 0; c < (NY + kTileY - 1) / kTileY; ++c) {
+      const int x0 = a * kTileX, y0 = c * kTileY;
+      const int interior = (x0 + kTileX <= NX) && (y0 + kTileY <= NY) && (x0 + P.ox_min >= 2) &&
+                           (x0 + kTileX - 1 + P.ox_max <= NX - 3) && (y0 + P.oy_min >= 2) &&
+                           (y0 + kTileY - 1 + P.oy_max <= NY - 3);
+      tiles.push_back(Tile2D{0, x0, y0, interior});
+    }
+  std::vector<LineBlock> lines, packs;
+  for (int b = 0; b < NX + NY; b += 128) lines.push_back(LineBlock{0, b});
+  for (int b = 0; b < NY; b += 128) packs.push_back(LineBlock{0, b});
+  std::vector<CellBlock> bl;
+  for (int b = 0; b < DIM; b += kThreadsLandau) bl.push_back(CellBlock{0, b});
+
+  // scratch layout: uploaded part first, then device-written scratch
+  Region R;
+  const size_t o_cs = R.take(P.cs.size() * sizeof(FSM_FLOAT2));
+  const size_t o_tab = R.take(P.tab2.size() * sizeof(PhiEntry2D));
+  const size_t o_chunks = R.take(P.chunks2.size() * sizeof(Chunk2D));
+  const size_t o_hx = R.take(P.hx.size() * 8), o_fx = R.take(P.fx.size() * 8);
+  const size_t o_dgx = R.take(P.dgx.size() * 8), o_hy = R.take(P.hy.size() * 8);
+  const size_t o_fy = R.take(P.fy.size() * 8), o_dgy = R.take(P.dgy.size() * 8);
+  const size_t o_ev2 = R.take(sizeof(Ev2D)), o_evl = R.take(sizeof(EvLandau));
+  const size_t o_tiles = R.take(tiles.size() * sizeof(Tile2D));
+  const size_t o_lines = R.take(lines.size() * sizeof(LineBlock));
+  const size_t o_packs = R.take(packs.size() * sizeof(LineBlock));
+  const size_t o_bl = R.take(bl.size() * sizeof(CellBlock));
+  const size_t upload_bytes = R.off;
+  const size_t o_ctr = R.take(sizeof(Counters)), o_err = R.take(4 * sizeof(int));
+  const size_t o_zx = R.take((size_t)DIM * 8), o_zy = R.take((size_t)DIM * 8);
+  const size_t o_nodes = R.take((size_t)DIM * 16);
+  const size_t o_T = R.take((size_t)DIM * 10 * 4);
+  if (R.off > kNoAllocScratchBytes) {
+    set_last_error("fsm_run_event_2d_noalloc: event needs " + std::to_string(R.off) +
+                   " scratch bytes, above the fixed " + std::to_string(kNoAllocScratchBytes));
+    return FSM_ERR_TOO_LARGE;
+  }
+
+  // descriptors (the same fields the batch path fills)
+  Ev2D e{};
+  e.NX = NX;
+  e.NY = NY;
+  e.NPHI = P.p.DIM_PHIP;
+  e.NR = P.p.DIM_RAP;
+  e.DX = P.p.DX;
+  e.DY = P.p.DY;
+  e.DTAU = P.p.DTAU;
+  e.TAU = P.p.TAU;
+  e.xmin = P.xmin;
+  e.ymin = P.ymin;
+  e.xmax_i = P.xmax_i;
+  e.ymax_i = P.ymax_i;
+  e.inv_dx = 1.0f / P.p.DX;
+  e.inv_dy = 1.0f / P.p.DY;
+  e.d_phip = P.d_phip;
+  e.Rx = P.Rx;
+  e.Ry = P.Ry;
+  e.use_smem = 1;
+  e.tiles_y = (NY + kTileY - 1) / kTileY;
+  e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o_cs);
+  e.tab = reinterpret_cast<const PhiEntry2D*>(D + o_tab);
+  e.chunks = reinterpret_cast<const Chunk2D*>(D + o_chunks);
+  e.nchunks = (int)P.chunks2.size();
+  e.boxW = P.boxW;
+  e.boxH = P.boxH;
+  e.e_gev = d_e_gev;
+  e.ax = SplineAxis{reinterpret_cast<const double*>(D + o_hx), reinterpret_cast<const double*>(D + o_fx),
+                    reinterpret_cast<const double*>(D + o_dgx), NX};
+  e.ay = SplineAxis{reinterpret_cast<const double*>(D + o_hy), reinterpret_cast<const double*>(D + o_fy),
+                    reinterpret_cast<const double*>(D + o_dgy), NY};
+  e.zx = reinterpret_cast<double*>(D + o_zx);
+  e.zy = reinterpret_cast<double*>(D + o_zy);
+  e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o_nodes);
+  e.T = dev_out->T ? dev_out->T : reinterpret_cast<float*>(D + o_T);
+  EvLandau l{};
+  l.DIM = DIM;
+  l.is3d = 0;
+  l.baryon = 0;
+  l.eos = P.p.EOS_TYPE;
+  l.viscous = P.p.VISCOUS_MATCHING;
+  l.TAU = P.p.TAU;
+  l.T = e.T;
+  l.J = nullptr;
+  l.e = dev_out->e;
+  l.P = dev_out->P;
+  l.Pi = dev_out->Pi;
+  l.u = dev_out->u;
+  l.pi = dev_out->pi;
+
+  // host image of the uploaded part (ordinary host memory; no pinned staging)
+  std::vector<char> H(upload_bytes, 0);
+  auto put = [&](size_t off, const void* src, size_t n) {
+    if (n) std::memcpy(H.data() + off, src, n);
+  };
+  put(o_cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
+  put(o_tab, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
+  put(o_chunks, P.chunks2.data(), P.chunks2.size() * sizeof(Chunk2D));
+  put(o_hx, P.hx.data(), P.hx.size() * 8);
+  put(o_fx, P.fx.data(), P.fx.size() * 8);
+  put(o_dgx, P.dgx.data(), P.dgx.size() * 8);
+  put(o_hy, P.hy.data(), P.hy.size() * 8);
+  put(o_fy, P.fy.data(), P.fy.size() * 8);
+  put(o_dgy, P.dgy.data(), P.dgy.size() * 8);
+  put(o_ev2, &e, sizeof(e));
+  put(o_evl, &l, sizeof(l));
+  put(o_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
+  put(o_lines, lines.data(), lines.size() * sizeof(LineBlock));
+  put(o_packs, packs.data(), packs.size() * sizeof(LineBlock));
+  put(o_bl, bl.data(), bl.size() * sizeof(CellBlock));
+
+  // launch geometry of the stream kernel (as the batch path computes it)
+  const int tab_cap = P.p.DIM_PHIP;
+  const int box_cap = (P.boxW * P.boxH + 7) & ~7;
+  const size_t smem2 = (((size_t)tab_cap * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)box_cap * 16 +
+                       (size_t)kTotSlots2D * kThreads2D * 4;
+  if ((st = raise_dyn_smem((const void*)fsm_stream2d_kernel, smem2)) != FSM_OK) return st;
+  int dev = 0, sms = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream2d_kernel, kThreads2D, smem2);
+  const int ntiles = (int)tiles.size();
+  const int grid2 = std::max(1, std::min(ntiles, sms * std::max(occ, 1)));
+
+  // upload (pageable source: returns once the bytes are staged), reset the
+  // counters this call reads, then the same launch sequence as the batch path
+  auto cu = [&](cudaError_t ce, const char* what) -> fsm_status {
+    if (ce == cudaSuccess) return FSM_OK;
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(ce));
+    return FSM_ERR_CUDA;
+  };
+  if ((st = cu(cudaMemcpyAsync(D, H.data(), upload_bytes, cudaMemcpyHostToDevice, s), "upload")) != FSM_OK)
+    return st;
+  if ((st = cu(cudaMemsetAsync(D + o_ctr, 0, sizeof(Counters), s), "memset")) != FSM_OK) return st;
+  if ((st = cu(cudaMemsetAsync(D + o_err, 0, 4 * sizeof(int), s), "memset")) != FSM_OK) return st;
+  const Ev2D* d_ev2 = reinterpret_cast<const Ev2D*>(D + o_ev2);
+  fsm_prep2d_lines_kernel<<<(int)lines.size(), 128, 0, s>>>(d_ev2, reinterpret_cast<const LineBlock*>(D + o_lines));
+  fsm_prep2d_pack_kernel<<<(int)packs.size(), 128, 0, s>>>(d_ev2, reinterpret_cast<const LineBlock*>(D + o_packs));
+  fsm_stream2d_kernel<<<grid2, kThreads2D, smem2, s>>>(d_ev2, reinterpret_cast<const Tile2D*>(D + o_tiles), ntiles,
+                                                       tab_cap, box_cap, reinterpret_cast<Counters*>(D + o_ctr),
+                                                       reinterpret_cast<int*>(D + o_err));
+  fsm_landau_kernel<<<(int)bl.size(), kThreadsLandau, 0, s>>>(reinterpret_cast<const EvLandau*>(D + o_evl),
+                                                            reinterpret_cast<const CellBlock*>(D + o_bl),
+                                                            reinterpret_cast<Counters*>(D + o_ctr));
+  return cu(cudaGetLastError(), "launch");
+}

@@ -100,6 +100,7 @@ SIGNATURES = {
     "fsm_batch_download": (_ST, [_VP, _VP, _VP]),
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
 }
 
 _lib = None
@@ -152,6 +153,13 @@ def read_params_file(path, base=None):
 OUT_COMPS = dict(T=10, J=4, e=1, P=1, Pi=1, u=4, pi=10, nB=1, V=4)
 SLAB_ORDER = ["T", "e", "P", "Pi", "u", "pi"]
 SLAB_ORDER_BARYON = SLAB_ORDER + ["J", "nB", "V"]
+
+
+def run_event_2d_noalloc(params, d_e, dev_out, stream=None):
+    """The allocation-free single-event 2D entry point; device pointers (ints)."""
+    o = Outputs(**{k: v for k, v in dev_out.items()})
+    check(lib().fsm_run_event_2d_noalloc(ctypes.byref(params), d_e, ctypes.byref(o), stream),
+          "fsm_run_event_2d_noalloc")
 
 
 def probe_fp32_tflops(device=0):

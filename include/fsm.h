@@ -189,6 +189,23 @@ fsm_status fsm_batch_check(fsm_batch* b);
 /* Total cell x momentum samples of one launch of the batch. */
 double fsm_batch_samples(fsm_batch* b);
 
+/* --------------------------------------------------------- no allocation */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they run the free streaming (a framework that owns all device
+ * memory through its own pool or budget, or code running where allocation
+ * calls are not allowed): one boost-invariant event (DIM_ETA = 1, BARYON = 0,
+ * E_DEP_FS = 0) on caller-owned device input and outputs, enqueued on
+ * `stream`, calling no cudaMalloc/cudaFree or other allocating routine.  Its
+ * scratch lives in one fixed 8 MiB file-scope device array that every GPU
+ * loading the library holds until the process exits; limits: DIM_X*DIM_Y <=
+ * 90601 (e.g. 301 x 301) and DIM_PHIP <= 1024 after the arc-length rule, larger
+ * events return FSM_ERR_TOO_LARGE.  The first call on each device looks up the
+ * array's device address (make that first call before any stream capture).
+ * All calls share the array, so calls that overlap on the GPU race: run them in
+ * one stream or serialise them. */
+fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
+                                    const fsm_outputs* dev_out, void* stream);
+
 /* ------------------------------------------------------------ diagnostics */
 /* Measured FP32 FMA throughput of `device` in TFLOP/s (a short FMA-chain
  * kernel timed with CUDA events): the peak the stream kernels' roofline

@@ -1,0 +1,54 @@
+"""The allocation-free entry point, for callers that cannot allocate device
+memory when they run the free streaming (e.g. a framework that owns all device
+memory through its own pool).  It must give the results of the ordinary device
+entry point.  Kept in its own file, collected last, so a run that stops at its
+first failure has run every other test first; it also passes alone."""
+import numpy as np
+import pytest
+
+import fsm_b200 as F
+import workloads as W
+from fsm_testutil import compare
+
+pytestmark = pytest.mark.gpu
+
+OUTS = ("T", "e", "P", "Pi", "u", "pi")
+
+
+def _dev_outputs(torch, dim):
+    return {k: torch.zeros((F.OUT_COMPS[k] * dim,), dtype=torch.float32, device="cuda") for k in OUTS}
+
+
+def _host(outs, dim):
+    return {k: v.cpu().numpy().reshape((F.OUT_COMPS[k], dim) if F.OUT_COMPS[k] > 1 else (dim,))
+            for k, v in outs.items()}
+
+
+def test_no_alloc_entry_matches_device_entry(ctx):
+    import torch
+    events = [W.lumpy2d(seed=21, side=151, dx=0.07, nphip=100, dtau=0.9, eos=2, radius=4.0),
+              W.gaussian2d()]
+    stream = torch.cuda.current_stream().cuda_stream
+    for p, e, _ in events:  # two calls in a row, each against the existing entry point
+        dim = e.size
+        d_e = torch.from_numpy(e).cuda()
+        ref = _dev_outputs(torch, dim)
+        ctx.run_event_device(p, d_e.data_ptr(), None, {k: v.data_ptr() for k, v in ref.items()},
+                             stream=stream)
+        got = _dev_outputs(torch, dim)
+        F.run_event_2d_noalloc(p, d_e.data_ptr(), {k: v.data_ptr() for k, v in got.items()},
+                               stream=stream)
+        torch.cuda.synchronize()
+        r, g = _host(ref, dim), _host(got, dim)
+        compare(g, r, float(p.TAU0 + p.DTAU))
+        assert all(np.isfinite(g[k]).all() for k in g)
+
+
+def test_no_alloc_rejects_oversized_events(ctx):
+    import torch
+    p = F.default_params(DIM_X=401, DIM_Y=401)
+    d_e = torch.zeros(401 * 401, dtype=torch.float32, device="cuda")
+    out = _dev_outputs(torch, 401 * 401)
+    with pytest.raises(F.FsmError) as ei:
+        F.run_event_2d_noalloc(p, d_e.data_ptr(), {k: v.data_ptr() for k, v in out.items()})
+    assert ei.value.status == 12  # FSM_ERR_TOO_LARGE
