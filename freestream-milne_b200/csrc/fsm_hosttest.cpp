@@ -1,8 +1,30 @@
 // fsm_hosttest.cpp -- TEST-ONLY build of the Landau-matching algorithm of
-// fsm_landau.cuh for the CPU, so unit tests can exercise the solver's logic
-// against the oracle without a GPU.  Not part of libfsm.so; the product runs
-// the same header only inside fsm_landau_kernel.
+// fsm_landau.cuh and the windowed spline slopes of fsm_spline.cuh for the CPU,
+// so unit tests can exercise their logic against the oracle without a GPU.
+// Not part of libfsm.so; the product runs the same headers only inside its
+// kernels.
+#include <vector>
+
 #include "fsm_landau.cuh"
+#include "fsm_plan.h"
+#include "fsm_spline.cuh"
+
+// Slopes dy/dx * d of the natural spline through y[0..n) on the float grid
+// i*d + lo, segment by segment as the prep kernels compute them.
+extern "C" void fsm_hosttest_line_slopes(const float* y, int n, float d, float lo, float* out) {
+  std::vector<fsm::AxisNode> ax;
+  fsm::build_axis(n, d, lo, ax);
+  const fsm::AxisNode* A = ax.data() + fsm::kPadLo;
+  std::vector<double> yp((size_t)n + fsm::kPadLo + fsm::kPadHi, 0.0);
+  for (int i = 0; i < n; ++i) yp[(size_t)fsm::kPadLo + i] = y[i];
+  const double* Y = yp.data() + fsm::kPadLo;
+  for (int a = 0; a < n; a += fsm::kSegP) {
+    float s[fsm::kSegP];
+    fsm::seg_slopes([&](int k) -> const fsm::AxisNode& { return A[k]; }, n, (double)d, a,
+                    [&](int i) { return Y[i]; }, s);
+    for (int t = 0; t < fsm::kSegP && a + t < n; ++t) out[a + t] = s[t];
+  }
+}
 
 extern "C" int fsm_hosttest_landau_cell(const float* T10, const float* J4, int is3d, int baryon,
                                         int eos, int viscous, float tau, float* out24) {

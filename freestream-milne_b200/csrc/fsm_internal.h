@@ -10,6 +10,7 @@
 //   Landau kernel.  Outputs e,P,Pi,u[4],pi[10],nB,V[4] are [comp][DIM] floats.
 #pragma once
 #include <stdint.h>
+#include <stddef.h>
 
 #ifndef __CUDACC__
 struct float2_h { float x, y; };
@@ -33,16 +34,43 @@ constexpr int kThreads3D = 256;
 constexpr int kThreadsLandau = 128;
 constexpr int kPhiChunk = 16;  // FP32 partial sums are folded into Kahan totals every 16 phi_p
 
-// Natural-spline axis data for the 2D prep kernels (host computed, double):
-// h[i] = x[i+1]-x[i] of the float grid coordinates, and the elimination
-// factors f[k] / modified diagonals dg[k] of the tridiagonal system for the
-// interior second derivatives (k = 0..n-3).
-struct SplineAxis {
-  const double* h;
-  const double* f;
-  const double* dg;
-  int n;
+// Natural-spline axis data for the 2D prep kernels (host computed, double),
+// one entry per interval / unknown k of an axis with n nodes, on the float grid
+// coordinates x_i: h = x[k+1] - x[k] and g = 6/h (k <= n-2); the elimination
+// factor f and the inverse modified diagonal 1/dg of the tridiagonal system for
+// the second derivative at node k+1 (k <= n-3).  Tables are stored with
+// kPadLo zero entries before k = 0 and kPadHi after the line, and all fields
+// outside the ranges above are 0.
+struct AxisNode {
+  double g, f, h, idg;
 };
+
+// Windowed natural-spline elimination of the prep kernels: a thread produces
+// the slopes of kSegP consecutive nodes from a forward/backward sweep over the
+// segment plus kWinP nodes on each side, started from zero.  The sweeps'
+// factors are the exact full-line ones and the influence of the truncated
+// start decays like (2 - sqrt 3)^kWinP < 1e-9.
+constexpr int kSegP = 8;
+constexpr int kWinP = 16;
+constexpr int kPadLo = kWinP + 4;           // table/line padding before node 0
+constexpr int kPadHi = kWinP + kSegP + 4;   // and after node n-1
+constexpr int kPrepRows = 4;  // y-lines (rows) per block of the long-row kernel, one warp each
+constexpr int kMaxNY2D = 5120;  // longest 2D row the long-row kernel stages in shared memory
+constexpr int kMaxStrip = 720;  // longest line of the 32-line strip kernels
+constexpr int kPrepThreads = 256;  // strip kernels
+
+// Dynamic shared memory of the strip kernels for lines of up to n nodes: the
+// padded axis table and two padded fields of 32 lines (odd line stride).
+inline int strip_ld(int n) { return (n + kPadLo + kPadHi) | 1; }
+inline size_t prep_strip_smem(int n) {
+  return (size_t)(n + kPadLo + kPadHi) * sizeof(AxisNode) + (size_t)2 * 32 * strip_ld(n) * 4;
+}
+
+// Dynamic shared memory of the long-row kernel: two padded rows of up to
+// ny_cap floats per warp.
+inline size_t prep_rows_smem(int ny_cap) {
+  return (size_t)kPrepRows * 2 * (size_t)(ny_cap + kPadLo + kPadHi + 2) * 4;
+}
 
 // Per-phi_p entry of the 2D stream table (6 float4, host computed).  With the
 // reference's float shift s = fl(cos(phi_p) * DTAU), the source point of cell ix
@@ -67,12 +95,20 @@ struct PhiEntry2D {
 // A run of consecutive phi_p nodes whose source offsets fit one staged window:
 // for a tile at (x0, y0) the window starts at row x0 + ox0 - 1, column
 // y0 + oy0 - 1 (a one-node margin on each side for samples decided with the
-// reference arithmetic).
+// reference arithmetic).  [ox0, ox1] x [oy0, oy1] is the run's offset range;
+// its window is win_h(c) rows of win_w(c) nodes.
 struct Chunk2D {
-  int p0, p1, ox0, oy0;
+  int p0, p1, ox0, oy0, ox1, oy1;
 };
+#if defined(__CUDACC__)
+#define FSM_HDI __host__ __device__ inline
+#else
+#define FSM_HDI inline
+#endif
+FSM_HDI int win_h(const Chunk2D& c) { return kTileX + (c.ox1 - c.ox0) + 3; }
+FSM_HDI int win_w(const Chunk2D& c) { return kTileY + (c.oy1 - c.oy0) + 3; }
 constexpr int kMaxChunks2D = 64;
-constexpr int kWindowBudget2D = 36 * 1024;  // bytes of one staged window
+constexpr int kWindowBudget2D = 32 * 1024;  // bytes of one staged window
 constexpr int kTotSlots2D = 5 * 4;          // per-thread moment totals kept in shared memory
 
 struct Ev2D {
@@ -91,9 +127,10 @@ struct Ev2D {
   int boxW, boxH;        // staged window (columns = y nodes, rows = x nodes)
   // prep
   const float* e_gev;    // input
-  SplineAxis ax, ay;
-  double* zx;            // scratch [DIM]
-  double* zy;            // scratch [DIM]
+  const AxisNode* ax;   // [NX] x-axis spline data
+  const AxisNode* ay;   // [NY] y-axis spline data
+  float* fa;             // scratch [DIM]: F = e/(2 pi)
+  float* sy;             // scratch [DIM]: y-slopes dF/dy * DY
   FSM_FLOAT4* nodes;     // [DIM]
   // outputs of the stream kernel
   float* T;              // [10][DIM]
@@ -146,9 +183,11 @@ struct EvLandau {
   long long cell_begin;   // first global cell index of this event in the Landau work list
 };
 
-// Work-list entries: a block of spline lines / cells of one event.
+// Work-list entries: a block of spline lines / cells of one event.  For the
+// row kernel `begin` is the first x row; for the column kernel `begin` is the
+// first y column and `seg` the first x segment (kSegP nodes) of the block.
 struct LineBlock {
-  int ev, begin;
+  int ev, begin, seg;
 };
 struct CellBlock {
   int ev, begin;

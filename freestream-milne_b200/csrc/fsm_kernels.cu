@@ -1,7 +1,8 @@
 // fsm_kernels.cu -- sm_100a kernels of the free-streaming + Landau-matching path.
 //
-//   fsm_prep2d_lines_kernel   natural-spline x- and y-derivatives of F = e/(2 pi)
-//   fsm_prep2d_pack_kernel    mixed derivative + float4 node packing
+//   fsm_prep2d_rows_kernel    F = e/(2 pi) and its natural-spline y-derivatives
+//   fsm_prep2d_cols_kernel    x- and mixed derivatives + float4 node packing
+//   fsm_prep2d_*_long_kernel  the same for grids whose lines exceed kMaxStrip
 //   fsm_prep3d_kernel         GeV/fm^3 -> fm^-4 conversion of 3D profiles
 //   fsm_stream2d_kernel       fused free streaming + moment quadrature, 2D
 //   fsm_stream3d_kernel       fused free streaming + moment quadrature, 3D (+baryon)
@@ -18,6 +19,7 @@
 
 #include "fsm_internal.h"
 #include "fsm_landau.cuh"
+#include "fsm_spline.cuh"
 
 namespace fsm {
 
@@ -40,100 +42,189 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
 }
 
 // ------------------------------------------------------------------ prep 2D
-// One natural-spline line solve.  `val(i)` returns the data at node i,
-// `scr(i)` is a double scratch slot per node; on return scr(i) holds the
-// derivative dy/dx at node i.
-template <class Val, class Scr>
-__device__ __forceinline__ void spline_line(const SplineAxis& ax, Val val, Scr scr) {
-  const int n = ax.n;
-  const int m = n - 2;
-  // forward elimination, r'_k stored at node k+1
-  double y0 = val(0), y1 = val(1);
-  double sl_prev = (y1 - y0) / ax.h[0];
-  double rp = 0.0;
-  for (int k = 0; k < m; ++k) {
-    double y2 = val(k + 2);
-    double sl = (y2 - y1) / ax.h[k + 1];
-    double rhs = 6.0 * (sl - sl_prev);
-    rp = (k == 0) ? rhs : rhs - ax.f[k] * rp;
-    scr(k + 1) = rp;
-    sl_prev = sl;
-    y1 = y2;
+// Strip kernels: a block owns 32 lines of one event and stages them whole in
+// shared memory (coalesced), zero-padded at both ends, together with the
+// padded axis table; lane l takes line l and warp w the segments w, w + 8, ...
+// of it, so the table reads are warp-uniform broadcasts and the line reads
+// conflict-free.  Line lengths up to kMaxStrip.
+__device__ __forceinline__ void stage_axis(AxisNode* dst, const AxisNode* __restrict__ src, int n) {
+  const double* s = reinterpret_cast<const double*>(src - kPadLo);
+  double* d = reinterpret_cast<double*>(dst);
+  for (int i = threadIdx.x; i < (n + kPadLo + kPadHi) * 4; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+// y-lines (rows ix0 .. ix0+31, contiguous in memory): F = e/(2 pi) -> fa and
+// its y-slopes -> sy.  Lines are staged with an odd stride.
+__global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_rows_kernel(
+    const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks) {
+  extern __shared__ __align__(16) unsigned char prep_smem[];
+  const LineBlock b = blocks[blockIdx.x];
+  const Ev2D& ev = evs[b.ev];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int NX = ev.NX, NY = ev.NY;
+  const int ix0 = b.begin;
+  const int nr = min(32, NX - ix0);
+  const int ld = (NY + kPadLo + kPadHi) | 1;
+  AxisNode* tab = reinterpret_cast<AxisNode*>(prep_smem);
+  float* Fs = reinterpret_cast<float*>(tab + NY + kPadLo + kPadHi);
+  float* Ss = Fs + 32 * ld;
+  stage_axis(tab, ev.ay, NY);
+  for (int r = warp; r < 32; r += kPrepThreads / 32) {
+    float* fl = Fs + r * ld;
+    for (int c = lane; c < ld; c += 32) fl[c] = 0.0f;  // padding (and rows past the grid)
   }
-  // back substitution: second derivatives M[1..n-2]
-  double Mnext = 0.0;  // M[n-1]
-  for (int k = m - 1; k >= 0; --k) {
-    double Mi = (scr(k + 1) - ((k == m - 1) ? 0.0 : ax.h[k + 1] * Mnext)) / ax.dg[k];
-    scr(k + 1) = Mi;
-    Mnext = Mi;
+  __syncthreads();
+  for (int r = warp; r < nr; r += kPrepThreads / 32) {
+    const size_t row = (size_t)(ix0 + r) * NY;
+    float* fl = Fs + r * ld + kPadLo;
+    for (int c = lane; c < NY; c += 32) {
+      const float f = F_of(__ldg(ev.e_gev + row + c));
+      fl[c] = f;
+      ev.fa[row + c] = f;
+    }
   }
-  // derivatives at the nodes (M[0] = M[n-1] = 0)
-  double Mi = 0.0, yi = val(0);
-  for (int i = 0; i < n - 1; ++i) {
-    double Mi1 = (i + 1 == n - 1) ? 0.0 : scr(i + 1);
-    double yi1 = val(i + 1);
-    double sl = (yi1 - yi) / ax.h[i];
-    scr(i) = sl - ax.h[i] * (2.0 * Mi + Mi1) / 6.0;
-    if (i == n - 2) scr(n - 1) = sl + ax.h[i] * (Mi + 2.0 * Mi1) / 6.0;
-    Mi = Mi1;
-    yi = yi1;
+  __syncthreads();
+  {
+    const float* fl = Fs + lane * ld + kPadLo;
+    float* sl = Ss + lane * ld;
+    const AxisNode* A = tab + kPadLo;
+    const int nseg = (NY + kSegP - 1) / kSegP;
+    for (int sg = warp; sg < nseg; sg += kPrepThreads / 32) {
+      float sv[kSegP];
+      seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NY, (double)ev.DY, sg * kSegP,
+                 [&](int j) { return (double)fl[j]; }, sv);
+#pragma unroll
+      for (int t = 0; t < kSegP; ++t)
+        if (sg * kSegP + t < NY) sl[sg * kSegP + t] = sv[t];
+    }
+  }
+  __syncthreads();
+  for (int r = warp; r < nr; r += kPrepThreads / 32) {
+    const size_t row = (size_t)(ix0 + r) * NY;
+    for (int c = lane; c < NY; c += 32) ev.sy[row + c] = Ss[r * ld + c];
   }
 }
 
-// Lines [0, NY): x-direction spline at fixed iy -> zx.  Lines [NY, NY+NX):
-// y-direction spline at fixed ix -> zy.
-__global__ void __launch_bounds__(128) fsm_prep2d_lines_kernel(const Ev2D* __restrict__ evs,
-                                                               const LineBlock* __restrict__ blocks) {
+// x-lines (columns iy0 .. iy0+31 at stride NY): x-slopes of F and of the
+// y-slope field (the mixed derivative), packed with F and F_y into the nodes.
+__global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_cols_kernel(
+    const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks) {
+  extern __shared__ __align__(16) unsigned char prep_smem[];
   const LineBlock b = blocks[blockIdx.x];
   const Ev2D& ev = evs[b.ev];
-  const int line = b.begin + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int NX = ev.NX, NY = ev.NY;
-  if (line >= NX + NY) return;
-  const float* e = ev.e_gev;
-  if (line < NY) {
-    const int iy = line;
-    double* zx = ev.zx;
-    spline_line(ev.ax, [&](int i) { return (double)F_of(__ldg(e + (size_t)i * NY + iy)); },
-                [&](int i) -> double& { return zx[(size_t)i * NY + iy]; });
-  } else {
-    const int ix = line - NY;
-    double* zy = ev.zy + (size_t)ix * NY;
-    const float* er = e + (size_t)ix * NY;
-    spline_line(ev.ay, [&](int j) { return (double)F_of(__ldg(er + j)); },
-                [&](int j) -> double& { return zy[j]; });
+  const int iy0 = b.begin;
+  const int nc = min(32, NY - iy0);
+  const int np = NX + kPadLo + kPadHi;
+  AxisNode* tab = reinterpret_cast<AxisNode*>(prep_smem);
+  float* Fs = reinterpret_cast<float*>(tab + np);
+  float* Ys = Fs + 32 * np;
+  stage_axis(tab, ev.ax, NX);
+  for (int i = warp; i < np; i += kPrepThreads / 32) {
+    const int ix = i - kPadLo;
+    float f = 0.0f, yv = 0.0f;
+    if (ix >= 0 && ix < NX && lane < nc) {
+      const size_t k = (size_t)ix * NY + iy0 + lane;
+      f = __ldg(ev.fa + k);
+      yv = __ldg(ev.sy + k);
+    }
+    Fs[i * 32 + lane] = f;
+    Ys[i * 32 + lane] = yv;
+  }
+  __syncthreads();
+  if (lane >= nc) return;
+  const float* fc = Fs + kPadLo * 32 + lane;
+  const float* yc = Ys + kPadLo * 32 + lane;
+  const AxisNode* A = tab + kPadLo;
+  float4* nodes = reinterpret_cast<float4*>(ev.nodes) + iy0 + lane;
+  const int nseg = (NX + kSegP - 1) / kSegP;
+  for (int sg = warp; sg < nseg; sg += kPrepThreads / 32) {
+    const int a = sg * kSegP;
+    float sx[kSegP], sxy[kSegP];
+    seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
+               [&](int i) { return (double)fc[i * 32]; }, sx);
+    __syncwarp();  // keeps the second sweep's loads after the first (register pressure)
+    seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
+               [&](int i) { return (double)yc[i * 32]; }, sxy);
+#pragma unroll
+    for (int t = 0; t < kSegP; ++t) {
+      const int i = a + t;
+      if (i < NX) nodes[(size_t)i * NY] = make_float4(fc[i * 32], sx[t], yc[i * 32], sxy[t]);
+    }
   }
 }
 
-// Mixed derivative zxy = d/dx of the zy field along x lines (fixed iy), then
-// pack the node float4 (F, zx*DX, zy*DY, zxy*DX*DY).  zx is overwritten with
-// the line scratch after it has been consumed.
-__global__ void __launch_bounds__(128) fsm_prep2d_pack_kernel(const Ev2D* __restrict__ evs,
-                                                              const LineBlock* __restrict__ blocks) {
+// Long lines.  y-lines: one warp per x row ix.  The row's F = e/(2 pi) is
+// staged in shared memory (coalesced, zero-padded), lane l takes segments l,
+// l+32, ..., and the slopes are stored back coalesced.
+__global__ void __launch_bounds__(kPrepRows * 32) fsm_prep2d_rows_long_kernel(
+    const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks, int ny_cap) {
+  extern __shared__ __align__(16) unsigned char prep_smem[];
   const LineBlock b = blocks[blockIdx.x];
   const Ev2D& ev = evs[b.ev];
-  const int iy = b.begin + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int NX = ev.NX, NY = ev.NY;
-  if (iy >= NY) return;
-  const double DX = ev.DX, DY = ev.DY;
-  const double* zy = ev.zy;
-  double* zx = ev.zx;
-  FSM_FLOAT4* nodes = ev.nodes;
-  const float* e = ev.e_gev;
-  // first consume zx into the nodes (x, y components), freeing zx as scratch
-  for (int ix = 0; ix < NX; ++ix) {
-    size_t k = (size_t)ix * NY + iy;
-    float4 nd;
-    nd.x = F_of(__ldg(e + k));
-    nd.y = (float)(zx[k] * DX);
-    nd.z = (float)(zy[k] * DY);
-    nd.w = 0.0f;
-    nodes[k] = nd;
+  const int ix = b.begin + warp;
+  if (ix >= NX) return;
+  const int stride = ny_cap + kPadLo + kPadHi + 2;
+  float* fr = reinterpret_cast<float*>(prep_smem) + (size_t)warp * 2 * stride;
+  float* sr = fr + stride;
+  const size_t row = (size_t)ix * NY;
+  for (int c = lane; c < NY + kPadLo + kPadHi; c += 32) fr[c] = 0.0f;
+  __syncwarp();
+  for (int c = lane; c < NY; c += 32) {
+    const float f = F_of(__ldg(ev.e_gev + row + c));
+    fr[kPadLo + c] = f;
+    ev.fa[row + c] = f;
   }
-  spline_line(ev.ax, [&](int i) { return zy[(size_t)i * NY + iy]; },
-              [&](int i) -> double& { return zx[(size_t)i * NY + iy]; });
-  for (int ix = 0; ix < NX; ++ix) {
-    size_t k = (size_t)ix * NY + iy;
-    nodes[k].w = (float)(zx[k] * DX * DY);
+  __syncwarp();
+  const float* fl = fr + kPadLo;
+  const AxisNode* A = ev.ay;
+  const int nseg = (NY + kSegP - 1) / kSegP;
+  for (int sg = lane; sg < nseg; sg += 32) {
+    float sv[kSegP];
+    seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NY, (double)ev.DY, sg * kSegP,
+               [&](int j) { return (double)fl[j]; }, sv);
+#pragma unroll
+    for (int t = 0; t < kSegP; ++t) {
+      const int c = sg * kSegP + t;
+      if (c < NY) sr[c] = sv[t];
+    }
+  }
+  __syncwarp();
+  for (int c = lane; c < NY; c += 32) ev.sy[row + c] = sr[c];
+}
+
+// Long x-lines and packing: thread (iy, segment) with consecutive iy in a warp,
+// so every global access is coalesced.
+__global__ void __launch_bounds__(128) fsm_prep2d_cols_long_kernel(
+    const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks) {
+  const LineBlock b = blocks[blockIdx.x];
+  const Ev2D& ev = evs[b.ev];
+  const int NX = ev.NX, NY = ev.NY;
+  const int iy = b.begin + (threadIdx.x & 31);
+  const int a = (b.seg + (threadIdx.x >> 5)) * kSegP;
+  if (iy >= NY || a >= NX) return;
+  const float* fa = ev.fa + iy;
+  const float* sy = ev.sy + iy;
+  const AxisNode* A = ev.ax;
+  auto at = [&](const float* p, int i) {
+    return (i >= 0 && i < NX) ? (double)__ldg(p + (size_t)i * NY) : 0.0;
+  };
+  float sx[kSegP], sxy[kSegP];
+  seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
+             [&](int i) { return at(fa, i); }, sx);
+  seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
+             [&](int i) { return at(sy, i); }, sxy);
+  float4* nodes = reinterpret_cast<float4*>(ev.nodes) + iy;
+#pragma unroll
+  for (int t = 0; t < kSegP; ++t) {
+    const int i = a + t;
+    if (i < NX) {
+      const size_t k = (size_t)i * NY;
+      nodes[k] = make_float4(__ldg(fa + k), sx[t], __ldg(sy + k), sxy[t]);
+    }
   }
 }
 
@@ -283,8 +374,13 @@ constexpr int kWaitLimit = 1 << 20;  // polls of one bounded mbarrier wait
 // positions samples relative to the float cell coordinate).  The y-direction
 // Hermite pass of a node row -- the (value, x-slope) pair, one packed-FMA chain
 // -- is shared by the two cells that use it, so a thread evaluates 5 node rows
-// for its 4 samples.  Moments accumulate in FP32 chunks of 16 phi_p folded
-// into FP32 totals (two-level summation).
+// for its 4 samples.  Where the spline is not positive the reference falls back
+// to bilinear interpolation (src/FreeStream.cpp:245-246); that is rare, so it
+// is evaluated only in warps where some sample needs it.  Moments accumulate
+// in FP32 chunks of 16 phi_p folded into FP32 totals (two-level summation).
+//
+// kInterior: every sample of the run provably lands inside the grid, so the
+// in-grid test (src/FreeStream.cpp:213) is skipped.
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
@@ -303,16 +399,13 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
     const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], mw = e[4], tu = e[5];
     const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
     const int oy = (int)(short)(oyn & 0xffff);
-    const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
     const int j = iy + oy, i0 = ixb + ox;
     // y weights of this lane, first-order corrected for its own coordinate
     const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
     const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
-    const float uu = tu.y + ey;
-    const bool in_y = kInterior || ((j >= 1) && (j <= NY - 2));
     const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
+    float cv[K];
     float2 VDp = make_float2(0.f, 0.f);
-    float Bp = 0.f;
 #pragma unroll
     for (int r = 0; r <= K; ++r) {
       const float4 n0 = rowp[r * boxW], n1 = rowp[r * boxW + 1];
@@ -321,52 +414,67 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       VD = __ffma2_rn(make_float2(Kp.y, Kp.y), make_float2(n1.x, n1.y), VD);
       VD = __ffma2_rn(make_float2(Lp.x, Lp.x), make_float2(n0.z, n0.w), VD);
       VD = __ffma2_rn(make_float2(Lp.y, Lp.y), make_float2(n1.z, n1.w), VD);
-      const float B = fmaf(uu, n1.x - n0.x, n0.x);
       if (r > 0) {
         const int k = r - 1;
         const float2 ex2 = make_float2(ex[k], ex[k]);
         const float2 HG0 = __ffma2_rn(ex2, make_float2(dwx.x, dwx.y), make_float2(wx.x, wx.y));
         const float2 HG1 = __ffma2_rn(ex2, make_float2(dwx.z, dwx.w), make_float2(wx.z, wx.w));
         const float2 cc = __ffma2_rn(HG1, VD, __fmul2_rn(HG0, VDp));
-        const float cval = cc.x + cc.y;                             // bicubic
-        const float lval = fmaf(tu.x + ex[k], B - Bp, Bp);          // bilinear
-        float v = (cval > 0.0f) ? cval : lval;                      // src/FreeStream.cpp:245-246
-        if (!kInterior) {
-          const int ik = i0 + k;
-          bool in = act[k] && in_y && (ik >= 1) && (ik <= NX - 2);
-          // samples whose in-grid decision depends on rounding: exact path below
-          if (nearx && (ik <= 1 || ik >= NX - 2)) in = false;
-          if (neary && (j <= 1 || j >= NY - 2)) in = false;
-          v = in ? v : 0.0f;
-        }
-        const float2 v2 = make_float2(v, v);
-        a0[k] += v;
-        a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
-        a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+        cv[k] = cc.x + cc.y;  // bicubic
       }
       VDp = VD;
-      Bp = B;
     }
-    if (!kInterior && (nearx || neary)) {
-      // the fraction lies within 1e-3 of an integer: a sample next to the grid
-      // boundary may fall in or out with the rounding of its float position, so
-      // those samples (excluded above) are decided and evaluated with the
-      // reference arithmetic
+    // bilinear where the bicubic value is not positive (or not a number)
+    const float cmin = fminf(fminf(cv[0], cv[1]), fminf(cv[2], cv[3]));
+    if (__any_sync(0xffffffffu, !(cmin > 0.0f) || (cv[0] != cv[0]) || (cv[1] != cv[1]) ||
+                                    (cv[2] != cv[2]) || (cv[3] != cv[3]))) {
+      const float uu = tu.y + ey;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const int ik = i0 + k;
-        const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-        const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-        const bool cx = (ik >= 1) && (ik <= NX - 2);
-        if (act[k] && (ux || uy) && (ux || cx) && (uy || in_y)) {
-          const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-          const float v = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
-          const float2 v2 = make_float2(v, v);
-          a0[k] += v;
-          a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
-          a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+        if (!(cv[k] > 0.0f)) {
+          const float4 a00 = rowp[k * boxW], a01 = rowp[k * boxW + 1];
+          const float4 a10 = rowp[(k + 1) * boxW], a11 = rowp[(k + 1) * boxW + 1];
+          const float B0 = fmaf(uu, a01.x - a00.x, a00.x);
+          const float B1 = fmaf(uu, a11.x - a10.x, a10.x);
+          cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0);
         }
       }
+    }
+    if (!kInterior) {
+      const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
+      const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+      if (!(nearx || neary)) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
+          cv[k] = in ? cv[k] : 0.0f;
+        }
+      } else {
+        // the fraction lies within 1e-3 of an integer: a sample next to the
+        // grid boundary may fall in or out with the rounding of its float
+        // position, so those samples are decided and evaluated with the
+        // reference arithmetic
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int ik = i0 + k;
+          const bool cx = (ik >= 1) && (ik <= NX - 2);
+          const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+          const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+          if (act[k] && (ux || uy) && (ux || cx) && (uy || in_y)) {
+            const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+            cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
+          } else {
+            cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float2 v2 = make_float2(cv[k], cv[k]);
+      a0[k] += cv[k];
+      a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
+      a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
     }
     if ((p & (kPhiChunk - 1)) == kPhiChunk - 1) {
       // second level of the two-level sum, thread-private slots in shared memory
@@ -420,16 +528,18 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     if (t >= ntiles) return;
     const Tile2D tl = tiles[t];
     const Ev2D& ev = evs[tl.ev];
-    const int nch = ev.nchunks, boxW = ev.boxW, boxH = ev.boxH;
+    const int nch = ev.nchunks;
     const Chunk2D* __restrict__ chunks = ev.chunks;
     const float4* __restrict__ gnodes = reinterpret_cast<const float4*>(ev.nodes);
     if (warp == 0) {
       const Chunk2D c0 = chunks[0];
-      stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, boxW, boxH,
+      stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, win_w(c0),
+                   win_h(c0),
                    stab, ev.tab, (uint32_t)ev.NPHI * kPhiTab2D * 16, &bars[0]);
     }
     // per-thread cell constants
     const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
+    const int x_hi = min(tl.x0 + kTileX, ev.NX) - 1, y_hi = min(tl.y0 + kTileY, ev.NY) - 1;
     const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
     const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
@@ -457,7 +567,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       if (warp == 0 && c + 1 < nch) {
         const Chunk2D cn = chunks[c + 1];
         stage_window(b ? buf0 : buf1, gnodes, ev.NX, ev.NY, tl.x0 + cn.ox0 - 1, tl.y0 + cn.oy0 - 1,
-                     boxW, boxH, nullptr, nullptr, 0u, &bars[b ^ 1]);
+                     win_w(cn), win_h(cn), nullptr, nullptr, 0u, &bars[b ^ 1]);
       }
       const uint32_t ph = b ? phase1 : phase0;
       const bool ok = mbar_wait(&bars[b], ph, kWaitLimit);
@@ -472,9 +582,13 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
         return;
       }
       const Chunk2D ch = chunks[c];
-      const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1;
+      const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1, boxW = win_w(ch);
       const float4* win = b ? buf1 : buf0;
-      if (tl.interior)
+      // every sample of this run lands at least one node inside the grid
+      // boundary (cells past the grid edge are computed but never stored)
+      const bool interior = (tl.x0 + ch.ox0 >= 2) && (x_hi + ch.ox1 <= ev.NX - 3) &&
+                            (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
+      if (interior)
         stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
                            a12, a34, stot, err);
       else
@@ -671,9 +785,15 @@ __global__ void __launch_bounds__(kThreadsLandau) fsm_landau_kernel(const EvLand
   const int is = b.begin + threadIdx.x;
   int fb = 0;
   if (is < DIM) {
-    float T[10], J[4] = {0, 0, 0, 0};
+    float T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}, J[4] = {0, 0, 0, 0};
+    if (ev.is3d) {
 #pragma unroll
-    for (int m = 0; m < 10; ++m) T[m] = __ldg(ev.T + (size_t)m * DIM + is);
+      for (int m = 0; m < 10; ++m) T[m] = __ldg(ev.T + (size_t)m * DIM + is);
+    } else {  // boost-invariant: the stream kernel wrote T^{tau eta} = T^{x eta} = T^{y eta} = T^{eta eta} = 0
+      constexpr int nz[6] = {0, 1, 2, 4, 5, 7};
+#pragma unroll
+      for (int m = 0; m < 6; ++m) T[nz[m]] = __ldg(ev.T + (size_t)nz[m] * DIM + is);
+    }
     if (ev.baryon && ev.J) {
 #pragma unroll
       for (int m = 0; m < 4; ++m) J[m] = __ldg(ev.J + (size_t)m * DIM + is);

@@ -7,12 +7,13 @@
 // g = diag(1,-1,-1,-tau^2) (src/LandauMatch.cpp:197-214).  Because g T g is
 // symmetric, T^mu_nu is self-adjoint in the Minkowski inner product, so the
 // Rayleigh quotient  e(u) = (u.g.M.u)/(u.g.u)  is stationary at every
-// eigenvector and Rayleigh-quotient iteration converges fast.  The iteration
-// starts from the energy-flux direction u0^mu = T^{mu tau} (timelike for any
-// T^{mu nu} built from non-negative phase-space densities); each step solves
-// (M - e I) y = u by Gaussian elimination with partial pivoting, which is
-// backward stable, so strongly boosted cells (entries ~ gamma^2 e, eigenvalues
-// ~ e) keep their accuracy.  Everything is FP64.
+// eigenvector and Rayleigh-quotient iteration converges fast (cubically).
+// The iteration starts from the energy-flux direction u0^mu = T^{mu tau}
+// (timelike for any T^{mu nu} built from non-negative phase-space densities);
+// each step solves (M - e I) y = u by Gaussian elimination with partial
+// pivoting, which is backward stable, so strongly boosted cells (entries ~
+// gamma^2 e, eigenvalues ~ e) keep their accuracy.  The first steps run in
+// FP32, the converging ones and the acceptance test in FP64.
 //
 // Acceptance mirrors src/LandauMatch.cpp:222-291: the eigenvalue must be real
 // and positive, the eigenvector timelike and the boost factor u^tau below 100;
@@ -21,27 +22,51 @@
 #pragma once
 #include <math.h>
 
+#ifndef FSM_HD
 #if defined(__CUDACC__)
 #define FSM_HD __host__ __device__ __forceinline__
 #else
 #define FSM_HD inline
 #endif
+#endif
 
 namespace fsm {
+
+FSM_HD double fsm_rsqrt(double x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+FSM_HD float fsm_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+template <typename R> FSM_HD R eps_of();
+template <> FSM_HD double eps_of<double>() { return 2.220446049250313e-16; }
+template <> FSM_HD float eps_of<float>() { return 1.1920929e-07f; }
+template <typename R> FSM_HD R tiny_of();
+template <> FSM_HD double tiny_of<double>() { return 1.0e-290; }
+template <> FSM_HD float tiny_of<float>() { return 1.0e-36f; }
 
 // Solve A y = b by Gaussian elimination with partial pivoting (backward
 // stable).  Pivoting is a sequence of conditional row swaps with compile-time
 // indices, so A stays in registers.  A pivot below eps*max|A| (the shift has
 // hit the eigenvalue to rounding) is replaced by eps*max|A|, the usual inverse-
 // iteration safeguard: y stays finite and only its direction is used.
-template <int N>
-FSM_HD void gepp_solve(double A[N][N], double b[N], double y[N]) {
-  double amax = 0.0;
+template <typename R, int N>
+FSM_HD void gepp_solve(R A[N][N], R b[N], R y[N]) {
+  R amax = 0;
 #pragma unroll
   for (int r = 0; r < N; ++r)
 #pragma unroll
     for (int c = 0; c < N; ++c) amax = fmax(amax, fabs(A[r][c]));
-  const double tiny = fmax(2.220446049250313e-16 * amax, 1.0e-290);
+  const R tiny = fmax(eps_of<R>() * amax, tiny_of<R>());
+  R inv[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
 #pragma unroll
@@ -49,49 +74,48 @@ FSM_HD void gepp_solve(double A[N][N], double b[N], double y[N]) {
       const bool sw = fabs(A[r][k]) > fabs(A[k][k]);
 #pragma unroll
       for (int c = k; c < N; ++c) {
-        const double a = A[k][c], z = A[r][c];
+        const R a = A[k][c], z = A[r][c];
         A[k][c] = sw ? z : a;
         A[r][c] = sw ? a : z;
       }
-      const double a = b[k], z = b[r];
+      const R a = b[k], z = b[r];
       b[k] = sw ? z : a;
       b[r] = sw ? a : z;
     }
-    double piv = A[k][k];
-    if (fabs(piv) < tiny) piv = (piv < 0.0) ? -tiny : tiny;
-    const double inv = 1.0 / piv;
+    R piv = A[k][k];
+    if (fabs(piv) < tiny) piv = (piv < 0) ? -tiny : tiny;
+    inv[k] = R(1) / piv;
 #pragma unroll
     for (int r = k + 1; r < N; ++r) {
-      const double f = A[r][k] * inv;
+      const R f = A[r][k] * inv[k];
 #pragma unroll
       for (int c = k + 1; c < N; ++c) A[r][c] -= f * A[k][c];
       b[r] -= f * b[k];
     }
-    A[k][k] = piv;
   }
 #pragma unroll
   for (int k = N - 1; k >= 0; --k) {
-    double s = b[k];
+    R s = b[k];
 #pragma unroll
     for (int c = k + 1; c < N; ++c) s -= A[k][c] * y[c];
-    y[k] = s / A[k][k];
+    y[k] = s * inv[k];
   }
 }
 
-template <int N>
-FSM_HD double mink_norm2(const double g[N], const double u[N]) {
-  double s = 0.0;
+template <typename R, int N>
+FSM_HD R mink_norm2(const R g[N], const R u[N]) {
+  R s = 0;
 #pragma unroll
   for (int r = 0; r < N; ++r) s += g[r] * u[r] * u[r];
   return s;
 }
 
-template <int N>
-FSM_HD double rayleigh(const double M[N][N], const double g[N], const double u[N]) {
-  double num = 0.0, den = 0.0;
+template <typename R, int N>
+FSM_HD R rayleigh(const R M[N][N], const R g[N], const R u[N]) {
+  R num = 0, den = 0;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
-    double mu = 0.0;
+    R mu = 0;
 #pragma unroll
     for (int c = 0; c < N; ++c) mu += M[r][c] * u[c];
     num += g[r] * u[r] * mu;
@@ -100,62 +124,111 @@ FSM_HD double rayleigh(const double M[N][N], const double g[N], const double u[N
   return num / den;
 }
 
-// Timelike eigenpair of M (N = 3 for boost-invariant 2D events, whose eta row
-// and column vanish identically; N = 4 in 3D).  Returns 1 and (e, u) with
-// u.g.u = 1, u^tau > 0 when an acceptable pair was found.
+// One Rayleigh-quotient-iteration step: u <- (M - e)^-1 u, normalised to
+// u.g.u = 1 with u^tau > 0, and e <- its Rayleigh quotient.  False when the
+// step leaves the light cone or is not finite.
+template <typename R, int N>
+FSM_HD bool rqi_step(const R M[N][N], const R g[N], R u[N], R& e) {
+  R A[N][N], rhs[N], y[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    rhs[r] = u[r];
+#pragma unroll
+    for (int c = 0; c < N; ++c) A[r][c] = M[r][c] - (r == c ? e : R(0));
+  }
+  gepp_solve<R, N>(A, rhs, y);
+  const R m2 = mink_norm2<R, N>(g, y);
+  if (!(m2 > 0) || !isfinite(m2)) return false;
+  R t = fsm_rsqrt(m2);
+  if (y[0] < 0) t = -t;
+#pragma unroll
+  for (int r = 0; r < N; ++r) u[r] = y[r] * t;
+  e = rayleigh<R, N>(M, g, u);
+  return true;
+}
+
+// max |M u - e u| and the scales max|M|, max|u| of a candidate eigenpair.
 template <int N>
-FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, double u_out[N]) {
-  double u[N];
-#pragma unroll
-  for (int r = 0; r < N; ++r) u[r] = M[r][0];
-  double n2 = mink_norm2<N>(g, u);
-  if (!(n2 > 0.0) || !isfinite(n2)) {
-#pragma unroll
-    for (int r = 0; r < N; ++r) u[r] = (r == 0) ? 1.0 : 0.0;
-    n2 = 1.0;
-  }
-  double s = 1.0 / sqrt(n2);
-  if (u[0] < 0.0) s = -s;
-#pragma unroll
-  for (int r = 0; r < N; ++r) u[r] *= s;
-  double e = rayleigh<N>(M, g, u);
-  for (int it = 0; it < 16; ++it) {
-    double A[N][N], rhs[N], y[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      rhs[r] = u[r];
-#pragma unroll
-      for (int c = 0; c < N; ++c) A[r][c] = M[r][c] - (r == c ? e : 0.0);
-    }
-    gepp_solve<N>(A, rhs, y);
-    double m2 = mink_norm2<N>(g, y);
-    if (!(m2 > 0.0) || !isfinite(m2)) break;  // degenerate step or left the light cone
-    double t = 1.0 / sqrt(m2);
-    if (y[0] < 0.0) t = -t;
-    double d = 0.0, umax = 0.0;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      y[r] *= t;
-      d = fmax(d, fabs(y[r] - u[r]));
-      umax = fmax(umax, fabs(y[r]));
-      u[r] = y[r];
-    }
-    e = rayleigh<N>(M, g, u);
-    if (d <= 1.0e-14 * umax) break;
-  }
-  // eigen-residual check: a converged pair has |M u - e u| at rounding level
-  double rmax = 0.0, mmax = 0.0, umax = 0.0;
+FSM_HD void eigen_residual(const double M[N][N], const double u[N], double e, double* rmax,
+                           double* mmax, double* umax) {
+  double rr = 0.0, mm = 0.0, uu = 0.0;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
     double mu = 0.0;
 #pragma unroll
     for (int c = 0; c < N; ++c) {
       mu += M[r][c] * u[c];
-      mmax = fmax(mmax, fabs(M[r][c]));
+      mm = fmax(mm, fabs(M[r][c]));
     }
-    rmax = fmax(rmax, fabs(mu - e * u[r]));
-    umax = fmax(umax, fabs(u[r]));
+    rr = fmax(rr, fabs(mu - e * u[r]));
+    uu = fmax(uu, fabs(u[r]));
   }
+  *rmax = rr;
+  *mmax = mm;
+  *umax = uu;
+}
+
+// Timelike eigenpair of M (N = 3 for boost-invariant 2D events, whose eta row
+// and column vanish identically; N = 4 in 3D).  Returns 1 and (e, u) with
+// u.g.u = 1, u^tau > 0 when an acceptable pair was found.  Three FP32 RQI
+// steps from the energy-flux direction bring u to single precision (RQI
+// converges cubically); FP64 steps then run until the eigen-residual is at
+// rounding level, normally after one.
+template <int N>
+FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, double u_out[N]) {
+  double u[N];
+  {
+    float Mf[N][N], gf[N], uf[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      gf[r] = (float)g[r];
+      uf[r] = (float)M[r][0];
+#pragma unroll
+      for (int c = 0; c < N; ++c) Mf[r][c] = (float)M[r][c];
+    }
+    float n2 = mink_norm2<float, N>(gf, uf);
+    bool ok = (n2 > 0.0f) && isfinite(n2);
+    if (ok) {
+      float s = fsm_rsqrt(n2);
+      if (uf[0] < 0.0f) s = -s;
+#pragma unroll
+      for (int r = 0; r < N; ++r) uf[r] *= s;
+      float ef = rayleigh<float, N>(Mf, gf, uf);
+      float keep[N];
+#pragma unroll
+      for (int r = 0; r < N; ++r) keep[r] = uf[r];
+      for (int it = 0; it < 3; ++it) {
+        if (!rqi_step<float, N>(Mf, gf, uf, ef) || !isfinite(ef)) {
+#pragma unroll
+          for (int r = 0; r < N; ++r) uf[r] = keep[r];
+          break;
+        }
+#pragma unroll
+        for (int r = 0; r < N; ++r) keep[r] = uf[r];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r) u[r] = ok ? (double)uf[r] : (double)M[r][0];
+  }
+  double n2 = mink_norm2<double, N>(g, u);
+  if (!(n2 > 0.0) || !isfinite(n2)) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) u[r] = (r == 0) ? 1.0 : 0.0;
+    n2 = 1.0;
+  }
+  double s = fsm_rsqrt(n2);
+  if (u[0] < 0.0) s = -s;
+#pragma unroll
+  for (int r = 0; r < N; ++r) u[r] *= s;
+  double e = rayleigh<double, N>(M, g, u);
+  double rmax, mmax, umax;
+  for (int it = 0; it < 12; ++it) {
+    if (!rqi_step<double, N>(M, g, u, e)) break;
+    eigen_residual<N>(M, u, e, &rmax, &mmax, &umax);
+    if (rmax <= 1.0e-13 * mmax * umax) break;
+  }
+  // acceptance: a converged pair has |M u - e u| at rounding level
+  eigen_residual<N>(M, u, e, &rmax, &mmax, &umax);
   if (!(isfinite(e) && (rmax <= 1.0e-9 * mmax * umax) && (e > 0.0))) return 0;
   *e_out = e;
 #pragma unroll

@@ -23,8 +23,10 @@
 #include "fsm_plan.h"
 
 namespace fsm {
-__global__ void fsm_prep2d_lines_kernel(const Ev2D*, const LineBlock*);
-__global__ void fsm_prep2d_pack_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_rows_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
+__global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 }  // namespace fsm
@@ -141,9 +143,16 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
                            (y0 + kTileY - 1 + P.oy_max <= NY - 3);
       tiles.push_back(Tile2D{0, x0, y0, interior});
     }
-  std::vector<LineBlock> lines, packs;
-  for (int b = 0; b < NX + NY; b += 128) lines.push_back(LineBlock{0, b});
-  for (int b = 0; b < NY; b += 128) packs.push_back(LineBlock{0, b});
+  std::vector<LineBlock> rows, cols;
+  const bool strip = NX <= kMaxStrip && NY <= kMaxStrip;
+  if (strip) {
+    for (int x = 0; x < NX; x += 32) rows.push_back(LineBlock{0, x, 0});
+    for (int y = 0; y < NY; y += 32) cols.push_back(LineBlock{0, y, 0});
+  } else {
+    for (int x = 0; x < NX; x += kPrepRows) rows.push_back(LineBlock{0, x, 0});
+    for (int y = 0; y < NY; y += 32)
+      for (int g = 0; g < (NX + kSegP - 1) / kSegP; g += 4) cols.push_back(LineBlock{0, y, g});
+  }
   std::vector<CellBlock> bl;
   for (int b = 0; b < DIM; b += kThreadsLandau) bl.push_back(CellBlock{0, b});
 
@@ -152,17 +161,16 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   const size_t o_cs = R.take(P.cs.size() * sizeof(FSM_FLOAT2));
   const size_t o_tab = R.take(P.tab2.size() * sizeof(PhiEntry2D));
   const size_t o_chunks = R.take(P.chunks2.size() * sizeof(Chunk2D));
-  const size_t o_hx = R.take(P.hx.size() * 8), o_fx = R.take(P.fx.size() * 8);
-  const size_t o_dgx = R.take(P.dgx.size() * 8), o_hy = R.take(P.hy.size() * 8);
-  const size_t o_fy = R.take(P.fy.size() * 8), o_dgy = R.take(P.dgy.size() * 8);
+  const size_t o_axx = R.take(P.axx.size() * sizeof(AxisNode));
+  const size_t o_axy = R.take(P.axy.size() * sizeof(AxisNode));
   const size_t o_ev2 = R.take(sizeof(Ev2D)), o_evl = R.take(sizeof(EvLandau));
   const size_t o_tiles = R.take(tiles.size() * sizeof(Tile2D));
-  const size_t o_lines = R.take(lines.size() * sizeof(LineBlock));
-  const size_t o_packs = R.take(packs.size() * sizeof(LineBlock));
+  const size_t o_rows = R.take(rows.size() * sizeof(LineBlock));
+  const size_t o_cols = R.take(cols.size() * sizeof(LineBlock));
   const size_t o_bl = R.take(bl.size() * sizeof(CellBlock));
   const size_t upload_bytes = R.off;
   const size_t o_ctr = R.take(sizeof(Counters)), o_err = R.take(4 * sizeof(int));
-  const size_t o_zx = R.take((size_t)DIM * 8), o_zy = R.take((size_t)DIM * 8);
+  const size_t o_fa = R.take((size_t)DIM * 4), o_sy = R.take((size_t)DIM * 4);
   const size_t o_nodes = R.take((size_t)DIM * 16);
   const size_t o_T = R.take((size_t)DIM * 10 * 4);
   if (R.off > kNoAllocScratchBytes) {
@@ -199,12 +207,10 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   e.boxW = P.boxW;
   e.boxH = P.boxH;
   e.e_gev = d_e_gev;
-  e.ax = SplineAxis{reinterpret_cast<const double*>(D + o_hx), reinterpret_cast<const double*>(D + o_fx),
-                    reinterpret_cast<const double*>(D + o_dgx), NX};
-  e.ay = SplineAxis{reinterpret_cast<const double*>(D + o_hy), reinterpret_cast<const double*>(D + o_fy),
-                    reinterpret_cast<const double*>(D + o_dgy), NY};
-  e.zx = reinterpret_cast<double*>(D + o_zx);
-  e.zy = reinterpret_cast<double*>(D + o_zy);
+  e.ax = reinterpret_cast<const AxisNode*>(D + o_axx) + kPadLo;
+  e.ay = reinterpret_cast<const AxisNode*>(D + o_axy) + kPadLo;
+  e.fa = reinterpret_cast<float*>(D + o_fa);
+  e.sy = reinterpret_cast<float*>(D + o_sy);
   e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o_nodes);
   e.T = dev_out->T ? dev_out->T : reinterpret_cast<float*>(D + o_T);
   EvLandau l{};
@@ -230,25 +236,28 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   put(o_cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
   put(o_tab, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
   put(o_chunks, P.chunks2.data(), P.chunks2.size() * sizeof(Chunk2D));
-  put(o_hx, P.hx.data(), P.hx.size() * 8);
-  put(o_fx, P.fx.data(), P.fx.size() * 8);
-  put(o_dgx, P.dgx.data(), P.dgx.size() * 8);
-  put(o_hy, P.hy.data(), P.hy.size() * 8);
-  put(o_fy, P.fy.data(), P.fy.size() * 8);
-  put(o_dgy, P.dgy.data(), P.dgy.size() * 8);
+  put(o_axx, P.axx.data(), P.axx.size() * sizeof(AxisNode));
+  put(o_axy, P.axy.data(), P.axy.size() * sizeof(AxisNode));
   put(o_ev2, &e, sizeof(e));
   put(o_evl, &l, sizeof(l));
   put(o_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
-  put(o_lines, lines.data(), lines.size() * sizeof(LineBlock));
-  put(o_packs, packs.data(), packs.size() * sizeof(LineBlock));
+  put(o_rows, rows.data(), rows.size() * sizeof(LineBlock));
+  put(o_cols, cols.data(), cols.size() * sizeof(LineBlock));
   put(o_bl, bl.data(), bl.size() * sizeof(CellBlock));
 
   // launch geometry of the stream kernel (as the batch path computes it)
   const int tab_cap = P.p.DIM_PHIP;
-  const int box_cap = (P.boxW * P.boxH + 7) & ~7;
+  const int box_cap = (P.box_elems + 7) & ~7;
   const size_t smem2 = (((size_t)tab_cap * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)box_cap * 16 +
                        (size_t)kTotSlots2D * kThreads2D * 4;
   if ((st = raise_dyn_smem((const void*)fsm_stream2d_kernel, smem2)) != FSM_OK) return st;
+  const size_t smem_rows = strip ? prep_strip_smem(std::max(NX, NY)) : prep_rows_smem(NY);
+  if (strip) {
+    if ((st = raise_dyn_smem((const void*)fsm_prep2d_rows_kernel, smem_rows)) != FSM_OK) return st;
+    if ((st = raise_dyn_smem((const void*)fsm_prep2d_cols_kernel, smem_rows)) != FSM_OK) return st;
+  } else if ((st = raise_dyn_smem((const void*)fsm_prep2d_rows_long_kernel, smem_rows)) != FSM_OK) {
+    return st;
+  }
   int dev = 0, sms = 0, occ = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -268,8 +277,15 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   if ((st = cu(cudaMemsetAsync(D + o_ctr, 0, sizeof(Counters), s), "memset")) != FSM_OK) return st;
   if ((st = cu(cudaMemsetAsync(D + o_err, 0, 4 * sizeof(int), s), "memset")) != FSM_OK) return st;
   const Ev2D* d_ev2 = reinterpret_cast<const Ev2D*>(D + o_ev2);
-  fsm_prep2d_lines_kernel<<<(int)lines.size(), 128, 0, s>>>(d_ev2, reinterpret_cast<const LineBlock*>(D + o_lines));
-  fsm_prep2d_pack_kernel<<<(int)packs.size(), 128, 0, s>>>(d_ev2, reinterpret_cast<const LineBlock*>(D + o_packs));
+  const LineBlock* d_rows = reinterpret_cast<const LineBlock*>(D + o_rows);
+  const LineBlock* d_cols = reinterpret_cast<const LineBlock*>(D + o_cols);
+  if (strip) {
+    fsm_prep2d_rows_kernel<<<(int)rows.size(), kPrepThreads, smem_rows, s>>>(d_ev2, d_rows);
+    fsm_prep2d_cols_kernel<<<(int)cols.size(), kPrepThreads, smem_rows, s>>>(d_ev2, d_cols);
+  } else {
+    fsm_prep2d_rows_long_kernel<<<(int)rows.size(), kPrepRows * 32, smem_rows, s>>>(d_ev2, d_rows, NY);
+    fsm_prep2d_cols_long_kernel<<<(int)cols.size(), 128, 0, s>>>(d_ev2, d_cols);
+  }
   fsm_stream2d_kernel<<<grid2, kThreads2D, smem2, s>>>(d_ev2, reinterpret_cast<const Tile2D*>(D + o_tiles), ntiles,
                                                        tab_cap, box_cap, reinterpret_cast<Counters*>(D + o_ctr),
                                                        reinterpret_cast<int*>(D + o_err));

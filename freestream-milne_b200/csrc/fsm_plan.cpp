@@ -23,6 +23,34 @@ static inline float tanmap_w(int irap, int NR) {  // src/FreeStream.cpp:174
   return (float)(-.9975 + (float)irap * (1.995 / (float)(NR - 1)));
 }
 
+// Natural-spline axis table on the float grid coordinates x_i = i*d + lo
+// (src/FreeStream.cpp:129-140): interval widths and the elimination factors of
+// the tridiagonal system, padded with zero entries (see AxisNode).
+void build_axis(int n, float d, float lo, std::vector<AxisNode>& ax) {
+  std::vector<double> xv(n);
+  for (int i = 0; i < n; ++i) {
+    float xf = (float)i * d + lo;
+    xv[i] = xf;
+  }
+  ax.assign((size_t)n + kPadLo + kPadHi, AxisNode{0.0, 0.0, 0.0, 0.0});
+  AxisNode* A = ax.data() + kPadLo;
+  for (int i = 0; i + 1 < n; ++i) {
+    A[i].h = xv[i + 1] - xv[i];
+    A[i].g = 6.0 / A[i].h;
+  }
+  const int m = n - 2;
+  double dgp = 0.0;
+  for (int k = 0; k < m; ++k) {
+    double dg = 2.0 * (A[k].h + A[k + 1].h);
+    if (k > 0) {
+      A[k].f = A[k].h / dgp;
+      dg -= A[k].f * A[k].h;
+    }
+    A[k].idg = 1.0 / dg;
+    dgp = dg;
+  }
+}
+
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
                       std::string* why) {
   EventPlan& E = *out;
@@ -46,6 +74,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     if (!(p.DETA > 0) || !(p.TAU0 > 0))
       return fail(FSM_ERR_INVALID_ARG, "3D needs DETA > 0 and TAU0 > 0");
   }
+  if (!E.is3d && p.DIM_Y > kMaxNY2D)
+    return fail(FSM_ERR_TOO_LARGE, "DIM_Y above 5120 on the 2D path");
   E.baryon = p.BARYON != 0;
   if (E.baryon && !E.is3d)
     return fail(FSM_ERR_UNSUPPORTED, "BARYON with DIM_ETA = 1 is not implemented on the GPU path");
@@ -100,26 +130,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
 
   if (!E.is3d) {
     // natural-spline axes on the float grid coordinates (src/FreeStream.cpp:129-140)
-    auto axis = [](int n, float d, float lo, std::vector<double>& h, std::vector<double>& f,
-                   std::vector<double>& dg) {
-      std::vector<double> xv(n);
-      for (int i = 0; i < n; ++i) {
-        float xf = (float)i * d + lo;
-        xv[i] = xf;
-      }
-      h.resize(n - 1);
-      for (int i = 0; i + 1 < n; ++i) h[i] = xv[i + 1] - xv[i];
-      int m = n - 2;
-      f.assign(std::max(m, 1), 0.0);
-      dg.assign(std::max(m, 1), 0.0);
-      for (int k = 0; k < m; ++k) dg[k] = 2.0 * (h[k] + h[k + 1]);
-      for (int k = 1; k < m; ++k) {
-        f[k] = h[k] / dg[k - 1];
-        dg[k] -= f[k] * h[k];
-      }
-    };
-    axis(NX, p.DX, E.xmin, E.hx, E.fx, E.dgx);
-    axis(NY, p.DY, E.ymin, E.hy, E.fy, E.dgy);
+    build_axis(NX, p.DX, E.xmin, E.axx);
+    build_axis(NY, p.DY, E.ymin, E.axy);
     // per-phi_p stream table (see PhiEntry2D)
     E.tab2.resize(NP);
     for (int k = 0; k < NP; ++k) {
@@ -177,9 +189,10 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
           }
         }
         if (flush) {
-          E.chunks2.push_back(Chunk2D{p0, k, lo_x, lo_y});
+          E.chunks2.push_back(Chunk2D{p0, k, lo_x, lo_y, hi_x, hi_y});
           E.boxH = std::max(E.boxH, kTileX + (hi_x - lo_x) + 3);
           E.boxW = std::max(E.boxW, kTileY + (hi_y - lo_y) + 3);
+          E.box_elems = std::max(E.box_elems, (kTileX + (hi_x - lo_x) + 3) * (kTileY + (hi_y - lo_y) + 3));
           if (k < NP) {
             p0 = k;
             lo_x = hi_x = E.tab2[k].ox;

@@ -20,10 +20,11 @@ struct EventPlan {
   std::vector<FSM_FLOAT2> cs;  // (cos, sin) of phi_p
   std::vector<PhiEntry2D> tab2;  // 2D stream table
   std::vector<Chunk2D> chunks2;  // phi_p runs staged as one window each
-  int boxW = 0, boxH = 0;        // staged window size (nodes)
+  int boxW = 0, boxH = 0;        // largest staged window width / height over the runs (nodes)
+  int box_elems = 0;             // largest staged window (nodes) of one run
   int ox_min = 0, ox_max = 0, oy_min = 0, oy_max = 0;  // offset range over all phi_p
   // 2D spline axes
-  std::vector<double> hx, fx, dgx, hy, fy, dgy;
+  std::vector<AxisNode> axx, axy;
   int Rx = 0, Ry = 0;
   // 3D tables
   std::vector<RapEta> re;
@@ -39,6 +40,10 @@ struct EventPlan {
 // and fills the tables.  Returns FSM_OK or an error with a message in *why.
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
                       std::string* why);
+
+// Natural-spline axis table of n float grid coordinates i*d + lo, with
+// kPadLo + kPadHi zero padding entries (entry k of the line at kPadLo + k).
+void build_axis(int n, float d, float lo, std::vector<AxisNode>& ax);
 
 // Output components of one event in the slab order used by batches:
 // T(10) e P Pi u(4) pi(10) [J(4) nB V(4)].

@@ -4,7 +4,7 @@
 // on the host, laid out in one device allocation (tables, scratch, descriptor
 // arrays, work lists and optionally input/output slabs), and run as a fixed
 // sequence of six launches on one stream:
-//   memset(counters) -> prep2d_lines -> prep2d_pack -> prep3d -> stream2d
+//   memset(counters) -> prep2d_rows -> prep2d_cols -> prep3d -> stream2d
 //   -> stream3d -> landau
 // The sequence is captured into a CUDA graph on the first fsm_batch_launch and
 // replayed afterwards.  The single-event entry points run a cached one-event
@@ -23,8 +23,10 @@
 #include "fsm_plan.h"
 
 namespace fsm {
-__global__ void fsm_prep2d_lines_kernel(const Ev2D*, const LineBlock*);
-__global__ void fsm_prep2d_pack_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_rows_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
+__global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
+__global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const CellBlock*, int, int, Counters*);
@@ -96,13 +98,13 @@ struct fsm_batch {
   Ev3D* d_ev3 = nullptr;
   EvLandau* d_evl = nullptr;
   Tile2D* d_tiles = nullptr;
-  LineBlock *d_lines = nullptr, *d_packs = nullptr;
+  LineBlock *d_rows = nullptr, *d_cols = nullptr, *d_rows_l = nullptr, *d_cols_l = nullptr;
   CellBlock *d_prep3 = nullptr, *d_b3 = nullptr, *d_bl = nullptr;
   Counters* d_ctr = nullptr;
   int* d_err = nullptr;
-  int ntiles = 0, nlines = 0, npacks = 0, nprep3 = 0, nb3 = 0, nbl = 0;
-  int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0;
-  size_t smem2 = 0, smem3 = 0;
+  int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, nb3 = 0, nbl = 0;
+  int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
+  size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
   int grid2 = 0, grid3 = 0;
   double samples = 0;
   cudaGraphExec_t graph = nullptr;
@@ -151,7 +153,8 @@ fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot) 
   }
   return FSM_OK;
 }
-int g_smem2[64] = {0}, g_smem3[64] = {0};
+int g_smem2[64] = {0}, g_smem3[64] = {0}, g_smem_rows[64] = {0}, g_smem_srows[64] = {0},
+    g_smem_scols[64] = {0};
 
 // Builds descriptors and uploads everything.  ext_in / ext_out (one event)
 // select external device buffers instead of owned slabs.
@@ -174,8 +177,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   // ---- layout
   Layout L;
   struct EvOffs {
-    size_t cs, tab2, chunks, hx, fx, dgx, hy, fy, dgy, re, rapf, rapfB, jac;
-    size_t zx, zy, nodes, efield, T, J, in_e, in_nB, out;
+    size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac;
+    size_t fa, sy, nodes, efield, T, J, in_e, in_nB, out;
   };
   std::vector<EvOffs> eo(n);
   int n2 = 0, n3 = 0;
@@ -201,12 +204,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     if (!P.is3d) {
       o.tab2 = L.take(P.tab2.size() * sizeof(PhiEntry2D));
       o.chunks = L.take(P.chunks2.size() * sizeof(Chunk2D));
-      o.hx = L.take(P.hx.size() * 8);
-      o.fx = L.take(P.fx.size() * 8);
-      o.dgx = L.take(P.dgx.size() * 8);
-      o.hy = L.take(P.hy.size() * 8);
-      o.fy = L.take(P.fy.size() * 8);
-      o.dgy = L.take(P.dgy.size() * 8);
+      o.axx = L.take(P.axx.size() * sizeof(AxisNode));
+      o.axy = L.take(P.axy.size() * sizeof(AxisNode));
     } else {
       o.re = L.take(P.re.size() * sizeof(RapEta));
       o.rapf = L.take(P.rapf.size() * 4);
@@ -216,7 +215,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   }
   // work lists (host side first, to know their sizes)
   std::vector<Tile2D> tiles;
-  std::vector<LineBlock> lines, packs;
+  std::vector<LineBlock> rows, cols, rows_l, cols_l;
   std::vector<CellBlock> prep3, b3, bl;
   {
     std::vector<int> order2;
@@ -243,9 +242,18 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
       if (P.is3d) continue;
-      int nl = P.p.DIM_X + P.p.DIM_Y;
-      for (int s = 0; s < nl; s += 128) lines.push_back(LineBlock{b->ev2_of[i], s});
-      for (int s = 0; s < P.p.DIM_Y; s += 128) packs.push_back(LineBlock{b->ev2_of[i], s});
+      const int e2 = b->ev2_of[i], NX = P.p.DIM_X, NY = P.p.DIM_Y;
+      if (NX <= kMaxStrip && NY <= kMaxStrip) {
+        for (int x = 0; x < NX; x += 32) rows.push_back(LineBlock{e2, x, 0});
+        for (int y = 0; y < NY; y += 32) cols.push_back(LineBlock{e2, y, 0});
+        b->strip_cap2 = std::max(b->strip_cap2, std::max(NX, NY));
+      } else {
+        for (int x = 0; x < NX; x += kPrepRows) rows_l.push_back(LineBlock{e2, x, 0});
+        const int nseg = (NX + kSegP - 1) / kSegP;
+        for (int y = 0; y < NY; y += 32)
+          for (int g = 0; g < nseg; g += 4) cols_l.push_back(LineBlock{e2, y, g});
+        b->ny_cap2 = std::max(b->ny_cap2, NY);
+      }
     }
     std::vector<int> order3;
     for (int i = 0; i < n; ++i)
@@ -270,8 +278,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   size_t o_ev3 = L.take(std::max(n3, 1) * sizeof(Ev3D));
   size_t o_evl = L.take(n * sizeof(EvLandau));
   size_t o_tiles = L.take(std::max<size_t>(tiles.size(), 1) * sizeof(Tile2D));
-  size_t o_lines = L.take(std::max<size_t>(lines.size(), 1) * sizeof(LineBlock));
-  size_t o_packs = L.take(std::max<size_t>(packs.size(), 1) * sizeof(LineBlock));
+  size_t o_rows = L.take(std::max<size_t>(rows.size(), 1) * sizeof(LineBlock));
+  size_t o_cols = L.take(std::max<size_t>(cols.size(), 1) * sizeof(LineBlock));
+  size_t o_rows_l = L.take(std::max<size_t>(rows_l.size(), 1) * sizeof(LineBlock));
+  size_t o_cols_l = L.take(std::max<size_t>(cols_l.size(), 1) * sizeof(LineBlock));
   size_t o_prep3 = L.take(std::max<size_t>(prep3.size(), 1) * sizeof(CellBlock));
   size_t o_b3 = L.take(std::max<size_t>(b3.size(), 1) * sizeof(CellBlock));
   size_t o_bl = L.take(bl.size() * sizeof(CellBlock));
@@ -283,8 +293,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     const EventPlan& P = b->plans[i];
     EvOffs& o = eo[i];
     if (!P.is3d) {
-      o.zx = L.take((size_t)P.DIM * 8);
-      o.zy = L.take((size_t)P.DIM * 8);
+      o.fa = L.take((size_t)P.DIM * 4);
+      o.sy = L.take((size_t)P.DIM * 4);
       o.nodes = L.take((size_t)P.DIM * 16);
     } else {
       o.efield = L.take((size_t)P.DIM * 4);
@@ -323,12 +333,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     if (!P.is3d) {
       std::memcpy(H + o.tab2, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
       std::memcpy(H + o.chunks, P.chunks2.data(), P.chunks2.size() * sizeof(Chunk2D));
-      std::memcpy(H + o.hx, P.hx.data(), P.hx.size() * 8);
-      std::memcpy(H + o.fx, P.fx.data(), P.fx.size() * 8);
-      std::memcpy(H + o.dgx, P.dgx.data(), P.dgx.size() * 8);
-      std::memcpy(H + o.hy, P.hy.data(), P.hy.size() * 8);
-      std::memcpy(H + o.fy, P.fy.data(), P.fy.size() * 8);
-      std::memcpy(H + o.dgy, P.dgy.data(), P.dgy.size() * 8);
+      std::memcpy(H + o.axx, P.axx.data(), P.axx.size() * sizeof(AxisNode));
+      std::memcpy(H + o.axy, P.axy.data(), P.axy.size() * sizeof(AxisNode));
     } else {
       std::memcpy(H + o.re, P.re.data(), P.re.size() * sizeof(RapEta));
       std::memcpy(H + o.rapf, P.rapf.data(), P.rapf.size() * 4);
@@ -412,20 +418,16 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.nchunks = (int)P.chunks2.size();
       e.boxW = P.boxW;
       e.boxH = P.boxH;
-      b->box_cap2 = std::max(b->box_cap2, P.boxW * P.boxH);
+      b->box_cap2 = std::max(b->box_cap2, P.box_elems);
       e.use_smem = fp <= smem_budget ? 1 : 0;
       if (e.use_smem) max_fp = std::max(max_fp, fp);
       e.tiles_y = (p.DIM_Y + kTileY - 1) / kTileY;
       e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o.cs);
       e.e_gev = b->d_in_e[i];
-      e.ax = SplineAxis{reinterpret_cast<const double*>(D + o.hx),
-                        reinterpret_cast<const double*>(D + o.fx),
-                        reinterpret_cast<const double*>(D + o.dgx), p.DIM_X};
-      e.ay = SplineAxis{reinterpret_cast<const double*>(D + o.hy),
-                        reinterpret_cast<const double*>(D + o.fy),
-                        reinterpret_cast<const double*>(D + o.dgy), p.DIM_Y};
-      e.zx = reinterpret_cast<double*>(D + o.zx);
-      e.zy = reinterpret_cast<double*>(D + o.zy);
+      e.ax = reinterpret_cast<const AxisNode*>(D + o.axx) + kPadLo;
+      e.ay = reinterpret_cast<const AxisNode*>(D + o.axy) + kPadLo;
+      e.fa = reinterpret_cast<float*>(D + o.fa);
+      e.sy = reinterpret_cast<float*>(D + o.sy);
       e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o.nodes);
       e.T = b->d_T[i];
       max_np2 = std::max(max_np2, p.DIM_PHIP);
@@ -486,6 +488,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->smem2 = (((size_t)b->cs_cap2 * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)b->box_cap2 * 16 +
              (size_t)kTotSlots2D * kThreads2D * 4;
   b->smem3 = (size_t)b->cs_cap3 * 8;
+  b->smem_rows = prep_rows_smem(b->ny_cap2);
+  b->smem_strip = prep_strip_smem(b->strip_cap2);
   (void)max_fp;
   // the kernels index their dynamic shared memory by these capacities
   if ((n2 && b->smem2 < (size_t)b->cs_cap2 * kPhiTab2D * 16 + 2 * (size_t)b->box_cap2 * 16) ||
@@ -497,8 +501,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   std::memcpy(H + o_ev3, b->ev3.data(), n3 * sizeof(Ev3D));
   std::memcpy(H + o_evl, b->evl.data(), n * sizeof(EvLandau));
   std::memcpy(H + o_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
-  std::memcpy(H + o_lines, lines.data(), lines.size() * sizeof(LineBlock));
-  std::memcpy(H + o_packs, packs.data(), packs.size() * sizeof(LineBlock));
+  std::memcpy(H + o_rows, rows.data(), rows.size() * sizeof(LineBlock));
+  std::memcpy(H + o_cols, cols.data(), cols.size() * sizeof(LineBlock));
+  std::memcpy(H + o_rows_l, rows_l.data(), rows_l.size() * sizeof(LineBlock));
+  std::memcpy(H + o_cols_l, cols_l.data(), cols_l.size() * sizeof(LineBlock));
   std::memcpy(H + o_prep3, prep3.data(), prep3.size() * sizeof(CellBlock));
   std::memcpy(H + o_b3, b3.data(), b3.size() * sizeof(CellBlock));
   std::memcpy(H + o_bl, bl.data(), bl.size() * sizeof(CellBlock));
@@ -506,21 +512,38 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->d_ev3 = reinterpret_cast<Ev3D*>(D + o_ev3);
   b->d_evl = reinterpret_cast<EvLandau*>(D + o_evl);
   b->d_tiles = reinterpret_cast<Tile2D*>(D + o_tiles);
-  b->d_lines = reinterpret_cast<LineBlock*>(D + o_lines);
-  b->d_packs = reinterpret_cast<LineBlock*>(D + o_packs);
+  b->d_rows = reinterpret_cast<LineBlock*>(D + o_rows);
+  b->d_cols = reinterpret_cast<LineBlock*>(D + o_cols);
+  b->d_rows_l = reinterpret_cast<LineBlock*>(D + o_rows_l);
+  b->d_cols_l = reinterpret_cast<LineBlock*>(D + o_cols_l);
   b->d_prep3 = reinterpret_cast<CellBlock*>(D + o_prep3);
   b->d_b3 = reinterpret_cast<CellBlock*>(D + o_b3);
   b->d_bl = reinterpret_cast<CellBlock*>(D + o_bl);
   b->d_ctr = reinterpret_cast<Counters*>(D + o_ctr);
   b->d_err = reinterpret_cast<int*>(D + o_err);
   b->ntiles = (int)tiles.size();
-  b->nlines = (int)lines.size();
-  b->npacks = (int)packs.size();
+  b->nrows = (int)rows.size();
+  b->ncols = (int)cols.size();
+  b->nrows_l = (int)rows_l.size();
+  b->ncols_l = (int)cols_l.size();
   b->nprep3 = (int)prep3.size();
   b->nb3 = (int)b3.size();
   b->nbl = (int)bl.size();
   FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
   // ---- launch geometry
+  if (b->nrows) {
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_prep2d_rows_kernel, ctx->device, b->smem_strip,
+                                    &g_smem_srows[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
+    ss = ensure_dyn_smem((const void*)fsm_prep2d_cols_kernel, ctx->device, b->smem_strip,
+                         &g_smem_scols[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
+  }
+  if (b->nrows_l) {
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_prep2d_rows_long_kernel, ctx->device,
+                                    b->smem_rows, &g_smem_rows[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
+  }
   if (b->ntiles) {
     fsm_status ss = ensure_dyn_smem((const void*)fsm_stream2d_kernel, ctx->device, b->smem2,
                                     &g_smem2[ctx->device & 63]);
@@ -566,8 +589,12 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
     cudaEventRecord(ts.ev[0], s);
   }
   FSM_CUDA_TRY(cudaMemsetAsync(b->d_ctr, 0, sizeof(Counters), s));
-  if (b->nlines) fsm_prep2d_lines_kernel<<<b->nlines, 128, 0, s>>>(b->d_ev2, b->d_lines);
-  if (b->npacks) fsm_prep2d_pack_kernel<<<b->npacks, 128, 0, s>>>(b->d_ev2, b->d_packs);
+  if (b->nrows) fsm_prep2d_rows_kernel<<<b->nrows, kPrepThreads, b->smem_strip, s>>>(b->d_ev2, b->d_rows);
+  if (b->nrows_l)
+    fsm_prep2d_rows_long_kernel<<<b->nrows_l, kPrepRows * 32, b->smem_rows, s>>>(
+        b->d_ev2, b->d_rows_l, b->ny_cap2);
+  if (b->ncols) fsm_prep2d_cols_kernel<<<b->ncols, kPrepThreads, b->smem_strip, s>>>(b->d_ev2, b->d_cols);
+  if (b->ncols_l) fsm_prep2d_cols_long_kernel<<<b->ncols_l, 128, 0, s>>>(b->d_ev2, b->d_cols_l);
   if (b->nprep3) fsm_prep3d_kernel<<<b->nprep3, 256, 0, s>>>(b->d_ev3, b->d_prep3);
   if (timing) cudaEventRecord(ts.ev[1], s);
   if (b->ntiles)
@@ -662,6 +689,16 @@ cudaStream_t pick_stream(fsm_ctx* ctx, void* stream) {
 }  // namespace
 
 // ====================================================================== C ABI
+extern "C" fsm_status fsm_device_count(int* n) {
+  if (!n) return FSM_ERR_INVALID_ARG;
+  *n = 0;
+  if (cudaGetDeviceCount(n) != cudaSuccess) {
+    cudaGetLastError();
+    *n = 0;
+  }
+  return FSM_OK;
+}
+
 extern "C" fsm_status fsm_ctx_create(fsm_ctx** out, const fsm_ctx_opts* opts) {
   if (!out) return FSM_ERR_INVALID_ARG;
   *out = nullptr;

@@ -78,6 +78,7 @@ SIGNATURES = {
     "fsm_params_read_file": (_ST, [ctypes.c_char_p, ctypes.POINTER(Params)]),
     "fsm_params_derive": (None, [ctypes.POINTER(Params)]),
     "fsm_ctx_create": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(CtxOpts)]),
+    "fsm_device_count": (_ST, [ctypes.POINTER(ctypes.c_int)]),
     "fsm_ctx_destroy": (None, [_VP]),
     "fsm_ctx_timing": (_ST, [_VP, ctypes.POINTER(Timing), ctypes.c_int]),
     "fsm_run_event": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP, ctypes.POINTER(Outputs),
@@ -101,6 +102,8 @@ SIGNATURES = {
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
+    "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
+                              ctypes.c_int]),
 }
 
 _lib = None
@@ -309,3 +312,19 @@ class Batch:
         self.check_errors()  # synchronises
         o = outs.numpy()
         return [{k: v.copy() for k, v in self.unpack_outputs(o, ev).items()} for ev in range(self.n)]
+
+
+def write_field(path, var, params, projection=False, nthreads=0):
+    """One per-cell field in the reference's text format (src/FileIO.cpp:11-131)."""
+    v = np.ascontiguousarray(var, dtype=np.float32)
+    if v.size != params.DIM_X * params.DIM_Y * params.DIM_ETA:
+        raise ValueError("field size does not match the grid")
+    check(lib().fsm_write_field(str(path).encode(), v.ctypes.data, ctypes.byref(params),
+                                int(bool(projection)), int(nthreads)), "fsm_write_field")
+
+
+def device_count():
+    """Visible CUDA devices (0 without a GPU or driver)."""
+    n = ctypes.c_int(0)
+    check(lib().fsm_device_count(ctypes.byref(n)), "fsm_device_count")
+    return n.value

@@ -102,6 +102,9 @@ typedef struct fsm_ctx_opts {
 } fsm_ctx_opts;
 
 fsm_status fsm_ctx_create(fsm_ctx** ctx, const fsm_ctx_opts* opts /* NULL = defaults */);
+/* Number of visible CUDA devices (0 when there is none or no driver); no
+ * counterpart in the reference, which has no device. */
+fsm_status fsm_device_count(int* n);
 void fsm_ctx_destroy(fsm_ctx* ctx);
 
 /* Accumulated device time per kernel family since the last reset, measured
@@ -205,6 +208,17 @@ double fsm_batch_samples(fsm_batch* b);
  * one stream or serialise them. */
 fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
                                     const fsm_outputs* dev_out, void* stream);
+
+/* ------------------------------------------------------------- text output */
+/* One per-cell field in the reference's text formats (src/FileIO.cpp:11-131,
+ * replacing writeScalarToFile / writeVectorToFile for one component when
+ * projection = 0: "x y eta value" per cell with coordinates rounded to the
+ * spacing; writeScalarToFileProjection / writeVectorToFileProjection when
+ * projection = 1: the eta-centre slice, rows = y, columns = x).  Formatted by
+ * nthreads host threads (0 = all hardware threads).  Unlike the reference,
+ * which fails silently, an unwritable path returns FSM_ERR_FILE. */
+fsm_status fsm_write_field(const char* path, const float* var, const fsm_params* p, int projection,
+                           int nthreads);
 
 /* ------------------------------------------------------------ diagnostics */
 /* Measured FP32 FMA throughput of `device` in TFLOP/s (a short FMA-chain

@@ -54,6 +54,23 @@ def test_gpu_lumpy_full_grid(ctx):
     print("lumpy2d vs float", errs, "vs FP64", errs64)
 
 
+@pytest.mark.parametrize("nx,ny", [(41, 833), (829, 37)])
+def test_gpu_long_lines(ctx, nx, ny):
+    """Grids with a line longer than the strip kernels stage: the long-line
+    spline kernels (both orientations) against the oracle."""
+    p, e, _ = W.lumpy2d(seed=7, side=41, dx=0.08, nphip=64, dtau=0.6, eos=1, radius=1.2)
+    p.DIM_X, p.DIM_Y = nx, ny
+    F.lib().fsm_params_derive(p)
+    rng = np.random.default_rng(8)
+    x, y = W.axis(nx, p.DX), W.axis(ny, p.DY)
+    e = W.hotspots(rng, x, y, radius=1.2).astype(np.float32).ravel()
+    got = ctx.run_event(p, e)
+    ref = _oracle(p, e)
+    ref64 = _oracle(p, e, fp64=2)
+    compare_parity(got, ref, ref64, ref["tau"])
+    compare(got, ref64, ref["tau"])
+
+
 def test_gpu_3d_baryon_reduced(ctx):
     """3D + baryon path on a reduced grid the oracle runs in seconds."""
     p, e, nB = W.baryon3d(seed=5, side=41, neta=21, nrap=21, nphip=40)
