@@ -35,6 +35,10 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
+# DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.6 MB read +
+# 163.8 MB written) / 713.26 M samples in one ncu capture of the 128-event
+# batch (profiles/kernels_2d_uneven128_full.md)
+TRAFFIC_BYTES_PER_SAMPLE_2D = (88.596736e6 + 163.761152e6) / 713258674
 WORKLOAD = ("uneven_batch: 512 seeded lumpy 2D events, side {101,151,201,261,301}, DX U[0.05,0.1], "
             "DIM_PHIP {64,100,200} + arc-length rule, DTAU U[0.3,1.5], EOS 1/2 50:50, TAU0 0.2")
 
@@ -308,7 +312,11 @@ def main():
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "measured FP32 FMA probe on this GPU (fsm_probe_fp32_tflops)",
                          "flops_per_sample": FLOPS_PER_SAMPLE_2D, "samples_per_launch": samples,
-                         "launch_ms": stream_ms, "traffic": None},
+                         "launch_ms": stream_ms,
+                         "traffic": TRAFFIC_BYTES_PER_SAMPLE_2D * samples,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                           "128-event launch, scaled by samples "
+                                           "(profiles/kernels_2d_uneven128_full.md)"},
             "kernel_ms_per_step": {"prep": tm["prep_ms"] / args.steps,
                                    "stream": tm["stream_ms"] / args.steps,
                                    "landau": tm["landau_ms"] / args.steps},

@@ -124,6 +124,20 @@ FSM_HD R rayleigh(const R M[N][N], const R g[N], const R u[N]) {
   return num / den;
 }
 
+// Rayleigh quotient of a vector already normalised to u.g.u = 1.
+template <typename R, int N>
+FSM_HD R rayleigh_unit(const R M[N][N], const R g[N], const R u[N]) {
+  R num = 0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    R mu = 0;
+#pragma unroll
+    for (int c = 0; c < N; ++c) mu += M[r][c] * u[c];
+    num += g[r] * u[r] * mu;
+  }
+  return num;
+}
+
 // One Rayleigh-quotient-iteration step: u <- (M - e)^-1 u, normalised to
 // u.g.u = 1 with u^tau > 0, and e <- its Rayleigh quotient.  False when the
 // step leaves the light cone or is not finite.
@@ -143,7 +157,7 @@ FSM_HD bool rqi_step(const R M[N][N], const R g[N], R u[N], R& e) {
   if (y[0] < 0) t = -t;
 #pragma unroll
   for (int r = 0; r < N; ++r) u[r] = y[r] * t;
-  e = rayleigh<R, N>(M, g, u);
+  e = rayleigh_unit<R, N>(M, g, u);
   return true;
 }
 
@@ -170,8 +184,8 @@ FSM_HD void eigen_residual(const double M[N][N], const double u[N], double e, do
 
 // Timelike eigenpair of M (N = 3 for boost-invariant 2D events, whose eta row
 // and column vanish identically; N = 4 in 3D).  Returns 1 and (e, u) with
-// u.g.u = 1, u^tau > 0 when an acceptable pair was found.  Three FP32 RQI
-// steps from the energy-flux direction bring u to single precision (RQI
+// u.g.u = 1, u^tau > 0 when an acceptable pair was found.  Two FP32 RQI
+// steps from the energy-flux direction bring u close to single precision (RQI
 // converges cubically); FP64 steps then run until the eigen-residual is at
 // rounding level, normally after one.
 template <int N>
@@ -197,7 +211,7 @@ FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, 
       float keep[N];
 #pragma unroll
       for (int r = 0; r < N; ++r) keep[r] = uf[r];
-      for (int it = 0; it < 3; ++it) {
+      for (int it = 0; it < 2; ++it) {
         if (!rqi_step<float, N>(Mf, gf, uf, ef) || !isfinite(ef)) {
 #pragma unroll
           for (int r = 0; r < N; ++r) uf[r] = keep[r];
@@ -244,11 +258,12 @@ FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, 
 FSM_HD int reference_normalise(const double w[4], float TAU, double u[4]) {
   const double n = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
   if (!(n > 0.0)) return 0;
-  const double v0 = w[0] / n, v1 = w[1] / n, v2 = w[2] / n, v3 = w[3] / n;
+  const double in = 1.0 / n;
+  const double v0 = w[0] * in, v1 = w[1] * in, v2 = w[2] * in, v3 = w[3] * in;
   const float tt = TAU * TAU;  // float product, as the reference
   if (!((2.0 * v0 * v0 - 1.0 - (v3 * v3 * (tt - 1.0))) > 0)) return 0;
   const double mink = v0 * v0 - (v1 * v1 + v2 * v2 + tt * v3 * v3);
-  double factor = 1.0 / sqrt(mink);
+  double factor = fsm_rsqrt(mink);
   if (v0 < 0) factor = -factor;
   if (!((v0 * factor) < 100.0)) return 0;
   u[0] = v0 * factor;

@@ -21,6 +21,7 @@
 #include "../../include/fsm.h"
 #include "fsm_internal.h"
 #include "fsm_plan.h"
+#include "fsm_runtime.h"
 
 namespace fsm {
 __global__ void fsm_prep2d_rows_kernel(const Ev2D*, const LineBlock*);
@@ -35,84 +36,10 @@ __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 
 using namespace fsm;
 
-#define FSM_CUDA_TRY(call)                                                        \
-  do {                                                                            \
-    cudaError_t e_ = (call);                                                      \
-    if (e_ != cudaSuccess) {                                                      \
-      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
-      return (e_ == cudaErrorMemoryAllocation) ? FSM_ERR_OUT_OF_MEMORY : FSM_ERR_CUDA; \
-    }                                                                             \
-  } while (0)
+using namespace fsm::rt;
 
-namespace {
-
-constexpr size_t kAlign = 256;
-inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
-
-struct TimingSet {
-  cudaEvent_t ev[4];
-  double samples;
-};
-
-}  // namespace
-
-struct fsm_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool timing = false;
-  int num_sms = 0;
-  int smem_optin = 0;
-  fsm_timing acc{};
-  std::vector<TimingSet> pending;
-  std::vector<cudaEvent_t> event_pool;
-  std::mutex mu;
-  // cached one-event batches
-  fsm_batch* single_host = nullptr;
-  fsm_batch* single_dev = nullptr;
-};
-
-struct fsm_batch {
-  fsm_ctx* ctx = nullptr;
-  std::vector<EventPlan> plans;
-  bool own_io = true;
-  // device allocation
-  char* d_mem = nullptr;
-  size_t bytes = 0;
-  // staging for descriptor uploads (pinned)
-  char* h_stage = nullptr;
-  size_t stage_bytes = 0;
-  size_t desc_off = 0, desc_bytes = 0;
-  // per-event device views
-  std::vector<float*> d_in_e, d_in_nB;
-  std::vector<fsm_outputs> d_out;
-  std::vector<size_t> in_off, out_off;  // element offsets inside the slabs
-  size_t in_slab_off = 0, in_slab_bytes = 0, out_slab_off = 0, out_slab_bytes = 0;
-  std::vector<float*> d_T, d_J;         // moment buffers the Landau kernel reads
-  // host copies of descriptors
-  std::vector<Ev2D> ev2;
-  std::vector<Ev3D> ev3;
-  std::vector<EvLandau> evl;
-  std::vector<int> ev2_of, ev3_of;      // event -> index in ev2/ev3 (or -1)
-  // device descriptor arrays and work lists
-  Ev2D* d_ev2 = nullptr;
-  Ev3D* d_ev3 = nullptr;
-  EvLandau* d_evl = nullptr;
-  Tile2D* d_tiles = nullptr;
-  LineBlock *d_rows = nullptr, *d_cols = nullptr, *d_rows_l = nullptr, *d_cols_l = nullptr;
-  CellBlock *d_prep3 = nullptr, *d_b3 = nullptr, *d_bl = nullptr;
-  Counters* d_ctr = nullptr;
-  int* d_err = nullptr;
-  int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, nb3 = 0, nbl = 0;
-  int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
-  size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
-  int grid2 = 0, grid3 = 0;
-  double samples = 0;
-  cudaGraphExec_t graph = nullptr;
-  cudaStream_t graph_stream = nullptr;
-  cudaStream_t last_stream = nullptr;  // stream of the most recent upload/launch/download
-};
-
-namespace {
+namespace fsm {
+namespace rt {
 
 struct Layout {
   size_t off = 0;
@@ -135,8 +62,10 @@ bool has_device() {
 void batch_free(fsm_batch* b) {
   if (!b) return;
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->d_mem) cudaFree(b->d_mem);
-  if (b->h_stage) cudaFreeHost(b->h_stage);
+  if (!b->ext_mem) {
+    if (b->d_mem) cudaFree(b->d_mem);
+    if (b->h_stage) cudaFreeHost(b->h_stage);
+  }
   delete b;
 }
 
@@ -160,7 +89,7 @@ int g_smem2[64] = {0}, g_smem3[64] = {0}, g_smem_rows[64] = {0}, g_smem_srows[64
 // select external device buffers instead of owned slabs.
 fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
                        const float* const* ext_in_e, const float* const* ext_in_nB,
-                       const fsm_outputs* ext_out, fsm_batch** out) {
+                       const fsm_outputs* ext_out, fsm_batch** out, const BatchMem* mem) {
   if (n <= 0 || !params) return FSM_ERR_INVALID_ARG;
   std::unique_ptr<fsm_batch, void (*)(fsm_batch*)> b(new fsm_batch(), batch_free);
   b->ctx = ctx;
@@ -311,16 +240,26 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     b->out_slab_bytes = out_elems * 4;
   }
   b->bytes = L.off;
-  cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
-  if (ce != cudaSuccess) {
-    cudaGetLastError();
-    set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
-                   cudaGetErrorString(ce));
-    return FSM_ERR_OUT_OF_MEMORY;
+  b->stage_bytes = upload_bytes;
+  if (mem) {
+    b->ext_mem = true;
+    b->d_mem = mem->dev(mem->user, b->bytes);
+    b->h_stage = b->d_mem ? mem->host(mem->user, b->stage_bytes) : nullptr;
+    if (!b->d_mem || !b->h_stage) {
+      set_last_error("batch memory pool exhausted");
+      return FSM_ERR_OUT_OF_MEMORY;
+    }
+  } else {
+    cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
+    if (ce != cudaSuccess) {
+      cudaGetLastError();
+      set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
+                     cudaGetErrorString(ce));
+      return FSM_ERR_OUT_OF_MEMORY;
+    }
+    FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
   }
   char* D = b->d_mem;
-  b->stage_bytes = upload_bytes;
-  FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
   char* H = b->h_stage;
   std::memset(H, 0, upload_bytes);
   b->desc_off = o_ev2;
@@ -529,7 +468,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->nprep3 = (int)prep3.size();
   b->nb3 = (int)b3.size();
   b->nbl = (int)bl.size();
-  FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
+  if (mem)
+    FSM_CUDA_TRY(cudaMemcpyAsync(D, H, upload_bytes, cudaMemcpyHostToDevice, mem->stream));
+  else
+    FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
   // ---- launch geometry
   if (b->nrows) {
     fsm_status ss = ensure_dyn_smem((const void*)fsm_prep2d_rows_kernel, ctx->device, b->smem_strip,
@@ -562,7 +504,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                                                                b->smem3));
     b->grid3 = std::max(1, std::min(b->nb3, ctx->num_sms * std::max(occ, 1)));
   }
-  FSM_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int) * 4));
+  if (mem)
+    FSM_CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int) * 4, mem->stream));
+  else
+    FSM_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int) * 4));
   *out = b.release();
   return FSM_OK;
 }
@@ -686,7 +631,8 @@ cudaStream_t pick_stream(fsm_ctx* ctx, void* stream) {
   return stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
 }
 
-}  // namespace
+}  // namespace rt
+}  // namespace fsm
 
 // ====================================================================== C ABI
 extern "C" fsm_status fsm_device_count(int* n) {

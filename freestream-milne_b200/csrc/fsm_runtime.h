@@ -1,0 +1,128 @@
+// fsm_runtime.h -- internal: context and batch objects and the batch
+// build/launch functions shared by the C ABI (fsm_runtime.cu) and the request
+// server (fsm_server.cu).  Not installed; the public interface is fsm.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fsm.h"
+#include "fsm_internal.h"
+#include "fsm_plan.h"
+
+#define FSM_CUDA_TRY(call)                                                        \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+      return (e_ == cudaErrorMemoryAllocation) ? FSM_ERR_OUT_OF_MEMORY : FSM_ERR_CUDA; \
+    }                                                                             \
+  } while (0)
+
+namespace fsm {
+namespace rt {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+struct TimingSet {
+  cudaEvent_t ev[4];
+  double samples;
+};
+
+}  // namespace rt
+}  // namespace fsm
+
+using fsm::CellBlock;
+using fsm::Counters;
+using fsm::Ev2D;
+using fsm::Ev3D;
+using fsm::EvLandau;
+using fsm::EventPlan;
+using fsm::LineBlock;
+using fsm::Tile2D;
+
+struct fsm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool timing = false;
+  int num_sms = 0;
+  int smem_optin = 0;
+  fsm_timing acc{};
+  std::vector<fsm::rt::TimingSet> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::mutex mu;
+  // cached one-event batches
+  fsm_batch* single_host = nullptr;
+  fsm_batch* single_dev = nullptr;
+};
+
+struct fsm_batch {
+  fsm_ctx* ctx = nullptr;
+  std::vector<EventPlan> plans;
+  bool own_io = true;
+  bool ext_mem = false;  // d_mem / h_stage belong to the caller (BatchMem)
+  // device allocation
+  char* d_mem = nullptr;
+  size_t bytes = 0;
+  // staging for descriptor uploads (pinned)
+  char* h_stage = nullptr;
+  size_t stage_bytes = 0;
+  size_t desc_off = 0, desc_bytes = 0;
+  // per-event device views
+  std::vector<float*> d_in_e, d_in_nB;
+  std::vector<fsm_outputs> d_out;
+  std::vector<size_t> in_off, out_off;  // element offsets inside the slabs
+  size_t in_slab_off = 0, in_slab_bytes = 0, out_slab_off = 0, out_slab_bytes = 0;
+  std::vector<float*> d_T, d_J;         // moment buffers the Landau kernel reads
+  // host copies of descriptors
+  std::vector<Ev2D> ev2;
+  std::vector<Ev3D> ev3;
+  std::vector<EvLandau> evl;
+  std::vector<int> ev2_of, ev3_of;      // event -> index in ev2/ev3 (or -1)
+  // device descriptor arrays and work lists
+  Ev2D* d_ev2 = nullptr;
+  Ev3D* d_ev3 = nullptr;
+  EvLandau* d_evl = nullptr;
+  Tile2D* d_tiles = nullptr;
+  LineBlock *d_rows = nullptr, *d_cols = nullptr, *d_rows_l = nullptr, *d_cols_l = nullptr;
+  CellBlock *d_prep3 = nullptr, *d_b3 = nullptr, *d_bl = nullptr;
+  Counters* d_ctr = nullptr;
+  int* d_err = nullptr;
+  int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, nb3 = 0, nbl = 0;
+  int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
+  size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
+  int grid2 = 0, grid3 = 0;
+  double samples = 0;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  cudaStream_t last_stream = nullptr;  // stream of the most recent upload/launch/download
+};
+
+namespace fsm {
+namespace rt {
+
+// Memory for a batch supplied by its owner instead of cudaMalloc /
+// cudaMallocHost (the server's pools).  dev/host return at least `bytes`
+// (256-byte aligned) or nullptr when the pool is exhausted; the descriptor
+// upload is then enqueued on `stream` instead of copied synchronously.
+struct BatchMem {
+  void* user = nullptr;
+  char* (*dev)(void* user, size_t bytes) = nullptr;
+  char* (*host)(void* user, size_t bytes) = nullptr;
+  cudaStream_t stream = nullptr;
+};
+
+bool has_device();
+void batch_free(fsm_batch* b);
+fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
+                       const float* const* ext_in_e, const float* const* ext_in_nB,
+                       const fsm_outputs* ext_out, fsm_batch** out, const BatchMem* mem = nullptr);
+fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing);
+fsm_status check_kernel_errors(fsm_batch* b);
+fsm_status fill_info(const EventPlan& P, fsm_run_info* info);
+
+}  // namespace rt
+}  // namespace fsm

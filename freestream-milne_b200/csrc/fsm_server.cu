@@ -1,0 +1,555 @@
+// fsm_server.cu -- continuous-batching request server (no counterpart in the
+// reference, which computes one event per call).
+//
+// Requests (one event each, host buffers copied in at submit) wait in a FIFO.
+// A scheduler thread forms launch waves from the head of the queue whenever one
+// of the server's streams is idle and the device / pinned-host budgets have
+// room, so requests that arrive while others run join the next wave; waves on
+// different streams overlap on the device (one wave's copies with another's
+// kernels).  Each wave is an ordinary batch (fsm_runtime) whose memory comes
+// from the server's pools: one device allocation of hbm_budget_bytes and one
+// pinned host allocation of host_budget_bytes, carved by a first-fit
+// allocator, so admitting a wave calls no allocator of the CUDA runtime.  A
+// host callback at the end of each wave's stream work timestamps its
+// completion; latency is submit -> outputs in host memory.
+//
+// Every cell's result depends only on its own event, so a request's outputs
+// are the same alone and in any mix of requests (tests/test_server.py).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "fsm_runtime.h"
+
+using namespace fsm;
+using namespace fsm::rt;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// First-fit allocator over one region, 256-byte granules, coalescing frees.
+class Pool {
+ public:
+  void reset(char* base, size_t size) {
+    base_ = base;
+    size_ = size;
+    free_.clear();
+    if (size) free_[0] = size;
+  }
+  char* alloc(size_t n) {
+    n = align_up(std::max<size_t>(n, 1));
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        const size_t off = it->first, len = it->second;
+        free_.erase(it);
+        if (len > n) free_[off + n] = len - n;
+        used_ += n;
+        return base_ + off;
+      }
+    }
+    return nullptr;
+  }
+  void release(char* p, size_t n) {
+    if (!p) return;
+    n = align_up(std::max<size_t>(n, 1));
+    size_t off = (size_t)(p - base_);
+    used_ -= n;
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + n == next->first) {
+      n += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += n;
+        return;
+      }
+    }
+    free_[off] = n;
+  }
+
+ private:
+  char* base_ = nullptr;
+  size_t size_ = 0, used_ = 0;
+  std::map<size_t, size_t> free_;
+};
+
+// Pinned output slab of a retired wave, shared by its requests until each has
+// been polled (the poller copies straight from it).
+struct OutBlock {
+  char* p = nullptr;
+  size_t bytes = 0;
+  int refs = 0;
+};
+
+struct Request {
+  long long id = 0;
+  fsm_params p{};
+  std::vector<float> e, nB;
+  Clock::time_point t_submit, t_done;
+  bool done = false;
+  fsm_status status = FSM_OK;
+  std::string msg;  // error message of a failed request
+  OutBlock* ob = nullptr;   // holds the event's outputs once done
+  const float* out = nullptr;  // T(10) e P Pi u(4) pi(10) [J(4) nB V(4)], component-major
+  fsm_run_info info{};
+  size_t dim = 0;
+  bool baryon = false;
+};
+
+struct Wave {
+  std::vector<Request*> reqs;
+  fsm_batch* b = nullptr;
+  int slot = 0;
+  // pool regions: the batch's own device and staging blocks, plus the host
+  // input and output slabs (+ 16 bytes of kernel error words after the outputs)
+  char *d = nullptr, *hs = nullptr, *hin = nullptr, *hout = nullptr;
+  size_t dbytes = 0, hsbytes = 0, hinbytes = 0, houtbytes = 0;
+  bool done = false;
+  Clock::time_point t_done;
+};
+
+}  // namespace
+
+struct fsm_server {
+  fsm_server_opts opts{};
+  fsm_ctx* ctx = nullptr;
+  char* d_pool = nullptr;
+  char* h_pool = nullptr;
+  Pool dpool, hpool;
+  std::vector<cudaStream_t> streams;
+  std::vector<Wave*> slot_wave;  // wave in flight per stream, or nullptr
+  std::mutex mu;
+  std::condition_variable cv;       // scheduler wake-ups
+  std::condition_variable cv_done;  // pollers
+  std::deque<Request*> queue;
+  std::unordered_map<long long, Request*> reqs;
+  long long next_id = 1;
+  bool stopping = false;
+  std::thread th;
+  // statistics
+  long long submitted = 0, completed = 0, failed = 0, waves = 0;
+  std::vector<double> lat_ms;
+  Clock::time_point t_first{}, t_last{};
+  bool have_first = false;
+};
+
+namespace {
+
+char* pool_dev(void* u, size_t n) {
+  auto* W = static_cast<std::pair<fsm_server*, Wave*>*>(u);
+  std::lock_guard<std::mutex> g(W->first->mu);
+  char* p = W->first->dpool.alloc(n);
+  if (p) {
+    W->second->d = p;
+    W->second->dbytes = n;
+  }
+  return p;
+}
+char* pool_host(void* u, size_t n) {
+  auto* W = static_cast<std::pair<fsm_server*, Wave*>*>(u);
+  std::lock_guard<std::mutex> g(W->first->mu);
+  char* p = W->first->hpool.alloc(n);
+  if (p) {
+    W->second->hs = p;
+    W->second->hsbytes = n;
+  }
+  return p;
+}
+
+void CUDART_CB wave_done_cb(void* user) {
+  auto* W = static_cast<std::pair<fsm_server*, Wave*>*>(user);
+  fsm_server* S = W->first;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    W->second->t_done = Clock::now();
+    W->second->done = true;
+  }
+  S->cv.notify_all();
+  delete W;
+}
+
+// Releases a wave's pool regions and batch (mu held); the output slab only
+// when keep_out is false.
+void wave_release(fsm_server* S, Wave* w, bool keep_out = false) {
+  if (w->b) batch_free(w->b);
+  S->dpool.release(w->d, w->dbytes);
+  S->hpool.release(w->hs, w->hsbytes);
+  S->hpool.release(w->hin, w->hinbytes);
+  if (!keep_out) S->hpool.release(w->hout, w->houtbytes);
+  w->b = nullptr;
+  w->d = w->hs = w->hin = w->hout = nullptr;
+}
+
+void drop_output(fsm_server* S, Request* r) {
+  if (r->ob && --r->ob->refs == 0) {
+    S->hpool.release(r->ob->p, r->ob->bytes);
+    delete r->ob;
+  }
+  r->ob = nullptr;
+  r->out = nullptr;
+}
+
+void finish_request(fsm_server* S, Request* r, fsm_status st, Clock::time_point t) {
+  r->status = st;
+  r->done = true;
+  r->t_done = t;
+  if (st == FSM_OK) {
+    ++S->completed;
+    S->lat_ms.push_back(std::chrono::duration<double, std::milli>(t - r->t_submit).count());
+    S->t_last = std::max(S->t_last, t);
+  } else {
+    ++S->failed;
+    r->msg = fsm_last_error();
+  }
+}
+
+// Outputs of a completed wave into its requests (mu held).
+void wave_retire(fsm_server* S, Wave* w) {
+  const int* err = reinterpret_cast<const int*>(w->hout + w->b->out_slab_bytes);
+  fsm_status st = FSM_OK;
+  if (err[1] != 0) st = FSM_ERR_TIMEOUT;
+  else if (err[0] != 0) st = FSM_ERR_CUDA;
+  if (st != FSM_OK) set_last_error("server wave: kernel error words set");
+  const float* out = reinterpret_cast<const float*>(w->hout);
+  auto* ob = new OutBlock{w->hout, w->houtbytes, (int)w->reqs.size()};
+  for (size_t i = 0; i < w->reqs.size(); ++i) {
+    Request* r = w->reqs[i];
+    const EventPlan& P = w->b->plans[i];
+    r->dim = (size_t)P.DIM;
+    r->baryon = P.baryon;
+    r->ob = ob;
+    r->out = out + w->b->out_off[i];
+    fill_info(P, &r->info);
+    finish_request(S, r, st, w->t_done);
+  }
+  wave_release(S, w, /*keep_out=*/true);
+  S->cv_done.notify_all();
+}
+
+// Builds and enqueues one wave from the head of the queue on stream `slot`
+// (mu held on entry and exit; released while planning).  Returns false when
+// nothing could be admitted for lack of memory.
+bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
+  const int cap = S->opts.max_wave_events;
+  std::vector<Request*> take;
+  while (!S->queue.empty() && (int)take.size() < cap) {
+    take.push_back(S->queue.front());
+    S->queue.pop_front();
+  }
+  cudaStream_t s = S->streams[slot];
+  while (!take.empty()) {
+    auto* w = new Wave();
+    w->slot = slot;
+    w->reqs = take;
+    std::vector<fsm_params> ps(take.size());
+    std::vector<const float*> he(take.size());
+    for (size_t i = 0; i < take.size(); ++i) {
+      ps[i] = take[i]->p;
+      he[i] = take[i]->e.data();
+    }
+    auto* user = new std::pair<fsm_server*, Wave*>(S, w);
+    BatchMem mem;
+    mem.user = user;
+    mem.dev = pool_dev;
+    mem.host = pool_host;
+    mem.stream = s;
+    fsm_batch* b = nullptr;
+    // planning runs without the lock; the pools are only touched by this thread
+    lk.unlock();
+    fsm_status st = batch_build(S->ctx, (int)take.size(), ps.data(), he.data(), nullptr, nullptr,
+                                nullptr, &b, &mem);
+    lk.lock();
+    if (st == FSM_OK) {
+      w->b = b;
+      w->hinbytes = b->in_slab_bytes;
+      w->houtbytes = b->out_slab_bytes + 16;
+      w->hin = S->hpool.alloc(w->hinbytes);
+      w->hout = w->hin ? S->hpool.alloc(w->houtbytes) : nullptr;
+      if (!w->hin || !w->hout) st = FSM_ERR_OUT_OF_MEMORY;
+    }
+    if (st == FSM_OK) {
+      // inputs into the pinned slab, then the stream work of the wave
+      for (size_t i = 0; i < take.size(); ++i) {
+        float* dst = reinterpret_cast<float*>(w->hin) + b->in_off[i];
+        const size_t n = take[i]->e.size();
+        std::memcpy(dst, take[i]->e.data(), n * 4);
+        if (b->plans[i].baryon) std::memcpy(dst + n, take[i]->nB.data(), n * 4);
+      }
+      cudaError_t ce = cudaMemcpyAsync(b->d_mem + b->in_slab_off, w->hin, b->in_slab_bytes,
+                                       cudaMemcpyHostToDevice, s);
+      if (ce == cudaSuccess) st = enqueue(b, s, false);
+      else st = FSM_ERR_CUDA;
+      if (st == FSM_OK) {
+        ce = cudaMemcpyAsync(w->hout, b->d_mem + b->out_slab_off, b->out_slab_bytes,
+                             cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess)
+          ce = cudaMemcpyAsync(w->hout + b->out_slab_bytes, b->d_err, 16, cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaLaunchHostFunc(s, wave_done_cb, user);
+        if (ce != cudaSuccess) {
+          set_last_error(std::string("server wave: ") + cudaGetErrorString(ce));
+          st = FSM_ERR_CUDA;
+        }
+      }
+      if (st != FSM_OK) {
+        // the stream may still be using the regions: wait before releasing them
+        lk.unlock();
+        cudaStreamSynchronize(s);
+        lk.lock();
+        wave_release(S, w);
+        for (Request* r : take) finish_request(S, r, st, Clock::now());
+        delete w;
+        delete user;
+        S->cv_done.notify_all();
+        return true;
+      }
+      ++S->waves;
+      S->slot_wave[slot] = w;
+      return true;
+    }
+    // planning error of some event, or the pools are full
+    wave_release(S, w);
+    delete w;
+    delete user;
+    if (st == FSM_ERR_OUT_OF_MEMORY) {
+      bool busy = false;
+      for (Wave* x : S->slot_wave) busy = busy || (x != nullptr);
+      if (take.size() > 1) {  // retry with the first half, requeue the rest in order
+        const size_t h = take.size() / 2;
+        for (size_t i = take.size(); i-- > h;) S->queue.push_front(take[i]);
+        take.resize(h);
+        continue;
+      }
+      if (busy) {  // wait for memory to come back
+        S->queue.push_front(take[0]);
+        return false;
+      }
+      set_last_error("request does not fit the server's memory budgets");
+      finish_request(S, take[0], FSM_ERR_TOO_LARGE, Clock::now());
+      S->cv_done.notify_all();
+      return true;
+    }
+    // invalid parameters: fail the requests one by one so that one bad event
+    // does not fail its neighbours
+    if (take.size() > 1) {
+      for (size_t i = take.size(); i-- > 1;) S->queue.push_front(take[i]);
+      take.resize(1);
+      continue;
+    }
+    finish_request(S, take[0], st, Clock::now());
+    S->cv_done.notify_all();
+    return true;
+  }
+  return true;
+}
+
+void scheduler(fsm_server* S) {
+  cudaSetDevice(S->ctx->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  bool mem_wait = false;
+  for (;;) {
+    // retire completed waves
+    for (size_t k = 0; k < S->slot_wave.size(); ++k) {
+      Wave* w = S->slot_wave[k];
+      if (w && w->done) {
+        wave_retire(S, w);
+        delete w;
+        S->slot_wave[k] = nullptr;
+        mem_wait = false;
+      }
+    }
+    bool inflight = false;
+    for (Wave* x : S->slot_wave) inflight = inflight || (x != nullptr);
+    if (S->stopping && S->queue.empty() && !inflight) break;
+    // admit
+    bool launched = false;
+    if (!mem_wait) {
+      for (size_t k = 0; k < S->slot_wave.size() && !S->queue.empty(); ++k) {
+        if (S->slot_wave[k]) continue;
+        if (!wave_launch(S, lk, (int)k)) {
+          mem_wait = true;
+          break;
+        }
+        launched = true;
+      }
+    }
+    if (launched) continue;
+    S->cv.wait(lk);
+  }
+}
+
+}  // namespace
+
+extern "C" fsm_status fsm_server_start(fsm_server** out, const fsm_server_opts* opts) {
+  if (!out) return FSM_ERR_INVALID_ARG;
+  *out = nullptr;
+  std::unique_ptr<fsm_server> S(new fsm_server());
+  if (opts) S->opts = *opts;
+  if (S->opts.hbm_budget_bytes == 0) S->opts.hbm_budget_bytes = (size_t)8 << 30;
+  if (S->opts.host_budget_bytes == 0) S->opts.host_budget_bytes = (size_t)2 << 30;
+  if (S->opts.max_wave_events <= 0) S->opts.max_wave_events = 512;
+  if (S->opts.streams <= 0) S->opts.streams = 2;
+  fsm_ctx_opts co{S->opts.device, 0};
+  fsm_status st = fsm_ctx_create(&S->ctx, &co);
+  if (st != FSM_OK) return st;
+  cudaError_t ce = cudaMalloc(&S->d_pool, S->opts.hbm_budget_bytes);
+  if (ce == cudaSuccess) ce = cudaHostAlloc(&S->h_pool, S->opts.host_budget_bytes, cudaHostAllocDefault);
+  if (ce != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("server pools: ") + cudaGetErrorString(ce));
+    if (S->d_pool) cudaFree(S->d_pool);
+    fsm_ctx_destroy(S->ctx);
+    return FSM_ERR_OUT_OF_MEMORY;
+  }
+  S->dpool.reset(S->d_pool, S->opts.hbm_budget_bytes);
+  S->hpool.reset(S->h_pool, S->opts.host_budget_bytes);
+  S->streams.resize(S->opts.streams);
+  for (auto& s : S->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  S->slot_wave.assign(S->opts.streams, nullptr);
+  fsm_server* raw = S.get();
+  S->th = std::thread(scheduler, raw);
+  *out = S.release();
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_server_submit(fsm_server* S, const fsm_params* p, const float* e_gev,
+                                        const float* nB, long long* id) {
+  if (!S || !p || !e_gev || !id) return FSM_ERR_INVALID_ARG;
+  const long long dim = (long long)p->DIM_X * p->DIM_Y * p->DIM_ETA;
+  if (p->DIM_X < 1 || p->DIM_Y < 1 || p->DIM_ETA < 1 || dim > (1ll << 30)) {
+    set_last_error("fsm_server_submit: invalid grid");
+    return FSM_ERR_INVALID_ARG;
+  }
+  if (p->BARYON && !nB) {
+    set_last_error("fsm_server_submit: BARYON = 1 needs the baryon density");
+    return FSM_ERR_INVALID_ARG;
+  }
+  auto* r = new Request();
+  r->p = *p;
+  fsm_params_derive(&r->p);
+  r->e.assign(e_gev, e_gev + dim);
+  if (p->BARYON) r->nB.assign(nB, nB + dim);
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    if (S->stopping) {
+      delete r;
+      set_last_error("fsm_server_submit: server is stopping");
+      return FSM_ERR_CANCELLED;
+    }
+    r->id = S->next_id++;
+    r->t_submit = Clock::now();
+    if (!S->have_first) {
+      S->t_first = r->t_submit;
+      S->have_first = true;
+    }
+    ++S->submitted;
+    S->reqs[r->id] = r;
+    S->queue.push_back(r);
+    *id = r->id;
+  }
+  S->cv.notify_all();
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_server_poll(fsm_server* S, long long id, const fsm_outputs* host_out,
+                                      fsm_run_info* info, double timeout_ms, int* done) {
+  if (!S || !done) return FSM_ERR_INVALID_ARG;
+  *done = 0;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) {
+    set_last_error("fsm_server_poll: unknown request id");
+    return FSM_ERR_INVALID_ARG;
+  }
+  Request* r = it->second;
+  if (!r->done && timeout_ms != 0.0) {
+    auto pred = [&] { return r->done; };
+    if (timeout_ms < 0) S->cv_done.wait(lk, pred);
+    else S->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), pred);
+  }
+  if (!r->done) return FSM_OK;
+  *done = 1;
+  const fsm_status st = r->status;
+  if (st == FSM_OK && host_out) {
+    const size_t n = r->dim;
+    const float* o = r->out;
+    auto put = [&](float* dst, size_t comp0, size_t ncomp) {
+      if (dst) std::memcpy(dst, o + comp0 * n, ncomp * n * 4);
+    };
+    put(host_out->T, 0, 10);
+    put(host_out->e, 10, 1);
+    put(host_out->P, 11, 1);
+    put(host_out->Pi, 12, 1);
+    put(host_out->u, 13, 4);
+    put(host_out->pi, 17, 10);
+    if (r->baryon) {
+      put(host_out->J, 27, 4);
+      put(host_out->nB, 31, 1);
+      put(host_out->V, 32, 4);
+    }
+  }
+  if (info) *info = r->info;
+  if (st != FSM_OK) set_last_error(r->msg);
+  drop_output(S, r);
+  S->reqs.erase(it);
+  delete r;
+  return st;
+}
+
+extern "C" fsm_status fsm_server_stats_get(fsm_server* S, fsm_server_stats* st) {
+  if (!S || !st) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(S->mu);
+  *st = fsm_server_stats{};
+  st->submitted = S->submitted;
+  st->completed = S->completed;
+  st->failed = S->failed;
+  st->waves = S->waves;
+  if (!S->lat_ms.empty()) {
+    std::vector<double> v = S->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto q = [&](double f) { return v[std::min(v.size() - 1, (size_t)(f * (double)v.size()))]; };
+    st->p50_ms = q(0.50);
+    st->p99_ms = q(0.99);
+    st->max_ms = v.back();
+    const double span = std::chrono::duration<double>(S->t_last - S->t_first).count();
+    st->events_per_s = span > 0 ? (double)S->completed / span : 0.0;
+  }
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_server_stop(fsm_server* S) {
+  if (!S) return FSM_ERR_INVALID_ARG;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    S->stopping = true;
+    // queued requests are cancelled; waves in flight finish
+    for (Request* r : S->queue) finish_request(S, r, FSM_ERR_CANCELLED, Clock::now());
+    S->queue.clear();
+  }
+  S->cv.notify_all();
+  S->cv_done.notify_all();
+  if (S->th.joinable()) S->th.join();
+  for (auto& kv : S->reqs) {
+    drop_output(S, kv.second);
+    delete kv.second;
+  }
+  for (auto& s : S->streams) cudaStreamDestroy(s);
+  cudaFreeHost(S->h_pool);
+  cudaFree(S->d_pool);
+  fsm_ctx_destroy(S->ctx);
+  delete S;
+  return FSM_OK;
+}

@@ -71,6 +71,19 @@ class Timing(ctypes.Structure):
 # Every symbol include/fsm.h declares, with (restype, argtypes).
 _VP = ctypes.c_void_p
 _ST = ctypes.c_int
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("host_budget_bytes", ctypes.c_size_t), ("max_wave_events", ctypes.c_int),
+                ("streams", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("waves", ctypes.c_longlong),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("events_per_s", ctypes.c_double)]
+
+
 SIGNATURES = {
     "fsm_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "fsm_last_error": (ctypes.c_char_p, []),
@@ -104,6 +117,13 @@ SIGNATURES = {
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
     "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
                               ctypes.c_int]),
+    "fsm_server_start": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(ServerOpts)]),
+    "fsm_server_submit": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP,
+                                ctypes.POINTER(ctypes.c_longlong)]),
+    "fsm_server_poll": (_ST, [_VP, ctypes.c_longlong, ctypes.POINTER(Outputs),
+                              ctypes.POINTER(RunInfo), ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
+    "fsm_server_stats_get": (_ST, [_VP, ctypes.POINTER(ServerStats)]),
+    "fsm_server_stop": (_ST, [_VP]),
 }
 
 _lib = None
@@ -328,3 +348,64 @@ def device_count():
     n = ctypes.c_int(0)
     check(lib().fsm_device_count(ctypes.byref(n)), "fsm_device_count")
     return n.value
+
+
+class Server:
+    """Continuous-batching request server (fsm_server_*): submit events as they
+    arrive, poll for their outputs; results equal Context.run_event's."""
+
+    def __init__(self, device=0, hbm_budget=0, host_budget=0, max_wave_events=0, streams=0):
+        self.h = ctypes.c_void_p()
+        opts = ServerOpts(device, int(hbm_budget), int(host_budget), int(max_wave_events),
+                          int(streams))
+        check(lib().fsm_server_start(ctypes.byref(self.h), ctypes.byref(opts)), "fsm_server_start")
+        self._pending = {}
+
+    def submit(self, params, e_gev, nB=None):
+        e_gev = np.ascontiguousarray(e_gev, dtype=np.float32).ravel()
+        nb_ptr = None
+        if params.BARYON:
+            nB = np.ascontiguousarray(nB, dtype=np.float32).ravel()
+            nb_ptr = nB.ctypes.data
+        rid = ctypes.c_longlong()
+        check(lib().fsm_server_submit(self.h, ctypes.byref(params), e_gev.ctypes.data, nb_ptr,
+                                      ctypes.byref(rid)), "fsm_server_submit")
+        dim = params.DIM_X * params.DIM_Y * params.DIM_ETA
+        self._pending[rid.value] = (dim, bool(params.BARYON))
+        return rid.value
+
+    def poll(self, rid, timeout_ms=-1.0):
+        """None while running; the outputs dict once done (FsmError if it failed)."""
+        dim, baryon = self._pending[rid]
+        names = list(OUT_COMPS) if baryon else [k for k in OUT_COMPS if k not in ("J", "nB", "V")]
+        arrs, o = {}, Outputs()
+        for k in names:
+            a = np.zeros((OUT_COMPS[k], dim) if OUT_COMPS[k] > 1 else (dim,), dtype=np.float32)
+            arrs[k] = a
+            setattr(o, k, a.ctypes.data)
+        info, done = RunInfo(), ctypes.c_int(0)
+        st = lib().fsm_server_poll(self.h, rid, ctypes.byref(o), ctypes.byref(info),
+                                   float(timeout_ms), ctypes.byref(done))
+        if not done.value:
+            check(st, "fsm_server_poll")
+            return None
+        del self._pending[rid]
+        check(st, "fsm_server_poll")
+        arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
+        return arrs
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().fsm_server_stats_get(self.h, ctypes.byref(st)), "fsm_server_stats_get")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def stop(self):
+        if self.h:
+            check(lib().fsm_server_stop(self.h), "fsm_server_stop")
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass

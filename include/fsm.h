@@ -209,6 +209,46 @@ double fsm_batch_samples(fsm_batch* b);
 fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
                                     const fsm_outputs* dev_out, void* stream);
 
+/* ---------------------------------------------------------- request server */
+/* No counterpart in the reference, which computes one event per call.  A
+ * continuous-batching server: fsm_server_submit queues one event (host
+ * buffers, copied in); a scheduler thread admits queued requests into launch
+ * waves whenever one of its streams is idle and its device / pinned-host
+ * budgets have room, so requests arriving while others run join the next
+ * wave, and waves on different streams overlap on the device.  A request's
+ * results are identical to fsm_run_event's on the same event.  The server's
+ * functions may be called from any thread, except that fsm_server_stop must
+ * not race with the others. */
+typedef struct fsm_server fsm_server;
+
+typedef struct fsm_server_opts {
+  int device;                /* CUDA device ordinal                                 */
+  size_t hbm_budget_bytes;   /* device memory held for waves in flight (0: 8 GiB)   */
+  size_t host_budget_bytes;  /* pinned host memory for inputs/outputs (0: 2 GiB)    */
+  int max_wave_events;       /* events per launch wave (0: 512)                     */
+  int streams;               /* waves in flight (0: 2)                              */
+} fsm_server_opts;
+
+typedef struct fsm_server_stats {
+  long long submitted, completed, failed, waves;
+  double p50_ms, p99_ms, max_ms;  /* latency submit -> outputs in host memory         */
+  double events_per_s;            /* completed / (last completion - first submission) */
+} fsm_server_stats;
+
+/* Allocates both budgets up front (one device and one pinned allocation). */
+fsm_status fsm_server_start(fsm_server** s, const fsm_server_opts* opts /* NULL = defaults */);
+fsm_status fsm_server_submit(fsm_server* s, const fsm_params* p, const float* e_gev,
+                             const float* nB, long long* id);
+/* Waits up to timeout_ms (< 0: until done, 0: no wait).  done = 1: the request
+ * finished, its outputs are copied into host_out (NULL fields skipped), it is
+ * forgotten, and the return value is its own status (FSM_ERR_TOO_LARGE when it
+ * cannot fit the budgets, FSM_ERR_CANCELLED when the server stopped first). */
+fsm_status fsm_server_poll(fsm_server* s, long long id, const fsm_outputs* host_out,
+                           fsm_run_info* info, double timeout_ms, int* done);
+fsm_status fsm_server_stats_get(fsm_server* s, fsm_server_stats* st);
+/* Finishes the waves in flight, cancels queued requests, frees everything. */
+fsm_status fsm_server_stop(fsm_server* s);
+
 /* ------------------------------------------------------------- text output */
 /* One per-cell field in the reference's text formats (src/FileIO.cpp:11-131,
  * replacing writeScalarToFile / writeVectorToFile for one component when
