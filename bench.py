@@ -35,6 +35,7 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
+FLOPS_PER_SAMPLE_3D_BARYON = 75  # shift 5 + 2 trilinear x 21 + 14 moments x 2
 # DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.6 MB read +
 # 163.8 MB written) / 713.26 M samples in one ncu capture of the 128-event
 # batch (profiles/kernels_2d_uneven128_full.md)
@@ -52,6 +53,11 @@ def parse():
     ap.add_argument("--events", type=int, default=512)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-3d", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=160)
+    ap.add_argument("--serve-load", type=float, default=0.7,
+                    help="Poisson arrival rate as a fraction of the measured burst capacity")
     return ap.parse_args()
 
 
@@ -126,6 +132,109 @@ def cpu_baseline(events, nthreads, budget_s=20.0):
         os.close(saved)
     dt = time.perf_counter() - t0
     return done / dt, kind, f"first {done} events of the workload, {nthreads} OpenMP threads, {dt:.1f} s"
+
+
+def serve_stream(args, F, W, local, rank, ctx, max_over_ranks):
+    """Mixed request stream (80 % 2D of sides 101-301, 20 % 3D of 131^2 x
+    {25, 51} with 21/31/41 rapidities) through the continuous-batching server:
+    a burst measures capacity, then Poisson arrivals at serve_load x capacity
+    give p50/p99 latency; the same requests one by one through fsm_run_event
+    give the plain path."""
+    import threading
+    reqs = W.stream_requests(args.serve_requests, rate_hz=1.0, seed=4 + 1000 * rank)
+    gaps = [reqs[0][0]] + [reqs[k][0] - reqs[k - 1][0] for k in range(1, len(reqs))]
+    events = [ev for _, ev in reqs]
+    hydro = ["e", "P", "Pi", "u", "pi", "nB", "V"]  # the fields the reference hands to hydro
+    budget = dict(hbm_budget=48 << 30, host_budget=8 << 30, streams=2, outputs=hydro)
+
+    def run(rate_hz):
+        srv = F.Server(local, **budget)
+        ids = []
+        t0 = time.perf_counter()
+
+        def feeder():
+            t = t0
+            for g, (p, e, nb) in zip(gaps, events):
+                if rate_hz:
+                    t += g / rate_hz
+                    d = t - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                ids.append(srv.submit(p, e, nb))
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        k = 0
+        while k < len(events):
+            if k < len(ids):
+                srv.poll_view(ids[k])  # zero-copy: the client reads the pinned outputs
+                srv.release(ids[k])
+                k += 1
+            else:
+                time.sleep(1e-4)
+        th.join()
+        st = srv.stats()
+        srv.stop()
+        return st
+
+    burst = run(0.0)
+    cap = burst["events_per_s"]
+    rate = args.serve_load * cap
+    st = run(rate)
+    # plain per-event path on the same requests
+    bufs = {}
+    t0 = time.perf_counter()
+    for p, e, nb in events:
+        key = (p.DIM_X, p.DIM_Y, p.DIM_ETA, p.BARYON)
+        bufs[key] = ctx.run_event(p, e, nb, outputs=hydro, into=bufs.get(key))
+    plain = len(events) / (time.perf_counter() - t0)
+    n3 = sum(1 for p, _, _ in events if p.DIM_ETA > 1)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"requests": len(events), "requests_3d": n3, "burst_events_per_s": cap,
+            "rate_hz": rate, "load": args.serve_load, "events_per_s": st["events_per_s"],
+            "p50_ms": max_over_ranks(st["p50_ms"]), "p99_ms": max_over_ranks(st["p99_ms"]),
+            "max_ms": max_over_ranks(st["max_ms"]), "waves": st["waves"],
+            "plain_events_per_s": plain, "burst_over_plain": cap / plain,
+            "per_rank": world > 1,
+            "outputs": hydro,
+            "budget": {"hbm_bytes": budget["hbm_budget"], "pinned_host_bytes": budget["host_budget"]}}
+
+
+def event_3d(F, W, local, sp, stream, args):
+    """The 3D configuration with baryon charge, one event device-resident:
+    131 x 131 x 51 cells, 21 rapidities (tan map), 100 phi_p, DTAU 0.8."""
+    import torch
+    p, e, nb = W.baryon3d()
+    ctx = F.Context(local, timing=True)
+    b = F.Batch(ctx, [p])
+    h_in = torch.from_numpy(b.pack_inputs([(e, nb)])).pin_memory()
+    b.upload(h_in.data_ptr(), sp)
+    for _ in range(2):
+        b.launch(sp)
+    stream.synchronize()
+    ctx.timing(reset=True)
+    n = max(3, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n):
+        b.launch(sp)
+    e1.record(stream)
+    stream.synchronize()
+    b.check_errors()
+    ms = e0.elapsed_time(e1) / n
+    tm = ctx.timing(reset=True)
+    live = b.samples()
+    ref = p.DIM_X * p.DIM_Y * p.DIM_ETA * p.DIM_RAP * b.info(0)["dim_phip"]
+    stream_ms = tm["stream_ms"] / max(tm["stream_launches"], 1)
+    out = {"config": "131x131x51, DIM_RAP 21 (tan map), DIM_PHIP 100, DTAU 0.8, BARYON 1, EOS 1",
+           "ms_per_event": ms, "stream_ms": stream_ms, "landau_ms": tm["landau_ms"] / n,
+           "live_samples": live, "reference_samples": ref,
+           "live_samples_per_s": live / (stream_ms * 1e-3),
+           "stream_tflops": live * FLOPS_PER_SAMPLE_3D_BARYON / (stream_ms * 1e-3) / 1e12,
+           "flops_per_sample": FLOPS_PER_SAMPLE_3D_BARYON}
+    b.close()
+    ctx.close()
+    return out
 
 
 def reference_arm(args):
@@ -285,6 +394,16 @@ def main():
         for s in singles:
             s.close()
 
+    # ---------------- served: Poisson stream of mixed 2D/3D requests through the server
+    served = None
+    if not args.no_serve:
+        served = serve_stream(args, F, W, local, rank, ctx, max_over_ranks)
+
+    # ---------------- one 3D event with baryon charge (131^2 x 51, 21 rapidities, 100 phi_p)
+    ev3d = None
+    if not args.no_3d:
+        ev3d = event_3d(F, W, local, sp, stream, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
@@ -324,6 +443,8 @@ def main():
             "e2e": {"value": e2e, "unit": "events/s", "h2d_bytes_per_step": batch.in_bytes,
                     "d2h_bytes_per_step": batch.out_bytes},
             "gpu_launches": launches_per_step * args.steps,
+            "served": served,
+            "event_3d": ev3d,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

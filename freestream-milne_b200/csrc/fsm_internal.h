@@ -134,6 +134,12 @@ struct Ev2D {
   FSM_FLOAT4* nodes;     // [DIM]
   // outputs of the stream kernel
   float* T;              // [10][DIM]
+  // charge pass of a boost-invariant event with BARYON = 1: the field is
+  // B = n_B * qnorm, the bilinear fallback is scaled by fb_scale, and the
+  // moments go to J = (S, S cos, S sin, 0) * jscale * DRAP * d_phip
+  int charge;
+  float qnorm, fb_scale, jscale, DRAP;
+  float* J;              // [4][DIM]
 };
 
 // Per-(ieta, irap) quantities of the 3D path, computed on the host with the

@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_rows_kernel(
     const size_t row = (size_t)(ix0 + r) * NY;
     float* fl = Fs + r * ld + kPadLo;
     for (int c = lane; c < NY; c += 32) {
-      const float f = F_of(__ldg(ev.e_gev + row + c));
+      const float in = __ldg(ev.e_gev + row + c);
+      const float f = ev.charge ? __fmul_rn(in, ev.qnorm) : F_of(in);
       fl[c] = f;
       ev.fa[row + c] = f;
     }
@@ -174,7 +175,8 @@ __global__ void __launch_bounds__(kPrepRows * 32) fsm_prep2d_rows_long_kernel(
   for (int c = lane; c < NY + kPadLo + kPadHi; c += 32) fr[c] = 0.0f;
   __syncwarp();
   for (int c = lane; c < NY; c += 32) {
-    const float f = F_of(__ldg(ev.e_gev + row + c));
+    const float in = __ldg(ev.e_gev + row + c);
+    const float f = ev.charge ? __fmul_rn(in, ev.qnorm) : F_of(in);
     fr[kPadLo + c] = f;
     ev.fa[row + c] = f;
   }
@@ -436,7 +438,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
           const float4 a10 = rowp[(k + 1) * boxW], a11 = rowp[(k + 1) * boxW + 1];
           const float B0 = fmaf(uu, a01.x - a00.x, a00.x);
           const float B1 = fmaf(uu, a11.x - a10.x, a10.x);
-          cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0);
+          cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0) * ev.fb_scale;
         }
       }
     }
@@ -601,6 +603,23 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     const float R = (float)ev.NR, dphi = ev.d_phip, TAU = ev.TAU;
     const size_t DIM = (size_t)ev.NX * ev.NY;
     float* T = ev.T;
+    if (ev.charge) {
+      // J = (rapidity sum) * DRAP * d_phip (src/LandauMatch.cpp:137-140);
+      // in 2D the hypertrig rows are (1, cos, sin, 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        const size_t is = (size_t)(ixb + k) * ev.NY + iy;
+        const float s0 = stot[(5 * k + 0) * kThreads2D] + a0[k];
+        const float s1 = stot[(5 * k + 1) * kThreads2D] + a12[k].x;
+        const float s2 = stot[(5 * k + 2) * kThreads2D] + a12[k].y;
+        ev.J[0 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s0, ev.jscale), ev.DRAP), dphi);
+        ev.J[1 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s1, ev.jscale), ev.DRAP), dphi);
+        ev.J[2 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s2, ev.jscale), ev.DRAP), dphi);
+        ev.J[3 * DIM + is] = 0.0f;
+      }
+      continue;
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (!act[k]) continue;

@@ -213,6 +213,8 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   e.sy = reinterpret_cast<float*>(D + o_sy);
   e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o_nodes);
   e.T = dev_out->T ? dev_out->T : reinterpret_cast<float*>(D + o_T);
+  e.charge = 0;
+  e.fb_scale = 1.0f;
   EvLandau l{};
   l.DIM = DIM;
   l.is3d = 0;

@@ -77,8 +77,6 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
   if (!E.is3d && p.DIM_Y > kMaxNY2D)
     return fail(FSM_ERR_TOO_LARGE, "DIM_Y above 5120 on the 2D path");
   E.baryon = p.BARYON != 0;
-  if (E.baryon && !E.is3d)
-    return fail(FSM_ERR_UNSUPPORTED, "BARYON with DIM_ETA = 1 is not implemented on the GPU path");
   long long dim = (long long)p.DIM_X * p.DIM_Y * p.DIM_ETA;
   if (dim > (1ll << 30)) return fail(FSM_ERR_TOO_LARGE, "grid too large");
   p.DIM = (int)dim;
@@ -213,6 +211,34 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     E.Ry = (int)std::ceil(p.DTAU / p.DY) + 2;
     E.samples = (double)p.DIM * NP;
     E.ref_samples = (double)p.DIM * NR * NP;
+    if (E.baryon) {
+      // Charge pass.  The reference splines the irap = 0 slice of
+      // J~ = n_B * normB * c_irap (src/FreeStream.cpp:137, 353-387) for every
+      // rapidity and falls back to each slice's own bilinear value, so per
+      // sample the rapidity sum is NR c_0 S(B) when the spline of B = n_B normB
+      // is positive and (sum_irap c_irap) L(B) otherwise, c_irap the uniform-
+      // grid rapidity weights at eta = 0.
+      float SIGMA_B = p.SIGMA_B;
+      float nb = std::sqrt(2.0 * M_PI) * SIGMA_B * std::exp(SIGMA_B * SIGMA_B / 2.0);
+      E.normB = 1.0 / (2.0 * M_PI * nb);  // src/FreeStream.cpp:365-366
+      const float rapmin = (-1.0) * ((float)(NR - 1) / 2.0) * p.DRAP;
+      const float eta = 0.0f * p.DETA + E.etamin;
+      double csum = 0.0;
+      float c0 = 0.0f;
+      for (int irap = 0; irap < NR; ++irap) {
+        float rap = (float)irap * p.DRAP + rapmin;
+        float c = std::cosh(eta - rap) * std::exp((-1.0) * (eta - rap) * (eta - rap) / (SIGMA_B * SIGMA_B));
+        csum += c;
+        if (irap == 0) c0 = c;
+      }
+      if (!(c0 > 0.0f) || !std::isfinite(csum))
+        return fail(FSM_ERR_UNSUPPORTED,
+                    "2D BARYON: the first rapidity weight underflows (DRAP * DIM_RAP too wide for SIGMA_B)");
+      E.fb_scale2 = (float)(csum / ((double)NR * (double)c0));
+      E.jscale2 = (float)NR * c0;
+      E.samples *= 2.0;
+      E.ref_samples *= 2.0;
+    }
     return FSM_OK;
   }
 

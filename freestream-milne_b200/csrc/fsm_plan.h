@@ -31,6 +31,8 @@ struct EventPlan {
   std::vector<float> rapf, rapfB, jac;
   int r_lo = 0, r_hi = 0;
   float norm = 0, normB = 0;
+  // 2D with BARYON: fallback and output scales of the charge pass (Ev2D)
+  float fb_scale2 = 1.0f, jscale2 = 0.0f;
   double samples = 0;  // cell x momentum samples the stream kernel evaluates
   double ref_samples = 0;  // DIM * DIM_RAP * DIM_PHIP, the reference's count
 };

@@ -108,11 +108,13 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   struct EvOffs {
     size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac;
     size_t fa, sy, nodes, efield, T, J, in_e, in_nB, out;
+    size_t qfa, qsy, qnodes;  // charge pass scratch (2D with BARYON)
   };
   std::vector<EvOffs> eo(n);
   int n2 = 0, n3 = 0;
   b->ev2_of.assign(n, -1);
   b->ev3_of.assign(n, -1);
+  b->evq_of.assign(n, -1);
   b->in_off.assign(n, 0);
   b->out_off.assign(n, 0);
   size_t in_elems = 0, out_elems = 0;
@@ -122,8 +124,12 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     in_elems += (size_t)P.DIM * (P.baryon ? 2 : 1);
     b->out_off[i] = out_elems;
     out_elems += (size_t)P.DIM * output_components(P.baryon);
-    if (P.is3d) b->ev3_of[i] = n3++;
-    else b->ev2_of[i] = n2++;
+    if (P.is3d) {
+      b->ev3_of[i] = n3++;
+    } else {
+      b->ev2_of[i] = n2++;
+      if (P.baryon) b->evq_of[i] = n2++;
+    }
   }
   // tables
   for (int i = 0; i < n; ++i) {
@@ -166,22 +172,26 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                                (x0 + kTileX - 1 + P.ox_max <= NX - 3) && (y0 + P.oy_min >= 2) &&
                                (y0 + kTileY - 1 + P.oy_max <= NY - 3);
           tiles.push_back(Tile2D{b->ev2_of[i], x0, y0, interior});
+          if (b->evq_of[i] >= 0) tiles.push_back(Tile2D{b->evq_of[i], x0, y0, interior});
         }
     }
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
       if (P.is3d) continue;
-      const int e2 = b->ev2_of[i], NX = P.p.DIM_X, NY = P.p.DIM_Y;
-      if (NX <= kMaxStrip && NY <= kMaxStrip) {
-        for (int x = 0; x < NX; x += 32) rows.push_back(LineBlock{e2, x, 0});
-        for (int y = 0; y < NY; y += 32) cols.push_back(LineBlock{e2, y, 0});
-        b->strip_cap2 = std::max(b->strip_cap2, std::max(NX, NY));
-      } else {
-        for (int x = 0; x < NX; x += kPrepRows) rows_l.push_back(LineBlock{e2, x, 0});
-        const int nseg = (NX + kSegP - 1) / kSegP;
-        for (int y = 0; y < NY; y += 32)
-          for (int g = 0; g < nseg; g += 4) cols_l.push_back(LineBlock{e2, y, g});
-        b->ny_cap2 = std::max(b->ny_cap2, NY);
+      const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
+      for (int e2 : {b->ev2_of[i], b->evq_of[i]}) {
+        if (e2 < 0) continue;
+        if (NX <= kMaxStrip && NY <= kMaxStrip) {
+          for (int x = 0; x < NX; x += 32) rows.push_back(LineBlock{e2, x, 0});
+          for (int y = 0; y < NY; y += 32) cols.push_back(LineBlock{e2, y, 0});
+          b->strip_cap2 = std::max(b->strip_cap2, std::max(NX, NY));
+        } else {
+          for (int x = 0; x < NX; x += kPrepRows) rows_l.push_back(LineBlock{e2, x, 0});
+          const int nseg = (NX + kSegP - 1) / kSegP;
+          for (int y = 0; y < NY; y += 32)
+            for (int g = 0; g < nseg; g += 4) cols_l.push_back(LineBlock{e2, y, g});
+          b->ny_cap2 = std::max(b->ny_cap2, NY);
+        }
       }
     }
     std::vector<int> order3;
@@ -224,6 +234,11 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     if (!P.is3d) {
       o.fa = L.take((size_t)P.DIM * 4);
       o.sy = L.take((size_t)P.DIM * 4);
+      if (P.baryon) {
+        o.qfa = L.take((size_t)P.DIM * 4);
+        o.qsy = L.take((size_t)P.DIM * 4);
+        o.qnodes = L.take((size_t)P.DIM * 16);
+      }
       o.nodes = L.take((size_t)P.DIM * 16);
     } else {
       o.efield = L.take((size_t)P.DIM * 4);
@@ -281,6 +296,43 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
     }
   }
+  // ---- output slab layout: per event (default) or group by group
+  b->grouped_out = mem && mem->grouped_out;
+  b->out_goff.assign(n, {});
+  {
+    size_t off = 0;
+    for (int g = 0; g < kOutGroups; ++g) {
+      b->group_off[g] = off;
+      size_t ge = 0;
+      for (int i = 0; i < n; ++i) {
+        const EventPlan& P = b->plans[i];
+        if (g >= 6 && !P.baryon) continue;
+        ge += (size_t)kOutGroupComps[g] * P.DIM;
+      }
+      b->group_elems[g] = ge;
+      off += ge;
+    }
+    size_t gcur[kOutGroups];
+    for (int g = 0; g < kOutGroups; ++g) gcur[g] = b->group_off[g];
+    for (int i = 0; i < n; ++i) {
+      const EventPlan& P = b->plans[i];
+      size_t within = 0;
+      for (int g = 0; g < kOutGroups; ++g) {
+        if (g >= 6 && !P.baryon) {
+          b->out_goff[i][g] = 0;
+          continue;
+        }
+        const size_t sz = (size_t)kOutGroupComps[g] * P.DIM;
+        if (b->grouped_out) {
+          b->out_goff[i][g] = gcur[g];
+          gcur[g] += sz;
+        } else {
+          b->out_goff[i][g] = b->out_off[i] + within;
+        }
+        within += sz;
+      }
+    }
+  }
   // ---- per-event io views
   b->d_in_e.assign(n, nullptr);
   b->d_in_nB.assign(n, nullptr);
@@ -294,18 +346,19 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       float* in = reinterpret_cast<float*>(D + b->in_slab_off) + b->in_off[i];
       b->d_in_e[i] = in;
       b->d_in_nB[i] = P.baryon ? in + DIM : nullptr;
-      float* o = reinterpret_cast<float*>(D + b->out_slab_off) + b->out_off[i];
+      float* o = reinterpret_cast<float*>(D + b->out_slab_off);
+      const auto& go = b->out_goff[i];
       fsm_outputs v{};
-      v.T = o;
-      v.e = o + 10 * DIM;
-      v.P = o + 11 * DIM;
-      v.Pi = o + 12 * DIM;
-      v.u = o + 13 * DIM;
-      v.pi = o + 17 * DIM;
+      v.T = o + go[0];
+      v.e = o + go[1];
+      v.P = o + go[2];
+      v.Pi = o + go[3];
+      v.u = o + go[4];
+      v.pi = o + go[5];
       if (P.baryon) {
-        v.J = o + 27 * DIM;
-        v.nB = o + 31 * DIM;
-        v.V = o + 32 * DIM;
+        v.J = o + go[6];
+        v.nB = o + go[7];
+        v.V = o + go[8];
       }
       b->d_out[i] = v;
       b->d_T[i] = v.T;
@@ -369,6 +422,23 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.sy = reinterpret_cast<float*>(D + o.sy);
       e.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o.nodes);
       e.T = b->d_T[i];
+      e.charge = 0;
+      e.fb_scale = 1.0f;
+      if (P.baryon) {  // charge pass: same geometry and tables, its own field and scratch
+        Ev2D& q = b->ev2[b->evq_of[i]];
+        q = e;
+        q.charge = 1;
+        q.qnorm = P.normB;
+        q.fb_scale = P.fb_scale2;
+        q.jscale = P.jscale2;
+        q.DRAP = p.DRAP;
+        q.e_gev = b->d_in_nB[i];
+        q.fa = reinterpret_cast<float*>(D + o.qfa);
+        q.sy = reinterpret_cast<float*>(D + o.qsy);
+        q.nodes = reinterpret_cast<FSM_FLOAT4*>(D + o.qnodes);
+        q.T = nullptr;
+        q.J = b->d_J[i];
+      }
       max_np2 = std::max(max_np2, p.DIM_PHIP);
     } else {
       Ev3D& e = b->ev3[b->ev3_of[i]];

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -44,6 +45,15 @@ using fsm::EventPlan;
 using fsm::LineBlock;
 using fsm::Tile2D;
 
+namespace fsm {
+namespace rt {
+// Output component groups of a batch's output slab, in slab order:
+// T(10) e P Pi u(4) pi(10) J(4) nB V(4); J, nB and V only for baryon events.
+constexpr int kOutGroups = 9;
+constexpr int kOutGroupComps[kOutGroups] = {10, 1, 1, 1, 4, 10, 4, 1, 4};
+}  // namespace rt
+}  // namespace fsm
+
 struct fsm_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -75,6 +85,11 @@ struct fsm_batch {
   std::vector<float*> d_in_e, d_in_nB;
   std::vector<fsm_outputs> d_out;
   std::vector<size_t> in_off, out_off;  // element offsets inside the slabs
+  // element offset of event i's component group g inside the output slab; with
+  // grouped_out the slab holds group by group (all events' T, then all e, ...)
+  std::vector<std::array<size_t, fsm::rt::kOutGroups>> out_goff;
+  bool grouped_out = false;
+  size_t group_off[fsm::rt::kOutGroups] = {}, group_elems[fsm::rt::kOutGroups] = {};
   size_t in_slab_off = 0, in_slab_bytes = 0, out_slab_off = 0, out_slab_bytes = 0;
   std::vector<float*> d_T, d_J;         // moment buffers the Landau kernel reads
   // host copies of descriptors
@@ -82,6 +97,7 @@ struct fsm_batch {
   std::vector<Ev3D> ev3;
   std::vector<EvLandau> evl;
   std::vector<int> ev2_of, ev3_of;      // event -> index in ev2/ev3 (or -1)
+  std::vector<int> evq_of;              // 2D baryon event -> its charge pass in ev2 (or -1)
   // device descriptor arrays and work lists
   Ev2D* d_ev2 = nullptr;
   Ev3D* d_ev3 = nullptr;
@@ -113,6 +129,7 @@ struct BatchMem {
   char* (*dev)(void* user, size_t bytes) = nullptr;
   char* (*host)(void* user, size_t bytes) = nullptr;
   cudaStream_t stream = nullptr;
+  bool grouped_out = false;  // output slab laid out group by group
 };
 
 bool has_device();

@@ -103,8 +103,8 @@ struct Request {
   bool done = false;
   fsm_status status = FSM_OK;
   std::string msg;  // error message of a failed request
-  OutBlock* ob = nullptr;   // holds the event's outputs once done
-  const float* out = nullptr;  // T(10) e P Pi u(4) pi(10) [J(4) nB V(4)], component-major
+  OutBlock* ob = nullptr;  // holds the event's outputs once done
+  const float* grp[kOutGroups] = {};  // its component groups in the block (nullptr: not kept)
   fsm_run_info info{};
   size_t dim = 0;
   bool baryon = false;
@@ -118,6 +118,7 @@ struct Wave {
   // input and output slabs (+ 16 bytes of kernel error words after the outputs)
   char *d = nullptr, *hs = nullptr, *hin = nullptr, *hout = nullptr;
   size_t dbytes = 0, hsbytes = 0, hinbytes = 0, houtbytes = 0;
+  size_t hgrp[kOutGroups];  // element offset of each kept output group in hout, or -1
   bool done = false;
   Clock::time_point t_done;
 };
@@ -200,7 +201,7 @@ void drop_output(fsm_server* S, Request* r) {
     delete r->ob;
   }
   r->ob = nullptr;
-  r->out = nullptr;
+  for (auto& g : r->grp) g = nullptr;
 }
 
 void finish_request(fsm_server* S, Request* r, fsm_status st, Clock::time_point t) {
@@ -219,7 +220,7 @@ void finish_request(fsm_server* S, Request* r, fsm_status st, Clock::time_point 
 
 // Outputs of a completed wave into its requests (mu held).
 void wave_retire(fsm_server* S, Wave* w) {
-  const int* err = reinterpret_cast<const int*>(w->hout + w->b->out_slab_bytes);
+  const int* err = reinterpret_cast<const int*>(w->hout + w->houtbytes - 16);
   fsm_status st = FSM_OK;
   if (err[1] != 0) st = FSM_ERR_TIMEOUT;
   else if (err[0] != 0) st = FSM_ERR_CUDA;
@@ -232,7 +233,10 @@ void wave_retire(fsm_server* S, Wave* w) {
     r->dim = (size_t)P.DIM;
     r->baryon = P.baryon;
     r->ob = ob;
-    r->out = out + w->b->out_off[i];
+    for (int g = 0; g < kOutGroups; ++g) {
+      const bool have = w->hgrp[g] != (size_t)-1 && (g < 6 || P.baryon);
+      r->grp[g] = have ? out + w->hgrp[g] + (w->b->out_goff[i][g] - w->b->group_off[g]) : nullptr;
+    }
     fill_info(P, &r->info);
     finish_request(S, r, st, w->t_done);
   }
@@ -267,6 +271,7 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
     mem.dev = pool_dev;
     mem.host = pool_host;
     mem.stream = s;
+    mem.grouped_out = true;
     fsm_batch* b = nullptr;
     // planning runs without the lock; the pools are only touched by this thread
     lk.unlock();
@@ -276,7 +281,13 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
     if (st == FSM_OK) {
       w->b = b;
       w->hinbytes = b->in_slab_bytes;
-      w->houtbytes = b->out_slab_bytes + 16;
+      size_t kept = 0;
+      for (int g = 0; g < kOutGroups; ++g) {
+        const bool keep = (S->opts.output_mask & (1u << g)) && b->group_elems[g] > 0;
+        w->hgrp[g] = keep ? kept : (size_t)-1;
+        if (keep) kept += b->group_elems[g];
+      }
+      w->houtbytes = kept * 4 + 16;
       w->hin = S->hpool.alloc(w->hinbytes);
       w->hout = w->hin ? S->hpool.alloc(w->houtbytes) : nullptr;
       if (!w->hin || !w->hout) st = FSM_ERR_OUT_OF_MEMORY;
@@ -294,10 +305,15 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
       if (ce == cudaSuccess) st = enqueue(b, s, false);
       else st = FSM_ERR_CUDA;
       if (st == FSM_OK) {
-        ce = cudaMemcpyAsync(w->hout, b->d_mem + b->out_slab_off, b->out_slab_bytes,
-                             cudaMemcpyDeviceToHost, s);
+        // only the output groups the server keeps, one copy per group
+        ce = cudaSuccess;
+        for (int g = 0; g < kOutGroups && ce == cudaSuccess; ++g) {
+          if (w->hgrp[g] == (size_t)-1) continue;
+          ce = cudaMemcpyAsync(w->hout + w->hgrp[g] * 4, b->d_mem + b->out_slab_off + b->group_off[g] * 4,
+                               b->group_elems[g] * 4, cudaMemcpyDeviceToHost, s);
+        }
         if (ce == cudaSuccess)
-          ce = cudaMemcpyAsync(w->hout + b->out_slab_bytes, b->d_err, 16, cudaMemcpyDeviceToHost, s);
+          ce = cudaMemcpyAsync(w->hout + w->houtbytes - 16, b->d_err, 16, cudaMemcpyDeviceToHost, s);
         if (ce == cudaSuccess) ce = cudaLaunchHostFunc(s, wave_done_cb, user);
         if (ce != cudaSuccess) {
           set_last_error(std::string("server wave: ") + cudaGetErrorString(ce));
@@ -402,6 +418,7 @@ extern "C" fsm_status fsm_server_start(fsm_server** out, const fsm_server_opts* 
   if (S->opts.host_budget_bytes == 0) S->opts.host_budget_bytes = (size_t)2 << 30;
   if (S->opts.max_wave_events <= 0) S->opts.max_wave_events = 512;
   if (S->opts.streams <= 0) S->opts.streams = 2;
+  if (S->opts.output_mask == 0) S->opts.output_mask = FSM_OUT_ALL;
   fsm_ctx_opts co{S->opts.device, 0};
   fsm_status st = fsm_ctx_create(&S->ctx, &co);
   if (st != FSM_OK) return st;
@@ -485,21 +502,10 @@ extern "C" fsm_status fsm_server_poll(fsm_server* S, long long id, const fsm_out
   const fsm_status st = r->status;
   if (st == FSM_OK && host_out) {
     const size_t n = r->dim;
-    const float* o = r->out;
-    auto put = [&](float* dst, size_t comp0, size_t ncomp) {
-      if (dst) std::memcpy(dst, o + comp0 * n, ncomp * n * 4);
-    };
-    put(host_out->T, 0, 10);
-    put(host_out->e, 10, 1);
-    put(host_out->P, 11, 1);
-    put(host_out->Pi, 12, 1);
-    put(host_out->u, 13, 4);
-    put(host_out->pi, 17, 10);
-    if (r->baryon) {
-      put(host_out->J, 27, 4);
-      put(host_out->nB, 31, 1);
-      put(host_out->V, 32, 4);
-    }
+    float* dst[kOutGroups] = {host_out->T, host_out->e,  host_out->P, host_out->Pi, host_out->u,
+                              host_out->pi, host_out->J, host_out->nB, host_out->V};
+    for (int g = 0; g < kOutGroups; ++g)
+      if (dst[g] && r->grp[g]) std::memcpy(dst[g], r->grp[g], (size_t)kOutGroupComps[g] * n * 4);
   }
   if (info) *info = r->info;
   if (st != FSM_OK) set_last_error(r->msg);
@@ -507,6 +513,46 @@ extern "C" fsm_status fsm_server_poll(fsm_server* S, long long id, const fsm_out
   S->reqs.erase(it);
   delete r;
   return st;
+}
+
+extern "C" fsm_status fsm_server_poll_view(fsm_server* S, long long id, fsm_outputs* views,
+                                           fsm_run_info* info, double timeout_ms, int* done) {
+  if (!S || !done || !views) return FSM_ERR_INVALID_ARG;
+  *done = 0;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) {
+    set_last_error("fsm_server_poll_view: unknown request id");
+    return FSM_ERR_INVALID_ARG;
+  }
+  Request* r = it->second;
+  if (!r->done && timeout_ms != 0.0) {
+    auto pred = [&] { return r->done; };
+    if (timeout_ms < 0) S->cv_done.wait(lk, pred);
+    else S->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), pred);
+  }
+  if (!r->done) return FSM_OK;
+  *done = 1;
+  float** dst[kOutGroups] = {&views->T, &views->e,  &views->P,  &views->Pi, &views->u,
+                             &views->pi, &views->J, &views->nB, &views->V};
+  for (int g = 0; g < kOutGroups; ++g) *dst[g] = const_cast<float*>(r->grp[g]);
+  if (info) *info = r->info;
+  if (r->status != FSM_OK) set_last_error(r->msg);
+  return r->status;
+}
+
+extern "C" fsm_status fsm_server_release(fsm_server* S, long long id) {
+  if (!S) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end() || !it->second->done) {
+    set_last_error("fsm_server_release: unknown or unfinished request id");
+    return FSM_ERR_INVALID_ARG;
+  }
+  drop_output(S, it->second);
+  delete it->second;
+  S->reqs.erase(it);
+  return FSM_OK;
 }
 
 extern "C" fsm_status fsm_server_stats_get(fsm_server* S, fsm_server_stats* st) {

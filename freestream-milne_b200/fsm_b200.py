@@ -74,7 +74,11 @@ _ST = ctypes.c_int
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
                 ("host_budget_bytes", ctypes.c_size_t), ("max_wave_events", ctypes.c_int),
-                ("streams", ctypes.c_int)]
+                ("streams", ctypes.c_int), ("output_mask", ctypes.c_uint)]
+
+
+# output groups of the server (FSM_OUT_* in fsm.h), in slab order
+OUT_GROUPS = ["T", "e", "P", "Pi", "u", "pi", "J", "nB", "V"]
 
 
 class ServerStats(ctypes.Structure):
@@ -122,6 +126,10 @@ SIGNATURES = {
                                 ctypes.POINTER(ctypes.c_longlong)]),
     "fsm_server_poll": (_ST, [_VP, ctypes.c_longlong, ctypes.POINTER(Outputs),
                               ctypes.POINTER(RunInfo), ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
+    "fsm_server_poll_view": (_ST, [_VP, ctypes.c_longlong, ctypes.POINTER(Outputs),
+                                   ctypes.POINTER(RunInfo), ctypes.c_double,
+                                   ctypes.POINTER(ctypes.c_int)]),
+    "fsm_server_release": (_ST, [_VP, ctypes.c_longlong]),
     "fsm_server_stats_get": (_ST, [_VP, ctypes.POINTER(ServerStats)]),
     "fsm_server_stop": (_ST, [_VP]),
 }
@@ -213,8 +221,10 @@ class Context:
         check(lib().fsm_ctx_timing(self.h, ctypes.byref(t), int(reset)), "fsm_ctx_timing")
         return {k: getattr(t, k) for k, _ in Timing._fields_}
 
-    def run_event(self, params, e_gev, nB=None, outputs=None):
-        """Plain per-event path with host buffers; returns {name: ndarray}."""
+    def run_event(self, params, e_gev, nB=None, outputs=None, into=None):
+        """Plain per-event path with host buffers; returns {name: ndarray}
+        (written into the arrays of `into`, a previous result of the same
+        shape, when given)."""
         e_gev = np.ascontiguousarray(e_gev, dtype=np.float32).ravel()
         dim = params.DIM_X * params.DIM_Y * params.DIM_ETA
         if e_gev.size != dim:
@@ -224,7 +234,10 @@ class Context:
         arrs = {}
         o = Outputs()
         for k in names:
-            a = np.zeros((OUT_COMPS[k], dim) if OUT_COMPS[k] > 1 else (dim,), dtype=np.float32)
+            if into is not None and k in into:
+                a = into[k]
+            else:
+                a = np.zeros((OUT_COMPS[k], dim) if OUT_COMPS[k] > 1 else (dim,), dtype=np.float32)
             arrs[k] = a
             setattr(o, k, a.ctypes.data)
         nb_ptr = None
@@ -354,10 +367,15 @@ class Server:
     """Continuous-batching request server (fsm_server_*): submit events as they
     arrive, poll for their outputs; results equal Context.run_event's."""
 
-    def __init__(self, device=0, hbm_budget=0, host_budget=0, max_wave_events=0, streams=0):
+    def __init__(self, device=0, hbm_budget=0, host_budget=0, max_wave_events=0, streams=0,
+                 outputs=None):
         self.h = ctypes.c_void_p()
+        self.outputs = list(outputs) if outputs else list(OUT_GROUPS)
+        mask = 0
+        for k in self.outputs:
+            mask |= 1 << OUT_GROUPS.index(k)
         opts = ServerOpts(device, int(hbm_budget), int(host_budget), int(max_wave_events),
-                          int(streams))
+                          int(streams), mask)
         check(lib().fsm_server_start(ctypes.byref(self.h), ctypes.byref(opts)), "fsm_server_start")
         self._pending = {}
 
@@ -377,7 +395,7 @@ class Server:
     def poll(self, rid, timeout_ms=-1.0):
         """None while running; the outputs dict once done (FsmError if it failed)."""
         dim, baryon = self._pending[rid]
-        names = list(OUT_COMPS) if baryon else [k for k in OUT_COMPS if k not in ("J", "nB", "V")]
+        names = [k for k in self.outputs if baryon or k not in ("J", "nB", "V")]
         arrs, o = {}, Outputs()
         for k in names:
             a = np.zeros((OUT_COMPS[k], dim) if OUT_COMPS[k] > 1 else (dim,), dtype=np.float32)
@@ -393,6 +411,34 @@ class Server:
         check(st, "fsm_server_poll")
         arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
         return arrs
+
+    def poll_view(self, rid, timeout_ms=-1.0):
+        """Zero-copy poll: None while running; once done, read-only arrays viewing
+        the server's pinned memory, valid until release(rid)."""
+        dim, baryon = self._pending[rid]
+        o, info, done = Outputs(), RunInfo(), ctypes.c_int(0)
+        st = lib().fsm_server_poll_view(self.h, rid, ctypes.byref(o), ctypes.byref(info),
+                                        float(timeout_ms), ctypes.byref(done))
+        if not done.value:
+            check(st, "fsm_server_poll_view")
+            return None
+        if st != FSM_OK:
+            self.release(rid)
+            check(st, "fsm_server_poll_view")
+        arrs = {}
+        for k in self.outputs:
+            ptr = getattr(o, k)
+            if ptr:
+                n = OUT_COMPS[k] * dim
+                a = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), (n,))
+                a.flags.writeable = False
+                arrs[k] = a.reshape((OUT_COMPS[k], dim)) if OUT_COMPS[k] > 1 else a
+        arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
+        return arrs
+
+    def release(self, rid):
+        check(lib().fsm_server_release(self.h, rid), "fsm_server_release")
+        self._pending.pop(rid, None)
 
     def stats(self):
         st = ServerStats()

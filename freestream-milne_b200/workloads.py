@@ -79,6 +79,16 @@ def lumpy2d(seed=1, side=261, dx=0.06, nphip=200, tau0=0.2, dtau=1.0, eos=2, rad
     return p, e.astype(np.float32).ravel(), None
 
 
+def lumpy2d_baryon(seed=1, side=101, dx=0.08, nphip=64, dtau=0.8, nrap=5, drap=0.3, sigma_b=0.8,
+                   eos=1, radius=3.0, **over):
+    """Boost-invariant event with baryon charge: lumpy T^00 and n_B = 0.1 x the
+    normalised profile, DIM_RAP uniform rapidity nodes for the charge."""
+    p, e, _ = lumpy2d(seed=seed, side=side, dx=dx, nphip=nphip, dtau=dtau, eos=eos, radius=radius,
+                      BARYON=1, IC_BARYON=3, DIM_RAP=nrap, DRAP=drap, SIGMA_B=sigma_b, **over)
+    nB = (0.1 * e / max(float(e.max()), 1e-30)).astype(np.float32)
+    return p, e, nB
+
+
 def baryon3d(seed=2, side=131, dx=0.1, neta=51, deta=0.2, nrap=21, nphip=100, tau0=0.1,
              dtau=0.8, eta_flat=4.0, eta_width=1.0, **over):
     rng = np.random.default_rng(seed)

@@ -221,12 +221,29 @@ fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
  * not race with the others. */
 typedef struct fsm_server fsm_server;
 
+/* Output groups a server returns (fsm_server_opts.output_mask; 0 = all). */
+enum {
+  FSM_OUT_T = 1u << 0,     /* T^{mu nu}                 */
+  FSM_OUT_E = 1u << 1,     /* e                         */
+  FSM_OUT_P = 1u << 2,     /* P                         */
+  FSM_OUT_BULK = 1u << 3,  /* Pi                        */
+  FSM_OUT_U = 1u << 4,     /* u^mu                      */
+  FSM_OUT_SHEAR = 1u << 5, /* pi^{mu nu}                */
+  FSM_OUT_J = 1u << 6,     /* J^mu (baryon events)      */
+  FSM_OUT_NB = 1u << 7,    /* n_B (baryon events)       */
+  FSM_OUT_V = 1u << 8,     /* V^mu (baryon events)      */
+  FSM_OUT_ALL = 0x1ffu
+};
+
 typedef struct fsm_server_opts {
   int device;                /* CUDA device ordinal                                 */
   size_t hbm_budget_bytes;   /* device memory held for waves in flight (0: 8 GiB)   */
   size_t host_budget_bytes;  /* pinned host memory for inputs/outputs (0: 2 GiB)    */
   int max_wave_events;       /* events per launch wave (0: 512)                     */
   int streams;               /* waves in flight (0: 2)                              */
+  unsigned output_mask;      /* FSM_OUT_* groups copied back (0: all); fields of
+                                fsm_server_poll's host_out outside it are left as
+                                they are                                            */
 } fsm_server_opts;
 
 typedef struct fsm_server_stats {
@@ -245,6 +262,13 @@ fsm_status fsm_server_submit(fsm_server* s, const fsm_params* p, const float* e_
  * cannot fit the budgets, FSM_ERR_CANCELLED when the server stopped first). */
 fsm_status fsm_server_poll(fsm_server* s, long long id, const fsm_outputs* host_out,
                            fsm_run_info* info, double timeout_ms, int* done);
+/* Zero-copy variant: on done = 1 the fields of `views` point at the request's
+ * outputs inside the server's pinned memory (NULL for groups outside the
+ * output mask), valid until fsm_server_release(s, id); the request stays
+ * known until then. */
+fsm_status fsm_server_poll_view(fsm_server* s, long long id, fsm_outputs* views,
+                                fsm_run_info* info, double timeout_ms, int* done);
+fsm_status fsm_server_release(fsm_server* s, long long id);
 fsm_status fsm_server_stats_get(fsm_server* s, fsm_server_stats* st);
 /* Finishes the waves in flight, cancels queued requests, frees everything. */
 fsm_status fsm_server_stop(fsm_server* s);

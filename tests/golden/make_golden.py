@@ -3,7 +3,7 @@
 Run from the repository root in a checkout where the reference is available:
 
     make -C oracle            # builds oracle/_ref/libfsm_ref.so from <reference>/src
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 
 Each fixture holds a seeded synthetic input, its parameters and the outputs of
 the reference pipeline (src/FreestreamMilne.cpp:251-506) compiled from the
@@ -93,6 +93,14 @@ def cases():
     tp = hotspots(rng, x, y, n=15, radius=1.5)
     e = (tp[:, :, None] * np.exp(-eta.astype(np.float64) ** 2 / 4)[None, None, :]).astype(np.float32)
     cs.append(("wb3d_21x21x11", p, e, None))
+    # 2D with baryon charge: five uniform rapidity nodes for the charge density
+    p = O.make_params(DIM_X=45, DIM_Y=41, DX=0.1, DY=0.1, DIM_PHIP=40, TAU0=0.2, DTAU=0.7,
+                      EOS_TYPE=1, BARYON=1, IC_BARYON=3, DIM_RAP=5, DRAP=0.3, SIGMA_B=0.8)
+    x, y = axis(45, 0.1), axis(41, 0.1)
+    tp = hotspots(rng, x, y, n=20, radius=1.4)
+    e = tp.astype(np.float32)
+    nB = (0.1 * tp / tp.max()).astype(np.float32)
+    cs.append(("baryon2d_45x41_rap5", p, e, nB))
     return cs
 
 
@@ -103,10 +111,12 @@ def params_dict(p):
     return {k: getattr(p, k) for k, _ in O.PARAM_FIELDS}
 
 
-def main():
+def main(only=None):
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libfsm_ref.so missing: build it with `make -C oracle`")
     for name, p, e, nB in cases():
+        if only and name not in only:
+            continue
         r = O.run(p, e.ravel(), nB=None if nB is None else nB.ravel(), impl="ref")
         arrays = {"e_gev": e.ravel().astype(np.float32)}
         if nB is not None:
@@ -124,7 +134,8 @@ def main():
         np.savez_compressed(OUT / f"{name}.npz", **arrays)
         print(name, "cells", e.size, "phi_p", r["dim_phip"], "fallback", r["n_fallback"])
     # the public entry point end to end, with its parameter file
-    full_case()
+    if not only or "full_entry_31x29" in only:
+        full_case()
 
 
 FULL_INPUT = """OUTPUTFORMAT 2
@@ -175,4 +186,4 @@ def full_case():
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)  # optional fixture names: regenerate only those

@@ -71,6 +71,18 @@ def test_gpu_long_lines(ctx, nx, ny):
     compare(got, ref64, ref["tau"])
 
 
+def test_gpu_2d_baryon(ctx):
+    """Boost-invariant event with baryon charge: J^mu from the charge pass
+    (spline of the first rapidity slice, per-slice bilinear fallback)."""
+    p, e, nB = W.lumpy2d_baryon(seed=13, side=81, dx=0.08, nphip=48, dtau=0.7, nrap=5)
+    got = ctx.run_event(p, e, nB)
+    ref = _oracle(p, e, nB)
+    ref64 = _oracle(p, e, nB, fp64=2)
+    errs = compare_parity(got, ref, ref64, ref["tau"], baryon=True)
+    errs64 = compare(got, ref64, ref["tau"], baryon=True)
+    print("baryon2d vs float", errs, "vs FP64", errs64)
+
+
 def test_gpu_3d_baryon_reduced(ctx):
     """3D + baryon path on a reduced grid the oracle runs in seconds."""
     p, e, nB = W.baryon3d(seed=5, side=41, neta=21, nrap=21, nphip=40)

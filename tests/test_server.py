@@ -85,3 +85,23 @@ def test_server_budget_splits_waves_and_rejects_oversize():
     assert all(o is not None for o in outs)
     assert st["completed"] == len(small) and st["failed"] == 1
     assert st["waves"] >= 2
+
+
+@pytest.mark.gpu
+def test_server_output_mask(ctx):
+    p, e, _ = W.lumpy2d(seed=21, side=71, dx=0.09, nphip=64, dtau=0.6, eos=2, radius=2.0)
+    srv = F.Server(outputs=["e", "u"])
+    try:
+        got = srv.poll(srv.submit(p, e))
+        rid = srv.submit(p, e)
+        view = srv.poll_view(rid)
+        viewed = {k: np.array(v) for k, v in view.items() if k != "info"}
+        srv.release(rid)
+    finally:
+        srv.stop()
+    for k in ("e", "u"):
+        np.testing.assert_array_equal(viewed[k], got[k])
+    assert set(k for k in got if k != "info") == {"e", "u"}
+    plain = ctx.run_event(p, e)
+    np.testing.assert_array_equal(got["e"], plain["e"])
+    np.testing.assert_array_equal(got["u"], plain["u"])
