@@ -230,6 +230,34 @@ __global__ void __launch_bounds__(128) fsm_prep2d_cols_long_kernel(
   }
 }
 
+// --------------------------------------------------- energy-dependent DTAU
+// The reference's sums for the energy-dependent free-streaming time: float
+// running sums of eps^2 and eps over the converted profile, in cell order
+// (src/FreeStream.cpp:404-409).  The rounding of a running float sum depends
+// on its order, so one thread adds the cells in that order.
+__global__ void fsm_edep_sums_kernel(const float* __restrict__ e_gev, int n, float* sums) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float num = 0.0f, den = 0.0f;
+  int i = 0;
+  for (; i + 8 <= n; i += 8) {
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = to_fm4(__ldg(e_gev + i + k));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      num = __fadd_rn(num, __fmul_rn(v[k], v[k]));
+      den = __fadd_rn(den, v[k]);
+    }
+  }
+  for (; i < n; ++i) {
+    const float v = to_fm4(__ldg(e_gev + i));
+    num = __fadd_rn(num, __fmul_rn(v, v));
+    den = __fadd_rn(den, v);
+  }
+  sums[0] = num;
+  sums[1] = den;
+}
+
 // ------------------------------------------------------------------ prep 3D
 __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict__ evs,
                                                          const CellBlock* __restrict__ blocks) {
@@ -841,6 +869,96 @@ __global__ void __launch_bounds__(kThreadsLandau) fsm_landau_kernel(const EvLand
   }
   const unsigned mask = __ballot_sync(0xffffffffu, fb);
   if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&ctr->fallback, __popc(mask));
+}
+
+// ------------------------------------------------------------- diagnostics
+// Hydro-validity and thermal-vorticity fields of the Landau-matched outputs
+// (src/HydroValidity.cpp:8-101, src/LandauMatch.cpp:395-489), thread per
+// cell, with the reference's float/double mixing spelled out (no
+// contraction).  beta and omega follow the reference's own indexing: the
+// interior (ix, iy) pairs at index DIM_Y * ix + iy.
+__global__ void __launch_bounds__(256) fsm_diag_kernel(int NX, int NY, int NE, float DX, float DY,
+                                                       float tau, const float* __restrict__ e,
+                                                       const float* __restrict__ P,
+                                                       const float* __restrict__ Pi,
+                                                       const float* __restrict__ u,
+                                                       const float* __restrict__ pi, float* rpi,
+                                                       float* rsh, float* pdu, float* pmm,
+                                                       float* beta, float* om) {
+  const size_t n = (size_t)NX * NY * NE;
+  const size_t is = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (is >= n) return;
+  auto S = [&](int m) { return __ldg(pi + m * n + is); };
+  const float tau2 = __fmul_rn(tau, tau);
+  {
+    const float p = __ldg(P + is);
+    const float pp = ((double)p < 1.0e-5) ? (float)1.0e-5 : p;
+    if (rpi) rpi[is] = __fdiv_rn(__ldg(Pi + is), pp);
+  }
+  if (rsh) {
+    const float s0 = S(0), s1 = S(1), s2 = S(2), s3 = S(3), s4 = S(4), s5 = S(5), s6 = S(6),
+                s7 = S(7), s8 = S(8), s9 = S(9);
+    const float b = __fadd_rn(__fadd_rn(__fmul_rn(s1, s1), __fmul_rn(s2, s2)),
+                              __fmul_rn(__fmul_rn(tau2, s3), s3));
+    const float c = __fadd_rn(__fadd_rn(__fmul_rn(s4, s4), __fmul_rn(s7, s7)),
+                              __fmul_rn(__fmul_rn(__fmul_rn(tau2, tau2), s9), s9));
+    const float d = __fadd_rn(__fadd_rn(__fmul_rn(s5, s5), __fmul_rn(__fmul_rn(tau2, s6), s6)),
+                              __fmul_rn(__fmul_rn(tau2, s8), s8));
+    double acc = __dsub_rn((double)__fmul_rn(s0, s0), __dmul_rn(2.0, (double)b));
+    acc = __dadd_rn(acc, (double)c);
+    acc = __dadd_rn(acc, __dmul_rn(2.0, (double)d));
+    const float num = (float)acc;
+    const float ev = __ldg(e + is), pv = __ldg(P + is);
+    float den;
+    if ((double)ev < 1.0e-5) den = (float)1.0e-5;
+    else den = (float)__dadd_rn((double)__fmul_rn(ev, ev), __dmul_rn(__dmul_rn(3.0, (double)pv), (double)pv));
+    rsh[is] = __fdiv_rn(__fsqrt_rn(fabsf(num)), __fsqrt_rn(fabsf(den)));
+  }
+  if (pdu || pmm) {
+    const float ut = __ldg(u + is), ux = -__ldg(u + n + is), uy = -__ldg(u + 2 * n + is);
+    const float un = __fmul_rn(__fmul_rn(-tau, tau), __ldg(u + 3 * n + is));
+    auto dot = [&](float a, float b2, float c2, float d2) {
+      return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a, ut), __fmul_rn(b2, ux)), __fmul_rn(c2, uy)),
+                       __fmul_rn(d2, un));
+    };
+    if (pdu) {
+      pdu[is] = dot(S(0), S(1), S(2), S(3));
+      pdu[n + is] = dot(S(1), S(4), S(5), S(6));
+      pdu[2 * n + is] = dot(S(2), S(5), S(7), S(8));
+      pdu[3 * n + is] = dot(S(3), S(6), S(8), S(9));
+    }
+    if (pmm) {
+      const float pxx = -S(4), pyy = -S(7), pnn = __fmul_rn(__fmul_rn(-tau, tau), S(9));
+      pmm[is] = __fadd_rn(__fadd_rn(__fadd_rn(S(0), pxx), pyy), pnn);
+    }
+  }
+  if (beta || om) {
+    float b[4] = {0.f, 0.f, 0.f, 0.f}, w_xy = 0.f;
+    if (is < (size_t)NX * NY) {
+      const int ix = (int)(is / NY), iy = (int)(is % NY);
+      if (ix >= 1 && ix < NX - 1 && iy >= 1 && iy < NY - 1) {
+        auto T = [&](size_t k) { return powf(__fdiv_rn(__ldg(e + k), 13.8997f), 0.25f); };
+        const size_t px = (size_t)NY * (ix + 1) + iy, mx = (size_t)NY * (ix - 1) + iy,
+                     py = (size_t)NY * ix + (iy + 1), my = (size_t)NY * ix + (iy - 1);
+        const float Tc = T(is);
+        b[0] = __fdiv_rn(__ldg(u + is), Tc);
+        b[1] = __fdiv_rn(-__ldg(u + n + is), Tc);
+        b[2] = __fdiv_rn(-__ldg(u + 2 * n + is), Tc);
+        b[3] = __fdiv_rn(0.0f, Tc);
+        const float bx_py = __fdiv_rn(-__ldg(u + n + py), T(py));
+        const float bx_my = __fdiv_rn(-__ldg(u + n + my), T(my));
+        const float by_px = __fdiv_rn(-__ldg(u + 2 * n + px), T(px));
+        const float by_mx = __fdiv_rn(-__ldg(u + 2 * n + mx), T(mx));
+        const double gy = __ddiv_rn(__ddiv_rn((double)__fsub_rn(bx_py, bx_my), 2.0), (double)DY);
+        const double gx = __ddiv_rn(__ddiv_rn((double)__fsub_rn(by_px, by_mx), 2.0), (double)DX);
+        w_xy = (float)__dmul_rn(0.5, __dsub_rn(gy, gx));
+      }
+    }
+    if (beta)
+      for (int m = 0; m < 4; ++m) beta[m * n + is] = b[m];
+    if (om)
+      for (int m = 0; m < 6; ++m) om[m * n + is] = (m == 3) ? w_xy : 0.0f;
+  }
 }
 
 }  // namespace fsm

@@ -51,6 +51,13 @@ void build_axis(int n, float d, float lo, std::vector<AxisNode>& ax) {
   }
 }
 
+float edep_dtau(const fsm_params& p, float numerator, float denominator) {
+  const float hbarc = 0.197326938;
+  float e_T = numerator / (denominator + 1.0e-7);  // src/FreeStream.cpp:411-415
+  e_T = e_T * hbarc;
+  return p.TAU_R * std::pow((e_T / p.E_R), p.ALPHA);
+}
+
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
                       std::string* why) {
   EventPlan& E = *out;
@@ -93,10 +100,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       numerator += (eps * eps);
       denominator += eps;
     }
-    float e_T = numerator / (denominator + 1.0e-7);
-    e_T = e_T * hbarc;
-    float tau_fs = p.TAU_R * std::pow((e_T / p.E_R), p.ALPHA);
-    p.DTAU = tau_fs;
+    p.DTAU = edep_dtau(p, numerator, denominator);
     p.TAU = p.TAU0 + p.DTAU;
   }
   if (!(p.TAU > 0)) return fail(FSM_ERR_INVALID_ARG, "TAU0 + DTAU must be > 0");

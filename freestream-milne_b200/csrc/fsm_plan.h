@@ -43,6 +43,11 @@ struct EventPlan {
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
                       std::string* why);
 
+// Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
+// reference's float sums of eps^2 and eps over the converted profile
+// (src/FreeStream.cpp:389-417).
+float edep_dtau(const fsm_params& p, float numerator, float denominator);
+
 // Natural-spline axis table of n float grid coordinates i*d + lo, with
 // kPadLo + kPadHi zero padding entries (entry k of the line at kPadLo + k).
 void build_axis(int n, float d, float lo, std::vector<AxisNode>& ax);

@@ -32,6 +32,10 @@ __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const CellBlock*, int, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
+__global__ void fsm_edep_sums_kernel(const float*, int, float*);
+__global__ void fsm_diag_kernel(int, int, int, float, float, float, const float*, const float*,
+                                const float*, const float*, const float*, float*, float*, float*,
+                                float*, float*, float*);
 }  // namespace fsm
 
 using namespace fsm;
@@ -744,6 +748,8 @@ extern "C" void fsm_ctx_destroy(fsm_ctx* ctx) {
   for (auto& t : ctx->pending)
     for (int k = 0; k < 4; ++k) cudaEventDestroy(t.ev[k]);
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->d_sums) cudaFree(ctx->d_sums);
+  if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -827,6 +833,24 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
   if (!ctx || !p || !d_e_gev || !dev_out) return FSM_ERR_INVALID_ARG;
   if (p->BARYON && !d_nB) return FSM_ERR_INVALID_ARG;
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  cudaStream_t st = pick_stream(ctx, stream);
+  fsm_params pe = *p;
+  if (pe.E_DEP_FS == 1) {
+    // the free-streaming time depends on the profile: its sums are taken on
+    // the device in the reference's order and read back before planning
+    fsm_params_derive(&pe);
+    if (pe.DIM <= 0) return FSM_ERR_INVALID_ARG;
+    if (!ctx->d_sums) {
+      FSM_CUDA_TRY(cudaMalloc(&ctx->d_sums, 2 * sizeof(float)));
+      FSM_CUDA_TRY(cudaMallocHost(&ctx->h_sums, 2 * sizeof(float)));
+    }
+    fsm_edep_sums_kernel<<<1, 32, 0, st>>>(d_e_gev, pe.DIM, ctx->d_sums);
+    FSM_CUDA_TRY(cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    FSM_CUDA_TRY(cudaStreamSynchronize(st));
+    pe.DTAU = edep_dtau(pe, ctx->h_sums[0], ctx->h_sums[1]);
+    pe.E_DEP_FS = 0;
+  }
+  p = &pe;
   EventPlan P;
   std::string why;
   fsm_status s = plan_event(*p, nullptr, &P, &why);
@@ -834,7 +858,6 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
     set_last_error(why);
     return s;
   }
-  cudaStream_t st = pick_stream(ctx, stream);
   fsm_batch* b = ctx->single_dev;
   const bool same_io = b && b->d_in_e[0] == d_e_gev && b->d_in_nB[0] == d_nB &&
                        std::memcmp(&b->d_out[0], dev_out, sizeof(fsm_outputs)) == 0;
@@ -961,4 +984,67 @@ extern "C" fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* str
 extern "C" fsm_status fsm_batch_check(fsm_batch* b) {
   if (!b) return FSM_ERR_INVALID_ARG;
   return check_kernel_errors(b);
+}
+
+// ============================================================ diagnostics
+extern "C" fsm_status fsm_diagnostics_device(const fsm_params* p, const fsm_outputs* in,
+                                             const fsm_diagnostics* out, void* stream) {
+  if (!p || !in || !out || !in->e || !in->P || !in->Pi || !in->u || !in->pi)
+    return FSM_ERR_INVALID_ARG;
+  const long long n = (long long)p->DIM_X * p->DIM_Y * p->DIM_ETA;
+  if (p->DIM_X < 1 || p->DIM_Y < 1 || p->DIM_ETA < 1 || n > (1ll << 30)) return FSM_ERR_INVALID_ARG;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int blocks = (int)((n + 255) / 256);
+  fsm_diag_kernel<<<blocks, 256, 0, s>>>(p->DIM_X, p->DIM_Y, p->DIM_ETA, p->DX, p->DY, p->TAU, in->e,
+                                         in->P, in->Pi, in->u, in->pi, out->R_Pi_Inv,
+                                         out->R_pimunu_Inv, out->pi_dot_u, out->pi_mu_mu, out->beta,
+                                         out->omega);
+  FSM_CUDA_TRY(cudaGetLastError());
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_diagnostics_host(fsm_ctx* ctx, const fsm_params* p, const fsm_outputs* hin,
+                                           const fsm_diagnostics* hout) {
+  if (!ctx || !p || !hin || !hout || !hin->e || !hin->P || !hin->Pi || !hin->u || !hin->pi)
+    return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)p->DIM_X * p->DIM_Y * p->DIM_ETA;
+  // inputs e P Pi u(4) pi(10), outputs 17 components
+  float* d = nullptr;
+  FSM_CUDA_TRY(cudaMalloc(&d, (17 + 17) * n * 4));
+  cudaStream_t st = ctx->stream;
+  fsm_status s = FSM_OK;
+  auto up = [&](float* dst, const float* src, size_t comps) {
+    if (cudaMemcpyAsync(dst, src, comps * n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      s = FSM_ERR_CUDA;
+  };
+  fsm_outputs din{};
+  din.e = d;
+  din.P = d + n;
+  din.Pi = d + 2 * n;
+  din.u = d + 3 * n;
+  din.pi = d + 7 * n;
+  up(din.e, hin->e, 1);
+  up(din.P, hin->P, 1);
+  up(din.Pi, hin->Pi, 1);
+  up(din.u, hin->u, 4);
+  up(din.pi, hin->pi, 10);
+  float* o = d + 17 * n;
+  fsm_diagnostics dout{o, o + n, o + 2 * n, o + 6 * n, o + 7 * n, o + 11 * n};
+  if (s == FSM_OK) s = fsm_diagnostics_device(p, &din, &dout, st);
+  auto down = [&](float* dst, const float* src, size_t comps) {
+    if (dst && s == FSM_OK &&
+        cudaMemcpyAsync(dst, src, comps * n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      s = FSM_ERR_CUDA;
+  };
+  down(hout->R_Pi_Inv, dout.R_Pi_Inv, 1);
+  down(hout->R_pimunu_Inv, dout.R_pimunu_Inv, 1);
+  down(hout->pi_dot_u, dout.pi_dot_u, 4);
+  down(hout->pi_mu_mu, dout.pi_mu_mu, 1);
+  down(hout->beta, dout.beta, 4);
+  down(hout->omega, dout.omega, 6);
+  if (cudaStreamSynchronize(st) != cudaSuccess && s == FSM_OK) s = FSM_ERR_CUDA;
+  cudaFree(d);
+  if (s != FSM_OK) set_last_error(std::string("fsm_diagnostics_host: ") + cudaGetErrorString(cudaGetLastError()));
+  return s;
 }

@@ -64,6 +64,9 @@ struct fsm_ctx {
   std::vector<fsm::rt::TimingSet> pending;
   std::vector<cudaEvent_t> event_pool;
   std::mutex mu;
+  // energy-dependent DTAU of device profiles: sums on the device, read back
+  float* d_sums = nullptr;
+  float* h_sums = nullptr;
   // cached one-event batches
   fsm_batch* single_host = nullptr;
   fsm_batch* single_dev = nullptr;

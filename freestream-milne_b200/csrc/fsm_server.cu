@@ -80,6 +80,7 @@ class Pool {
     }
     free_[off] = n;
   }
+  size_t used() const { return used_; }
 
  private:
   char* base_ = nullptr;
@@ -140,6 +141,7 @@ struct fsm_server {
   std::unordered_map<long long, Request*> reqs;
   long long next_id = 1;
   bool stopping = false;
+  bool mem_wait = false;  // admission waits for pool memory (a wave or a poll frees it)
   std::thread th;
   // statistics
   long long submitted = 0, completed = 0, failed = 0, waves = 0;
@@ -199,6 +201,8 @@ void drop_output(fsm_server* S, Request* r) {
   if (r->ob && --r->ob->refs == 0) {
     S->hpool.release(r->ob->p, r->ob->bytes);
     delete r->ob;
+    S->mem_wait = false;  // pinned memory came back: admission may proceed
+    S->cv.notify_all();
   }
   r->ob = nullptr;
   for (auto& g : r->grp) g = nullptr;
@@ -341,15 +345,14 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
     delete w;
     delete user;
     if (st == FSM_ERR_OUT_OF_MEMORY) {
-      bool busy = false;
-      for (Wave* x : S->slot_wave) busy = busy || (x != nullptr);
       if (take.size() > 1) {  // retry with the first half, requeue the rest in order
         const size_t h = take.size() / 2;
         for (size_t i = take.size(); i-- > h;) S->queue.push_front(take[i]);
         take.resize(h);
         continue;
       }
-      if (busy) {  // wait for memory to come back
+      if (S->dpool.used() != 0 || S->hpool.used() != 0) {
+        // memory is held by waves in flight or by outputs not yet polled: wait
         S->queue.push_front(take[0]);
         return false;
       }
@@ -375,7 +378,6 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
 void scheduler(fsm_server* S) {
   cudaSetDevice(S->ctx->device);
   std::unique_lock<std::mutex> lk(S->mu);
-  bool mem_wait = false;
   for (;;) {
     // retire completed waves
     for (size_t k = 0; k < S->slot_wave.size(); ++k) {
@@ -384,7 +386,7 @@ void scheduler(fsm_server* S) {
         wave_retire(S, w);
         delete w;
         S->slot_wave[k] = nullptr;
-        mem_wait = false;
+        S->mem_wait = false;
       }
     }
     bool inflight = false;
@@ -392,11 +394,11 @@ void scheduler(fsm_server* S) {
     if (S->stopping && S->queue.empty() && !inflight) break;
     // admit
     bool launched = false;
-    if (!mem_wait) {
+    if (!S->mem_wait) {
       for (size_t k = 0; k < S->slot_wave.size() && !S->queue.empty(); ++k) {
         if (S->slot_wave[k]) continue;
         if (!wave_launch(S, lk, (int)k)) {
-          mem_wait = true;
+          S->mem_wait = true;
           break;
         }
         launched = true;

@@ -88,6 +88,14 @@ class ServerStats(ctypes.Structure):
                 ("max_ms", ctypes.c_double), ("events_per_s", ctypes.c_double)]
 
 
+class Diagnostics(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in
+                ("R_Pi_Inv", "R_pimunu_Inv", "pi_dot_u", "pi_mu_mu", "beta", "omega")]
+
+
+DIAG_COMPS = {"R_Pi_Inv": 1, "R_pimunu_Inv": 1, "pi_dot_u": 4, "pi_mu_mu": 1, "beta": 4, "omega": 6}
+
+
 SIGNATURES = {
     "fsm_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "fsm_last_error": (ctypes.c_char_p, []),
@@ -121,6 +129,10 @@ SIGNATURES = {
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
     "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
                               ctypes.c_int]),
+    "fsm_diagnostics_device": (_ST, [ctypes.POINTER(Params), ctypes.POINTER(Outputs),
+                                     ctypes.POINTER(Diagnostics), _VP]),
+    "fsm_diagnostics_host": (_ST, [_VP, ctypes.POINTER(Params), ctypes.POINTER(Outputs),
+                                   ctypes.POINTER(Diagnostics)]),
     "fsm_server_start": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(ServerOpts)]),
     "fsm_server_submit": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP,
                                 ctypes.POINTER(ctypes.c_longlong)]),
@@ -248,6 +260,29 @@ class Context:
         check(lib().fsm_run_event(self.h, ctypes.byref(params), e_gev.ctypes.data, nb_ptr,
                                   ctypes.byref(o), ctypes.byref(info)), "fsm_run_event")
         arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
+        return arrs
+
+    def diagnostics(self, params, result):
+        """Hydro-validity and vorticity fields of a run_event result (TAU taken
+        from its info); returns {name: ndarray}."""
+        p = Params.from_buffer_copy(params)
+        F_ = lib()
+        F_.fsm_params_derive(ctypes.byref(p))
+        p.TAU = result["info"]["tau"]
+        dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        o = Outputs()
+        keep = []
+        for k in ("e", "P", "Pi", "u", "pi"):
+            a = np.ascontiguousarray(result[k], dtype=np.float32)
+            keep.append(a)
+            setattr(o, k, a.ctypes.data)
+        arrs, dg = {}, Diagnostics()
+        for k, c in DIAG_COMPS.items():
+            a = np.zeros((c, dim) if c > 1 else (dim,), dtype=np.float32)
+            arrs[k] = a
+            setattr(dg, k, a.ctypes.data)
+        check(F_.fsm_diagnostics_host(self.h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(dg)),
+              "fsm_diagnostics_host")
         return arrs
 
     def run_event_device(self, params, d_e, d_nB, dev_out, stream=None):

@@ -151,8 +151,9 @@ fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
                          const float* nB, const fsm_outputs* host_out, fsm_run_info* info);
 
 /* One event on device-resident buffers, enqueued on `stream`; returns without
- * synchronising.  E_DEP_FS=1 needs a host-visible profile and is rejected here
- * (use fsm_run_event). */
+ * synchronising, except with E_DEP_FS = 1: the free-streaming time depends on
+ * the profile, so its sums (src/FreeStream.cpp:389-417) are taken on the
+ * device and read back before the event is planned. */
 fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* d_e_gev,
                                 const float* d_nB, const fsm_outputs* dev_out, void* stream,
                                 fsm_run_info* info);
@@ -272,6 +273,28 @@ fsm_status fsm_server_release(fsm_server* s, long long id);
 fsm_status fsm_server_stats_get(fsm_server* s, fsm_server_stats* st);
 /* Finishes the waves in flight, cancels queued requests, frees everything. */
 fsm_status fsm_server_stop(fsm_server* s);
+
+/* ------------------------------------------------------------- diagnostics */
+/* Hydro-validity and thermal-vorticity fields of Landau-matched outputs, as the
+ * reference computes them before writing its *_projection / beta / w_xy files
+ * (src/HydroValidity.cpp:8-101, src/LandauMatch.cpp:395-489,
+ * src/FreestreamMilne.cpp:561-611).  Any field may be NULL. */
+typedef struct fsm_diagnostics {
+  float* R_Pi_Inv;      /* [DIM]     Pi / max(P, 1e-5)                          */
+  float* R_pimunu_Inv;  /* [DIM]     sqrt|pi_{mu nu} pi^{mu nu}| / sqrt(e^2+3P^2) */
+  float* pi_dot_u;      /* [4][DIM]  pi^{mu nu} u_nu                            */
+  float* pi_mu_mu;      /* [DIM]     pi^mu_mu                                   */
+  float* beta;          /* [4][DIM]  u_mu / T on interior (ix, iy), else 0      */
+  float* omega;         /* [6][DIM]  thermal vorticity; only w_xy is non-zero   */
+} fsm_diagnostics;
+
+/* From device outputs (e, P, Pi, u, pi of fsm_outputs) on `stream`; p->TAU is
+ * the Landau-matching time (fsm_run_info.tau). */
+fsm_status fsm_diagnostics_device(const fsm_params* p, const fsm_outputs* dev_in,
+                                  const fsm_diagnostics* dev_out, void* stream);
+/* Same from host arrays (copied to the device and back; synchronous). */
+fsm_status fsm_diagnostics_host(fsm_ctx* ctx, const fsm_params* p, const fsm_outputs* host_in,
+                                const fsm_diagnostics* host_out);
 
 /* ------------------------------------------------------------- text output */
 /* One per-cell field in the reference's text formats (src/FileIO.cpp:11-131,

@@ -509,3 +509,61 @@ extern "C" int oracle_eig(int n, const double* A, double* wr, double* wi, double
 extern "C" int oracle_landau_cell(const float* T10, float tau, float* e, float* u4) {
   return landau_cell<float>(T10, tau, e, u4);
 }
+
+// ---- diagnostics: restated from src/HydroValidity.cpp:8-101 and
+// src/LandauMatch.cpp:395-489 with the reference's float/double mixing.
+extern "C" void oracle_diagnostics(const oracle_params* p, float tau, const float* e,
+                                   const float* P, const float* Pi, const float* u,
+                                   const float* pi, float* out) {
+  const int NX = p->DIM_X, NY = p->DIM_Y, NE = p->DIM_ETA;
+  const size_t n = (size_t)NX * NY * NE;
+  for (size_t k = 0; k < 17 * n; ++k) out[k] = 0.0f;
+  float* rpi = out;
+  float* rsh = out + n;
+  float* pdu = out + 2 * n;
+  float* pmm = out + 6 * n;
+  float* beta = out + 7 * n;
+  float* om = out + 11 * n;
+  const float tau2 = tau * tau;
+  for (size_t is = 0; is < n; ++is) {
+    // bulk inverse Reynolds number (HydroValidity.cpp:8-19)
+    float pp = (P[is] < 1.0e-5) ? 1.0e-5 : P[is];
+    rpi[is] = Pi[is] / pp;
+    // shear inverse Reynolds number (HydroValidity.cpp:21-38)
+    const float* s = pi;
+    auto S = [&](int m) { return s[m * n + is]; };
+    float num = S(0) * S(0) - 2.0 * (S(1) * S(1) + S(2) * S(2) + tau2 * S(3) * S(3)) +
+                (S(4) * S(4) + S(7) * S(7) + tau2 * tau2 * S(9) * S(9)) +
+                2.0 * (S(5) * S(5) + tau2 * S(6) * S(6) + tau2 * S(8) * S(8));
+    float den;
+    if (e[is] < 1.0e-5) den = 1.0e-5;
+    else den = e[is] * e[is] + 3.0 * P[is] * P[is];
+    rsh[is] = std::sqrt(std::fabs(num)) / std::sqrt(std::fabs(den));
+    // pi^{mu nu} u_nu (HydroValidity.cpp:40-79)
+    float ut = u[is], ux = -u[n + is], uy = -u[2 * n + is], un = -tau * tau * u[3 * n + is];
+    pdu[is] = S(0) * ut + S(1) * ux + S(2) * uy + S(3) * un;
+    pdu[n + is] = S(1) * ut + S(4) * ux + S(5) * uy + S(6) * un;
+    pdu[2 * n + is] = S(2) * ut + S(5) * ux + S(7) * uy + S(8) * un;
+    pdu[3 * n + is] = S(3) * ut + S(6) * ux + S(8) * uy + S(9) * un;
+    // pi^mu_mu (HydroValidity.cpp:81-101)
+    float pxx = -S(4), pyy = -S(7), pnn = -tau * tau * S(9);
+    pmm[is] = S(0) + pxx + pyy + pnn;
+  }
+  // thermal velocity and vorticity (LandauMatch.cpp:395-489): interior (ix, iy),
+  // cell index DIM_Y * ix + iy as in the reference
+  auto T = [&](size_t k) { return std::pow((e[k] / 13.8997f), 0.25f); };
+  for (int ix = 1; ix < NX - 1; ++ix)
+    for (int iy = 1; iy < NY - 1; ++iy) {
+      const size_t is = (size_t)NY * ix + iy, px = (size_t)NY * (ix + 1) + iy,
+                   mx = (size_t)NY * (ix - 1) + iy, py = (size_t)NY * ix + (iy + 1),
+                   my = (size_t)NY * ix + (iy - 1);
+      float Tc = T(is), Tpx = T(px), Tmx = T(mx), Tpy = T(py), Tmy = T(my);
+      beta[is] = u[is] / Tc;
+      beta[n + is] = -u[n + is] / Tc;
+      beta[2 * n + is] = -u[2 * n + is] / Tc;
+      beta[3 * n + is] = 0.0f / Tc;
+      float bx_py = -u[n + py] / Tpy, bx_my = -u[n + my] / Tmy;
+      float by_px = -u[2 * n + px] / Tpx, by_mx = -u[2 * n + mx] / Tmx;
+      om[3 * n + is] = 0.5 * ((bx_py - bx_my) / 2.0 / p->DY - (by_px - by_mx) / 2.0 / p->DX);
+    }
+}

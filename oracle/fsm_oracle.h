@@ -95,6 +95,13 @@ int oracle_eig(int n, const double* A, double* wr, double* wi, double* vr);
  * T^{mu nu} components; returns 1 if an eigenvector was accepted. */
 int oracle_landau_cell(const float* T10, float tau, float* e, float* u4);
 
+/* Hydro-validity and thermal-vorticity diagnostics of the Landau-matched
+ * fields (src/HydroValidity.cpp:8-101, src/LandauMatch.cpp:395-489) at
+ * proper time tau: out has 17 components of DIM floats: R_Pi_Inv,
+ * R_pimunu_Inv, pi.u (4), pi^mu_mu, beta (4), omega (6). */
+void oracle_diagnostics(const oracle_params* p, float tau, const float* e, const float* P,
+                        const float* Pi, const float* u, const float* pi, float* out17);
+
 #ifdef __cplusplus
 }
 #endif

@@ -188,3 +188,20 @@ def landau_cell(T10, tau):
     ok = lib().oracle_landau_cell(T10.ctypes.data, ctypes.c_float(tau), e.ctypes.data,
                                   u.ctypes.data)
     return ok, float(e[0]), u
+
+
+DIAG_NAMES = ["R_Pi_Inv", "R_pimunu_Inv", "pi_dot_u", "pi_mu_mu", "beta", "omega"]
+DIAG_COMPS = {"R_Pi_Inv": 1, "R_pimunu_Inv": 1, "pi_dot_u": 4, "pi_mu_mu": 1, "beta": 4, "omega": 6}
+
+
+def diagnostics(p, tau, e, P, Pi, u, pi, impl="oracle"):
+    """Hydro-validity and vorticity diagnostics (17 x DIM floats) of the
+    oracle's restatement or of the reference's own functions."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float32).ravel() for a in (e, P, Pi, u, pi)]
+    n = arrs[0].size
+    out = np.zeros(17 * n, np.float32)
+    fn = (lib().oracle_diagnostics if impl == "oracle" else ref().ref_diagnostics)
+    fn.argtypes = [ctypes.POINTER(Params), ctypes.c_float] + [ctypes.c_void_p] * 6
+    fn.restype = None
+    fn(ctypes.byref(p), ctypes.c_float(tau), *[a.ctypes.data for a in arrs], out.ctypes.data)
+    return out.reshape(17, n)

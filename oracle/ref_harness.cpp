@@ -166,3 +166,35 @@ extern "C" int ref_run_full(const char* workdir, const float* e_gev, int n, doub
   if (chdir(old) != 0) return 3;
   return rc;
 }
+
+// The reference's own diagnostic functions (src/HydroValidity.cpp:8-101,
+// src/LandauMatch.cpp:395-489) on given Landau-matched fields; out as
+// oracle_diagnostics.
+extern "C" void ref_diagnostics(const oracle_params* pin, float tau, const float* e, const float* P,
+                                const float* Pi, const float* u, const float* pi, float* out) {
+  parameters params;
+  std::memcpy(&params, pin, sizeof(params));
+  params.DIM = params.DIM_X * params.DIM_Y * params.DIM_ETA;
+  params.TAU = tau;
+  const int n = params.DIM;
+  std::vector<float> ev(e, e + n), Pv(P, P + n), Piv(Pi, Pi + n);
+  float** uu = calloc2dArrayf(nullptr, 4, n);
+  float** sh = calloc2dArrayf(nullptr, 10, n);
+  for (int m = 0; m < 4; ++m) std::memcpy(uu[m], u + (size_t)m * n, n * 4);
+  for (int m = 0; m < 10; ++m) std::memcpy(sh[m], pi + (size_t)m * n, n * 4);
+  float* o = out;
+  std::fill(o, o + (size_t)17 * n, 0.0f);
+  calculateBulkInvReynolds(Pv.data(), Piv.data(), o, params);
+  calculateShearInvReynolds(ev.data(), Pv.data(), sh, o + n, params);
+  calculate_pi_dot_u(uu, sh, o + 2 * n, o + 3 * n, o + 4 * n, o + 5 * n, params);
+  calculate_pi_mu_mu(sh, o + 6 * n, params);
+  float** beta = calloc2dArrayf(nullptr, 4, n);
+  float** om = calloc2dArrayf(nullptr, 6, n);
+  calculateThermalVorticityTensor(ev.data(), uu, beta, om, params);
+  for (int m = 0; m < 4; ++m) std::memcpy(o + (size_t)(7 + m) * n, beta[m], n * 4);
+  for (int m = 0; m < 6; ++m) std::memcpy(o + (size_t)(11 + m) * n, om[m], n * 4);
+  free2dArrayf(uu, 4);
+  free2dArrayf(sh, 10);
+  free2dArrayf(beta, 4);
+  free2dArrayf(om, 6);
+}

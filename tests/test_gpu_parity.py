@@ -140,6 +140,52 @@ def test_energy_dependent_tau(ctx):
     compare_parity(got, ref, O.run(oracle_params(d), e, fp64=2), meta[2])
 
 
+def test_energy_dependent_tau_device_entry(ctx):
+    """E_DEP_FS with a device-resident profile: the device sums reproduce the
+    reference's float running sums, so DTAU and every output match the host
+    entry point's (and the reference's DTAU) exactly."""
+    import torch
+    d, e, nB, ref, meta = load_golden("edepfs2d_45")
+    p = fsm_params(d)
+    host = ctx.run_event(p, e)
+    dim = e.size
+    d_e = torch.from_numpy(np.ascontiguousarray(e)).cuda()
+    outs = {k: torch.zeros((F.OUT_COMPS[k] * dim,), dtype=torch.float32, device="cuda")
+            for k in ("T", "e", "P", "Pi", "u", "pi")}
+    info = ctx.run_event_device(p, d_e.data_ptr(), None, {k: v.data_ptr() for k, v in outs.items()},
+                                stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert info["dtau"] == float(meta[1]) == host["info"]["dtau"]
+    for k, v in outs.items():
+        assert np.array_equal(v.cpu().numpy().reshape(host[k].shape), host[k]), k
+
+
+@pytest.mark.parametrize("case", ["lumpy2d", "baryon3d"])
+def test_gpu_diagnostics(ctx, case):
+    """Hydro-validity and vorticity fields on the GPU against the oracle's
+    restatement (itself bit-exact with the reference's functions) on the same
+    matched fields."""
+    if case == "lumpy2d":
+        p, e, nB = W.lumpy2d(seed=2, side=91, dx=0.08, nphip=64, dtau=0.8, eos=2, radius=3.0)
+    else:
+        p, e, nB = W.baryon3d(seed=5, side=31, neta=15, nrap=11, nphip=24)
+    got = ctx.run_event(p, e, nB)
+    dg = ctx.diagnostics(p, got)
+    po = O.Params(**p.as_dict())
+    po.DIM = p.DIM_X * p.DIM_Y * p.DIM_ETA
+    ref = O.diagnostics(po, got["info"]["tau"], got["e"], got["P"], got["Pi"], got["u"], got["pi"])
+    off = 0
+    for k, c in F.DIAG_COMPS.items():
+        a = np.asarray(dg[k], np.float32).reshape(c, -1)
+        b = ref[off:off + c]
+        off += c
+        if k in ("beta", "omega"):  # powf of the temperature may differ by an ulp
+            scale = np.abs(b).max() + 1e-30
+            assert np.max(np.abs(a - b)) <= 1e-5 * scale, k
+        else:
+            np.testing.assert_array_equal(a, b, err_msg=k)
+
+
 def test_invalid_inputs_are_rejected(ctx):
     p = F.default_params(DIM_X=3)
     with pytest.raises(F.FsmError):

@@ -128,3 +128,19 @@ def test_2d_conformal_trace_and_energy():
     before = e_fm.sum() * dx * dx
     after = r["tau"] * T[0].sum() * dx * dx
     assert abs(after / before - 1) < 2e-3
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("name", ["lumpy2d_wb_61x53", "baryon3d_25x23x15"])
+def test_diagnostics_match_reference(name):
+    """The diagnostics restatement (hydro validity, thermal vorticity) against
+    the reference's own functions on the reference's Landau-matched fields:
+    bit for bit."""
+    d, e, nB, ref, meta = load_golden(name)
+    p = oracle_params(d)
+    p.DIM = p.DIM_X * p.DIM_Y * p.DIM_ETA
+    args = (p, float(np.float32(meta[2])), ref["e"], ref["P"], ref["Pi"], ref["u"], ref["pi"])
+    a = O.diagnostics(*args, impl="oracle")
+    b = O.diagnostics(*args, impl="ref")
+    np.testing.assert_array_equal(a, b)
+    assert np.isfinite(a).all() and np.abs(a[1]).max() > 0
