@@ -108,7 +108,8 @@ struct Chunk2D {
 FSM_HDI int win_h(const Chunk2D& c) { return kTileX + (c.ox1 - c.ox0) + 3; }
 FSM_HDI int win_w(const Chunk2D& c) { return kTileY + (c.oy1 - c.oy0) + 3; }
 constexpr int kMaxChunks2D = 64;
-constexpr int kWindowBudget2D = 32 * 1024;  // bytes of one staged window
+constexpr int kWindowBudget2D = 32 * 1024;  // bytes of one staged window (default)
+constexpr int kMaxWindow2D = 64 * 1024;     // largest staged window the planner raises to
 constexpr int kTotSlots2D = 5 * 4;          // per-thread moment totals kept in shared memory
 
 struct Ev2D {

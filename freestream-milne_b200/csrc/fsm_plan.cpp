@@ -59,7 +59,7 @@ float edep_dtau(const fsm_params& p, float numerator, float denominator) {
 }
 
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why) {
+                      std::string* why, int window_budget) {
   EventPlan& E = *out;
   E = EventPlan();
   fsm_params p = in;
@@ -168,12 +168,15 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
     }
     // phi_p runs whose staged window (tile + offset spread + 1-node margins)
-    // fits the window budget; consecutive nodes have neighbouring offsets
-    {
+    // fits the window budget; consecutive nodes have neighbouring offsets.  A
+    // budget that would need more than kMaxChunks2D runs is raised (a tuned
+    // small window must not make long free-streaming distances unplannable).
+    for (int budget = window_budget;; budget = budget * 3 / 2) {
       auto win_bytes = [](int dox, int doy) {
         return (size_t)(kTileX + dox + 3) * (size_t)(kTileY + doy + 3) * 16;
       };
       E.chunks2.clear();
+      E.boxW = E.boxH = E.box_elems = 0;
       int p0 = 0;
       auto oy_of = [&](int k) { return (int)(short)(E.tab2[k].oy_near & 0xffff); };
       int lo_x = E.tab2[0].ox, hi_x = lo_x, lo_y = oy_of(0), hi_y = lo_y;
@@ -184,7 +187,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
         if (!flush) {
           int nlx = std::min(lo_x, E.tab2[k].ox), nhx = std::max(hi_x, E.tab2[k].ox);
           int nly = std::min(lo_y, oy_of(k)), nhy = std::max(hi_y, oy_of(k));
-          if (win_bytes(nhx - nlx, nhy - nly) > (size_t)kWindowBudget2D) {
+          if (win_bytes(nhx - nlx, nhy - nly) > (size_t)budget) {
             flush = true;
           } else {
             lo_x = nlx; hi_x = nhx; lo_y = nly; hi_y = nhy;
@@ -208,7 +211,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
           E.oy_max = std::max(E.oy_max, oy_of(k));
         }
       }
-      if ((int)E.chunks2.size() > kMaxChunks2D || E.boxW > 256 || E.boxH > 256)
+      if ((int)E.chunks2.size() <= kMaxChunks2D && E.boxW <= 256 && E.boxH <= 256) break;
+      if ((int)E.chunks2.size() <= kMaxChunks2D || budget > kMaxWindow2D)
         return fail(FSM_ERR_TOO_LARGE, "free-streaming distance too large for the staged windows");
     }
     E.Rx = (int)std::ceil(p.DTAU / p.DX) + 2;

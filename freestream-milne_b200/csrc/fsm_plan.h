@@ -39,9 +39,11 @@ struct EventPlan {
 
 // Validates `in`, applies the energy-dependent free-streaming time (needs the
 // host profile; pass NULL to reject E_DEP_FS=1) and the phi_p arc-length rule,
-// and fills the tables.  Returns FSM_OK or an error with a message in *why.
+// and fills the tables; 2D phi_p runs are cut so that each run's staged window
+// stays within window_budget bytes.  Returns FSM_OK or an error with a message
+// in *why.
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why);
+                      std::string* why, int window_budget = kWindowBudget2D);
 
 // Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
 // reference's float sums of eps^2 and eps over the converted profile

@@ -101,7 +101,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->plans.resize(n);
   for (int i = 0; i < n; ++i) {
     std::string why;
-    fsm_status s = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why);
+    fsm_status s = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why,
+                              ctx->window_budget);
     if (s != FSM_OK) {
       set_last_error("event " + std::to_string(i) + ": " + why);
       return s;
@@ -786,7 +787,7 @@ extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const flo
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
   EventPlan P;
   std::string why;
-  fsm_status s = plan_event(*p, e_gev, &P, &why);
+  fsm_status s = plan_event(*p, e_gev, &P, &why, ctx->window_budget);
   if (s != FSM_OK) {
     set_last_error(why);
     return s;
@@ -853,7 +854,7 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
   p = &pe;
   EventPlan P;
   std::string why;
-  fsm_status s = plan_event(*p, nullptr, &P, &why);
+  fsm_status s = plan_event(*p, nullptr, &P, &why, ctx->window_budget);
   if (s != FSM_OK) {
     set_last_error(why);
     return s;
@@ -1047,4 +1048,86 @@ extern "C" fsm_status fsm_diagnostics_host(fsm_ctx* ctx, const fsm_params* p, co
   cudaFree(d);
   if (s != FSM_OK) set_last_error(std::string("fsm_diagnostics_host: ") + cudaGetErrorString(cudaGetLastError()));
   return s;
+}
+
+// ============================================================== autotuning
+extern "C" fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t) {
+  if (!ctx || !t) return FSM_ERR_INVALID_ARG;
+  const int minimum = (kTileX + 3) * (kTileY + 3) * 16;
+  if (t->window_bytes < minimum || t->window_bytes > 96 * 1024) {
+    set_last_error("fsm_ctx_set_tuning: window_bytes outside [" + std::to_string(minimum) + ", 98304]");
+    return FSM_ERR_INVALID_ARG;
+  }
+  ctx->window_budget = t->window_bytes;
+  // cached one-event batches were planned with the old windows
+  batch_free(ctx->single_host);
+  ctx->single_host = nullptr;
+  batch_free(ctx->single_dev);
+  ctx->single_dev = nullptr;
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_autotune(fsm_ctx* ctx, int n, const fsm_params* params,
+                                   const float* const* host_e, const float* const* host_nB,
+                                   fsm_tuning* out) {
+  if (!ctx || n <= 0 || !params || !out) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  static const int cand_kb[] = {20, 24, 28, 32, 40, 48};
+  const int saved = ctx->window_budget;
+  double best_ms = 0.0;
+  int best = saved;
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t e0, e1;
+  FSM_CUDA_TRY(cudaEventCreate(&e0));
+  FSM_CUDA_TRY(cudaEventCreate(&e1));
+  fsm_status status = FSM_OK;
+  for (int kb : cand_kb) {
+    ctx->window_budget = kb * 1024;
+    fsm_batch* b = nullptr;
+    fsm_status s = batch_build(ctx, n, params, host_e, nullptr, nullptr, nullptr, &b);
+    if (s != FSM_OK) {
+      batch_free(b);
+      continue;  // e.g. too many runs for this window: not a candidate
+    }
+    // inputs: the caller's profiles (or zeros) in the batch's own input slab
+    for (int i = 0; i < n && host_e; ++i) {
+      const size_t dim = (size_t)b->plans[i].DIM;
+      cudaMemcpyAsync(b->d_in_e[i], host_e[i], dim * 4, cudaMemcpyHostToDevice, st);
+      if (b->plans[i].baryon && host_nB && host_nB[i])
+        cudaMemcpyAsync(b->d_in_nB[i], host_nB[i], dim * 4, cudaMemcpyHostToDevice, st);
+    }
+    if (!host_e) cudaMemsetAsync(b->d_mem + b->in_slab_off, 0, b->in_slab_bytes, st);
+    double ms = 0.0;
+    for (int rep = 0; rep < 4 && s == FSM_OK; ++rep) {
+      cudaEventRecord(e0, st);
+      s = enqueue(b, st, false);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) s = FSM_ERR_CUDA;
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep >= 1) ms += t;  // the first launch warms up
+    }
+    if (s == FSM_OK) s = check_kernel_errors(b);
+    batch_free(b);
+    if (s != FSM_OK) {
+      status = s;
+      break;
+    }
+    ms /= 3.0;
+    if (best_ms == 0.0 || ms < best_ms) {
+      best_ms = ms;
+      best = kb * 1024;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->window_budget = saved;
+  if (status != FSM_OK) return status;
+  if (best_ms == 0.0) {
+    set_last_error("fsm_autotune: no candidate window could be planned");
+    return FSM_ERR_INVALID_ARG;
+  }
+  out->window_bytes = best;
+  out->ms = best_ms;
+  return fsm_ctx_set_tuning(ctx, out);
 }

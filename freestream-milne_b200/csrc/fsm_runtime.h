@@ -64,6 +64,7 @@ struct fsm_ctx {
   std::vector<fsm::rt::TimingSet> pending;
   std::vector<cudaEvent_t> event_pool;
   std::mutex mu;
+  int window_budget = fsm::kWindowBudget2D;  // staged window of a 2D phi_p run (autotuned)
   // energy-dependent DTAU of device profiles: sums on the device, read back
   float* d_sums = nullptr;
   float* h_sums = nullptr;

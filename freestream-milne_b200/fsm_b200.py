@@ -71,6 +71,10 @@ class Timing(ctypes.Structure):
 # Every symbol include/fsm.h declares, with (restype, argtypes).
 _VP = ctypes.c_void_p
 _ST = ctypes.c_int
+class Tuning(ctypes.Structure):
+    _fields_ = [("window_bytes", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
                 ("host_budget_bytes", ctypes.c_size_t), ("max_wave_events", ctypes.c_int),
@@ -133,6 +137,9 @@ SIGNATURES = {
                                      ctypes.POINTER(Diagnostics), _VP]),
     "fsm_diagnostics_host": (_ST, [_VP, ctypes.POINTER(Params), ctypes.POINTER(Outputs),
                                    ctypes.POINTER(Diagnostics)]),
+    "fsm_autotune": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(_VP),
+                           ctypes.POINTER(_VP), ctypes.POINTER(Tuning)]),
+    "fsm_ctx_set_tuning": (_ST, [_VP, ctypes.POINTER(Tuning)]),
     "fsm_server_start": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(ServerOpts)]),
     "fsm_server_submit": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP,
                                 ctypes.POINTER(ctypes.c_longlong)]),
@@ -261,6 +268,30 @@ class Context:
                                   ctypes.byref(o), ctypes.byref(info)), "fsm_run_event")
         arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
         return arrs
+
+    def autotune(self, params_list, inputs=None):
+        """Times the candidate staged-window sizes on these events (inputs: list
+        of (e, nB) or None for zeros) and keeps the fastest for this context."""
+        n = len(params_list)
+        arr = (Params * n)(*params_list)
+        keep, pe, pn = [], None, None
+        if inputs is not None:
+            pe, pn = (_VP * n)(), (_VP * n)()
+            for i, (e, nb) in enumerate(inputs):
+                a = np.ascontiguousarray(e, dtype=np.float32).ravel()
+                keep.append(a)
+                pe[i] = a.ctypes.data
+                if nb is not None:
+                    b = np.ascontiguousarray(nb, dtype=np.float32).ravel()
+                    keep.append(b)
+                    pn[i] = b.ctypes.data
+        t = Tuning()
+        check(lib().fsm_autotune(self.h, n, arr, pe, pn, ctypes.byref(t)), "fsm_autotune")
+        return {"window_bytes": t.window_bytes, "ms": t.ms}
+
+    def set_tuning(self, window_bytes):
+        t = Tuning(int(window_bytes), 0.0)
+        check(lib().fsm_ctx_set_tuning(self.h, ctypes.byref(t)), "fsm_ctx_set_tuning")
 
     def diagnostics(self, params, result):
         """Hydro-validity and vorticity fields of a run_event result (TAU taken

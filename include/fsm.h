@@ -210,6 +210,23 @@ double fsm_batch_samples(fsm_batch* b);
 fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
                                     const fsm_outputs* dev_out, void* stream);
 
+/* ------------------------------------------------------------- autotuning */
+/* Launch-shape tuning of a context (no counterpart in the reference).  The 2D
+ * stream kernel stages, per output tile, one source window per run of
+ * consecutive phi_p; window_bytes bounds a window (larger windows: fewer runs
+ * and barriers, more shared memory per block and possibly fewer blocks per
+ * SM).  fsm_autotune times the full launch sequence of the given events for a
+ * set of candidate sizes, keeps the fastest for every later batch and event of
+ * ctx and returns it; the result can be stored and restored with
+ * fsm_ctx_set_tuning.  host_e / host_nB may be NULL (zero profiles). */
+typedef struct fsm_tuning {
+  int window_bytes;  /* staged window bound of a 2D phi_p run (default 32768)   */
+  double ms;         /* measured launch-sequence time with it (fsm_autotune)    */
+} fsm_tuning;
+fsm_status fsm_autotune(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
+                        const float* const* host_nB, fsm_tuning* out);
+fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t);
+
 /* ---------------------------------------------------------- request server */
 /* No counterpart in the reference, which computes one event per call.  A
  * continuous-batching server: fsm_server_submit queues one event (host

@@ -186,6 +186,26 @@ def test_gpu_diagnostics(ctx, case):
             np.testing.assert_array_equal(a, b, err_msg=k)
 
 
+def test_autotune_keeps_results():
+    """The autotuner only changes launch shapes: results with the tuned window
+    equal those with the default, bit for bit."""
+    evs = [W.lumpy2d(seed=30 + k, side=81 + 20 * k, dx=0.07, nphip=64, dtau=0.5 + 0.4 * k,
+                     eos=1 + k % 2, radius=2.5) for k in range(3)]
+    base = F.Context(0)
+    ref = [base.run_event(p, e) for p, e, _ in evs]
+    base.close()
+    c = F.Context(0)
+    t = c.autotune([p for p, _, _ in evs], [(e, nb) for _, e, nb in evs])
+    assert 20 * 1024 <= t["window_bytes"] <= 48 * 1024 and t["ms"] > 0
+    for k in (20 * 1024, 48 * 1024):  # 20 KB: the planner raises it where runs would be too many
+        c.set_tuning(k)
+        for (p, e, _), r in zip(evs, ref):
+            got = c.run_event(p, e)
+            for name in ("T", "e", "u", "pi"):
+                np.testing.assert_array_equal(got[name], r[name], err_msg=f"{k} {name}")
+    c.close()
+
+
 def test_invalid_inputs_are_rejected(ctx):
     p = F.default_params(DIM_X=3)
     with pytest.raises(F.FsmError):
