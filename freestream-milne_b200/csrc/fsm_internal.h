@@ -156,6 +156,22 @@ struct RapEta {
   float E;      // tanh(d)^2/TAU^2                          (row 9)
 };
 
+// Per-(ieta, irap, phi_p) entry of the 3D stream table (host computed): with
+// the reference's float shift s = fl(cos(phi_p) * D), the source point of cell
+// ix is ix + sx, sx = -s/DX, split into the integer offset ox = floor(sx) and
+// the fraction t (likewise y), and flags telling whether t or u lies within
+// 1e-3 of an integer.
+struct PhiEntry3D {
+  float t, u;
+  int ox;
+  int oy_near;  // low 16 bits: oy (signed); bit 16: near in x; bit 17: near in y
+};
+
+// A 3D output tile: 32 x 32 cells of one eta slice of one event.
+struct Tile3D {
+  int ev, x0, y0, ieta;
+};
+
 struct Ev3D {
   int NX, NY, NE, NR, NPHI;
   int r_lo, r_hi;  // live rapidity nodes [r_lo, r_hi)
@@ -169,9 +185,11 @@ struct Ev3D {
   const float* rapf;      // [NE*NR] energy rapidity weight  cosh^2 d exp(-d^2/2 sigma^2)
   const float* rapfB;     // [NE*NR] baryon weight on the uniform rapidity grid
   const float* jac;       // [NR] tan-map Jacobian (src/LandauMatch.cpp:92-93)
+  const PhiEntry3D* tab3; // [NE*NR*NPHI]
   const float* e_gev;     // input
-  float* efield;          // converted energy density (fm^-4)
+  float* efield;          // converted energy density (fm^-4), eta-slice major [NE][NX][NY]
   const float* nB;        // input baryon density
+  float* bfield;          // baryon density, eta-slice major [NE][NX][NY]
   float* T;               // [10][DIM]
   float* J;               // [4][DIM]
   long long cell_begin;   // first global cell index of this event in the 3D work list

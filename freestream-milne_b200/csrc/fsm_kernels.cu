@@ -34,12 +34,6 @@ __device__ __forceinline__ float F_of(float e_gev) {
   return (float)(__ddiv_rn((double)to_fm4(e_gev), 6.283185307179586));
 }
 
-__device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
-  float y = __fsub_rn(x, comp);
-  float t = __fadd_rn(sum, y);
-  comp = __fsub_rn(__fsub_rn(t, sum), y);
-  sum = t;
-}
 
 // ------------------------------------------------------------------ prep 2D
 // Strip kernels: a block owns 32 lines of one event and stages them whole in
@@ -265,7 +259,14 @@ __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict_
   const Ev3D& ev = evs[b.ev];
   const int DIM = ev.NX * ev.NY * ev.NE;
   const int is = b.begin + threadIdx.x;
-  if (is < DIM) ev.efield[is] = to_fm4(__ldg(ev.e_gev + is));
+  if (is >= DIM) return;
+  // eta-slice-major copies: slice ieta is a contiguous NX x NY plane, so the
+  // stream kernel's lanes (consecutive y) read consecutive addresses
+  const int NE = ev.NE, NYE = ev.NY * NE;
+  const int ix = is / NYE, iy = (is - ix * NYE) / NE, ieta = is - ix * NYE - iy * NE;
+  const size_t dst = ((size_t)ieta * ev.NX + ix) * ev.NY + iy;
+  ev.efield[dst] = to_fm4(__ldg(ev.e_gev + is));
+  if (ev.baryon) ev.bfield[dst] = __ldg(ev.nB + is);
 }
 
 // ---------------------------------------------------------------- stream 2D
@@ -675,147 +676,265 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
 }
 
 // ---------------------------------------------------------------- stream 3D
-// One thread per cell; cells of a CTA are consecutive in the reference order
-// (eta fastest), so the trilinear corner loads of a warp are coalesced.
-__global__ void __launch_bounds__(kThreads3D) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
-                                                                  const CellBlock* __restrict__ blocks,
-                                                                  int nblocks, int cs_cap,
-                                                                  Counters* ctr) {
-  extern __shared__ float4 smem4[];
-  __shared__ int s_blk;
-  float2* scs = reinterpret_cast<float2*>(smem4);
-  for (;;) {
-    if (threadIdx.x == 0) s_blk = atomicAdd(&ctr->block3d, 1);
-    __syncthreads();
-    const int bi = s_blk;
-    if (bi >= nblocks) return;
-    const CellBlock b = blocks[bi];
-    const Ev3D& ev = evs[b.ev];
-    const int NPHI = ev.NPHI;
-    for (int k = threadIdx.x; k < NPHI; k += blockDim.x) {
-      const FSM_FLOAT2 c = ev.cs[k];
-      scs[k] = make_float2(c.x, c.y);
+// One sample with the reference's own float arithmetic (src/FreeStream.cpp:
+// 193-276): shifted point, correctly rounded index division, in-grid test and
+// trilinear interpolation (the eta fraction and slice from the host table).
+// Used for the rare samples whose in-grid decision depends on the rounding.
+// Returns false for a sample outside the grid.
+__device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const float* __restrict__ P0,
+                                               const float* __restrict__ Q0, float x, float y,
+                                               float c, float s, float D, float et, float rf0,
+                                               float rf1, float rb0, float rb1, float& v, float& vb) {
+  const int NX = ev.NX, NY = ev.NY;
+  const float xn = __fsub_rn(x, __fmul_rn(c, D));
+  const float yn = __fsub_rn(y, __fmul_rn(s, D));
+  const float qx = __fdiv_rn(__fsub_rn(xn, ev.xmin), ev.DX);
+  const float qy = __fdiv_rn(__fsub_rn(yn, ev.ymin), ev.DY);
+  const float fx = floorf(qx), fy = floorf(qy);
+  if (!(fx >= 1.0f && fx < (float)(NX - 1) && fy >= 1.0f && fy < (float)(NY - 1))) return false;
+  const int i = (int)fx, j = (int)fy;
+  const float t = qx - fx, u = qy - fy;
+  const size_t plane = (size_t)NX * NY, k = (size_t)i * NY + j;
+  auto lin = [&](const float* a) {
+    return (1.0f - t) * (1.0f - u) * __ldg(a + k) + t * (1.0f - u) * __ldg(a + k + NY) +
+           (1.0f - t) * u * __ldg(a + k + 1) + t * u * __ldg(a + k + NY + 1);
+  };
+  v = (1.0f - et) * (lin(P0) * rf0) + et * (lin(P0 + plane) * rf1);
+  if (Q0) vb = (1.0f - et) * (lin(Q0) * rb0) + et * (lin(Q0 + plane) * rb1);
+  return true;
+}
+
+// Persistent kernel over 32 x 32 output tiles of one eta slice (largest
+// rapidity count first).  For a fixed slice and rapidity node the shift length
+// D is the same for every cell, so for each phi_p the whole tile shifts by one
+// vector: the host table gives the integer offset and the fractions once, each
+// cell corrects the fraction for its own float-rounded coordinate, and the
+// lanes (consecutive y) read consecutive addresses of the eta-slice-major
+// copies.  Lane l of warp w owns the cells (x0 + 4w + k, y0 + l); a thread
+// interpolates 5 x rows of two eta slices for its 4 samples.  phi_p whose
+// whole tile lands outside the grid are skipped; runs inside it skip the
+// in-grid test.  Moments: FP32 partial sums over 16 phi_p folded into
+// per-rapidity sums, then into T^{mu nu} / J^mu with the rapidity factors
+// (src/LandauMatch.cpp:76-143), all in thread-private shared-memory slots.
+template <bool kInterior>
+__device__ __forceinline__ void stream3d_phi(const Ev3D& ev, const float* __restrict__ P0,
+                                             const float* __restrict__ Q0, int i0, int j, float t,
+                                             float uc, const float (&ex)[kCellsPerThread], float et,
+                                             float rf0, float rf1, float rb0, float rb1,
+                                             bool baryon, float (&v)[kCellsPerThread],
+                                             float (&vb)[kCellsPerThread]) {
+  constexpr int K = kCellsPerThread;
+  const int NX = ev.NX, NY = ev.NY;
+  const size_t plane = (size_t)NX * NY;
+  const int jj = kInterior ? j : min(max(j, 0), NY - 2);
+  float B0p = 0.f, B1p = 0.f, C0p = 0.f, C1p = 0.f;
+#pragma unroll
+  for (int r = 0; r <= K; ++r) {
+    const int i = kInterior ? i0 + r : min(max(i0 + r, 0), NX - 1);
+    const size_t k = (size_t)i * NY + jj;
+    // y interpolation of the row on both eta slices
+    const float a0 = __ldg(P0 + k), a1 = __ldg(P0 + k + 1);
+    const float b0 = __ldg(P0 + plane + k), b1 = __ldg(P0 + plane + k + 1);
+    const float B0 = fmaf(uc, a1 - a0, a0), B1 = fmaf(uc, b1 - b0, b0);
+    float C0 = 0.f, C1 = 0.f;
+    if (baryon) {
+      const float c0 = __ldg(Q0 + k), c1 = __ldg(Q0 + k + 1);
+      const float d0 = __ldg(Q0 + plane + k), d1 = __ldg(Q0 + plane + k + 1);
+      C0 = fmaf(uc, c1 - c0, c0);
+      C1 = fmaf(uc, d1 - d0, d0);
     }
+    if (r > 0) {
+      const int q = r - 1;
+      const float tk = t + ex[q];
+      const float L0 = fmaf(tk, B0 - B0p, B0p), L1 = fmaf(tk, B1 - B1p, B1p);
+      v[q] = (1.0f - et) * (L0 * rf0) + et * (L1 * rf1);
+      if (baryon) {
+        const float M0 = fmaf(tk, C0 - C0p, C0p), M1 = fmaf(tk, C1 - C1p, C1p);
+        vb[q] = (1.0f - et) * (M0 * rb0) + et * (M1 * rb1);
+      }
+    }
+    B0p = B0;
+    B1p = B1;
+    C0p = C0;
+    C1p = C1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
+                                                                     const Tile3D* __restrict__ tiles,
+                                                                     int ntiles, Counters* ctr) {
+  extern __shared__ float slots3[];  // thread-private slots, [slot][thread]
+  __shared__ int s_tile;
+  constexpr int K = kCellsPerThread;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* const sl = slots3 + threadIdx.x;
+  auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
+  // slot layout per cell k: Q 0..5 (per-rapidity sums), T 6..15, Qb 16..18, J 19..22
+  constexpr int kSlotsPerCell = 23;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->block3d, 1);
     __syncthreads();
-    const int NX = ev.NX, NY = ev.NY, NE = ev.NE, NR = ev.NR;
-    const int DIM = NX * NY * NE;
-    const int is = b.begin + threadIdx.x;
-    if (is < DIM) {
-      const int ix = is / (NY * NE);
-      const int iy = (is - NY * NE * ix) / NE;
-      const int ieta = is - NY * NE * ix - NE * iy;
-      const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
-      const float inv_dx = ev.inv_dx, inv_dy = ev.inv_dy;
-      const float NXm1 = (float)(NX - 1), NYm1 = (float)(NY - 1);
+    const int tix = s_tile;
+    if (tix >= ntiles) return;
+    const Tile3D tl = tiles[tix];
+    const Ev3D& ev = evs[tl.ev];
+    const int NX = ev.NX, NY = ev.NY, NE = ev.NE, NR = ev.NR, NP = ev.NPHI;
+    const int ieta = tl.ieta;
+    const bool baryon = ev.baryon != 0;
+    const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
+    const int x_hi = min(tl.x0 + kTileX, NX) - 1, y_hi = min(tl.y0 + kTileY, NY) - 1;
+    const bool full = (tl.x0 + kTileX <= NX) && (tl.y0 + kTileY <= NY);
+    const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
+    const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
+    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
+    float ex[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int ix = ixb + k;
       const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
-      const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);
-      const float* __restrict__ ef = ev.efield;
-      const float* __restrict__ nb = ev.nB;
-      const bool baryon = ev.baryon != 0;
-      const int sx = NY * NE;
-      float Tt[10], Tc[10], Jt[4], Jc[4];
+      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
+      act[k] = (ix < NX) && (iy < NY);
+    }
 #pragma unroll
-      for (int m = 0; m < 10; ++m) Tt[m] = Tc[m] = 0.0f;
+    for (int m = 0; m < K * kSlotsPerCell; ++m) S(m) = 0.0f;
+    const size_t plane = (size_t)NX * NY;
+    for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
+      const RapEta re = ev.re[ieta * NR + irap];
+      if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D)) continue;
+      const float et = re.efrac, D = re.D;
+      const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
+      const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
+      float rb0 = 0.f, rb1 = 0.f;
+      if (baryon) {
+        rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
+        rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
+      }
+      const float* P0 = ev.efield + (size_t)re.efl * plane;
+      const float* Q0 = baryon ? ev.bfield + (size_t)re.efl * plane : nullptr;
+      const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
+      float a[K][6], ab[K][3];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) Jt[m] = Jc[m] = 0.0f;
-      for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
-        const RapEta re = ev.re[ieta * NR + irap];
-        if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D)) continue;
-        const float D = re.D, et = re.efrac;
-        const float rf0 = __ldg(ev.rapf + re.efl * NR + irap), rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
-        float rb0 = 0.f, rb1 = 0.f;
-        if (baryon) {
-          rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
-          rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
-        }
-        float a[6] = {0, 0, 0, 0, 0, 0}, st[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
-        float ab[3] = {0, 0, 0}, sbt[3] = {0, 0, 0}, sbc[3] = {0, 0, 0};
-        for (int p = 0; p < NPHI; ++p) {
-          const float2 cs = scs[p];
-          // (src/FreeStream.cpp:193-199)
-          const float xn = __fsub_rn(x, __fmul_rn(cs.x, D));
-          const float yn = __fsub_rn(y, __fmul_rn(cs.y, D));
-          float qx = __fmul_rn(__fsub_rn(xn, xmin), inv_dx);
-          float qy = __fmul_rn(__fsub_rn(yn, ymin), inv_dy);
-          if (fabsf(qx - 1.0f) < 1.0e-3f || fabsf(qx - NXm1) < 1.0e-3f)
-            qx = __fdiv_rn(__fsub_rn(xn, xmin), DX);
-          if (fabsf(qy - 1.0f) < 1.0e-3f || fabsf(qy - NYm1) < 1.0e-3f)
-            qy = __fdiv_rn(__fsub_rn(yn, ymin), DY);
-          const float fxf = floorf(qx), fyf = floorf(qy);
-          if (fxf >= 1.0f && fxf < NXm1 && fyf >= 1.0f && fyf < NYm1) {
-            const int i = (int)fxf, j = (int)fyf;
-            const float t = qx - fxf, u = qy - fyf;
-            const int k = i * sx + j * NE + re.efl;
-            const float w00 = (1.0f - t) * (1.0f - u), w10 = t * (1.0f - u), w01 = (1.0f - t) * u,
-                        w11 = t * u;
-            const float l0 = w00 * __ldg(ef + k) + w10 * __ldg(ef + k + sx) + w01 * __ldg(ef + k + NE) +
-                             w11 * __ldg(ef + k + sx + NE);
-            const float l1 = w00 * __ldg(ef + k + 1) + w10 * __ldg(ef + k + sx + 1) +
-                             w01 * __ldg(ef + k + NE + 1) + w11 * __ldg(ef + k + sx + NE + 1);
-            const float v = (1.0f - et) * (l0 * rf0) + et * (l1 * rf1);
-            a[0] += v;
-            a[1] += v * cs.x;
-            a[2] += v * cs.y;
-            a[3] += v * (cs.x * cs.x);
-            a[4] += v * (cs.x * cs.y);
-            a[5] += v * (cs.y * cs.y);
-            if (baryon) {
-              const float b0 = w00 * __ldg(nb + k) + w10 * __ldg(nb + k + sx) +
-                               w01 * __ldg(nb + k + NE) + w11 * __ldg(nb + k + sx + NE);
-              const float b1 = w00 * __ldg(nb + k + 1) + w10 * __ldg(nb + k + sx + 1) +
-                               w01 * __ldg(nb + k + NE + 1) + w11 * __ldg(nb + k + sx + NE + 1);
-              const float vb = (1.0f - et) * (b0 * rb0) + et * (b1 * rb1);
-              ab[0] += vb;
-              ab[1] += vb * cs.x;
-              ab[2] += vb * cs.y;
+      for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) a[k][m] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) ab[k][m] = 0.0f;
+      }
+      for (int p = 0; p < NP; ++p) {
+        const PhiEntry3D e = tab[p];
+        const int ox = e.ox;
+        const int oy = (int)(short)(e.oy_near & 0xffff);
+        // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
+        // more either side when the fraction is near an integer)
+        const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
+        const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
+        if (!skip) {
+          const FSM_FLOAT2 cs = ev.cs[p];
+          // (a full tile, so that no lane past the grid edge reads outside it)
+          const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
+          const int i0 = ixb + ox, j = iy + oy;
+          const float uc = e.u + ey;
+          float v[K], vb[K];
+          if (interior) {
+            stream3d_phi<true>(ev, P0, Q0, i0, j, e.t, uc, ex, et, rf0, rf1, rb0, rb1, baryon, v, vb);
+          } else {
+            stream3d_phi<false>(ev, P0, Q0, i0, j, e.t, uc, ex, et, rf0, rf1, rb0, rb1, baryon, v, vb);
+            const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
+            const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              const int ik = i0 + k;
+              const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+              const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+              bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
+              if (act[k] && (ux || uy)) {
+                // the in-grid decision depends on the rounding: reference arithmetic
+                const float x = __fadd_rn(__fmul_rn((float)(ixb + k), DX), xmin);
+                in = exact_sample3d(ev, P0, Q0, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k],
+                                    vb[k]);
+              }
+              if (!in) {
+                v[k] = 0.0f;
+                vb[k] = 0.0f;
+              }
             }
           }
-          if ((p & (kPhiChunk - 1)) == kPhiChunk - 1) {
+          const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            a[k][0] += v[k];
+            a[k][1] = fmaf(v[k], cs.x, a[k][1]);
+            a[k][2] = fmaf(v[k], cs.y, a[k][2]);
+            a[k][3] = fmaf(v[k], cc, a[k][3]);
+            a[k][4] = fmaf(v[k], csn, a[k][4]);
+            a[k][5] = fmaf(v[k], ss, a[k][5]);
+            if (baryon) {
+              ab[k][0] += vb[k];
+              ab[k][1] = fmaf(vb[k], cs.x, ab[k][1]);
+              ab[k][2] = fmaf(vb[k], cs.y, ab[k][2]);
+            }
+          }
+        }
+        if ((p & (kPhiChunk - 1)) == kPhiChunk - 1 || p == NP - 1) {
+          // second level of the two-level sum: per-rapidity sums in slots
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
 #pragma unroll
             for (int m = 0; m < 6; ++m) {
-              kahan_add(st[m], sc[m], a[m]);
-              a[m] = 0.0f;
+              S(k * kSlotsPerCell + m) += a[k][m];
+              a[k][m] = 0.0f;
             }
+            if (baryon) {
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-              kahan_add(sbt[m], sbc[m], ab[m]);
-              ab[m] = 0.0f;
+              for (int m = 0; m < 3; ++m) {
+                S(k * kSlotsPerCell + 16 + m) += ab[k][m];
+                ab[k][m] = 0.0f;
+              }
             }
           }
         }
+      }
+      // rows of the hypertrig table (src/LandauMatch.cpp:46-55) times the
+      // rapidity Jacobian (src/LandauMatch.cpp:101) and the profile norm
+      const float jw = ev.jac[irap] * ev.norm;
 #pragma unroll
-        for (int m = 0; m < 6; ++m) kahan_add(st[m], sc[m], a[m]);
-#pragma unroll
-        for (int m = 0; m < 3; ++m) kahan_add(sbt[m], sbc[m], ab[m]);
-        // rows of the hypertrig table (src/LandauMatch.cpp:46-55) times the
-        // rapidity Jacobian (src/LandauMatch.cpp:101) and the profile norm
-        const float jw = ev.jac[irap] * ev.norm;
-        const float S1 = st[0] * jw, Sc = st[1] * jw, Ss = st[2] * jw;
-        kahan_add(Tt[0], Tc[0], S1);
-        kahan_add(Tt[1], Tc[1], Sc * re.A);
-        kahan_add(Tt[2], Tc[2], Ss * re.A);
-        kahan_add(Tt[3], Tc[3], S1 * re.Dt);
-        kahan_add(Tt[4], Tc[4], st[3] * jw * re.B);
-        kahan_add(Tt[5], Tc[5], st[4] * jw * re.B);
-        kahan_add(Tt[6], Tc[6], Sc * re.C);
-        kahan_add(Tt[7], Tc[7], st[5] * jw * re.B);
-        kahan_add(Tt[8], Tc[8], Ss * re.C);
-        kahan_add(Tt[9], Tc[9], S1 * re.E);
+      for (int k = 0; k < K; ++k) {
+        const int b = k * kSlotsPerCell;
+        const float S1 = S(b + 0) * jw, Sc = S(b + 1) * jw, Ss = S(b + 2) * jw;
+        const float Scc = S(b + 3) * jw, Scs = S(b + 4) * jw, Sss = S(b + 5) * jw;
+        S(b + 6) += S1;
+        S(b + 7) += Sc * re.A;
+        S(b + 8) += Ss * re.A;
+        S(b + 9) += S1 * re.Dt;
+        S(b + 10) += Scc * re.B;
+        S(b + 11) += Scs * re.B;
+        S(b + 12) += Sc * re.C;
+        S(b + 13) += Sss * re.B;
+        S(b + 14) += Ss * re.C;
+        S(b + 15) += S1 * re.E;
+        for (int m = 0; m < 6; ++m) S(b + m) = 0.0f;
         if (baryon) {
-          const float B1 = sbt[0] * ev.normB, Bc = sbt[1] * ev.normB, Bs = sbt[2] * ev.normB;
-          kahan_add(Jt[0], Jc[0], B1);
-          kahan_add(Jt[1], Jc[1], Bc * re.A);
-          kahan_add(Jt[2], Jc[2], Bs * re.A);
-          kahan_add(Jt[3], Jc[3], B1 * re.Dt);
+          const float B1 = S(b + 16) * ev.normB, Bc = S(b + 17) * ev.normB, Bs = S(b + 18) * ev.normB;
+          S(b + 19) += B1;
+          S(b + 20) += Bc * re.A;
+          S(b + 21) += Bs * re.A;
+          S(b + 22) += B1 * re.Dt;
+          for (int m = 16; m < 19; ++m) S(b + m) = 0.0f;
         }
       }
-      const float dphi = ev.d_phip;
+    }
+    const float dphi = ev.d_phip;
+    const size_t DIM = (size_t)NX * NY * NE;
 #pragma unroll
-      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = Tt[m] * dphi;  // (LandauMatch.cpp:105)
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      const size_t is = ((size_t)(ixb + k) * NY + iy) * NE + ieta;
+      const int b = k * kSlotsPerCell;
+      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = S(b + 6 + m) * dphi;  // (LandauMatch.cpp:105)
       if (baryon) {
         const float jf = ev.DRAP * dphi;  // (LandauMatch.cpp:140)
-#pragma unroll
-        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = Jt[m] * jf;
+        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = S(b + 19 + m) * jf;
       }
     }
     __syncthreads();

@@ -329,6 +329,34 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     }
   E.samples = live_pairs * (double)NX * NY * NP;
   E.ref_samples = (double)p.DIM * NR * NP;
+  // 3D stream table: integer offsets and fractions of the shifted points
+  // (src/FreeStream.cpp:193-212) for every live (ieta, irap) and phi_p
+  E.tab3.assign((size_t)NE * NR * NP, PhiEntry3D{0.0f, 0.0f, 0, 0});
+  E.live_eta.assign(NE, 0);
+  for (int ieta = 0; ieta < NE; ++ieta)
+    for (int irap = E.r_lo; irap < E.r_hi; ++irap) {
+      const RapEta& r = E.re[(size_t)ieta * NR + irap];
+      if (!(r.efl >= 1 && r.efl < NE - 1 && std::isfinite(r.D))) continue;
+      E.live_eta[ieta] += 1;
+      for (int k = 0; k < NP; ++k) {
+        const float shx = E.cs[k].x * r.D, shy = E.cs[k].y * r.D;  // reference float products
+        const double sx = -(double)shx / (double)p.DX, sy = -(double)shy / (double)p.DY;
+        const double ox = std::floor(sx), oy = std::floor(sy);
+        PhiEntry3D& w = E.tab3[((size_t)ieta * NR + irap) * NP + k];
+        const double t = sx - ox, u = sy - oy;
+        w.t = (float)t;
+        w.u = (float)u;
+        if (!(std::fabs(ox) < 30000.0 && std::fabs(oy) < 30000.0)) {  // far outside any grid
+          w.ox = 1 << 20;
+          w.oy_near = 0;
+          continue;
+        }
+        w.ox = (int)ox;
+        const int nearx = (t < 1e-3 || t > 1.0 - 1e-3) ? 1 : 0;
+        const int neary = (u < 1e-3 || u > 1.0 - 1e-3) ? 1 : 0;
+        w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
+      }
+    }
   return FSM_OK;
 }
 

@@ -28,6 +28,8 @@ struct EventPlan {
   int Rx = 0, Ry = 0;
   // 3D tables
   std::vector<RapEta> re;
+  std::vector<PhiEntry3D> tab3;  // [NE*NR*NPHI]
+  std::vector<int> live_eta;     // live rapidity nodes per eta slice
   std::vector<float> rapf, rapfB, jac;
   int r_lo = 0, r_hi = 0;
   float norm = 0, normB = 0;

@@ -30,7 +30,7 @@ __global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
 __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
-__global__ void fsm_stream3d_kernel(const Ev3D*, const CellBlock*, int, int, Counters*);
+__global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_edep_sums_kernel(const float*, int, float*);
 __global__ void fsm_diag_kernel(int, int, int, float, float, float, const float*, const float*,
@@ -111,8 +111,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   // ---- layout
   Layout L;
   struct EvOffs {
-    size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac;
-    size_t fa, sy, nodes, efield, T, J, in_e, in_nB, out;
+    size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac, tab3;
+    size_t fa, sy, nodes, efield, bfield, T, J, in_e, in_nB, out;
     size_t qfa, qsy, qnodes;  // charge pass scratch (2D with BARYON)
   };
   std::vector<EvOffs> eo(n);
@@ -151,12 +151,14 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       o.rapf = L.take(P.rapf.size() * 4);
       o.rapfB = L.take(P.rapfB.size() * 4);
       o.jac = L.take(P.jac.size() * 4);
+      o.tab3 = L.take(P.tab3.size() * sizeof(PhiEntry3D));
     }
   }
   // work lists (host side first, to know their sizes)
   std::vector<Tile2D> tiles;
   std::vector<LineBlock> rows, cols, rows_l, cols_l;
-  std::vector<CellBlock> prep3, b3, bl;
+  std::vector<CellBlock> prep3, bl;
+  std::vector<Tile3D> tiles3;
   {
     std::vector<int> order2;
     for (int i = 0; i < n; ++i)
@@ -206,10 +208,24 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       const EventPlan &A = b->plans[a], &C = b->plans[c];
       return A.samples / std::max(1, A.DIM) > C.samples / std::max(1, C.DIM);
     });
+    // 3D tiles: 32 x 32 cells of one eta slice, slices with the most live
+    // rapidity nodes first
+    std::vector<std::pair<int, Tile3D>> t3;
     for (int i : order3) {
       const EventPlan& P = b->plans[i];
-      for (int s = 0; s < P.DIM; s += kThreads3D) b3.push_back(CellBlock{b->ev3_of[i], s});
+      const int NX = P.p.DIM_X, NY = P.p.DIM_Y, NE = P.p.DIM_ETA;
+      for (int ie = 0; ie < NE; ++ie) {
+        // slices without a live rapidity node still get tiles: they write zeros
+        for (int x0 = 0; x0 < NX; x0 += kTileX)
+          for (int y0 = 0; y0 < NY; y0 += kTileY)
+            t3.push_back({P.live_eta[ie] * P.p.DIM_PHIP, Tile3D{b->ev3_of[i], x0, y0, ie}});
+      }
     }
+    std::stable_sort(t3.begin(), t3.end(),
+                     [](const std::pair<int, Tile3D>& a, const std::pair<int, Tile3D>& c) {
+                       return a.first > c.first;
+                     });
+    for (auto& t : t3) tiles3.push_back(t.second);
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
       if (P.is3d)
@@ -227,7 +243,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   size_t o_rows_l = L.take(std::max<size_t>(rows_l.size(), 1) * sizeof(LineBlock));
   size_t o_cols_l = L.take(std::max<size_t>(cols_l.size(), 1) * sizeof(LineBlock));
   size_t o_prep3 = L.take(std::max<size_t>(prep3.size(), 1) * sizeof(CellBlock));
-  size_t o_b3 = L.take(std::max<size_t>(b3.size(), 1) * sizeof(CellBlock));
+  size_t o_tiles3 = L.take(std::max<size_t>(tiles3.size(), 1) * sizeof(Tile3D));
   size_t o_bl = L.take(bl.size() * sizeof(CellBlock));
   size_t o_ctr = L.take(sizeof(Counters));
   size_t o_err = L.take(sizeof(int) * 4);
@@ -247,6 +263,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       o.nodes = L.take((size_t)P.DIM * 16);
     } else {
       o.efield = L.take((size_t)P.DIM * 4);
+      o.bfield = P.baryon ? L.take((size_t)P.DIM * 4) : 0;
     }
     if (!b->own_io) {
       o.T = L.take((size_t)P.DIM * 10 * 4);
@@ -299,6 +316,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       std::memcpy(H + o.rapf, P.rapf.data(), P.rapf.size() * 4);
       std::memcpy(H + o.rapfB, P.rapfB.data(), P.rapfB.size() * 4);
       std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
+      std::memcpy(H + o.tab3, P.tab3.data(), P.tab3.size() * sizeof(PhiEntry3D));
     }
   }
   // ---- output slab layout: per event (default) or group by group
@@ -472,6 +490,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.jac = reinterpret_cast<const float*>(D + o.jac);
       e.e_gev = b->d_in_e[i];
       e.efield = reinterpret_cast<float*>(D + o.efield);
+      e.bfield = P.baryon ? reinterpret_cast<float*>(D + o.bfield) : nullptr;
+      e.tab3 = reinterpret_cast<const PhiEntry3D*>(D + o.tab3);
       e.nB = b->d_in_nB[i];
       e.T = b->d_T[i];
       e.J = b->d_J[i];
@@ -501,13 +521,13 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->box_cap2 = (b->box_cap2 + 7) & ~7;  // float4 units, 128-byte multiple
   b->smem2 = (((size_t)b->cs_cap2 * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)b->box_cap2 * 16 +
              (size_t)kTotSlots2D * kThreads2D * 4;
-  b->smem3 = (size_t)b->cs_cap3 * 8;
+  b->smem3 = (size_t)kThreads3D * kCellsPerThread * 23 * 4;  // thread-private moment slots
   b->smem_rows = prep_rows_smem(b->ny_cap2);
   b->smem_strip = prep_strip_smem(b->strip_cap2);
   (void)max_fp;
   // the kernels index their dynamic shared memory by these capacities
   if ((n2 && b->smem2 < (size_t)b->cs_cap2 * kPhiTab2D * 16 + 2 * (size_t)b->box_cap2 * 16) ||
-      (n3 && b->smem3 < (size_t)max_np3 * 8)) {
+      (n3 && b->smem3 == 0)) {
     set_last_error("internal error: dynamic shared memory below the staged tables");
     return FSM_ERR_CUDA;
   }
@@ -520,7 +540,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   std::memcpy(H + o_rows_l, rows_l.data(), rows_l.size() * sizeof(LineBlock));
   std::memcpy(H + o_cols_l, cols_l.data(), cols_l.size() * sizeof(LineBlock));
   std::memcpy(H + o_prep3, prep3.data(), prep3.size() * sizeof(CellBlock));
-  std::memcpy(H + o_b3, b3.data(), b3.size() * sizeof(CellBlock));
+  std::memcpy(H + o_tiles3, tiles3.data(), tiles3.size() * sizeof(Tile3D));
   std::memcpy(H + o_bl, bl.data(), bl.size() * sizeof(CellBlock));
   b->d_ev2 = reinterpret_cast<Ev2D*>(D + o_ev2);
   b->d_ev3 = reinterpret_cast<Ev3D*>(D + o_ev3);
@@ -531,7 +551,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->d_rows_l = reinterpret_cast<LineBlock*>(D + o_rows_l);
   b->d_cols_l = reinterpret_cast<LineBlock*>(D + o_cols_l);
   b->d_prep3 = reinterpret_cast<CellBlock*>(D + o_prep3);
-  b->d_b3 = reinterpret_cast<CellBlock*>(D + o_b3);
+  b->d_tiles3 = reinterpret_cast<Tile3D*>(D + o_tiles3);
   b->d_bl = reinterpret_cast<CellBlock*>(D + o_bl);
   b->d_ctr = reinterpret_cast<Counters*>(D + o_ctr);
   b->d_err = reinterpret_cast<int*>(D + o_err);
@@ -541,7 +561,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->nrows_l = (int)rows_l.size();
   b->ncols_l = (int)cols_l.size();
   b->nprep3 = (int)prep3.size();
-  b->nb3 = (int)b3.size();
+  b->ntiles3 = (int)tiles3.size();
   b->nbl = (int)bl.size();
   if (mem)
     FSM_CUDA_TRY(cudaMemcpyAsync(D, H, upload_bytes, cudaMemcpyHostToDevice, mem->stream));
@@ -570,14 +590,14 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                                                                b->smem2));
     b->grid2 = std::max(1, std::min(b->ntiles, ctx->num_sms * std::max(occ, 1)));
   }
-  if (b->nb3) {
+  if (b->ntiles3) {
     fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_kernel, ctx->device, b->smem3,
                                     &g_smem3[ctx->device & 63]);
     if (ss != FSM_OK) return ss;
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_kernel, kThreads3D,
                                                                b->smem3));
-    b->grid3 = std::max(1, std::min(b->nb3, ctx->num_sms * std::max(occ, 1)));
+    b->grid3 = std::max(1, std::min(b->ntiles3, ctx->num_sms * std::max(occ, 1)));
   }
   if (mem)
     FSM_CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int) * 4, mem->stream));
@@ -621,9 +641,9 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
     fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
                                                                b->cs_cap2, b->box_cap2, b->d_ctr,
                                                                b->d_err);
-  if (b->nb3)
-    fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_b3, b->nb3,
-                                                               b->cs_cap3, b->d_ctr);
+  if (b->ntiles3)
+    fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3, b->ntiles3,
+                                                               b->d_ctr);
   if (timing) cudaEventRecord(ts.ev[2], s);
   if (b->nbl) fsm_landau_kernel<<<b->nbl, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl, b->d_ctr);
   if (timing) {

@@ -44,6 +44,8 @@ using fsm::EvLandau;
 using fsm::EventPlan;
 using fsm::LineBlock;
 using fsm::Tile2D;
+using fsm::Tile3D;
+using fsm::PhiEntry3D;
 
 namespace fsm {
 namespace rt {
@@ -108,10 +110,11 @@ struct fsm_batch {
   EvLandau* d_evl = nullptr;
   Tile2D* d_tiles = nullptr;
   LineBlock *d_rows = nullptr, *d_cols = nullptr, *d_rows_l = nullptr, *d_cols_l = nullptr;
-  CellBlock *d_prep3 = nullptr, *d_b3 = nullptr, *d_bl = nullptr;
+  CellBlock *d_prep3 = nullptr, *d_bl = nullptr;
+  fsm::Tile3D* d_tiles3 = nullptr;
   Counters* d_ctr = nullptr;
   int* d_err = nullptr;
-  int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, nb3 = 0, nbl = 0;
+  int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, ntiles3 = 0, nbl = 0;
   int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
   size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
   int grid2 = 0, grid3 = 0;
