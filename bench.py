@@ -11,7 +11,8 @@ family, replayed from a CUDA graph.  Each rank runs its own 512 events
 Printed JSON line (rank 0):
   value        events/s over all ranks, inputs resident in HBM
   e2e          events/s through the C ABI with the host round trip inside the
-               timed region (pinned input slab H2D, launch, full output slab D2H)
+               timed region (pinned input slab H2D, launch, D2H of the fields
+               the reference returns to its caller: e, P, Pi, u, pi)
   plain_*      the same events one at a time (one launch sequence per event)
   roofline     fused stream kernel, FP32 pipe: algorithmic FLOPs / measured
                launch time vs the measured FP32 FMA peak of the same GPU
@@ -134,14 +135,14 @@ def cpu_baseline(events, nthreads, budget_s=20.0):
     return done / dt, kind, f"first {done} events of the workload, {nthreads} OpenMP threads, {dt:.1f} s"
 
 
-def serve_stream(args, F, W, local, rank, ctx, max_over_ranks):
+def serve_stream(args, F, W, local, rank, ctx, reps):
     """Mixed request stream (80 % 2D of sides 101-301, 20 % 3D of 131^2 x
     {25, 51} with 21/31/41 rapidities) through the continuous-batching server:
     a burst measures capacity, then Poisson arrivals at serve_load x capacity
     give p50/p99 latency; the same requests one by one through fsm_run_event
     give the plain path."""
     import threading
-    reqs = W.stream_requests(args.serve_requests, rate_hz=1.0, seed=4 + 1000 * rank)
+    reqs = W.stream_requests(args.serve_requests, rate_hz=1.0, seed=reps.seed(4))
     gaps = [reqs[0][0]] + [reqs[k][0] - reqs[k - 1][0] for k in range(1, len(reqs))]
     events = [ev for _, ev in reqs]
     hydro = ["e", "P", "Pi", "u", "pi", "nB", "V"]  # the fields the reference hands to hydro
@@ -189,13 +190,14 @@ def serve_stream(args, F, W, local, rank, ctx, max_over_ranks):
         bufs[key] = ctx.run_event(p, e, nb, outputs=hydro, into=bufs.get(key))
     plain = len(events) / (time.perf_counter() - t0)
     n3 = sum(1 for p, _, _ in events if p.DIM_ETA > 1)
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    return {"requests": len(events), "requests_3d": n3, "burst_events_per_s": cap,
-            "rate_hz": rate, "load": args.serve_load, "events_per_s": st["events_per_s"],
-            "p50_ms": max_over_ranks(st["p50_ms"]), "p99_ms": max_over_ranks(st["p99_ms"]),
-            "max_ms": max_over_ranks(st["max_ms"]), "waves": st["waves"],
-            "plain_events_per_s": plain, "burst_over_plain": cap / plain,
-            "per_rank": world > 1,
+    # whole job: rates summed over the replicas, latencies the worst rank's
+    cap_all, plain_all = reps.sum(cap), reps.sum(plain)
+    return {"requests": len(events) * reps.world, "requests_3d": n3, "burst_events_per_s": cap_all,
+            "rate_hz": reps.sum(rate), "load": args.serve_load,
+            "events_per_s": reps.sum(st["events_per_s"]),
+            "p50_ms": reps.max(st["p50_ms"]), "p99_ms": reps.max(st["p99_ms"]),
+            "max_ms": reps.max(st["max_ms"]), "waves": st["waves"],
+            "plain_events_per_s": plain_all, "burst_over_plain": cap_all / plain_all,
             "outputs": hydro,
             "budget": {"hbm_bytes": budget["hbm_budget"], "pinned_host_bytes": budget["host_budget"]}}
 
@@ -277,40 +279,25 @@ def main():
         return reference_arm(args)
 
     import numpy as np
+    import numpy as np
     import torch
     import fsm_b200 as F
     import workloads as W
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    reps = Replicas(backend="nccl")  # one process per GPU, own events; timing reductions only
+    rank, world = reps.rank, reps.world
+    barrier, max_over_ranks = reps.barrier, reps.max
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    events = W.uneven_batch(n=args.events, seed=3 + 1000 * rank)
+    events = W.uneven_batch(n=args.events, seed=reps.seed(3))
     params = [p for p, _, _ in events]
     ctx = F.Context(local)
     tuning = ctx.autotune(params, [(e, nb) for _, e, nb in events])  # staged-window size
     batch = F.Batch(ctx, params)
     n = len(events)
     h_in = torch.from_numpy(batch.pack_inputs([(e, nb) for _, e, nb in events])).pin_memory()
-    h_out = torch.empty(batch.out_bytes // 4, dtype=torch.float32).pin_memory()
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     batch.upload(h_in.data_ptr(), sp)
@@ -338,25 +325,53 @@ def main():
     t_ms = max_over_ranks(sum(step_ms))
     value = world * n * args.steps / (t_ms / 1e3)
 
-    # ---------------- end to end through the C ABI, host buffers
-    for _ in range(max(1, args.warmup // 2)):
-        batch.upload(h_in.data_ptr(), sp)
-        batch.launch(sp)
-        batch.download(h_out.data_ptr(), sp)
-    stream.synchronize()
+    # ---------------- end to end through the C ABI, host buffers.  Two grouped
+    # batches on two streams alternate steps, so one step's copies overlap the
+    # other's kernels; each step uploads its input slab and copies back the
+    # fields the reference hands its caller (output_to_vectors,
+    # src/FreestreamMilne.cpp:700-716: e, P, Pi, u^mu, pi^{mu nu}).
+    e2e_groups = ["e", "P", "Pi", "u", "pi"]
+    pair = [F.Batch(ctx, params, grouped=True) for _ in range(2)]
+    e2e_streams = [stream, torch.cuda.Stream()]
+    d2h_bytes = pair[0].groups_bytes(e2e_groups)
+    h_outs = [torch.empty(d2h_bytes // 4, dtype=torch.float32).pin_memory() for _ in range(2)]
+
+    def e2e_step(k):
+        b, s = pair[k % 2], e2e_streams[k % 2].cuda_stream
+        b.upload(h_in.data_ptr(), s)
+        b.launch(s)
+        b.download_groups(e2e_groups, h_outs[k % 2].data_ptr(), s)
+
+    for k in range(max(2, args.warmup)):
+        e2e_step(k)
+    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        batch.upload(h_in.data_ptr(), sp)
-        batch.launch(sp)
-        batch.download(h_out.data_ptr(), sp)
-    e1.record(stream)
-    stream.synchronize()
-    batch.check_errors()
+    e0.record(e2e_streams[0])
+    e2e_streams[1].wait_event(e0)
+    for k in range(args.steps):
+        e2e_step(k)
+    e2e_streams[0].wait_stream(e2e_streams[1])
+    e1.record(e2e_streams[0])
+    torch.cuda.synchronize()
+    for b in pair:
+        b.check_errors()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e = world * n * args.steps / (e2e_ms / 1e3)
+    # the packed host copy holds the same values as the device-resident run
+    got = pair[(args.steps - 1) % 2].unpack_groups(h_outs[(args.steps - 1) % 2].numpy(),
+                                                   e2e_groups, 0)
+    h_full = torch.empty(batch.out_bytes // 4, dtype=torch.float32).pin_memory()
+    batch.download(h_full.data_ptr(), sp)
+    batch.check_errors()
+    ref0 = batch.unpack_outputs(h_full.numpy(), 0)
+    for k in e2e_groups:
+        if not np.array_equal(got[k], ref0[k]):
+            raise RuntimeError(f"e2e copy of {k} differs from the device-resident result")
+    del h_full
+    for b in pair:
+        b.close()
 
     # ---------------- kernel timing pass for the roofline (CUDA events per kernel family)
     tctx = F.Context(local, timing=True)
@@ -399,7 +414,7 @@ def main():
     # ---------------- served: Poisson stream of mixed 2D/3D requests through the server
     served = None
     if not args.no_serve:
-        served = serve_stream(args, F, W, local, rank, ctx, max_over_ranks)
+        served = serve_stream(args, F, W, local, rank, ctx, reps)
 
     # ---------------- one 3D event with baryon charge (131^2 x 51, 21 rapidities, 100 phi_p)
     ev3d = None
@@ -444,7 +459,8 @@ def main():
                                    "landau": tm["landau_ms"] / args.steps},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "events/s", "h2d_bytes_per_step": batch.in_bytes,
-                    "d2h_bytes_per_step": batch.out_bytes},
+                    "d2h_bytes_per_step": d2h_bytes, "d2h_fields": e2e_groups,
+                    "pipeline": "2 batches on 2 streams, alternating steps"},
             "gpu_launches": launches_per_step * args.steps,
             "served": served,
             "event_3d": ev3d,
@@ -455,9 +471,7 @@ def main():
     tctx.close()
     batch.close()
     ctx.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 

@@ -278,7 +278,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   }
   b->bytes = L.off;
   b->stage_bytes = upload_bytes;
-  if (mem) {
+  if (mem && mem->dev) {
     b->ext_mem = true;
     b->d_mem = mem->dev(mem->user, b->bytes);
     b->h_stage = b->d_mem ? mem->host(mem->user, b->stage_bytes) : nullptr;
@@ -563,7 +563,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->nprep3 = (int)prep3.size();
   b->ntiles3 = (int)tiles3.size();
   b->nbl = (int)bl.size();
-  if (mem)
+  if (mem && mem->dev)
     FSM_CUDA_TRY(cudaMemcpyAsync(D, H, upload_bytes, cudaMemcpyHostToDevice, mem->stream));
   else
     FSM_CUDA_TRY(cudaMemcpy(D, H, upload_bytes, cudaMemcpyHostToDevice));
@@ -599,7 +599,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                                                                b->smem3));
     b->grid3 = std::max(1, std::min(b->ntiles3, ctx->num_sms * std::max(occ, 1)));
   }
-  if (mem)
+  if (mem && mem->dev)
     FSM_CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int) * 4, mem->stream));
   else
     FSM_CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int) * 4));
@@ -899,10 +899,52 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
 
 extern "C" fsm_status fsm_batch_create(fsm_ctx* ctx, int n, const fsm_params* params,
                                        fsm_batch** out) {
+  return fsm_batch_create_ex(ctx, n, params, 0, out);
+}
+
+extern "C" fsm_status fsm_batch_create_ex(fsm_ctx* ctx, int n, const fsm_params* params,
+                                          int grouped_outputs, fsm_batch** out) {
   if (!ctx || !params || !out || n <= 0) return FSM_ERR_INVALID_ARG;
   *out = nullptr;
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
-  return batch_build(ctx, n, params, nullptr, nullptr, nullptr, nullptr, out);
+  BatchMem layout;  // no pools: only the output layout
+  layout.grouped_out = grouped_outputs != 0;
+  return batch_build(ctx, n, params, nullptr, nullptr, nullptr, nullptr, out, &layout);
+}
+
+extern "C" fsm_status fsm_batch_group_offset(fsm_batch* b, unsigned mask, int group, int ev,
+                                             size_t* elem) {
+  if (!b || !elem || !b->own_io || !b->grouped_out || group < 0 || group >= kOutGroups || ev < 0 ||
+      ev >= (int)b->plans.size() || !(mask & (1u << group)))
+    return FSM_ERR_INVALID_ARG;
+  if (group >= 6 && !b->plans[ev].baryon) return FSM_ERR_INVALID_ARG;
+  size_t before = 0;
+  for (int g = 0; g < group; ++g)
+    if (mask & (1u << g)) before += b->group_elems[g];
+  *elem = before + (b->out_goff[ev][group] - b->group_off[group]);
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_batch_download_groups(fsm_batch* b, unsigned mask, void* host_out,
+                                                void* stream) {
+  if (!b || !b->own_io || !b->grouped_out || !host_out) return FSM_ERR_INVALID_ARG;
+  b->last_stream = pick_stream(b->ctx, stream);
+  char* h = static_cast<char*>(host_out);
+  for (int g = 0; g < kOutGroups; ++g) {
+    if (!(mask & (1u << g)) || b->group_elems[g] == 0) continue;
+    FSM_CUDA_TRY(cudaMemcpyAsync(h, b->d_mem + b->out_slab_off + b->group_off[g] * 4,
+                                 b->group_elems[g] * 4, cudaMemcpyDeviceToHost, b->last_stream));
+    h += b->group_elems[g] * 4;
+  }
+  return FSM_OK;
+}
+
+extern "C" size_t fsm_batch_groups_bytes(fsm_batch* b, unsigned mask) {
+  if (!b) return 0;
+  size_t n = 0;
+  for (int g = 0; g < kOutGroups; ++g)
+    if (mask & (1u << g)) n += b->group_elems[g] * 4;
+  return n;
 }
 
 extern "C" void fsm_batch_destroy(fsm_batch* b) {
@@ -982,7 +1024,7 @@ extern "C" fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_e
                                               size_t* out_elem) {
   if (!b || !b->own_io || ev < 0 || ev >= (int)b->plans.size()) return FSM_ERR_INVALID_ARG;
   if (in_elem) *in_elem = b->in_off[ev];
-  if (out_elem) *out_elem = b->out_off[ev];
+  if (out_elem) *out_elem = b->grouped_out ? (size_t)-1 : b->out_off[ev];
   return FSM_OK;
 }
 

@@ -130,7 +130,8 @@ namespace rt {
 // Memory for a batch supplied by its owner instead of cudaMalloc /
 // cudaMallocHost (the server's pools).  dev/host return at least `bytes`
 // (256-byte aligned) or nullptr when the pool is exhausted; the descriptor
-// upload is then enqueued on `stream` instead of copied synchronously.
+// upload is then enqueued on `stream` instead of copied synchronously.  With
+// dev null the batch allocates its own memory and only grouped_out applies.
 struct BatchMem {
   void* user = nullptr;
   char* (*dev)(void* user, size_t bytes) = nullptr;

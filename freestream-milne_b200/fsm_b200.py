@@ -128,6 +128,12 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_size_t)]),
     "fsm_batch_upload": (_ST, [_VP, _VP, _VP]),
     "fsm_batch_download": (_ST, [_VP, _VP, _VP]),
+    "fsm_batch_create_ex": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
+                                  ctypes.POINTER(_VP)]),
+    "fsm_batch_download_groups": (_ST, [_VP, ctypes.c_uint, _VP, _VP]),
+    "fsm_batch_groups_bytes": (ctypes.c_size_t, [_VP, ctypes.c_uint]),
+    "fsm_batch_group_offset": (_ST, [_VP, ctypes.c_uint, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_size_t)]),
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
@@ -325,14 +331,24 @@ class Context:
         return {k: getattr(info, k) for k, _ in RunInfo._fields_}
 
 
+def out_mask(groups):
+    """OR of the FSM_OUT_* bits of the named output groups (OUT_GROUPS names)."""
+    m = 0
+    for k in groups:
+        m |= 1 << OUT_GROUPS.index(k)
+    return m
+
+
 class Batch:
-    def __init__(self, ctx, params_list):
+    def __init__(self, ctx, params_list, grouped=False):
         self.ctx = ctx
         n = len(params_list)
         arr = (Params * n)(*params_list)
         self.params = list(params_list)
+        self.grouped = bool(grouped)
         self.h = ctypes.c_void_p()
-        check(lib().fsm_batch_create(ctx.h, n, arr, ctypes.byref(self.h)), "fsm_batch_create")
+        check(lib().fsm_batch_create_ex(ctx.h, n, arr, int(self.grouped), ctypes.byref(self.h)),
+              "fsm_batch_create_ex")
         self.n = n
         ib, ob = ctypes.c_size_t(), ctypes.c_size_t()
         check(lib().fsm_batch_slabs(self.h, ctypes.byref(ib), ctypes.byref(ob)), "fsm_batch_slabs")
@@ -372,6 +388,34 @@ class Batch:
     def launch(self, stream=None):
         check(lib().fsm_batch_launch(self.h, stream), "fsm_batch_launch")
 
+    def groups_bytes(self, groups):
+        return lib().fsm_batch_groups_bytes(self.h, out_mask(groups))
+
+    def download_groups(self, groups, host_ptr, stream=None):
+        """Grouped batches: copy back only `groups`, packed in OUT_GROUPS order."""
+        check(lib().fsm_batch_download_groups(self.h, out_mask(groups), host_ptr, stream),
+              "fsm_batch_download_groups")
+
+    def group_offset(self, groups, group, ev):
+        o = ctypes.c_size_t()
+        check(lib().fsm_batch_group_offset(self.h, out_mask(groups), OUT_GROUPS.index(group), ev,
+                                           ctypes.byref(o)), "fsm_batch_group_offset")
+        return o.value
+
+    def unpack_groups(self, packed, groups, ev):
+        """Per-event dict of the `groups` arrays from a download_groups buffer."""
+        p = self.params[ev]
+        dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        res = {}
+        for k in OUT_GROUPS:
+            if k not in groups or (k in ("J", "nB", "V") and not p.BARYON):
+                continue
+            c = OUT_COMPS[k]
+            off = self.group_offset(groups, k, ev)
+            a = packed[off:off + c * dim]
+            res[k] = a.reshape(c, dim) if c > 1 else a
+        return res
+
     def check_errors(self):
         check(lib().fsm_batch_check(self.h), "fsm_batch_check")
 
@@ -388,6 +432,8 @@ class Batch:
 
     def unpack_outputs(self, slab, ev):
         """Per-event dict of output arrays from a downloaded output slab."""
+        if self.grouped:
+            return self.unpack_groups(slab, OUT_GROUPS, ev)
         p = self.params[ev]
         dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
         _, off = self.offsets(ev)
@@ -437,9 +483,7 @@ class Server:
                  outputs=None):
         self.h = ctypes.c_void_p()
         self.outputs = list(outputs) if outputs else list(OUT_GROUPS)
-        mask = 0
-        for k in self.outputs:
-            mask |= 1 << OUT_GROUPS.index(k)
+        mask = out_mask(self.outputs)
         opts = ServerOpts(device, int(hbm_budget), int(host_budget), int(max_wave_events),
                           int(streams), mask)
         check(lib().fsm_server_start(ctypes.byref(self.h), ctypes.byref(opts)), "fsm_server_start")

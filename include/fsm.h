@@ -166,6 +166,13 @@ typedef struct fsm_batch fsm_batch;
 
 fsm_status fsm_batch_create(fsm_ctx* ctx, int n_events, const fsm_params* params,
                             fsm_batch** batch);
+/* As fsm_batch_create; grouped_outputs != 0 lays the output slab out group by
+ * group (all events' T, then all events' e, ... in FSM_OUT_* order, events in
+ * batch order inside a group) so that a caller can copy back only the groups
+ * it reads with fsm_batch_download_groups.  fsm_batch_event_offsets then
+ * reports (size_t)-1 as the output offset; use fsm_batch_group_offset. */
+fsm_status fsm_batch_create_ex(fsm_ctx* ctx, int n_events, const fsm_params* params,
+                               int grouped_outputs, fsm_batch** batch);
 void fsm_batch_destroy(fsm_batch* b);
 /* Device views of event `ev`: input slots (d_e, d_nB) and outputs. */
 fsm_status fsm_batch_views(fsm_batch* b, int ev, float** d_e, float** d_nB,
@@ -187,6 +194,14 @@ fsm_status fsm_batch_event_offsets(fsm_batch* b, int ev, size_t* in_elem, size_t
  * whole output slab, enqueued on `stream` (pinned host memory makes them async). */
 fsm_status fsm_batch_upload(fsm_batch* b, const void* host_in, void* stream);
 fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream);
+/* Grouped batches only: copies the groups in `mask` (an OR of FSM_OUT_*
+ * values, defined below) back to host_out, packed in group order, one copy per
+ * group.  Bytes written: fsm_batch_groups_bytes(b, mask).  Offset (in floats)
+ * of event ev's part of group g (FSM_OUT_* == 1 << g) inside that packed
+ * buffer: fsm_batch_group_offset. */
+fsm_status fsm_batch_download_groups(fsm_batch* b, unsigned mask, void* host_out, void* stream);
+size_t fsm_batch_groups_bytes(fsm_batch* b, unsigned mask);
+fsm_status fsm_batch_group_offset(fsm_batch* b, unsigned mask, int group, int ev, size_t* elem);
 /* Waits for the stream the batch last used (upload, launch or download) and
  * checks the kernels' internal error counters. */
 fsm_status fsm_batch_check(fsm_batch* b);

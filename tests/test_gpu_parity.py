@@ -117,6 +117,50 @@ def test_batch_equals_single_events(ctx):
     b.close()
 
 
+def test_grouped_batch_downloads(ctx):
+    """A batch with grouped outputs gives the same results as a per-event one,
+    and download_groups copies back exactly the groups asked for."""
+    evs = []
+    for name in golden_names():
+        d, e, nB, _, _ = load_golden(name)
+        if not d["E_DEP_FS"]:
+            evs.append((fsm_params(d), e, nB))
+    inputs = [(e, nB) for _, e, nB in evs]
+    plain = F.Batch(ctx, [p for p, _, _ in evs])
+    want = plain.run_host(inputs)
+    plain.close()
+    b = F.Batch(ctx, [p for p, _, _ in evs], grouped=True)
+    got = b.run_host(inputs)
+    for w, g in zip(want, got):
+        assert sorted(w) == sorted(g)
+        for k in w:
+            assert np.array_equal(w[k], g[k]), k
+    import torch
+    groups = ["e", "u", "pi", "nB"]
+    nbytes = b.groups_bytes(groups)
+    expect = 0
+    for p, _, _ in evs:
+        dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        expect += 4 * dim * (1 + 4 + 10 + (1 if p.BARYON else 0))
+    assert nbytes == expect
+    host = torch.full((nbytes // 4,), np.nan, dtype=torch.float32).pin_memory()
+    b.upload(torch.from_numpy(b.pack_inputs(inputs)).pin_memory().data_ptr())
+    b.launch()
+    b.download_groups(groups, host.data_ptr())
+    b.check_errors()
+    packed = host.numpy()
+    assert not np.isnan(packed).any()
+    for ev, w in enumerate(want):
+        part = b.unpack_groups(packed, groups, ev)
+        assert sorted(part) == sorted(k for k in groups if k in w)
+        for k in part:
+            assert np.array_equal(part[k], w[k]), (ev, k)
+    assert b.offsets(0)[1] == 2**64 - 1  # no per-event output block in a grouped slab
+    with pytest.raises(F.FsmError):
+        b.group_offset(groups, "T", 0)  # T was not downloaded
+    b.close()
+
+
 def test_device_entry_point(ctx):
     import torch
     p, e, _ = W.lumpy2d(seed=9, side=101, dx=0.08, nphip=64, dtau=0.7)
