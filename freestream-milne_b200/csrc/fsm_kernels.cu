@@ -15,6 +15,7 @@
 // src/LandauMatch.cpp:76-107).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 #include <cuda.h>
 
 #include "fsm_internal.h"
@@ -412,6 +413,13 @@ constexpr int kWaitLimit = 1 << 20;  // polls of one bounded mbarrier wait
 //
 // kInterior: every sample of the run provably lands inside the grid, so the
 // in-grid test (src/FreeStream.cpp:213) is skipped.
+//
+// Consecutive phi_p often share the integer offset (the source point moves by
+// at most about one cell per phi_p step): the thread keeps the 2 x (K + 1)
+// nodes of the last offset in registers (nd0/nd1, node values of the grid,
+// the same in every staged window) and reloads them only when the offset
+// changes.  Out-of-grid window entries are never copied; samples that would
+// read them are masked below, whatever the registers hold.
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
@@ -421,7 +429,9 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
                                              float (&a0)[kCellsPerThread],
                                              float2 (&a12)[kCellsPerThread],
                                              float2 (&a34)[kCellsPerThread],
-                                             float* __restrict__ stot, int* err) {
+                                             float4 (&nd0)[kCellsPerThread + 1],
+                                             float4 (&nd1)[kCellsPerThread + 1], int& pox,
+                                             int& poy, float* __restrict__ stot, int* err) {
   constexpr int K = kCellsPerThread;
   const int NX = ev.NX, NY = ev.NY;
   const float2 ey2 = make_float2(ey, ey);
@@ -435,11 +445,20 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
     const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
     const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
     const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
+    if (ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+#pragma unroll
+      for (int r = 0; r <= K; ++r) {
+        nd0[r] = rowp[r * boxW];
+        nd1[r] = rowp[r * boxW + 1];
+      }
+      pox = ox;
+      poy = oy;
+    }
     float cv[K];
     float2 VDp = make_float2(0.f, 0.f);
 #pragma unroll
     for (int r = 0; r <= K; ++r) {
-      const float4 n0 = rowp[r * boxW], n1 = rowp[r * boxW + 1];
+      const float4 n0 = nd0[r], n1 = nd1[r];
       // y pass of the node row: (value, x-slope) interpolated to the sample's y
       float2 VD = __fmul2_rn(make_float2(Kp.x, Kp.x), make_float2(n0.x, n0.y));
       VD = __ffma2_rn(make_float2(Kp.y, Kp.y), make_float2(n1.x, n1.y), VD);
@@ -463,8 +482,8 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!(cv[k] > 0.0f)) {
-          const float4 a00 = rowp[k * boxW], a01 = rowp[k * boxW + 1];
-          const float4 a10 = rowp[(k + 1) * boxW], a11 = rowp[(k + 1) * boxW + 1];
+          const float4 a00 = nd0[k], a01 = nd1[k];
+          const float4 a10 = nd0[k + 1], a11 = nd1[k + 1];
           const float B0 = fmaf(uu, a01.x - a00.x, a00.x);
           const float B1 = fmaf(uu, a11.x - a10.x, a10.x);
           cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0) * ev.fb_scale;
@@ -592,6 +611,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     }
 #pragma unroll
     for (int m = 0; m < kTotSlots2D; ++m) stot[m * kThreads2D] = 0.0f;
+    float4 nd0[K + 1], nd1[K + 1];
+    int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
+    // warps whose cells all lie past the grid's x edge skip the runs
+    const bool live = ixb <= x_hi;
 
     for (int c = 0; c < nch; ++c) {
       const int b = c & 1;
@@ -619,12 +642,14 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       // boundary (cells past the grid edge are computed but never stored)
       const bool interior = (tl.x0 + ch.ox0 >= 2) && (x_hi + ch.ox1 <= ev.NX - 3) &&
                             (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
-      if (interior)
+      if (!live) {
+      } else if (interior) {
         stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
-                           a12, a34, stot, err);
-      else
+                           a12, a34, nd0, nd1, pox, poy, stot, err);
+      } else {
         stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
-                            a12, a34, stot, err);
+                            a12, a34, nd0, nd1, pox, poy, stot, err);
+      }
       __syncthreads();  // buffer b is free for the load of run c + 2
     }
     // T = (sum over DIM_RAP identical rapidity copies) * d_phip / TAU
