@@ -30,6 +30,7 @@ constexpr int kWarps2D = 8;
 constexpr int kTileX = kWarps2D * kCellsPerThread;  // 2D output tile: x extent (slow index)
 constexpr int kThreads2D = kWarps2D * 32;
 constexpr int kPhiTab2D = 6;         // float4 per phi_p entry of the 2D table
+constexpr int kMaxRunPhi2D = 64;     // phi_p per staged run (the run's table slice is staged with it)
 constexpr int kThreads3D = 256;
 constexpr int kThreadsLandau = 128;
 constexpr int kPhiChunk = 16;  // FP32 partial sums are folded into Kahan totals every 16 phi_p
@@ -111,6 +112,12 @@ constexpr int kMaxChunks2D = 64;
 constexpr int kWindowBudget2D = 32 * 1024;  // bytes of one staged window (default)
 constexpr int kMaxWindow2D = 64 * 1024;     // largest staged window the planner raises to
 constexpr int kTotSlots2D = 5 * 4;          // per-thread moment totals kept in shared memory
+// Dynamic shared memory of the 2D stream kernel with staged windows of up to
+// box_cap nodes: two run tables, two windows, the moment totals.
+inline size_t stream2d_smem(int box_cap) {
+  return ((size_t)2 * kMaxRunPhi2D * kPhiTab2D + 2 * (size_t)box_cap) * 16 +
+         (size_t)kTotSlots2D * kThreads2D * 4;
+}
 
 struct Ev2D {
   int NX, NY, NPHI, NR;

@@ -420,12 +420,13 @@ constexpr int kWaitLimit = 1 << 20;  // polls of one bounded mbarrier wait
 // the same in every staged window) and reloads them only when the offset
 // changes.  Out-of-grid window entries are never copied; samples that would
 // read them are masked below, whatever the registers hold.
+//
+// `stab` holds the table entries of the run's phi_p p0 .. p1 - 1.
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
-                                             int p0, int p1, int ixb, int iy, float y, float ey,
+                                             int p0, int p1, int ixb, int iy, float ey,
                                              const float (&ex)[kCellsPerThread],
-                                             const bool (&act)[kCellsPerThread],
                                              float (&a0)[kCellsPerThread],
                                              float2 (&a12)[kCellsPerThread],
                                              float2 (&a34)[kCellsPerThread],
@@ -436,7 +437,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
   const int NX = ev.NX, NY = ev.NY;
   const float2 ey2 = make_float2(ey, ey);
   for (int p = p0; p < p1; ++p) {
-    const float4* e = stab + kPhiTab2D * p;
+    const float4* e = stab + kPhiTab2D * (p - p0);
     const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], mw = e[4], tu = e[5];
     const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
     const int oy = (int)(short)(oyn & 0xffff);
@@ -475,9 +476,10 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       VDp = VD;
     }
     // bilinear where the bicubic value is not positive (or not a number)
-    const float cmin = fminf(fminf(cv[0], cv[1]), fminf(cv[2], cv[3]));
-    if (__any_sync(0xffffffffu, !(cmin > 0.0f) || (cv[0] != cv[0]) || (cv[1] != cv[1]) ||
-                                    (cv[2] != cv[2]) || (cv[3] != cv[3]))) {
+    bool pos = true;
+#pragma unroll
+    for (int k = 0; k < K; ++k) pos = pos && (cv[k] > 0.0f);
+    if (__any_sync(0xffffffffu, !pos)) {
       const float uu = tu.y + ey;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -510,8 +512,9 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
           const bool cx = (ik >= 1) && (ik <= NX - 2);
           const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
           const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-          if (act[k] && (ux || uy) && (ux || cx) && (uy || in_y)) {
+          if (ixb + k < NX && iy < NY && (ux || uy) && (ux || cx) && (uy || in_y)) {
             const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+            const float y = __fadd_rn(__fmul_rn((float)iy, ev.DY), ev.ymin);
             cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
           } else {
             cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
@@ -551,15 +554,16 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
 // error and leaves.
 __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D* __restrict__ evs,
                                                                      const Tile2D* __restrict__ tiles,
-                                                                     int ntiles, int tab_cap,
-                                                                     int box_cap, Counters* ctr,
-                                                                     int* err) {
+                                                                     int ntiles, int box_cap,
+                                                                     Counters* ctr, int* err) {
   extern __shared__ __align__(128) float4 smem4[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ int s_tile;
-  float4* stab = smem4;
-  const size_t tab_f4 = ((size_t)tab_cap * kPhiTab2D + 7) & ~(size_t)7;  // 128-byte aligned
-  float4* const buf0 = smem4 + tab_f4;
+  constexpr int kTabF4 = kMaxRunPhi2D * kPhiTab2D;  // one run table (a 128-byte multiple)
+  static_assert(kTabF4 % 8 == 0, "run tables keep the windows 128-byte aligned");
+  float4* const tab0 = smem4;
+  float4* const tab1 = smem4 + kTabF4;
+  float4* const buf0 = smem4 + 2 * kTabF4;
   float4* const buf1 = buf0 + box_cap;
   float* const stot = reinterpret_cast<float*>(buf1 + box_cap) + threadIdx.x;
   if (threadIdx.x == 0) {
@@ -584,8 +588,8 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     if (warp == 0) {
       const Chunk2D c0 = chunks[0];
       stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, win_w(c0),
-                   win_h(c0),
-                   stab, ev.tab, (uint32_t)ev.NPHI * kPhiTab2D * 16, &bars[0]);
+                   win_h(c0), tab0, ev.tab + c0.p0,
+                   (uint32_t)(c0.p1 - c0.p0) * (uint32_t)sizeof(PhiEntry2D), &bars[0]);
     }
     // per-thread cell constants
     const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
@@ -594,13 +598,11 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
     const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
     float ex[K];
-    bool act[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int ix = ixb + k;
       const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
       ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
-      act[k] = (ix < ev.NX) && (iy < ev.NY);
     }
     float a0[K];
     float2 a12[K], a34[K];
@@ -621,7 +623,8 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       if (warp == 0 && c + 1 < nch) {
         const Chunk2D cn = chunks[c + 1];
         stage_window(b ? buf0 : buf1, gnodes, ev.NX, ev.NY, tl.x0 + cn.ox0 - 1, tl.y0 + cn.oy0 - 1,
-                     win_w(cn), win_h(cn), nullptr, nullptr, 0u, &bars[b ^ 1]);
+                     win_w(cn), win_h(cn), b ? tab0 : tab1, ev.tab + cn.p0,
+                     (uint32_t)(cn.p1 - cn.p0) * (uint32_t)sizeof(PhiEntry2D), &bars[b ^ 1]);
       }
       const uint32_t ph = b ? phase1 : phase0;
       const bool ok = mbar_wait(&bars[b], ph, kWaitLimit);
@@ -638,16 +641,17 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       const Chunk2D ch = chunks[c];
       const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1, boxW = win_w(ch);
       const float4* win = b ? buf1 : buf0;
+      const float4* stab = b ? tab1 : tab0;
       // every sample of this run lands at least one node inside the grid
       // boundary (cells past the grid edge are computed but never stored)
       const bool interior = (tl.x0 + ch.ox0 >= 2) && (x_hi + ch.ox1 <= ev.NX - 3) &&
                             (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
       if (!live) {
       } else if (interior) {
-        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
+        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
                            a12, a34, nd0, nd1, pox, poy, stot, err);
       } else {
-        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, y, ey, ex, act, a0,
+        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
                             a12, a34, nd0, nd1, pox, poy, stot, err);
       }
       __syncthreads();  // buffer b is free for the load of run c + 2
@@ -662,7 +666,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       // in 2D the hypertrig rows are (1, cos, sin, 0)
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        if (!act[k]) continue;
+        if (ixb + k >= ev.NX || iy >= ev.NY) continue;
         const size_t is = (size_t)(ixb + k) * ev.NY + iy;
         const float s0 = stot[(5 * k + 0) * kThreads2D] + a0[k];
         const float s1 = stot[(5 * k + 1) * kThreads2D] + a12[k].x;
@@ -676,7 +680,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      if (!act[k]) continue;
+      if (ixb + k >= ev.NX || iy >= ev.NY) continue;
       const float tot[5] = {stot[(5 * k + 0) * kThreads2D] + a0[k],
                             stot[(5 * k + 1) * kThreads2D] + a12[k].x,
                             stot[(5 * k + 2) * kThreads2D] + a12[k].y,

@@ -27,7 +27,7 @@ __global__ void fsm_prep2d_rows_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
 __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
-__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 }  // namespace fsm
 
@@ -248,10 +248,8 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   put(o_bl, bl.data(), bl.size() * sizeof(CellBlock));
 
   // launch geometry of the stream kernel (as the batch path computes it)
-  const int tab_cap = P.p.DIM_PHIP;
   const int box_cap = (P.box_elems + 7) & ~7;
-  const size_t smem2 = (((size_t)tab_cap * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)box_cap * 16 +
-                       (size_t)kTotSlots2D * kThreads2D * 4;
+  const size_t smem2 = stream2d_smem(box_cap);
   if ((st = raise_dyn_smem((const void*)fsm_stream2d_kernel, smem2)) != FSM_OK) return st;
   const size_t smem_rows = strip ? prep_strip_smem(std::max(NX, NY)) : prep_rows_smem(NY);
   if (strip) {
@@ -289,7 +287,7 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
     fsm_prep2d_cols_long_kernel<<<(int)cols.size(), 128, 0, s>>>(d_ev2, d_cols);
   }
   fsm_stream2d_kernel<<<grid2, kThreads2D, smem2, s>>>(d_ev2, reinterpret_cast<const Tile2D*>(D + o_tiles), ntiles,
-                                                       tab_cap, box_cap, reinterpret_cast<Counters*>(D + o_ctr),
+                                                       box_cap, reinterpret_cast<Counters*>(D + o_ctr),
                                                        reinterpret_cast<int*>(D + o_err));
   fsm_landau_kernel<<<(int)bl.size(), kThreadsLandau, 0, s>>>(reinterpret_cast<const EvLandau*>(D + o_evl),
                                                             reinterpret_cast<const CellBlock*>(D + o_bl),

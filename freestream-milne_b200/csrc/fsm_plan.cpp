@@ -167,10 +167,12 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       const int neary = (u < 1e-3 || u > 1.0 - 1e-3) ? 1 : 0;
       w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
     }
-    // phi_p runs whose staged window (tile + offset spread + 1-node margins)
-    // fits the window budget; consecutive nodes have neighbouring offsets.  A
-    // budget that would need more than kMaxChunks2D runs is raised (a tuned
-    // small window must not make long free-streaming distances unplannable).
+    // phi_p runs of at most kMaxRunPhi2D nodes whose staged window (tile +
+    // offset spread + 1-node margins) fits the window budget; consecutive
+    // nodes have neighbouring offsets.  A budget that cuts the circle into
+    // more than kMaxChunks2D runs is raised up to kMaxWindow2D (fewer, larger
+    // windows for long free-streaming distances).
+    const int min_runs = (NP + kMaxRunPhi2D - 1) / kMaxRunPhi2D;
     for (int budget = window_budget;; budget = budget * 3 / 2) {
       auto win_bytes = [](int dox, int doy) {
         return (size_t)(kTileX + dox + 3) * (size_t)(kTileY + doy + 3) * 16;
@@ -183,7 +185,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       E.ox_min = E.ox_max = lo_x;
       E.oy_min = E.oy_max = lo_y;
       for (int k = 1; k <= NP; ++k) {
-        bool flush = (k == NP);
+        bool flush = (k == NP) || (k - p0 == kMaxRunPhi2D);
         if (!flush) {
           int nlx = std::min(lo_x, E.tab2[k].ox), nhx = std::max(hi_x, E.tab2[k].ox);
           int nly = std::min(lo_y, oy_of(k)), nhy = std::max(hi_y, oy_of(k));
@@ -211,9 +213,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
           E.oy_max = std::max(E.oy_max, oy_of(k));
         }
       }
-      if ((int)E.chunks2.size() <= kMaxChunks2D && E.boxW <= 256 && E.boxH <= 256) break;
-      if ((int)E.chunks2.size() <= kMaxChunks2D || budget > kMaxWindow2D)
-        return fail(FSM_ERR_TOO_LARGE, "free-streaming distance too large for the staged windows");
+      const bool few = (int)E.chunks2.size() <= std::max(kMaxChunks2D, 2 * min_runs);
+      if (few || budget * 3 / 2 > kMaxWindow2D) break;
     }
     E.Rx = (int)std::ceil(p.DTAU / p.DX) + 2;
     E.Ry = (int)std::ceil(p.DTAU / p.DY) + 2;

@@ -29,7 +29,7 @@ __global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
 __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
-__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, int, Counters*, int*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_edep_sums_kernel(const float*, int, float*);
@@ -519,15 +519,13 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->cs_cap2 = max_np2;
   b->cs_cap3 = (max_np3 + 1) & ~1;
   b->box_cap2 = (b->box_cap2 + 7) & ~7;  // float4 units, 128-byte multiple
-  b->smem2 = (((size_t)b->cs_cap2 * kPhiTab2D + 7) & ~(size_t)7) * 16 + 2 * (size_t)b->box_cap2 * 16 +
-             (size_t)kTotSlots2D * kThreads2D * 4;
+  b->smem2 = stream2d_smem(b->box_cap2);
   b->smem3 = (size_t)kThreads3D * kCellsPerThread * 23 * 4;  // thread-private moment slots
   b->smem_rows = prep_rows_smem(b->ny_cap2);
   b->smem_strip = prep_strip_smem(b->strip_cap2);
   (void)max_fp;
   // the kernels index their dynamic shared memory by these capacities
-  if ((n2 && b->smem2 < (size_t)b->cs_cap2 * kPhiTab2D * 16 + 2 * (size_t)b->box_cap2 * 16) ||
-      (n3 && b->smem3 == 0)) {
+  if (n3 && b->smem3 == 0) {
     set_last_error("internal error: dynamic shared memory below the staged tables");
     return FSM_ERR_CUDA;
   }
@@ -639,8 +637,7 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
   if (timing) cudaEventRecord(ts.ev[1], s);
   if (b->ntiles)
     fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
-                                                               b->cs_cap2, b->box_cap2, b->d_ctr,
-                                                               b->d_err);
+                                                               b->box_cap2, b->d_ctr, b->d_err);
   if (b->ntiles3)
     fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3, b->ntiles3,
                                                                b->d_ctr);

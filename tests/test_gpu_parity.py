@@ -71,6 +71,17 @@ def test_gpu_long_lines(ctx, nx, ny):
     compare(got, ref64, ref["tau"])
 
 
+def test_gpu_many_phi_nodes(ctx):
+    """DIM_PHIP far above one staged run (2000 phi_p: 32 runs of the table)."""
+    p, e, _ = W.lumpy2d(seed=21, side=61, dx=0.08, nphip=2000, dtau=0.7, eos=1, radius=1.5)
+    got = ctx.run_event(p, e)
+    assert got["info"]["dim_phip"] == 2000
+    ref = _oracle(p, e)
+    ref64 = _oracle(p, e, fp64=2)
+    compare_parity(got, ref, ref64, ref["tau"])
+    compare(got, ref64, ref["tau"])
+
+
 def test_gpu_2d_baryon(ctx):
     """Boost-invariant event with baryon charge: J^mu from the charge pass
     (spline of the first rapidity slice, per-slice bilinear fallback)."""
