@@ -50,7 +50,7 @@ __device__ __forceinline__ void stage_axis(AxisNode* dst, const AxisNode* __rest
 
 // y-lines (rows ix0 .. ix0+31, contiguous in memory): F = e/(2 pi) -> fa and
 // its y-slopes -> sy.  Lines are staged with an odd stride.
-__global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_rows_kernel(
+__global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_rows_kernel(
     const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks) {
   extern __shared__ __align__(16) unsigned char prep_smem[];
   const LineBlock b = blocks[blockIdx.x];
@@ -103,7 +103,9 @@ __global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_rows_kernel(
 
 // x-lines (columns iy0 .. iy0+31 at stride NY): x-slopes of F and of the
 // y-slope field (the mixed derivative), packed with F and F_y into the nodes.
-__global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_cols_kernel(
+// A job is one field of one segment: (F, F_x) fills the first half of the
+// node float4, (F_y, F_xy) the second.
+__global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_cols_kernel(
     const Ev2D* __restrict__ evs, const LineBlock* __restrict__ blocks) {
   extern __shared__ __align__(16) unsigned char prep_smem[];
   const LineBlock b = blocks[blockIdx.x];
@@ -133,20 +135,18 @@ __global__ void __launch_bounds__(kPrepThreads, 1) fsm_prep2d_cols_kernel(
   const float* fc = Fs + kPadLo * 32 + lane;
   const float* yc = Ys + kPadLo * 32 + lane;
   const AxisNode* A = tab + kPadLo;
-  float4* nodes = reinterpret_cast<float4*>(ev.nodes) + iy0 + lane;
+  float2* nodes = reinterpret_cast<float2*>(reinterpret_cast<float4*>(ev.nodes) + iy0 + lane);
   const int nseg = (NX + kSegP - 1) / kSegP;
-  for (int sg = warp; sg < nseg; sg += kPrepThreads / 32) {
-    const int a = sg * kSegP;
-    float sx[kSegP], sxy[kSegP];
+  for (int job = warp; job < 2 * nseg; job += kPrepThreads / 32) {
+    const int a = (job >> 1) * kSegP, half = job & 1;
+    const float* vc = half ? yc : fc;
+    float sv[kSegP];
     seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
-               [&](int i) { return (double)fc[i * 32]; }, sx);
-    __syncwarp();  // keeps the second sweep's loads after the first (register pressure)
-    seg_slopes([&](int k) -> const AxisNode& { return A[k]; }, NX, (double)ev.DX, a,
-               [&](int i) { return (double)yc[i * 32]; }, sxy);
+               [&](int i) { return (double)vc[i * 32]; }, sv);
 #pragma unroll
     for (int t = 0; t < kSegP; ++t) {
       const int i = a + t;
-      if (i < NX) nodes[(size_t)i * NY] = make_float4(fc[i * 32], sx[t], yc[i * 32], sxy[t]);
+      if (i < NX) nodes[(size_t)i * NY * 2 + half] = make_float2(vc[i * 32], sv[t]);
     }
   }
 }

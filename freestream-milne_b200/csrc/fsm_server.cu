@@ -142,6 +142,11 @@ struct fsm_server {
   long long next_id = 1;
   bool stopping = false;
   bool mem_wait = false;  // admission waits for pool memory (a wave or a poll frees it)
+  // Bumped under mu by every event the scheduler waits for (a wave done, a
+  // submit, freed output memory, stop).  The scheduler releases mu while it
+  // plans a wave, and a notify in that window finds nobody waiting; comparing
+  // the count before it sleeps catches such events.
+  unsigned long long wake_gen = 0;
   std::thread th;
   // statistics
   long long submitted = 0, completed = 0, failed = 0, waves = 0;
@@ -180,6 +185,7 @@ void CUDART_CB wave_done_cb(void* user) {
     std::lock_guard<std::mutex> g(S->mu);
     W->second->t_done = Clock::now();
     W->second->done = true;
+    ++S->wake_gen;
   }
   S->cv.notify_all();
   delete W;
@@ -202,6 +208,7 @@ void drop_output(fsm_server* S, Request* r) {
     S->hpool.release(r->ob->p, r->ob->bytes);
     delete r->ob;
     S->mem_wait = false;  // pinned memory came back: admission may proceed
+    ++S->wake_gen;
     S->cv.notify_all();
   }
   r->ob = nullptr;
@@ -379,6 +386,7 @@ void scheduler(fsm_server* S) {
   cudaSetDevice(S->ctx->device);
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
+    const unsigned long long gen = S->wake_gen;
     // retire completed waves
     for (size_t k = 0; k < S->slot_wave.size(); ++k) {
       Wave* w = S->slot_wave[k];
@@ -397,14 +405,17 @@ void scheduler(fsm_server* S) {
     if (!S->mem_wait) {
       for (size_t k = 0; k < S->slot_wave.size() && !S->queue.empty(); ++k) {
         if (S->slot_wave[k]) continue;
+        const unsigned long long g0 = S->wake_gen;
         if (!wave_launch(S, lk, (int)k)) {
-          S->mem_wait = true;
+          // wait for memory only if none was freed while the wave was planned
+          if (S->wake_gen == g0) S->mem_wait = true;
           break;
         }
         launched = true;
       }
     }
     if (launched) continue;
+    if (S->wake_gen != gen) continue;  // something happened while mu was released
     S->cv.wait(lk);
   }
 }
@@ -478,6 +489,7 @@ extern "C" fsm_status fsm_server_submit(fsm_server* S, const fsm_params* p, cons
     S->reqs[r->id] = r;
     S->queue.push_back(r);
     *id = r->id;
+    ++S->wake_gen;
   }
   S->cv.notify_all();
   return FSM_OK;
@@ -586,6 +598,7 @@ extern "C" fsm_status fsm_server_stop(fsm_server* S) {
     // queued requests are cancelled; waves in flight finish
     for (Request* r : S->queue) finish_request(S, r, FSM_ERR_CANCELLED, Clock::now());
     S->queue.clear();
+    ++S->wake_gen;
   }
   S->cv.notify_all();
   S->cv_done.notify_all();
