@@ -1,11 +1,12 @@
 // fsm_internal.h -- descriptors shared by the host planner and the sm_100a kernels.
 //
-// Layout in HBM (per event, all in the reference cell order
+// Layout in HBM (per event; fields in the reference cell order
 // is = (DIM_Y*DIM_ETA)*ix + DIM_ETA*iy + ieta):
 //   2D: nodes[is]  float4 (F, F_x*DX, F_y*DY, F_xy*DX*DY): the bicubic node data
-//       of F = e/(2 pi), 16 B/cell, read by the stream kernel through a shared-
-//       memory footprint of each output tile.
-//   3D: efield[is] float e (fm^-4) and the caller's nB[is] float, read through L1.
+//       of F = e/(2 pi), 16 B/cell, read by the stream kernel through staged
+//       shared-memory windows of each output tile.
+//   3D: nodes3[e][ix][iy] eta-pair nodes (e in fm^-4 of slices e and e+1, and
+//       n_B of both with BARYON), float2 / float4, read through L1.
 //   T[10][DIM], J[4][DIM]: moments written by the stream kernels, read by the
 //   Landau kernel.  Outputs e,P,Pi,u[4],pi[10],nB,V[4] are [comp][DIM] floats.
 #pragma once
@@ -194,9 +195,10 @@ struct Ev3D {
   const float* jac;       // [NR] tan-map Jacobian (src/LandauMatch.cpp:92-93)
   const PhiEntry3D* tab3; // [NE*NR*NPHI]
   const float* e_gev;     // input
-  float* efield;          // converted energy density (fm^-4), eta-slice major [NE][NX][NY]
   const float* nB;        // input baryon density
-  float* bfield;          // baryon density, eta-slice major [NE][NX][NY]
+  // eta-pair nodes [NE-1][NX][NY]: (E[e], E[e+1], B[e], B[e+1]) float4 with
+  // BARYON, (E[e], E[e+1]) float2 without; E in fm^-4
+  void* nodes3;
   float* T;               // [10][DIM]
   float* J;               // [4][DIM]
   long long cell_begin;   // first global cell index of this event in the 3D work list

@@ -254,20 +254,27 @@ __global__ void fsm_edep_sums_kernel(const float* __restrict__ e_gev, int n, flo
 }
 
 // ------------------------------------------------------------------ prep 3D
+// Eta-pair node arrays of a 3D event: node (e, ix, iy) holds the converted
+// energy density of slices e and e+1 at (ix, iy) (and the baryon density of
+// both with BARYON), [NE-1][NX][NY], so that the stream kernel reads both
+// slices of a sample with one vector load and its lanes (consecutive y) read
+// consecutive nodes.  Thread per node.
 __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict__ evs,
                                                          const CellBlock* __restrict__ blocks) {
   const CellBlock b = blocks[blockIdx.x];
   const Ev3D& ev = evs[b.ev];
-  const int DIM = ev.NX * ev.NY * ev.NE;
-  const int is = b.begin + threadIdx.x;
-  if (is >= DIM) return;
-  // eta-slice-major copies: slice ieta is a contiguous NX x NY plane, so the
-  // stream kernel's lanes (consecutive y) read consecutive addresses
-  const int NE = ev.NE, NYE = ev.NY * NE;
-  const int ix = is / NYE, iy = (is - ix * NYE) / NE, ieta = is - ix * NYE - iy * NE;
-  const size_t dst = ((size_t)ieta * ev.NX + ix) * ev.NY + iy;
-  ev.efield[dst] = to_fm4(__ldg(ev.e_gev + is));
-  if (ev.baryon) ev.bfield[dst] = __ldg(ev.nB + is);
+  const int NX = ev.NX, NY = ev.NY, NE = ev.NE;
+  const int plane = NX * NY;
+  const int q = b.begin + threadIdx.x;  // (e * NX + ix) * NY + iy
+  if (q >= (NE - 1) * plane) return;
+  const int e = q / plane, r = q - e * plane;
+  const int ix = r / NY, iy = r - ix * NY;
+  const size_t is = ((size_t)ix * NY + iy) * NE + e;  // the reference's cell order
+  const float E0 = to_fm4(__ldg(ev.e_gev + is)), E1 = to_fm4(__ldg(ev.e_gev + is + 1));
+  if (ev.baryon)
+    reinterpret_cast<float4*>(ev.nodes3)[q] = make_float4(E0, E1, __ldg(ev.nB + is), __ldg(ev.nB + is + 1));
+  else
+    reinterpret_cast<float2*>(ev.nodes3)[q] = make_float2(E0, E1);
 }
 
 // ---------------------------------------------------------------- stream 2D
@@ -705,15 +712,27 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
 }
 
 // ---------------------------------------------------------------- stream 3D
+// Node of the eta-pair arrays: (E[e], E[e+1], B[e], B[e+1]) with baryons,
+// (E[e], E[e+1]) without.
+template <bool kB> struct Node3D;
+template <> struct Node3D<true> { using T = float4; };
+template <> struct Node3D<false> { using T = float2; };
+__device__ __forceinline__ float node_b0(const float4& n) { return n.z; }
+__device__ __forceinline__ float node_b1(const float4& n) { return n.w; }
+__device__ __forceinline__ float node_b0(const float2&) { return 0.0f; }
+__device__ __forceinline__ float node_b1(const float2&) { return 0.0f; }
+
 // One sample with the reference's own float arithmetic (src/FreeStream.cpp:
 // 193-276): shifted point, correctly rounded index division, in-grid test and
 // trilinear interpolation (the eta fraction and slice from the host table).
 // Used for the rare samples whose in-grid decision depends on the rounding.
-// Returns false for a sample outside the grid.
-__device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const float* __restrict__ P0,
-                                               const float* __restrict__ Q0, float x, float y,
-                                               float c, float s, float D, float et, float rf0,
-                                               float rf1, float rb0, float rb1, float& v, float& vb) {
+// N points at the eta pair of the sample's slice.  Returns false for a sample
+// outside the grid.
+template <bool kB>
+__device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const typename Node3D<kB>::T* __restrict__ N,
+                                               float x, float y, float c, float s, float D, float et,
+                                               float rf0, float rf1, float rb0, float rb1, float& v,
+                                               float& vb) {
   const int NX = ev.NX, NY = ev.NY;
   const float xn = __fsub_rn(x, __fmul_rn(c, D));
   const float yn = __fsub_rn(y, __fmul_rn(s, D));
@@ -723,13 +742,17 @@ __device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const float* __re
   if (!(fx >= 1.0f && fx < (float)(NX - 1) && fy >= 1.0f && fy < (float)(NY - 1))) return false;
   const int i = (int)fx, j = (int)fy;
   const float t = qx - fx, u = qy - fy;
-  const size_t plane = (size_t)NX * NY, k = (size_t)i * NY + j;
-  auto lin = [&](const float* a) {
-    return (1.0f - t) * (1.0f - u) * __ldg(a + k) + t * (1.0f - u) * __ldg(a + k + NY) +
-           (1.0f - t) * u * __ldg(a + k + 1) + t * u * __ldg(a + k + NY + 1);
+  const size_t k = (size_t)i * NY + j;
+  const auto n00 = __ldg(N + k), n10 = __ldg(N + k + NY), n01 = __ldg(N + k + 1),
+             n11 = __ldg(N + k + NY + 1);
+  auto lin = [&](float a00, float a10, float a01, float a11) {
+    return (1.0f - t) * (1.0f - u) * a00 + t * (1.0f - u) * a10 + (1.0f - t) * u * a01 + t * u * a11;
   };
-  v = (1.0f - et) * (lin(P0) * rf0) + et * (lin(P0 + plane) * rf1);
-  if (Q0) vb = (1.0f - et) * (lin(Q0) * rb0) + et * (lin(Q0 + plane) * rb1);
+  v = (1.0f - et) * (lin(n00.x, n10.x, n01.x, n11.x) * rf0) +
+      et * (lin(n00.y, n10.y, n01.y, n11.y) * rf1);
+  if (kB)
+    vb = (1.0f - et) * (lin(node_b0(n00), node_b0(n10), node_b0(n01), node_b0(n11)) * rb0) +
+         et * (lin(node_b1(n00), node_b1(n10), node_b1(n01), node_b1(n11)) * rb1);
   return true;
 }
 
@@ -738,54 +761,155 @@ __device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const float* __re
 // D is the same for every cell, so for each phi_p the whole tile shifts by one
 // vector: the host table gives the integer offset and the fractions once, each
 // cell corrects the fraction for its own float-rounded coordinate, and the
-// lanes (consecutive y) read consecutive addresses of the eta-slice-major
-// copies.  Lane l of warp w owns the cells (x0 + 4w + k, y0 + l); a thread
-// interpolates 5 x rows of two eta slices for its 4 samples.  phi_p whose
-// whole tile lands outside the grid are skipped; runs inside it skip the
-// in-grid test.  Moments: FP32 partial sums over 16 phi_p folded into
-// per-rapidity sums, then into T^{mu nu} / J^mu with the rapidity factors
-// (src/LandauMatch.cpp:76-143), all in thread-private shared-memory slots.
-template <bool kInterior>
-__device__ __forceinline__ void stream3d_phi(const Ev3D& ev, const float* __restrict__ P0,
-                                             const float* __restrict__ Q0, int i0, int j, float t,
-                                             float uc, const float (&ex)[kCellsPerThread], float et,
+// lanes (consecutive y) read consecutive nodes of the eta-pair array, one
+// vector load per node for both eta slices (and both fields).  Lane l of warp
+// w owns the cells (x0 + 4w + k, y0 + l); a thread interpolates 5 x rows for
+// its 4 samples and, without baryons, keeps those 2 x 5 nodes in registers
+// while consecutive phi_p share the offset.  phi_p whose whole tile lands outside the grid are
+// skipped; runs inside it skip the in-grid test.  Moments: FP32 partial sums
+// over 16 phi_p folded into per-rapidity sums, then into T^{mu nu} / J^mu
+// with the rapidity factors (src/LandauMatch.cpp:76-143), all in
+// thread-private shared-memory slots.
+constexpr int kSlotsPerCell3D = 23;  // per cell: Q 0..5, T 6..15, Qb 16..18, J 19..22
+
+// The phi_p loop of one rapidity node for one tile (nodes of eta pair efl).
+template <bool kB>
+__device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, int ixb, int iy,
+                                             int x_hi, int y_hi, bool full, float y, float ey,
+                                             const float (&ex)[kCellsPerThread],
+                                             const bool (&act)[kCellsPerThread],
+                                             const typename Node3D<kB>::T* __restrict__ N,
+                                             const PhiEntry3D* __restrict__ tab, float D, float et,
                                              float rf0, float rf1, float rb0, float rb1,
-                                             bool baryon, float (&v)[kCellsPerThread],
-                                             float (&vb)[kCellsPerThread]) {
+                                             float* __restrict__ sl) {
+  using NodeT = typename Node3D<kB>::T;
   constexpr int K = kCellsPerThread;
-  const int NX = ev.NX, NY = ev.NY;
-  const size_t plane = (size_t)NX * NY;
-  const int jj = kInterior ? j : min(max(j, 0), NY - 2);
-  float B0p = 0.f, B1p = 0.f, C0p = 0.f, C1p = 0.f;
+  const int NX = ev.NX, NY = ev.NY, NP = ev.NPHI;
+  auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
+  float a[K][6], ab[K][3];
 #pragma unroll
-  for (int r = 0; r <= K; ++r) {
-    const int i = kInterior ? i0 + r : min(max(i0 + r, 0), NX - 1);
-    const size_t k = (size_t)i * NY + jj;
-    // y interpolation of the row on both eta slices
-    const float a0 = __ldg(P0 + k), a1 = __ldg(P0 + k + 1);
-    const float b0 = __ldg(P0 + plane + k), b1 = __ldg(P0 + plane + k + 1);
-    const float B0 = fmaf(uc, a1 - a0, a0), B1 = fmaf(uc, b1 - b0, b0);
-    float C0 = 0.f, C1 = 0.f;
-    if (baryon) {
-      const float c0 = __ldg(Q0 + k), c1 = __ldg(Q0 + k + 1);
-      const float d0 = __ldg(Q0 + plane + k), d1 = __ldg(Q0 + plane + k + 1);
-      C0 = fmaf(uc, c1 - c0, c0);
-      C1 = fmaf(uc, d1 - d0, d0);
-    }
-    if (r > 0) {
-      const int q = r - 1;
-      const float tk = t + ex[q];
-      const float L0 = fmaf(tk, B0 - B0p, B0p), L1 = fmaf(tk, B1 - B1p, B1p);
-      v[q] = (1.0f - et) * (L0 * rf0) + et * (L1 * rf1);
-      if (baryon) {
-        const float M0 = fmaf(tk, C0 - C0p, C0p), M1 = fmaf(tk, C1 - C1p, C1p);
-        vb[q] = (1.0f - et) * (M0 * rb0) + et * (M1 * rb1);
+  for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a[k][m] = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) ab[k][m] = 0.0f;
+  }
+  // float2 nodes of the last offset stay in registers; float4 nodes (with
+  // baryons) are reloaded for every phi_p (kept, they would not fit the
+  // registers of two CTAs per SM)
+  constexpr bool kCache = !kB;
+  NodeT n0[K + 1], n1[K + 1];
+  int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
+  for (int p = 0; p < NP; ++p) {
+    const PhiEntry3D e = tab[p];
+    const int ox = e.ox;
+    const int oy = (int)(short)(e.oy_near & 0xffff);
+    // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
+    // more either side when the fraction is near an integer)
+    const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
+    const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
+    if (!skip) {
+      // (a full tile, so that no lane past the grid edge reads outside it)
+      const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
+      const int i0 = ixb + ox, j = iy + oy;
+      if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+        // clamped indices keep the loads of edge lanes inside the arrays
+        // (their samples are masked below); inside the grid they are exact
+        const int jj = min(max(j, 0), NY - 2);
+#pragma unroll
+        for (int r = 0; r <= K; ++r) {
+          const int i = min(max(i0 + r, 0), NX - 1);
+          const NodeT* q = N + (size_t)i * NY + jj;
+          n0[r] = __ldg(q);
+          n1[r] = __ldg(q + 1);
+        }
+        pox = ox;
+        poy = oy;
+      }
+      const float uc = e.u + ey;
+      float v[K], vb[K];
+      float B0p = 0.f, B1p = 0.f, C0p = 0.f, C1p = 0.f;
+#pragma unroll
+      for (int r = 0; r <= K; ++r) {
+        // y interpolation of the row on both eta slices
+        const float B0 = fmaf(uc, n1[r].x - n0[r].x, n0[r].x);
+        const float B1 = fmaf(uc, n1[r].y - n0[r].y, n0[r].y);
+        float C0 = 0.f, C1 = 0.f;
+        if (kB) {
+          C0 = fmaf(uc, node_b0(n1[r]) - node_b0(n0[r]), node_b0(n0[r]));
+          C1 = fmaf(uc, node_b1(n1[r]) - node_b1(n0[r]), node_b1(n0[r]));
+        }
+        if (r > 0) {
+          const int q = r - 1;
+          const float tk = e.t + ex[q];
+          const float L0 = fmaf(tk, B0 - B0p, B0p), L1 = fmaf(tk, B1 - B1p, B1p);
+          v[q] = (1.0f - et) * (L0 * rf0) + et * (L1 * rf1);
+          vb[q] = 0.0f;
+          if (kB) {
+            const float M0 = fmaf(tk, C0 - C0p, C0p), M1 = fmaf(tk, C1 - C1p, C1p);
+            vb[q] = (1.0f - et) * (M0 * rb0) + et * (M1 * rb1);
+          }
+        }
+        B0p = B0;
+        B1p = B1;
+        C0p = C0;
+        C1p = C1;
+      }
+      const FSM_FLOAT2 cs = ev.cs[p];
+      if (!interior) {
+        const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
+        const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int ik = i0 + k;
+          const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+          const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+          bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
+          if (act[k] && (ux || uy)) {
+            // the in-grid decision depends on the rounding: reference arithmetic
+            const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+            in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+          }
+          if (!in) {
+            v[k] = 0.0f;
+            vb[k] = 0.0f;
+          }
+        }
+      }
+      const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        a[k][0] += v[k];
+        a[k][1] = fmaf(v[k], cs.x, a[k][1]);
+        a[k][2] = fmaf(v[k], cs.y, a[k][2]);
+        a[k][3] = fmaf(v[k], cc, a[k][3]);
+        a[k][4] = fmaf(v[k], csn, a[k][4]);
+        a[k][5] = fmaf(v[k], ss, a[k][5]);
+        if (kB) {
+          ab[k][0] += vb[k];
+          ab[k][1] = fmaf(vb[k], cs.x, ab[k][1]);
+          ab[k][2] = fmaf(vb[k], cs.y, ab[k][2]);
+        }
       }
     }
-    B0p = B0;
-    B1p = B1;
-    C0p = C0;
-    C1p = C1;
+    if ((p & (kPhiChunk - 1)) == kPhiChunk - 1 || p == NP - 1) {
+      // second level of the two-level sum: per-rapidity sums in slots
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          S(k * kSlotsPerCell3D + m) += a[k][m];
+          a[k][m] = 0.0f;
+        }
+        if (kB) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            S(k * kSlotsPerCell3D + 16 + m) += ab[k][m];
+            ab[k][m] = 0.0f;
+          }
+        }
+      }
+    }
   }
 }
 
@@ -798,8 +922,6 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* const sl = slots3 + threadIdx.x;
   auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
-  // slot layout per cell k: Q 0..5 (per-rapidity sums), T 6..15, Qb 16..18, J 19..22
-  constexpr int kSlotsPerCell = 23;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->block3d, 1);
     __syncthreads();
@@ -826,110 +948,31 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
       act[k] = (ix < NX) && (iy < NY);
     }
 #pragma unroll
-    for (int m = 0; m < K * kSlotsPerCell; ++m) S(m) = 0.0f;
+    for (int m = 0; m < K * kSlotsPerCell3D; ++m) S(m) = 0.0f;
     const size_t plane = (size_t)NX * NY;
     for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
       const RapEta re = ev.re[ieta * NR + irap];
       if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D)) continue;
-      const float et = re.efrac, D = re.D;
       const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
       const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
-      float rb0 = 0.f, rb1 = 0.f;
-      if (baryon) {
-        rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
-        rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
-      }
-      const float* P0 = ev.efield + (size_t)re.efl * plane;
-      const float* Q0 = baryon ? ev.bfield + (size_t)re.efl * plane : nullptr;
       const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
-      float a[K][6], ab[K][3];
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-#pragma unroll
-        for (int m = 0; m < 6; ++m) a[k][m] = 0.0f;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) ab[k][m] = 0.0f;
-      }
-      for (int p = 0; p < NP; ++p) {
-        const PhiEntry3D e = tab[p];
-        const int ox = e.ox;
-        const int oy = (int)(short)(e.oy_near & 0xffff);
-        // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
-        // more either side when the fraction is near an integer)
-        const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
-        const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
-        if (!skip) {
-          const FSM_FLOAT2 cs = ev.cs[p];
-          // (a full tile, so that no lane past the grid edge reads outside it)
-          const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
-          const int i0 = ixb + ox, j = iy + oy;
-          const float uc = e.u + ey;
-          float v[K], vb[K];
-          if (interior) {
-            stream3d_phi<true>(ev, P0, Q0, i0, j, e.t, uc, ex, et, rf0, rf1, rb0, rb1, baryon, v, vb);
-          } else {
-            stream3d_phi<false>(ev, P0, Q0, i0, j, e.t, uc, ex, et, rf0, rf1, rb0, rb1, baryon, v, vb);
-            const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
-            const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const int ik = i0 + k;
-              const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-              const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-              bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
-              if (act[k] && (ux || uy)) {
-                // the in-grid decision depends on the rounding: reference arithmetic
-                const float x = __fadd_rn(__fmul_rn((float)(ixb + k), DX), xmin);
-                in = exact_sample3d(ev, P0, Q0, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k],
-                                    vb[k]);
-              }
-              if (!in) {
-                v[k] = 0.0f;
-                vb[k] = 0.0f;
-              }
-            }
-          }
-          const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            a[k][0] += v[k];
-            a[k][1] = fmaf(v[k], cs.x, a[k][1]);
-            a[k][2] = fmaf(v[k], cs.y, a[k][2]);
-            a[k][3] = fmaf(v[k], cc, a[k][3]);
-            a[k][4] = fmaf(v[k], csn, a[k][4]);
-            a[k][5] = fmaf(v[k], ss, a[k][5]);
-            if (baryon) {
-              ab[k][0] += vb[k];
-              ab[k][1] = fmaf(vb[k], cs.x, ab[k][1]);
-              ab[k][2] = fmaf(vb[k], cs.y, ab[k][2]);
-            }
-          }
-        }
-        if ((p & (kPhiChunk - 1)) == kPhiChunk - 1 || p == NP - 1) {
-          // second level of the two-level sum: per-rapidity sums in slots
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-#pragma unroll
-            for (int m = 0; m < 6; ++m) {
-              S(k * kSlotsPerCell + m) += a[k][m];
-              a[k][m] = 0.0f;
-            }
-            if (baryon) {
-#pragma unroll
-              for (int m = 0; m < 3; ++m) {
-                S(k * kSlotsPerCell + 16 + m) += ab[k][m];
-                ab[k][m] = 0.0f;
-              }
-            }
-          }
-        }
+      if (baryon) {
+        const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
+        const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
+        const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
+        stream3d_rap<true>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
+                           re.efrac, rf0, rf1, rb0, rb1, sl);
+      } else {
+        const float2* N = reinterpret_cast<const float2*>(ev.nodes3) + (size_t)re.efl * plane;
+        stream3d_rap<false>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
+                            re.efrac, rf0, rf1, 0.f, 0.f, sl);
       }
       // rows of the hypertrig table (src/LandauMatch.cpp:46-55) times the
       // rapidity Jacobian (src/LandauMatch.cpp:101) and the profile norm
       const float jw = ev.jac[irap] * ev.norm;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const int b = k * kSlotsPerCell;
+        const int b = k * kSlotsPerCell3D;
         const float S1 = S(b + 0) * jw, Sc = S(b + 1) * jw, Ss = S(b + 2) * jw;
         const float Scc = S(b + 3) * jw, Scs = S(b + 4) * jw, Sss = S(b + 5) * jw;
         S(b + 6) += S1;
@@ -959,7 +1002,7 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
     for (int k = 0; k < K; ++k) {
       if (!act[k]) continue;
       const size_t is = ((size_t)(ixb + k) * NY + iy) * NE + ieta;
-      const int b = k * kSlotsPerCell;
+      const int b = k * kSlotsPerCell3D;
       for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = S(b + 6 + m) * dphi;  // (LandauMatch.cpp:105)
       if (baryon) {
         const float jf = ev.DRAP * dphi;  // (LandauMatch.cpp:140)

@@ -112,7 +112,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   Layout L;
   struct EvOffs {
     size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac, tab3;
-    size_t fa, sy, nodes, efield, bfield, T, J, in_e, in_nB, out;
+    size_t fa, sy, nodes, nodes3, T, J, in_e, in_nB, out;
     size_t qfa, qsy, qnodes;  // charge pass scratch (2D with BARYON)
   };
   std::vector<EvOffs> eo(n);
@@ -229,7 +229,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
       if (P.is3d)
-        for (int s = 0; s < P.DIM; s += 256) prep3.push_back(CellBlock{b->ev3_of[i], s});
+        for (int s = 0; s < (P.p.DIM_ETA - 1) * P.p.DIM_X * P.p.DIM_Y; s += 256)
+          prep3.push_back(CellBlock{b->ev3_of[i], s});
       for (int s = 0; s < P.DIM; s += kThreadsLandau) bl.push_back(CellBlock{i, s});
     }
   }
@@ -262,8 +263,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       }
       o.nodes = L.take((size_t)P.DIM * 16);
     } else {
-      o.efield = L.take((size_t)P.DIM * 4);
-      o.bfield = P.baryon ? L.take((size_t)P.DIM * 4) : 0;
+      o.nodes3 = L.take((size_t)(P.p.DIM_ETA - 1) * P.p.DIM_X * P.p.DIM_Y * (P.baryon ? 16 : 8));
     }
     if (!b->own_io) {
       o.T = L.take((size_t)P.DIM * 10 * 4);
@@ -489,8 +489,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.rapfB = reinterpret_cast<const float*>(D + o.rapfB);
       e.jac = reinterpret_cast<const float*>(D + o.jac);
       e.e_gev = b->d_in_e[i];
-      e.efield = reinterpret_cast<float*>(D + o.efield);
-      e.bfield = P.baryon ? reinterpret_cast<float*>(D + o.bfield) : nullptr;
+      e.nodes3 = D + o.nodes3;
       e.tab3 = reinterpret_cast<const PhiEntry3D*>(D + o.tab3);
       e.nB = b->d_in_nB[i];
       e.T = b->d_T[i];
