@@ -721,6 +721,16 @@ __device__ __forceinline__ float node_b0(const float4& n) { return n.z; }
 __device__ __forceinline__ float node_b1(const float4& n) { return n.w; }
 __device__ __forceinline__ float node_b0(const float2&) { return 0.0f; }
 __device__ __forceinline__ float node_b1(const float2&) { return 0.0f; }
+// (energy slice e, slice e+1) and (baryon slice e, slice e+1) pairs of a node
+__device__ __forceinline__ float2 node_e(const float4& n) { return make_float2(n.x, n.y); }
+__device__ __forceinline__ float2 node_e(const float2& n) { return n; }
+__device__ __forceinline__ float2 node_b(const float4& n) { return make_float2(n.z, n.w); }
+__device__ __forceinline__ float2 node_b(const float2&) { return make_float2(0.f, 0.f); }
+// Linear interpolation a + w (b - a) of both components, with b - a rounded
+// once (b + (-1) a is exact before the rounding) as the scalar fmaf(w, b - a, a).
+__device__ __forceinline__ float2 lerp2(float2 w, float2 a, float2 b) {
+  return __ffma2_rn(w, __ffma2_rn(a, make_float2(-1.0f, -1.0f), b), a);
+}
 
 // One sample with the reference's own float arithmetic (src/FreeStream.cpp:
 // 193-276): shifted point, correctly rounded index division, in-grid test and
@@ -785,15 +795,17 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
   using NodeT = typename Node3D<kB>::T;
   constexpr int K = kCellsPerThread;
   const int NX = ev.NX, NY = ev.NY, NP = ev.NPHI;
-  auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
-  float a[K][6], ab[K][3];
+  // moment partial sums: (energy, baryon) pairs of the weights 1, cos, sin
+  // and the energy-only cos^2, cos sin, sin^2
+  float2 a01[K], a1c[K], a1s[K];
+  float a3[K], a4[K], a5[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-#pragma unroll
-    for (int m = 0; m < 6; ++m) a[k][m] = 0.0f;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) ab[k][m] = 0.0f;
+    a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
+    a3[k] = a4[k] = a5[k] = 0.0f;
   }
+  const float omet = 1.0f - et;
+  const float2 rf = make_float2(rf0, rf1), rb = make_float2(rb0, rb1);
   // float2 nodes of the last offset stay in registers; float4 nodes (with
   // baryons) are reloaded for every phi_p (kept, they would not fit the
   // registers of two CTAs per SM)
@@ -827,33 +839,30 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
         poy = oy;
       }
       const float uc = e.u + ey;
+      const float2 uc2 = make_float2(uc, uc);
       float v[K], vb[K];
-      float B0p = 0.f, B1p = 0.f, C0p = 0.f, C1p = 0.f;
+      float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
 #pragma unroll
       for (int r = 0; r <= K; ++r) {
-        // y interpolation of the row on both eta slices
-        const float B0 = fmaf(uc, n1[r].x - n0[r].x, n0[r].x);
-        const float B1 = fmaf(uc, n1[r].y - n0[r].y, n0[r].y);
-        float C0 = 0.f, C1 = 0.f;
-        if (kB) {
-          C0 = fmaf(uc, node_b0(n1[r]) - node_b0(n0[r]), node_b0(n0[r]));
-          C1 = fmaf(uc, node_b1(n1[r]) - node_b1(n0[r]), node_b1(n0[r]));
-        }
+        // y interpolation of the row on both eta slices (packed pairs)
+        const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
+        float2 C = make_float2(0.f, 0.f);
+        if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
         if (r > 0) {
           const int q = r - 1;
           const float tk = e.t + ex[q];
-          const float L0 = fmaf(tk, B0 - B0p, B0p), L1 = fmaf(tk, B1 - B1p, B1p);
-          v[q] = (1.0f - et) * (L0 * rf0) + et * (L1 * rf1);
+          const float2 tk2 = make_float2(tk, tk);
+          // x interpolation, then the eta interpolation with the rapidity weights
+          const float2 L = __fmul2_rn(lerp2(tk2, Bp, B), rf);
+          v[q] = fmaf(omet, L.x, et * L.y);
           vb[q] = 0.0f;
           if (kB) {
-            const float M0 = fmaf(tk, C0 - C0p, C0p), M1 = fmaf(tk, C1 - C1p, C1p);
-            vb[q] = (1.0f - et) * (M0 * rb0) + et * (M1 * rb1);
+            const float2 M = __fmul2_rn(lerp2(tk2, Cp, C), rb);
+            vb[q] = fmaf(omet, M.x, et * M.y);
           }
         }
-        B0p = B0;
-        B1p = B1;
-        C0p = C0;
-        C1p = C1;
+        Bp = B;
+        Cp = C;
       }
       const FSM_FLOAT2 cs = ev.cs[p];
       if (!interior) {
@@ -877,37 +886,36 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
         }
       }
       const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+      const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        a[k][0] += v[k];
-        a[k][1] = fmaf(v[k], cs.x, a[k][1]);
-        a[k][2] = fmaf(v[k], cs.y, a[k][2]);
-        a[k][3] = fmaf(v[k], cc, a[k][3]);
-        a[k][4] = fmaf(v[k], csn, a[k][4]);
-        a[k][5] = fmaf(v[k], ss, a[k][5]);
-        if (kB) {
-          ab[k][0] += vb[k];
-          ab[k][1] = fmaf(vb[k], cs.x, ab[k][1]);
-          ab[k][2] = fmaf(vb[k], cs.y, ab[k][2]);
-        }
+        const float2 w = make_float2(v[k], vb[k]);
+        a01[k] = __fadd2_rn(a01[k], w);
+        a1c[k] = __ffma2_rn(w, c2, a1c[k]);
+        a1s[k] = __ffma2_rn(w, s2, a1s[k]);
+        a3[k] = fmaf(v[k], cc, a3[k]);
+        a4[k] = fmaf(v[k], csn, a4[k]);
+        a5[k] = fmaf(v[k], ss, a5[k]);
       }
     }
     if ((p & (kPhiChunk - 1)) == kPhiChunk - 1 || p == NP - 1) {
       // second level of the two-level sum: per-rapidity sums in slots
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-          S(k * kSlotsPerCell3D + m) += a[k][m];
-          a[k][m] = 0.0f;
-        }
+        float* q = sl + k * kSlotsPerCell3D * kThreads3D;
+        q[0 * kThreads3D] += a01[k].x;
+        q[1 * kThreads3D] += a1c[k].x;
+        q[2 * kThreads3D] += a1s[k].x;
+        q[3 * kThreads3D] += a3[k];
+        q[4 * kThreads3D] += a4[k];
+        q[5 * kThreads3D] += a5[k];
         if (kB) {
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            S(k * kSlotsPerCell3D + 16 + m) += ab[k][m];
-            ab[k][m] = 0.0f;
-          }
+          q[16 * kThreads3D] += a01[k].y;
+          q[17 * kThreads3D] += a1c[k].y;
+          q[18 * kThreads3D] += a1s[k].y;
         }
+        a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
+        a3[k] = a4[k] = a5[k] = 0.0f;
       }
     }
   }
