@@ -235,14 +235,16 @@ FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, 
 #pragma unroll
   for (int r = 0; r < N; ++r) u[r] *= s;
   double e = rayleigh<double, N>(M, g, u);
-  double rmax, mmax, umax;
+  double rmax = 0.0, mmax = 0.0, umax = 0.0;
+  bool have = false;  // the residual of the current (e, u) is at hand
   for (int it = 0; it < 12; ++it) {
-    if (!rqi_step<double, N>(M, g, u, e)) break;
+    if (!rqi_step<double, N>(M, g, u, e)) break;  // a failed step leaves (e, u) unchanged
     eigen_residual<N>(M, u, e, &rmax, &mmax, &umax);
+    have = true;
     if (rmax <= 1.0e-13 * mmax * umax) break;
   }
   // acceptance: a converged pair has |M u - e u| at rounding level
-  eigen_residual<N>(M, u, e, &rmax, &mmax, &umax);
+  if (!have) eigen_residual<N>(M, u, e, &rmax, &mmax, &umax);
   if (!(isfinite(e) && (rmax <= 1.0e-9 * mmax * umax) && (e > 0.0))) return 0;
   *e_out = e;
 #pragma unroll
