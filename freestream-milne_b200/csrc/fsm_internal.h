@@ -226,6 +226,13 @@ struct LineBlock {
 struct CellBlock {
   int ev, begin;
 };
+// One contiguous run of a packed download: len floats from src (output-slab
+// element offset) to dst (packed element offset).
+struct CopySeg {
+  long long src, dst;
+  int len, pad;
+};
+constexpr int kMaxCopySeg = 1 << 16;  // floats per segment (one block each)
 
 // One 2D output tile of one event; interior = 1 when every sample of every
 // cell of the tile provably lands inside the grid (no bounds logic needed).

@@ -1021,6 +1021,18 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
   }
 }
 
+// ------------------------------------------------------------- packing
+// Gathers the output-slab segments a packed download asks for into one
+// contiguous device buffer (block per segment, coalesced).
+__global__ void __launch_bounds__(256) fsm_pack_kernel(const float* __restrict__ slab,
+                                                       float* __restrict__ out,
+                                                       const CopySeg* __restrict__ segs) {
+  const CopySeg sg = segs[blockIdx.x];
+  const float* a = slab + sg.src;
+  float* d = out + sg.dst;
+  for (int i = threadIdx.x; i < sg.len; i += blockDim.x) d[i] = __ldg(a + i);
+}
+
 // ----------------------------------------------------------------- Landau
 // Seven 128-thread blocks per SM (73 registers, some spilled to L1): the
 // solver is latency-bound, and the extra warps gain more than the spills cost

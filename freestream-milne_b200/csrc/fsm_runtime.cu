@@ -32,6 +32,7 @@ __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
+__global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
 __global__ void fsm_edep_sums_kernel(const float*, int, float*);
 __global__ void fsm_diag_kernel(int, int, int, float, float, float, const float*, const float*,
                                 const float*, const float*, const float*, float*, float*, float*,
@@ -66,6 +67,8 @@ bool has_device() {
 void batch_free(fsm_batch* b) {
   if (!b) return;
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_segs) cudaFree(b->d_segs);
+  if (b->d_pack) cudaFree(b->d_pack);
   if (!b->ext_mem) {
     if (b->d_mem) cudaFree(b->d_mem);
     if (b->h_stage) cudaFreeHost(b->h_stage);
@@ -932,6 +935,125 @@ extern "C" fsm_status fsm_batch_download_groups(fsm_batch* b, unsigned mask, voi
                                  b->group_elems[g] * 4, cudaMemcpyDeviceToHost, b->last_stream));
     h += b->group_elems[g] * 4;
   }
+  return FSM_OK;
+}
+
+namespace {
+
+// Components of a boost-invariant event that vanish by symmetry, per output
+// group (bit c: component c): T^{tau eta}, T^{x eta}, T^{y eta}, T^{eta eta};
+// u^eta; pi^{tau eta}, pi^{x eta}, pi^{y eta}; J^eta; V^eta.
+constexpr unsigned kZeroEta2D[kOutGroups] = {(1u << 3) | (1u << 6) | (1u << 8) | (1u << 9), 0, 0, 0,
+                                             1u << 3, (1u << 3) | (1u << 6) | (1u << 8), 1u << 3, 0,
+                                             1u << 3};
+
+bool pack_keeps(const fsm_batch* b, unsigned flags, int g, int c, int ev) {
+  const EventPlan& P = b->plans[ev];
+  if (g >= 6 && !P.baryon) return false;
+  if ((flags & FSM_PACK_SKIP_ETA) && !P.is3d && ((kZeroEta2D[g] >> c) & 1u)) return false;
+  return true;
+}
+
+// Walks the packed layout (groups in mask, events in order, kept components
+// in order); f(g, c, ev, src, dst, len) per component, in packed order.
+template <class F>
+size_t pack_walk(const fsm_batch* b, unsigned mask, unsigned flags, F f) {
+  size_t dst = 0;
+  const size_t base = b->out_slab_off / 4;
+  for (int g = 0; g < kOutGroups; ++g) {
+    if (!(mask & (1u << g))) continue;
+    for (int i = 0; i < (int)b->plans.size(); ++i) {
+      const size_t dim = (size_t)b->plans[i].DIM;
+      for (int c = 0; c < kOutGroupComps[g]; ++c) {
+        if (!pack_keeps(b, flags, g, c, i)) continue;
+        f(g, c, i, base + b->out_goff[i][g] + (size_t)c * dim, dst, dim);
+        dst += dim;
+      }
+    }
+  }
+  return dst;
+}
+
+// Copy list of (mask, flags) on the device (built on first use).
+fsm_status pack_prepare(fsm_batch* b, unsigned mask, unsigned flags) {
+  if (b->pack_ready && b->pack_mask == mask && b->pack_flags == flags) return FSM_OK;
+  std::vector<CopySeg> segs;
+  const size_t total = pack_walk(b, mask, flags, [&](int, int, int, size_t src, size_t dst, size_t len) {
+    if (!segs.empty()) {  // extend the previous run when both sides continue it
+      CopySeg& l = segs.back();
+      if ((size_t)l.src + l.len == src && (size_t)l.dst + l.len == dst && l.len < kMaxCopySeg) {
+        const size_t add = std::min(len, (size_t)(kMaxCopySeg - l.len));
+        l.len += (int)add;
+        src += add;
+        dst += add;
+        len -= add;
+      }
+    }
+    for (size_t o = 0; o < len; o += kMaxCopySeg)
+      segs.push_back(CopySeg{(long long)(src + o), (long long)(dst + o),
+                             (int)std::min((size_t)kMaxCopySeg, len - o), 0});
+  });
+  if (segs.size() > b->seg_cap) {
+    if (b->d_segs) cudaFree(b->d_segs);
+    b->d_segs = nullptr;
+    b->seg_cap = 0;
+    FSM_CUDA_TRY(cudaMalloc(&b->d_segs, segs.size() * sizeof(CopySeg)));
+    b->seg_cap = segs.size();
+  }
+  if (total > b->pack_cap) {
+    if (b->d_pack) cudaFree(b->d_pack);
+    b->d_pack = nullptr;
+    b->pack_cap = 0;
+    FSM_CUDA_TRY(cudaMalloc(&b->d_pack, std::max<size_t>(total, 1) * 4));
+    b->pack_cap = total;
+  }
+  if (!segs.empty())
+    FSM_CUDA_TRY(cudaMemcpy(b->d_segs, segs.data(), segs.size() * sizeof(CopySeg),
+                            cudaMemcpyHostToDevice));
+  b->nsegs = (int)segs.size();
+  b->pack_elems = total;
+  b->pack_mask = mask;
+  b->pack_flags = flags;
+  b->pack_ready = true;
+  return FSM_OK;
+}
+
+}  // namespace
+
+extern "C" size_t fsm_batch_packed_bytes(fsm_batch* b, unsigned mask, unsigned flags) {
+  if (!b || !b->own_io) return 0;
+  return pack_walk(b, mask, flags, [](int, int, int, size_t, size_t, size_t) {}) * 4;
+}
+
+extern "C" fsm_status fsm_batch_packed_offset(fsm_batch* b, unsigned mask, unsigned flags, int group,
+                                              int comp, int ev, size_t* elem) {
+  if (!b || !elem || !b->own_io || group < 0 || group >= kOutGroups || comp < 0 ||
+      comp >= kOutGroupComps[group] || ev < 0 || ev >= (int)b->plans.size() ||
+      !(mask & (1u << group)) || !pack_keeps(b, flags, group, comp, ev))
+    return FSM_ERR_INVALID_ARG;
+  bool found = false;
+  pack_walk(b, mask, flags, [&](int g, int c, int i, size_t, size_t dst, size_t) {
+    if (g == group && c == comp && i == ev) {
+      *elem = dst;
+      found = true;
+    }
+  });
+  return found ? FSM_OK : FSM_ERR_INVALID_ARG;
+}
+
+extern "C" fsm_status fsm_batch_download_packed(fsm_batch* b, unsigned mask, unsigned flags,
+                                                void* host_out, void* stream) {
+  if (!b || !b->own_io || !host_out) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  fsm_status s = pack_prepare(b, mask, flags);
+  if (s != FSM_OK) return s;
+  b->last_stream = pick_stream(b->ctx, stream);
+  if (b->nsegs == 0) return FSM_OK;
+  fsm_pack_kernel<<<b->nsegs, 256, 0, b->last_stream>>>(reinterpret_cast<const float*>(b->d_mem), b->d_pack,
+                                                        b->d_segs);
+  FSM_CUDA_TRY(cudaGetLastError());
+  FSM_CUDA_TRY(cudaMemcpyAsync(host_out, b->d_pack, b->pack_elems * 4, cudaMemcpyDeviceToHost,
+                               b->last_stream));
   return FSM_OK;
 }
 

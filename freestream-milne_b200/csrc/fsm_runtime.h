@@ -122,6 +122,14 @@ struct fsm_batch {
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   cudaStream_t last_stream = nullptr;  // stream of the most recent upload/launch/download
+  // packed downloads: copy list of the last (mask, flags) and the staging buffer
+  unsigned pack_mask = 0, pack_flags = 0;
+  bool pack_ready = false;
+  fsm::CopySeg* d_segs = nullptr;
+  int nsegs = 0;
+  size_t seg_cap = 0;
+  float* d_pack = nullptr;
+  size_t pack_elems = 0, pack_cap = 0;
 };
 
 namespace fsm {

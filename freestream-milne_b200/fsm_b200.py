@@ -83,6 +83,7 @@ class ServerOpts(ctypes.Structure):
 
 # output groups of the server (FSM_OUT_* in fsm.h), in slab order
 OUT_GROUPS = ["T", "e", "P", "Pi", "u", "pi", "J", "nB", "V"]
+PACK_SKIP_ETA = 1  # FSM_PACK_SKIP_ETA
 
 
 class ServerStats(ctypes.Structure):
@@ -134,6 +135,10 @@ SIGNATURES = {
     "fsm_batch_groups_bytes": (ctypes.c_size_t, [_VP, ctypes.c_uint]),
     "fsm_batch_group_offset": (_ST, [_VP, ctypes.c_uint, ctypes.c_int, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_size_t)]),
+    "fsm_batch_download_packed": (_ST, [_VP, ctypes.c_uint, ctypes.c_uint, _VP, _VP]),
+    "fsm_batch_packed_bytes": (ctypes.c_size_t, [_VP, ctypes.c_uint, ctypes.c_uint]),
+    "fsm_batch_packed_offset": (_ST, [_VP, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
@@ -401,6 +406,42 @@ class Batch:
         check(lib().fsm_batch_group_offset(self.h, out_mask(groups), OUT_GROUPS.index(group), ev,
                                            ctypes.byref(o)), "fsm_batch_group_offset")
         return o.value
+
+    def packed_bytes(self, groups, skip_eta=False):
+        return lib().fsm_batch_packed_bytes(self.h, out_mask(groups), PACK_SKIP_ETA if skip_eta else 0)
+
+    def download_packed(self, groups, host_ptr, skip_eta=False, stream=None):
+        """Gather `groups` on the device and copy them back with one copy; with
+        skip_eta the components of 2D events that vanish by symmetry are left out."""
+        check(lib().fsm_batch_download_packed(self.h, out_mask(groups),
+                                              PACK_SKIP_ETA if skip_eta else 0, host_ptr, stream),
+              "fsm_batch_download_packed")
+
+    def packed_offset(self, groups, group, comp, ev, skip_eta=False):
+        """Offset (floats) of component `comp` of `group` of event `ev` in a
+        packed download, or None when the component is left out."""
+        o = ctypes.c_size_t()
+        st = lib().fsm_batch_packed_offset(self.h, out_mask(groups), PACK_SKIP_ETA if skip_eta else 0,
+                                           OUT_GROUPS.index(group), comp, ev, ctypes.byref(o))
+        return o.value if st == 0 else None
+
+    def unpack_packed(self, packed, groups, ev, skip_eta=False):
+        """Per-event dict of the `groups` arrays from a packed download; left-out
+        components (zero by symmetry) come back as zeros."""
+        p = self.params[ev]
+        dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        res = {}
+        for k in OUT_GROUPS:
+            if k not in groups or (k in ("J", "nB", "V") and not p.BARYON):
+                continue
+            c = OUT_COMPS[k]
+            a = np.zeros((c, dim), np.float32)
+            for m in range(c):
+                off = self.packed_offset(groups, k, m, ev, skip_eta)
+                if off is not None:
+                    a[m] = packed[off:off + dim]
+            res[k] = a if c > 1 else a[0]
+        return res
 
     def unpack_groups(self, packed, groups, ev):
         """Per-event dict of the `groups` arrays from a download_groups buffer."""

@@ -202,6 +202,22 @@ fsm_status fsm_batch_download(fsm_batch* b, void* host_out, void* stream);
 fsm_status fsm_batch_download_groups(fsm_batch* b, unsigned mask, void* host_out, void* stream);
 size_t fsm_batch_groups_bytes(fsm_batch* b, unsigned mask);
 fsm_status fsm_batch_group_offset(fsm_batch* b, unsigned mask, int group, int ev, size_t* elem);
+/* Packed copy of the fields a caller reads, for either slab layout: the groups
+ * in `mask` one after the other, events in batch order, components in order,
+ * gathered on the device into one buffer and copied to host_out with one
+ * device->host copy on `stream`.  flags FSM_PACK_SKIP_ETA leaves out the
+ * components of boost-invariant (DIM_ETA = 1) events that vanish by symmetry:
+ * T^{tau eta}, T^{x eta}, T^{y eta}, T^{eta eta}, u^eta, pi^{tau eta},
+ * pi^{x eta}, pi^{y eta}, J^eta, V^eta (pi^{eta eta} does not vanish and is
+ * kept).  The first call for a (mask, flags) pair allocates the device copy
+ * list and the staging buffer.  Offsets are in floats; a left-out component
+ * has none (FSM_ERR_INVALID_ARG). */
+enum { FSM_PACK_SKIP_ETA = 1 };
+fsm_status fsm_batch_download_packed(fsm_batch* b, unsigned mask, unsigned flags, void* host_out,
+                                     void* stream);
+size_t fsm_batch_packed_bytes(fsm_batch* b, unsigned mask, unsigned flags);
+fsm_status fsm_batch_packed_offset(fsm_batch* b, unsigned mask, unsigned flags, int group, int comp,
+                                   int ev, size_t* elem);
 /* Waits for the stream the batch last used (upload, launch or download) and
  * checks the kernels' internal error counters. */
 fsm_status fsm_batch_check(fsm_batch* b);

@@ -172,6 +172,39 @@ def test_grouped_batch_downloads(ctx):
     b.close()
 
 
+@pytest.mark.parametrize("grouped", [False, True])
+def test_packed_downloads(ctx, grouped):
+    """Packed downloads (device gather + one copy) give the fields of the
+    regular download; the components left out for 2D events are zero there."""
+    evs = []
+    for name in golden_names():
+        d, e, nB, _, _ = load_golden(name)
+        if not d["E_DEP_FS"]:
+            evs.append((fsm_params(d), e, nB))
+    inputs = [(e, nB) for _, e, nB in evs]
+    b = F.Batch(ctx, [p for p, _, _ in evs], grouped=grouped)
+    want = b.run_host(inputs)
+    import torch
+    for groups in (["e", "P", "Pi", "u", "pi"], list(F.OUT_GROUPS)):
+        for skip in (False, True):
+            nbytes = b.packed_bytes(groups, skip)
+            host = torch.full((nbytes // 4,), np.nan, dtype=torch.float32).pin_memory()
+            b.download_packed(groups, host.data_ptr(), skip)
+            b.check_errors()
+            packed = host.numpy()
+            assert not np.isnan(packed).any()
+            for ev, w in enumerate(want):
+                got = b.unpack_packed(packed, groups, ev, skip)
+                assert sorted(got) == sorted(k for k in groups if k in w)
+                for k in got:
+                    assert np.array_equal(got[k], w[k]), (grouped, skip, ev, k)
+    full = b.packed_bytes(["u", "pi"])
+    less = b.packed_bytes(["u", "pi"], True)
+    n2d = sum(p.DIM_X * p.DIM_Y for p, _, _ in evs if p.DIM_ETA == 1)
+    assert full - less == 4 * 4 * n2d  # u^eta, pi^{tau eta}, pi^{x eta}, pi^{y eta}
+    b.close()
+
+
 def test_device_entry_point(ctx):
     import torch
     p, e, _ = W.lumpy2d(seed=9, side=101, dx=0.08, nphip=64, dtau=0.7)
