@@ -102,6 +102,37 @@ FSM_HD void gepp_solve(R A[N][N], R b[N], R y[N]) {
   }
 }
 
+// a*d - b*c with one rounding error on the result (Kahan's algorithm): the
+// error of w = b*c is recovered exactly by an FMA, so the cancellation of the
+// two products (large for the minors of strongly boosted cells) costs nothing.
+FSM_HD double det2(double a, double b, double c, double d) {
+  const double w = b * c;
+  const double e = fma(-b, c, w);
+  const double f = fma(a, d, -w);
+  return f + e;
+}
+FSM_HD float det2(float a, float b, float c, float d) { return a * d - b * c; }
+
+// y = adj(A) b = det(A) A^-1 b for 3 x 3 A: the direction an inverse-
+// iteration step needs, without division or pivoting.  The cofactors are 2 x 2
+// determinants (det2); near an eigenvalue adj(A) is the outer product of the
+// right and left null vectors, so y keeps its direction to rounding level.
+template <typename R>
+FSM_HD void adj_solve3(const R A[3][3], const R b[3], R y[3]) {
+  const R c00 = det2(A[1][1], A[1][2], A[2][1], A[2][2]);
+  const R c01 = det2(A[1][2], A[1][0], A[2][2], A[2][0]);
+  const R c02 = det2(A[1][0], A[1][1], A[2][0], A[2][1]);
+  const R c10 = det2(A[0][2], A[0][1], A[2][2], A[2][1]);
+  const R c11 = det2(A[0][0], A[0][2], A[2][0], A[2][2]);
+  const R c12 = det2(A[0][1], A[0][0], A[2][1], A[2][0]);
+  const R c20 = det2(A[0][1], A[0][2], A[1][1], A[1][2]);
+  const R c21 = det2(A[0][2], A[0][0], A[1][2], A[1][0]);
+  const R c22 = det2(A[0][0], A[0][1], A[1][0], A[1][1]);
+  y[0] = c00 * b[0] + c10 * b[1] + c20 * b[2];
+  y[1] = c01 * b[0] + c11 * b[1] + c21 * b[2];
+  y[2] = c02 * b[0] + c12 * b[1] + c22 * b[2];
+}
+
 template <typename R, int N>
 FSM_HD R mink_norm2(const R g[N], const R u[N]) {
   R s = 0;
@@ -150,7 +181,8 @@ FSM_HD bool rqi_step(const R M[N][N], const R g[N], R u[N], R& e) {
 #pragma unroll
     for (int c = 0; c < N; ++c) A[r][c] = M[r][c] - (r == c ? e : R(0));
   }
-  gepp_solve<R, N>(A, rhs, y);
+  if constexpr (N == 3) adj_solve3<R>(A, rhs, y);
+  else gepp_solve<R, N>(A, rhs, y);
   const R m2 = mink_norm2<R, N>(g, y);
   if (!(m2 > 0) || !isfinite(m2)) return false;
   R t = fsm_rsqrt(m2);
