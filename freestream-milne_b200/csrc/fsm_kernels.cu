@@ -1034,10 +1034,10 @@ __global__ void __launch_bounds__(256) fsm_pack_kernel(const float* __restrict__
 }
 
 // ----------------------------------------------------------------- Landau
-// Seven 128-thread blocks per SM (73 registers, some spilled to L1): the
+// Eight 128-thread blocks per SM (64 registers, some spilled to L1): the
 // solver is latency-bound, and the extra warps gain more than the spills cost
-// (measured against 4, 5, 6 and 8 blocks, and 64- and 256-thread blocks).
-__global__ void __launch_bounds__(kThreadsLandau, 7) fsm_landau_kernel(const EvLandau* __restrict__ evs,
+// (measured against 4 to 7 blocks, and 64- and 256-thread blocks).
+__global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvLandau* __restrict__ evs,
                                                                     const CellBlock* __restrict__ blocks,
                                                                     Counters* ctr) {
   const CellBlock b = blocks[blockIdx.x];

@@ -266,7 +266,7 @@ FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, 
   if (u[0] < 0.0) s = -s;
 #pragma unroll
   for (int r = 0; r < N; ++r) u[r] *= s;
-  double e = rayleigh<double, N>(M, g, u);
+  double e = rayleigh_unit<double, N>(M, g, u);  // u.g.u = 1 up to rounding
   double rmax = 0.0, mmax = 0.0, umax = 0.0;
   bool have = false;  // the residual of the current (e, u) is at hand
   for (int it = 0; it < 12; ++it) {
