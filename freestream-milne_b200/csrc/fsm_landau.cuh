@@ -289,21 +289,21 @@ FSM_HD int landau_eigen(const double M[N][N], const double g[N], double* e_out, 
 // timelike iff 2 v0^2 - 1 - v3^2 (tau^2 - 1) > 0 and u = v / sqrt(v0^2 -
 // (v1^2 + v2^2 + tau^2 v3^2)), where tau^2 is the float product TAU*TAU (the
 // index itself was lowered with the double product).  Accept iff u^tau < 100.
+// Both tests and u are invariant under a positive rescaling of v, so they are
+// evaluated on w itself (multiplied through by |w|^2) without normalising it.
 FSM_HD int reference_normalise(const double w[4], float TAU, double u[4]) {
-  const double n = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-  if (!(n > 0.0)) return 0;
-  const double in = 1.0 / n;
-  const double v0 = w[0] * in, v1 = w[1] * in, v2 = w[2] * in, v3 = w[3] * in;
+  const double n2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
+  if (!(n2 > 0.0)) return 0;
   const float tt = TAU * TAU;  // float product, as the reference
-  if (!((2.0 * v0 * v0 - 1.0 - (v3 * v3 * (tt - 1.0))) > 0)) return 0;
-  const double mink = v0 * v0 - (v1 * v1 + v2 * v2 + tt * v3 * v3);
+  if (!((2.0 * w[0] * w[0] - n2 - (w[3] * w[3] * (tt - 1.0))) > 0)) return 0;
+  const double mink = w[0] * w[0] - (w[1] * w[1] + w[2] * w[2] + tt * w[3] * w[3]);
   double factor = fsm_rsqrt(mink);
-  if (v0 < 0) factor = -factor;
-  if (!((v0 * factor) < 100.0)) return 0;
-  u[0] = v0 * factor;
-  u[1] = v1 * factor;
-  u[2] = v2 * factor;
-  u[3] = v3 * factor;
+  if (w[0] < 0) factor = -factor;
+  if (!((w[0] * factor) < 100.0)) return 0;
+  u[0] = w[0] * factor;
+  u[1] = w[1] * factor;
+  u[2] = w[2] * factor;
+  u[3] = w[3] * factor;
   return 1;
 }
 
