@@ -69,14 +69,33 @@ __global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_rows_kernel(
     for (int c = lane; c < ld; c += 32) fl[c] = 0.0f;  // padding (and rows past the grid)
   }
   __syncthreads();
-  for (int r = warp; r < nr; r += kPrepThreads / 32) {
-    const size_t row = (size_t)(ix0 + r) * NY;
-    float* fl = Fs + r * ld + kPadLo;
-    for (int c = lane; c < NY; c += 32) {
-      const float in = __ldg(ev.e_gev + row + c);
-      const float f = ev.charge ? __fmul_rn(in, ev.qnorm) : F_of(in);
-      fl[c] = f;
-      ev.fa[row + c] = f;
+  {
+    // 8 independent loads in flight per thread before their stores (the
+    // descriptor's pointers may alias as far as the compiler knows, so it
+    // would not hoist a load above the preceding store by itself)
+    const float* __restrict__ src = ev.e_gev;
+    float* __restrict__ fa = ev.fa;
+    constexpr int kB = 8;
+    for (int r = warp; r < nr; r += kPrepThreads / 32) {
+      const size_t row = (size_t)(ix0 + r) * NY;
+      float* fl = Fs + r * ld + kPadLo;
+      for (int c0 = lane; c0 < NY; c0 += 32 * kB) {
+        float in[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          const int c = c0 + 32 * u;
+          in[u] = c < NY ? __ldg(src + row + c) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          const int c = c0 + 32 * u;
+          if (c < NY) {
+            const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u]);
+            fl[c] = f;
+            fa[row + c] = f;
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -119,16 +138,31 @@ __global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_cols_kernel(
   float* Fs = reinterpret_cast<float*>(tab + np);
   float* Ys = Fs + 32 * np;
   stage_axis(tab, ev.ax, NX);
-  for (int i = warp; i < np; i += kPrepThreads / 32) {
-    const int ix = i - kPadLo;
-    float f = 0.0f, yv = 0.0f;
-    if (ix >= 0 && ix < NX && lane < nc) {
-      const size_t k = (size_t)ix * NY + iy0 + lane;
-      f = __ldg(ev.fa + k);
-      yv = __ldg(ev.sy + k);
+  {
+    constexpr int kB = 4;  // independent loads in flight per thread
+    const float* __restrict__ fa = ev.fa;
+    const float* __restrict__ sy = ev.sy;
+    for (int i0 = warp; i0 < np; i0 += (kPrepThreads / 32) * kB) {
+      float f[kB], yv[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int i = i0 + (kPrepThreads / 32) * u, ix = i - kPadLo;
+        f[u] = yv[u] = 0.0f;
+        if (i < np && ix >= 0 && ix < NX && lane < nc) {
+          const size_t k = (size_t)ix * NY + iy0 + lane;
+          f[u] = __ldg(fa + k);
+          yv[u] = __ldg(sy + k);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int i = i0 + (kPrepThreads / 32) * u;
+        if (i < np) {
+          Fs[i * 32 + lane] = f[u];
+          Ys[i * 32 + lane] = yv[u];
+        }
+      }
     }
-    Fs[i * 32 + lane] = f;
-    Ys[i * 32 + lane] = yv;
   }
   __syncthreads();
   if (lane >= nc) return;
@@ -445,7 +479,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
   const float2 ey2 = make_float2(ey, ey);
   for (int p = p0; p < p1; ++p) {
     const float4* e = stab + kPhiTab2D * (p - p0);
-    const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], mw = e[4], tu = e[5];
+    const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
     const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
     const int oy = (int)(short)(oyn & 0xffff);
     const int j = iy + oy, i0 = ixb + ox;
@@ -499,6 +533,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
         }
       }
     }
+    const float4 mw = e[4];
     if (!kInterior) {
       const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
       const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
