@@ -203,11 +203,27 @@ __global__ void __launch_bounds__(kPrepRows * 32) fsm_prep2d_rows_long_kernel(
   const size_t row = (size_t)ix * NY;
   for (int c = lane; c < NY + kPadLo + kPadHi; c += 32) fr[c] = 0.0f;
   __syncwarp();
-  for (int c = lane; c < NY; c += 32) {
-    const float in = __ldg(ev.e_gev + row + c);
-    const float f = ev.charge ? __fmul_rn(in, ev.qnorm) : F_of(in);
-    fr[kPadLo + c] = f;
-    ev.fa[row + c] = f;
+  {
+    const float* __restrict__ src = ev.e_gev;
+    float* __restrict__ fa = ev.fa;
+    constexpr int kB = 8;  // independent loads in flight per thread
+    for (int c0 = lane; c0 < NY; c0 += 32 * kB) {
+      float in[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int c = c0 + 32 * u;
+        in[u] = c < NY ? __ldg(src + row + c) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int c = c0 + 32 * u;
+        if (c < NY) {
+          const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u]);
+          fr[kPadLo + c] = f;
+          fa[row + c] = f;
+        }
+      }
+    }
   }
   __syncwarp();
   const float* fl = fr + kPadLo;

@@ -11,11 +11,112 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
+#include <mutex>
+#include <functional>
+#include <condition_variable>
+#include <atomic>
 
 namespace fsm {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int& parallel_depth();
+
+namespace {
+
+// Worker threads started on first use and kept for the life of the process
+// (blocked on a condition variable between jobs).
+struct WorkerPool {
+  std::mutex busy;  // one job at a time
+  std::mutex m;
+  std::condition_variable cv, cv_done;
+  const std::function<void(int)>* f = nullptr;
+  int n = 0, want = 0, running = 0;
+  std::atomic<int> next{0};
+  unsigned long long gen = 0;
+  std::vector<std::thread> th;
+
+  explicit WorkerPool(int workers) {
+    for (int t = 0; t < workers; ++t) th.emplace_back([this, t] { loop(t); });
+  }
+  void drain() {
+    for (int i; (i = next.fetch_add(1)) < n;) (*f)(i);
+  }
+  void loop(int t) {
+    unsigned long long seen = 0;
+    std::unique_lock<std::mutex> lk(m);
+    for (;;) {
+      cv.wait(lk, [&] { return gen != seen; });
+      seen = gen;
+      if (t >= want) continue;  // this job uses fewer threads
+      lk.unlock();
+      ++parallel_depth();
+      drain();
+      --parallel_depth();
+      lk.lock();
+      if (--running == 0) cv_done.notify_all();
+    }
+  }
+};
+
+WorkerPool& worker_pool() {
+  static WorkerPool* pool = new WorkerPool(host_threads() - 1);  // kept until exit
+  return *pool;
+}
+
+}  // namespace
+
+int host_threads() {
+  static const int n = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+  return n;
+}
+
+int& parallel_depth() {
+  static thread_local int d = 0;
+  return d;
+}
+
+void run_parallel(int n, int threads, const std::function<void(int)>& f) {
+  threads = std::min(std::min(threads, n), host_threads());
+  if (threads <= 1 || parallel_depth() > 0) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  WorkerPool& P = worker_pool();
+  std::unique_lock<std::mutex> job(P.busy, std::try_to_lock);
+  if (!job.owns_lock()) {  // another host thread is using the pool
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  {
+    std::lock_guard<std::mutex> g(P.m);
+    P.f = &f;
+    P.n = n;
+    P.next = 0;
+    P.want = threads - 1;
+    P.running = threads - 1;
+    ++P.gen;
+  }
+  P.cv.notify_all();
+  ++parallel_depth();
+  P.drain();
+  --parallel_depth();
+  std::unique_lock<std::mutex> lk(P.m);
+  P.cv_done.wait(lk, [&] { return P.running == 0; });
+  P.f = nullptr;
+}
+
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPiece = (size_t)1 << 20;
+  const int pieces = (int)((bytes + kPiece - 1) / kPiece);
+  parallel_for(pieces, bytes >= 4 * kPiece ? host_threads() : 1, [&](int k) {
+    const size_t o = (size_t)k * kPiece;
+    std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o,
+                std::min(kPiece, bytes - o));
+  });
+}
 
 int output_components(bool baryon) { return baryon ? 36 : 27; }
 
@@ -273,7 +374,9 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
   const float rapmin = (-1.0) * ((float)(NR - 1) / 2.0) * p.DRAP;
   const float SIGMA = p.SIGMA, SIGMA_B = p.SIGMA_B;
   std::vector<int> live_cnt(NR, 0);
-  for (int ieta = 0; ieta < NE; ++ieta) {
+  std::vector<char> live_pair((size_t)NE * NR, 0);
+  const int plan_threads = (double)NE * NR * NP > 1.0e5 ? host_threads() : 1;
+  parallel_for(NE, plan_threads, [&](int ieta) {
     float eta = (float)ieta * DETA + E.etamin;
     for (int irap = 0; irap < NR; ++irap) {
       float w = tanmap_w(irap, NR);
@@ -309,11 +412,12 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       float du = eta - rapu;
       E.rapfB[(size_t)ieta * NR + irap] =
           std::cosh(du) * std::exp((-1.0) * du * du / (SIGMA_B * SIGMA_B));
-      bool live = (r.efl >= 1 && r.efl < NE - 1) && std::isfinite(D) &&
-                  std::fabs(D) <= (float)(NX + NY) * std::max(p.DX, p.DY);
-      if (live) live_cnt[irap] += 1;
+      live_pair[(size_t)ieta * NR + irap] = (r.efl >= 1 && r.efl < NE - 1) && std::isfinite(D) &&
+                                             std::fabs(D) <= (float)(NX + NY) * std::max(p.DX, p.DY);
     }
-  }
+  });
+  for (int ieta = 0; ieta < NE; ++ieta)
+    for (int irap = 0; irap < NR; ++irap) live_cnt[irap] += live_pair[(size_t)ieta * NR + irap];
   E.r_lo = NR;
   E.r_hi = 0;
   double live_pairs = 0;
@@ -334,7 +438,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
   // (src/FreeStream.cpp:193-212) for every live (ieta, irap) and phi_p
   E.tab3.assign((size_t)NE * NR * NP, PhiEntry3D{0.0f, 0.0f, 0, 0});
   E.live_eta.assign(NE, 0);
-  for (int ieta = 0; ieta < NE; ++ieta)
+  parallel_for(NE, plan_threads, [&](int ieta) {
     for (int irap = E.r_lo; irap < E.r_hi; ++irap) {
       const RapEta& r = E.re[(size_t)ieta * NR + irap];
       if (!(r.efl >= 1 && r.efl < NE - 1 && std::isfinite(r.D))) continue;
@@ -358,6 +462,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
         w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
       }
     }
+  });
   return FSM_OK;
 }
 

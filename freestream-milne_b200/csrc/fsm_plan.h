@@ -3,6 +3,7 @@
 // compiled by the host compiler with FMA contraction disabled so that every
 // table entry is rounded exactly as the reference computes it.
 #pragma once
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -10,6 +11,20 @@
 #include "fsm_internal.h"
 
 namespace fsm {
+
+// Host threads for planning and staging copies (at most 16).
+int host_threads();
+// Runs f(i) for i in [0, n) on up to `threads` threads of a process-wide
+// worker pool (the caller's thread included).  Serial for threads <= 1,
+// inside another parallel_for (nested loops never multiply the thread count)
+// and while another host thread has the pool.
+void run_parallel(int n, int threads, const std::function<void(int)>& f);
+template <class F>
+void parallel_for(int n, int threads, F f) {
+  run_parallel(n, threads, std::function<void(int)>(f));
+}
+// memcpy in 1 MiB pieces on several threads when it is large.
+void parallel_copy(void* dst, const void* src, size_t bytes);
 
 struct EventPlan {
   fsm_params p;  // effective parameters (E_DEP_FS and phi_p rule applied, DIM/TAU set)

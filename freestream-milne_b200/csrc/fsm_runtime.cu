@@ -102,14 +102,24 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->ctx = ctx;
   b->own_io = (ext_in_e == nullptr);
   b->plans.resize(n);
-  for (int i = 0; i < n; ++i) {
-    std::string why;
-    fsm_status s = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why,
-                              ctx->window_budget);
-    if (s != FSM_OK) {
-      set_last_error("event " + std::to_string(i) + ": " + why);
-      return s;
-    }
+  {
+    // events are planned independently: several host threads when the tables
+    // are large (3D events: one entry per eta slice x rapidity x phi_p)
+    double work = 0;
+    for (int i = 0; i < n; ++i)
+      work += (double)std::max(1, params[i].DIM_ETA) * std::max(1, params[i].DIM_RAP) *
+              std::max(1, params[i].DIM_PHIP);
+    std::vector<fsm_status> st(n, FSM_OK);
+    std::vector<std::string> why(n);
+    parallel_for(n, work > 2.0e5 ? host_threads() : 1, [&](int i) {
+      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i],
+                         ctx->window_budget);
+    });
+    for (int i = 0; i < n; ++i)
+      if (st[i] != FSM_OK) {  // the first failing event, as a serial loop would report
+        set_last_error("event " + std::to_string(i) + ": " + why[i]);
+        return st[i];
+      }
   }
   // ---- layout
   Layout L;
@@ -304,10 +314,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   std::memset(H, 0, upload_bytes);
   b->desc_off = o_ev2;
   b->desc_bytes = o_tiles - o_ev2;
-  // ---- fill tables
-  for (int i = 0; i < n; ++i) {
+  // ---- fill tables (per event; several threads for large tables)
+  parallel_for(n, upload_bytes > ((size_t)8 << 20) ? host_threads() : 1, [&](int i) {
     const EventPlan& P = b->plans[i];
-    EvOffs& o = eo[i];
+    const EvOffs& o = eo[i];
     std::memcpy(H + o.cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
     if (!P.is3d) {
       std::memcpy(H + o.tab2, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
@@ -319,9 +329,9 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       std::memcpy(H + o.rapf, P.rapf.data(), P.rapf.size() * 4);
       std::memcpy(H + o.rapfB, P.rapfB.data(), P.rapfB.size() * 4);
       std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
-      std::memcpy(H + o.tab3, P.tab3.data(), P.tab3.size() * sizeof(PhiEntry3D));
+      parallel_copy(H + o.tab3, P.tab3.data(), P.tab3.size() * sizeof(PhiEntry3D));
     }
-  }
+  });
   // ---- output slab layout: per event (default) or group by group
   b->grouped_out = mem && mem->grouped_out;
   b->out_goff.assign(n, {});

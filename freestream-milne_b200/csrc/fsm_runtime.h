@@ -4,8 +4,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 

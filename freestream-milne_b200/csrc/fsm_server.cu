@@ -304,13 +304,17 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
       if (!w->hin || !w->hout) st = FSM_ERR_OUT_OF_MEMORY;
     }
     if (st == FSM_OK) {
-      // inputs into the pinned slab, then the stream work of the wave
+      // inputs into the pinned slab, without the lock (the slab is this
+      // wave's, the requests' inputs are read-only after submit), large ones
+      // on several threads; then the stream work of the wave
+      lk.unlock();
       for (size_t i = 0; i < take.size(); ++i) {
         float* dst = reinterpret_cast<float*>(w->hin) + b->in_off[i];
         const size_t n = take[i]->e.size();
-        std::memcpy(dst, take[i]->e.data(), n * 4);
-        if (b->plans[i].baryon) std::memcpy(dst + n, take[i]->nB.data(), n * 4);
+        parallel_copy(dst, take[i]->e.data(), n * 4);
+        if (b->plans[i].baryon) parallel_copy(dst + n, take[i]->nB.data(), n * 4);
       }
+      lk.lock();
       cudaError_t ce = cudaMemcpyAsync(b->d_mem + b->in_slab_off, w->hin, b->in_slab_bytes,
                                        cudaMemcpyHostToDevice, s);
       if (ce == cudaSuccess) st = enqueue(b, s, false);
