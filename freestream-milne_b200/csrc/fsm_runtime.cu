@@ -814,22 +814,29 @@ extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const flo
   if (!ctx || !p || !e_gev || !host_out) return FSM_ERR_INVALID_ARG;
   if (p->BARYON && !nB) return FSM_ERR_INVALID_ARG;
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
-  EventPlan P;
-  std::string why;
-  fsm_status s = plan_event(*p, e_gev, &P, &why, ctx->window_budget);
-  if (s != FSM_OK) {
-    set_last_error(why);
-    return s;
-  }
+  fsm_status s;
   fsm_batch* b = ctx->single_host;
-  if (!b || !same_params(b->plans[0].p, P.p)) {
-    batch_free(ctx->single_host);
-    ctx->single_host = nullptr;
-    const float* he[1] = {e_gev};
-    s = batch_build(ctx, 1, p, he, nullptr, nullptr, nullptr, &ctx->single_host);
-    if (s != FSM_OK) return s;
-    b = ctx->single_host;
+  // the cached batch serves the same parameters again without planning (an
+  // energy-dependent DTAU depends on the profile, so those events re-plan)
+  if (!b || p->E_DEP_FS != 0 || !same_params(ctx->single_host_raw, *p)) {
+    EventPlan P;
+    std::string why;
+    s = plan_event(*p, e_gev, &P, &why, ctx->window_budget);
+    if (s != FSM_OK) {
+      set_last_error(why);
+      return s;
+    }
+    if (!b || !same_params(b->plans[0].p, P.p)) {
+      batch_free(ctx->single_host);
+      ctx->single_host = nullptr;
+      const float* he[1] = {e_gev};
+      s = batch_build(ctx, 1, p, he, nullptr, nullptr, nullptr, &ctx->single_host);
+      if (s != FSM_OK) return s;
+      b = ctx->single_host;
+    }
+    ctx->single_host_raw = *p;
   }
+  const EventPlan& P = b->plans[0];
   cudaStream_t st = ctx->stream;
   const size_t DIM = P.DIM;
   FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_e[0], e_gev, DIM * 4, cudaMemcpyHostToDevice, st));
@@ -854,7 +861,7 @@ extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const flo
   }
   FSM_CUDA_TRY(cudaStreamSynchronize(st));
   if ((s = check_kernel_errors(b)) != FSM_OK) return s;
-  return fill_info(b->plans[0], info);
+  return fill_info(P, info);
 }
 
 extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* d_e_gev,

@@ -73,9 +73,10 @@ struct fsm_ctx {
   // energy-dependent DTAU of device profiles: sums on the device, read back
   float* d_sums = nullptr;
   float* h_sums = nullptr;
-  // cached one-event batches
+  // cached one-event batches (single_host_raw: the caller's parameters it was built for)
   fsm_batch* single_host = nullptr;
   fsm_batch* single_dev = nullptr;
+  fsm_params single_host_raw{};
 };
 
 struct fsm_batch {
