@@ -16,6 +16,7 @@
 #include <functional>
 #include <condition_variable>
 #include <atomic>
+#include <unistd.h>
 
 namespace fsm {
 
@@ -27,8 +28,10 @@ int& parallel_depth();
 namespace {
 
 // Worker threads started on first use and kept for the life of the process
-// (blocked on a condition variable between jobs).
+// (blocked on a condition variable between jobs).  A child created by fork()
+// inherits the pool object but none of its threads: it runs loops serially.
 struct WorkerPool {
+  const pid_t owner = getpid();
   std::mutex busy;  // one job at a time
   std::mutex m;
   std::condition_variable cv, cv_done;
@@ -86,7 +89,7 @@ void run_parallel(int n, int threads, const std::function<void(int)>& f) {
   }
   WorkerPool& P = worker_pool();
   std::unique_lock<std::mutex> job(P.busy, std::try_to_lock);
-  if (!job.owns_lock()) {  // another host thread is using the pool
+  if (!job.owns_lock() || P.owner != getpid()) {  // in use by another host thread, or forked
     for (int i = 0; i < n; ++i) f(i);
     return;
   }
