@@ -81,6 +81,16 @@ def test_no_cpu_fallback_without_device():
     assert st == 6  # FSM_ERR_NO_DEVICE: the library never computes on the CPU
 
 
+def test_batch_download_entry_points_reject_null_batches():
+    L = F.lib()
+    assert L.fsm_batch_create_ex(None, 1, None, 0, None) == 1  # FSM_ERR_INVALID_ARG
+    assert L.fsm_batch_download_groups(None, 1, None, None) == 1
+    assert L.fsm_batch_download_packed(None, 1, F.PACK_SKIP_ETA, None, None) == 1
+    assert L.fsm_batch_packed_offset(None, 1, 0, 0, 0, 0, None) == 1
+    assert L.fsm_batch_group_offset(None, 1, 0, 0, None) == 1
+    assert L.fsm_batch_groups_bytes(None, 1) == 0 and L.fsm_batch_packed_bytes(None, 1, 0) == 0
+
+
 def _host_landau():
     L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
     L.fsm_hosttest_landau_cell.argtypes = ([ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 +
