@@ -3,6 +3,7 @@
 // so unit tests can exercise their logic against the oracle without a GPU.
 // Not part of libfsm.so; the product runs the same headers only inside its
 // kernels.
+#include <string>
 #include <vector>
 
 #include "fsm_landau.cuh"
@@ -40,4 +41,32 @@ extern "C" int fsm_hosttest_landau_cell(const float* T10, const float* J4, int i
   for (int k = 0; k < 4; ++k) out24[18 + k] = o.V[k];
   out24[22] = (float)o.fallback;
   return o.fallback ? 0 : 1;
+}
+
+// FNV-1a digest of the tables plan_event builds for *p, planned on the worker
+// pool (serial = 0) or on the calling thread only (serial = 1).  Returns the
+// plan status.
+extern "C" int fsm_hosttest_plan_digest(const fsm_params* p, int serial, unsigned long long* digest) {
+  fsm::EventPlan E;
+  std::string why;
+  if (serial) ++fsm::parallel_depth();
+  const fsm_status s = fsm::plan_event(*p, nullptr, &E, &why);
+  if (serial) --fsm::parallel_depth();
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](const void* data, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  mix(E.cs.data(), E.cs.size() * sizeof(E.cs[0]));
+  mix(E.tab2.data(), E.tab2.size() * sizeof(E.tab2[0]));
+  mix(E.chunks2.data(), E.chunks2.size() * sizeof(E.chunks2[0]));
+  mix(E.re.data(), E.re.size() * sizeof(E.re[0]));
+  mix(E.rapf.data(), E.rapf.size() * 4);
+  mix(E.rapfB.data(), E.rapfB.size() * 4);
+  mix(E.tab3.data(), E.tab3.size() * sizeof(E.tab3[0]));
+  mix(E.live_eta.data(), E.live_eta.size() * sizeof(E.live_eta[0]));
+  mix(&E.r_lo, sizeof(E.r_lo));
+  mix(&E.r_hi, sizeof(E.r_hi));
+  *digest = h;
+  return (int)s;
 }

@@ -124,16 +124,10 @@ struct Ev2D {
   int NX, NY, NPHI, NR;
   float DX, DY, DTAU, TAU;
   float xmin, ymin, xmax_i, ymax_i;  // grid origin and spline domain (src/FreeStream.cpp:113,142-146)
-  float inv_dx, inv_dy;
   float d_phip;
-  int Rx, Ry;        // footprint halo in cells
-  int use_smem;      // footprint fits the block's shared memory
-  int tiles_y;       // tiles along y
-  const FSM_FLOAT2* cs;  // [NPHI] (cos phi_p, sin phi_p), float as the reference computes them
   const PhiEntry2D* tab; // [NPHI]
   const Chunk2D* chunks; // [nchunks]
   int nchunks;
-  int boxW, boxH;        // staged window (columns = y nodes, rows = x nodes)
   // prep
   const float* e_gev;    // input
   const AxisNode* ax;   // [NX] x-axis spline data
@@ -186,7 +180,6 @@ struct Ev3D {
   int baryon;
   float DX, DY;
   float xmin, ymin;
-  float inv_dx, inv_dy;
   float norm, normB, d_phip, DRAP;
   const FSM_FLOAT2* cs;   // [NPHI]
   const RapEta* re;       // [NE*NR]

@@ -10,10 +10,12 @@
 // eigenvector and Rayleigh-quotient iteration converges fast (cubically).
 // The iteration starts from the energy-flux direction u0^mu = T^{mu tau}
 // (timelike for any T^{mu nu} built from non-negative phase-space densities);
-// each step solves (M - e I) y = u by Gaussian elimination with partial
-// pivoting, which is backward stable, so strongly boosted cells (entries ~
-// gamma^2 e, eigenvalues ~ e) keep their accuracy.  The first steps run in
-// FP32, the converging ones and the acceptance test in FP64.
+// each step solves (M - e I) y = u: in 3D by Gaussian elimination with partial
+// pivoting (backward stable), for the 3 x 3 boost-invariant problem through
+// the adjugate with FMA-exact 2 x 2 cofactors (no division, no pivoting), so
+// strongly boosted cells (entries ~ gamma^2 e, eigenvalues ~ e) keep their
+// accuracy either way.  The first steps run in FP32, the converging ones and
+// the acceptance test in FP64.
 //
 // Acceptance mirrors src/LandauMatch.cpp:222-291: the eigenvalue must be real
 // and positive, the eigenvector timelike and the boost factor u^tau below 100;

@@ -193,19 +193,10 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   e.ymin = P.ymin;
   e.xmax_i = P.xmax_i;
   e.ymax_i = P.ymax_i;
-  e.inv_dx = 1.0f / P.p.DX;
-  e.inv_dy = 1.0f / P.p.DY;
   e.d_phip = P.d_phip;
-  e.Rx = P.Rx;
-  e.Ry = P.Ry;
-  e.use_smem = 1;
-  e.tiles_y = (NY + kTileY - 1) / kTileY;
-  e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o_cs);
   e.tab = reinterpret_cast<const PhiEntry2D*>(D + o_tab);
   e.chunks = reinterpret_cast<const Chunk2D*>(D + o_chunks);
   e.nchunks = (int)P.chunks2.size();
-  e.boxW = P.boxW;
-  e.boxH = P.boxH;
   e.e_gev = d_e_gev;
   e.ax = reinterpret_cast<const AxisNode*>(D + o_axx) + kPadLo;
   e.ay = reinterpret_cast<const AxisNode*>(D + o_axy) + kPadLo;

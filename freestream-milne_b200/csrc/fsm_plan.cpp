@@ -23,8 +23,6 @@ namespace fsm {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-int& parallel_depth();
-
 namespace {
 
 // Worker threads started on first use and kept for the life of the process
@@ -282,7 +280,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
         return (size_t)(kTileX + dox + 3) * (size_t)(kTileY + doy + 3) * 16;
       };
       E.chunks2.clear();
-      E.boxW = E.boxH = E.box_elems = 0;
+      E.box_elems = 0;
       int p0 = 0;
       auto oy_of = [&](int k) { return (int)(short)(E.tab2[k].oy_near & 0xffff); };
       int lo_x = E.tab2[0].ox, hi_x = lo_x, lo_y = oy_of(0), hi_y = lo_y;
@@ -301,8 +299,6 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
         }
         if (flush) {
           E.chunks2.push_back(Chunk2D{p0, k, lo_x, lo_y, hi_x, hi_y});
-          E.boxH = std::max(E.boxH, kTileX + (hi_x - lo_x) + 3);
-          E.boxW = std::max(E.boxW, kTileY + (hi_y - lo_y) + 3);
           E.box_elems = std::max(E.box_elems, (kTileX + (hi_x - lo_x) + 3) * (kTileY + (hi_y - lo_y) + 3));
           if (k < NP) {
             p0 = k;
@@ -320,8 +316,6 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       const bool few = (int)E.chunks2.size() <= std::max(kMaxChunks2D, 2 * min_runs);
       if (few || budget * 3 / 2 > kMaxWindow2D) break;
     }
-    E.Rx = (int)std::ceil(p.DTAU / p.DX) + 2;
-    E.Ry = (int)std::ceil(p.DTAU / p.DY) + 2;
     E.samples = (double)p.DIM * NP;
     E.ref_samples = (double)p.DIM * NR * NP;
     if (E.baryon) {

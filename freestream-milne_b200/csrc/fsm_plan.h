@@ -14,6 +14,8 @@ namespace fsm {
 
 // Host threads for planning and staging copies (at most 16).
 int host_threads();
+// Nesting depth of parallel_for on this thread (loops run serially above 0).
+int& parallel_depth();
 // Runs f(i) for i in [0, n) on up to `threads` threads of a process-wide
 // worker pool (the caller's thread included).  Serial for threads <= 1,
 // inside another parallel_for (nested loops never multiply the thread count)
@@ -35,12 +37,10 @@ struct EventPlan {
   std::vector<FSM_FLOAT2> cs;  // (cos, sin) of phi_p
   std::vector<PhiEntry2D> tab2;  // 2D stream table
   std::vector<Chunk2D> chunks2;  // phi_p runs staged as one window each
-  int boxW = 0, boxH = 0;        // largest staged window width / height over the runs (nodes)
   int box_elems = 0;             // largest staged window (nodes) of one run
   int ox_min = 0, ox_max = 0, oy_min = 0, oy_max = 0;  // offset range over all phi_p
   // 2D spline axes
   std::vector<AxisNode> axx, axy;
-  int Rx = 0, Ry = 0;
   // 3D tables
   std::vector<RapEta> re;
   std::vector<PhiEntry3D> tab3;  // [NE*NR*NPHI]

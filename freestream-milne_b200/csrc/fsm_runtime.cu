@@ -413,8 +413,6 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->ev3.assign(n3, Ev3D{});
   b->evl.assign(n, EvLandau{});
   int max_np2 = 0, max_np3 = 0;
-  size_t max_fp = 0;
-  const size_t smem_budget = 84 * 1024;  // footprint bytes staged per CTA (2 CTAs/SM with the table)
   for (int i = 0; i < n; ++i) {
     const EventPlan& P = b->plans[i];
     const EvOffs& o = eo[i];
@@ -433,24 +431,11 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.ymin = P.ymin;
       e.xmax_i = P.xmax_i;
       e.ymax_i = P.ymax_i;
-      e.inv_dx = 1.0f / p.DX;
-      e.inv_dy = 1.0f / p.DY;
       e.d_phip = P.d_phip;
-      e.Rx = P.Rx;
-      e.Ry = P.Ry;
-      size_t fpw = std::min(p.DIM_Y, kTileY + 2 * P.Ry + 1);
-      size_t fph = std::min(p.DIM_X, kTileX + 2 * P.Rx + 1);
-      size_t fp = fpw * fph * 16;
       e.tab = reinterpret_cast<const PhiEntry2D*>(D + o.tab2);
       e.chunks = reinterpret_cast<const Chunk2D*>(D + o.chunks);
       e.nchunks = (int)P.chunks2.size();
-      e.boxW = P.boxW;
-      e.boxH = P.boxH;
       b->box_cap2 = std::max(b->box_cap2, P.box_elems);
-      e.use_smem = fp <= smem_budget ? 1 : 0;
-      if (e.use_smem) max_fp = std::max(max_fp, fp);
-      e.tiles_y = (p.DIM_Y + kTileY - 1) / kTileY;
-      e.cs = reinterpret_cast<const FSM_FLOAT2*>(D + o.cs);
       e.e_gev = b->d_in_e[i];
       e.ax = reinterpret_cast<const AxisNode*>(D + o.axx) + kPadLo;
       e.ay = reinterpret_cast<const AxisNode*>(D + o.axy) + kPadLo;
@@ -490,8 +475,6 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.DY = p.DY;
       e.xmin = P.xmin;
       e.ymin = P.ymin;
-      e.inv_dx = 1.0f / p.DX;
-      e.inv_dy = 1.0f / p.DY;
       e.norm = P.norm;
       e.normB = P.normB;
       e.d_phip = P.d_phip;
@@ -535,7 +518,6 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->smem3 = (size_t)kThreads3D * kCellsPerThread * 23 * 4;  // thread-private moment slots
   b->smem_rows = prep_rows_smem(b->ny_cap2);
   b->smem_strip = prep_strip_smem(b->strip_cap2);
-  (void)max_fp;
   // the kernels index their dynamic shared memory by these capacities
   if (n3 && b->smem3 == 0) {
     set_last_error("internal error: dynamic shared memory below the staged tables");

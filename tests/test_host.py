@@ -91,6 +91,25 @@ def test_batch_download_entry_points_reject_null_batches():
     assert L.fsm_batch_groups_bytes(None, 1) == 0 and L.fsm_batch_packed_bytes(None, 1, 0) == 0
 
 
+def test_parallel_planning_matches_serial():
+    """The planner's tables are identical whether the worker pool plans the
+    eta slices of a 3D event in parallel or one thread plans them."""
+    import workloads as W
+    L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
+    L.fsm_hosttest_plan_digest.argtypes = [ctypes.POINTER(F.Params), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_ulonglong)]
+    cases = [W.baryon3d(seed=1, side=41, neta=51, nrap=41)[0],
+             W.baryon3d(seed=2, side=31, neta=25, nrap=21, nphip=40)[0],
+             W.lumpy2d(seed=3, side=61, nphip=300)[0]]
+    for p in cases:
+        d = []
+        for serial in (1, 0, 0):
+            h = ctypes.c_ulonglong()
+            assert L.fsm_hosttest_plan_digest(ctypes.byref(p), serial, ctypes.byref(h)) == 0
+            d.append(h.value)
+        assert d[0] == d[1] == d[2], (p.DIM_ETA, p.DIM_RAP, d)
+
+
 def _host_landau():
     L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
     L.fsm_hosttest_landau_cell.argtypes = ([ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 +
@@ -127,8 +146,9 @@ def _boosted_fluid(rng, is3d, tau):
 
 
 def test_landau_algorithm_matches_oracle_on_boosted_fluids():
-    """RQI + partial-pivoting solver (the kernel's algorithm) vs the oracle's
-    Francis-QR solver with the reference's selection rules."""
+    """The kernel's Rayleigh-quotient iteration (adjugate steps for the 3 x 3
+    boost-invariant problem, partial pivoting in 3D) vs the oracle's Francis-QR
+    solver with the reference's selection rules."""
     L = _host_landau()
     rng = np.random.default_rng(5)
     tau = 1.3
