@@ -493,101 +493,106 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
   constexpr int K = kCellsPerThread;
   const int NX = ev.NX, NY = ev.NY;
   const float2 ey2 = make_float2(ey, ey);
-  for (int p = p0; p < p1; ++p) {
-    const float4* e = stab + kPhiTab2D * (p - p0);
-    const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
-    const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
-    const int oy = (int)(short)(oyn & 0xffff);
-    const int j = iy + oy, i0 = ixb + ox;
-    // y weights of this lane, first-order corrected for its own coordinate
-    const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
-    const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
-    const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
-    if (ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+  // phi_p in pieces that end at the fold points of the two-level sum, so the
+  // inner loop carries no fold test
+  for (int pc = p0; pc < p1;) {
+    const int pe = min(p1, (pc | (kPhiChunk - 1)) + 1);
+    for (int p = pc; p < pe; ++p) {
+      const float4* e = stab + kPhiTab2D * (p - p0);
+      const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
+      const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
+      const int oy = (int)(short)(oyn & 0xffff);
+      const int j = iy + oy, i0 = ixb + ox;
+      // y weights of this lane, first-order corrected for its own coordinate
+      const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
+      const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
+      const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
+      if (ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+#pragma unroll
+        for (int r = 0; r <= K; ++r) {
+          nd0[r] = rowp[r * boxW];
+          nd1[r] = rowp[r * boxW + 1];
+        }
+        pox = ox;
+        poy = oy;
+      }
+      float cv[K];
+      float2 VDp = make_float2(0.f, 0.f);
 #pragma unroll
       for (int r = 0; r <= K; ++r) {
-        nd0[r] = rowp[r * boxW];
-        nd1[r] = rowp[r * boxW + 1];
-      }
-      pox = ox;
-      poy = oy;
-    }
-    float cv[K];
-    float2 VDp = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int r = 0; r <= K; ++r) {
-      const float4 n0 = nd0[r], n1 = nd1[r];
-      // y pass of the node row: (value, x-slope) interpolated to the sample's y
-      float2 VD = __fmul2_rn(make_float2(Kp.x, Kp.x), make_float2(n0.x, n0.y));
-      VD = __ffma2_rn(make_float2(Kp.y, Kp.y), make_float2(n1.x, n1.y), VD);
-      VD = __ffma2_rn(make_float2(Lp.x, Lp.x), make_float2(n0.z, n0.w), VD);
-      VD = __ffma2_rn(make_float2(Lp.y, Lp.y), make_float2(n1.z, n1.w), VD);
-      if (r > 0) {
-        const int k = r - 1;
-        const float2 ex2 = make_float2(ex[k], ex[k]);
-        const float2 HG0 = __ffma2_rn(ex2, make_float2(dwx.x, dwx.y), make_float2(wx.x, wx.y));
-        const float2 HG1 = __ffma2_rn(ex2, make_float2(dwx.z, dwx.w), make_float2(wx.z, wx.w));
-        const float2 cc = __ffma2_rn(HG1, VD, __fmul2_rn(HG0, VDp));
-        cv[k] = cc.x + cc.y;  // bicubic
-      }
-      VDp = VD;
-    }
-    // bilinear where the bicubic value is not positive (or not a number)
-    bool pos = true;
-#pragma unroll
-    for (int k = 0; k < K; ++k) pos = pos && (cv[k] > 0.0f);
-    if (__any_sync(0xffffffffu, !pos)) {
-      const float uu = tu.y + ey;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (!(cv[k] > 0.0f)) {
-          const float4 a00 = nd0[k], a01 = nd1[k];
-          const float4 a10 = nd0[k + 1], a11 = nd1[k + 1];
-          const float B0 = fmaf(uu, a01.x - a00.x, a00.x);
-          const float B1 = fmaf(uu, a11.x - a10.x, a10.x);
-          cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0) * ev.fb_scale;
+        const float4 n0 = nd0[r], n1 = nd1[r];
+        // y pass of the node row: (value, x-slope) interpolated to the sample's y
+        float2 VD = __fmul2_rn(make_float2(Kp.x, Kp.x), make_float2(n0.x, n0.y));
+        VD = __ffma2_rn(make_float2(Kp.y, Kp.y), make_float2(n1.x, n1.y), VD);
+        VD = __ffma2_rn(make_float2(Lp.x, Lp.x), make_float2(n0.z, n0.w), VD);
+        VD = __ffma2_rn(make_float2(Lp.y, Lp.y), make_float2(n1.z, n1.w), VD);
+        if (r > 0) {
+          const int k = r - 1;
+          const float2 ex2 = make_float2(ex[k], ex[k]);
+          const float2 HG0 = __ffma2_rn(ex2, make_float2(dwx.x, dwx.y), make_float2(wx.x, wx.y));
+          const float2 HG1 = __ffma2_rn(ex2, make_float2(dwx.z, dwx.w), make_float2(wx.z, wx.w));
+          const float2 cc = __ffma2_rn(HG1, VD, __fmul2_rn(HG0, VDp));
+          cv[k] = cc.x + cc.y;  // bicubic
         }
+        VDp = VD;
       }
-    }
-    const float4 mw = e[4];
-    if (!kInterior) {
-      const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
-      const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
-      if (!(nearx || neary)) {
+      // bilinear where the bicubic value is not positive (or not a number)
+      bool pos = true;
+#pragma unroll
+      for (int k = 0; k < K; ++k) pos = pos && (cv[k] > 0.0f);
+      if (__any_sync(0xffffffffu, !pos)) {
+        const float uu = tu.y + ey;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
-          cv[k] = in ? cv[k] : 0.0f;
-        }
-      } else {
-        // the fraction lies within 1e-3 of an integer: a sample next to the
-        // grid boundary may fall in or out with the rounding of its float
-        // position, so those samples are decided and evaluated with the
-        // reference arithmetic
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int ik = i0 + k;
-          const bool cx = (ik >= 1) && (ik <= NX - 2);
-          const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-          const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-          if (ixb + k < NX && iy < NY && (ux || uy) && (ux || cx) && (uy || in_y)) {
-            const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-            const float y = __fadd_rn(__fmul_rn((float)iy, ev.DY), ev.ymin);
-            cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
-          } else {
-            cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
+          if (!(cv[k] > 0.0f)) {
+            const float4 a00 = nd0[k], a01 = nd1[k];
+            const float4 a10 = nd0[k + 1], a11 = nd1[k + 1];
+            const float B0 = fmaf(uu, a01.x - a00.x, a00.x);
+            const float B1 = fmaf(uu, a11.x - a10.x, a10.x);
+            cv[k] = fmaf(tu.x + ex[k], B1 - B0, B0) * ev.fb_scale;
           }
         }
       }
-    }
+      const float4 mw = e[4];
+      if (!kInterior) {
+        const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
+        const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+        if (!(nearx || neary)) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const float2 v2 = make_float2(cv[k], cv[k]);
-      a0[k] += cv[k];
-      a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
-      a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+          for (int k = 0; k < K; ++k) {
+            const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
+            cv[k] = in ? cv[k] : 0.0f;
+          }
+        } else {
+          // the fraction lies within 1e-3 of an integer: a sample next to the
+          // grid boundary may fall in or out with the rounding of its float
+          // position, so those samples are decided and evaluated with the
+          // reference arithmetic
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int ik = i0 + k;
+            const bool cx = (ik >= 1) && (ik <= NX - 2);
+            const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+            const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+            if (ixb + k < NX && iy < NY && (ux || uy) && (ux || cx) && (uy || in_y)) {
+              const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+              const float y = __fadd_rn(__fmul_rn((float)iy, ev.DY), ev.ymin);
+              cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
+            } else {
+              cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const float2 v2 = make_float2(cv[k], cv[k]);
+        a0[k] += cv[k];
+        a12[k] = __ffma2_rn(v2, make_float2(mw.x, mw.y), a12[k]);
+        a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
+      }
     }
-    if ((p & (kPhiChunk - 1)) == kPhiChunk - 1) {
+    if ((pe & (kPhiChunk - 1)) == 0) {
       // second level of the two-level sum, thread-private slots in shared memory
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -600,6 +605,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
         a12[k] = a34[k] = make_float2(0.f, 0.f);
       }
     }
+    pc = pe;
   }
 }
 
@@ -863,93 +869,97 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
   constexpr bool kCache = !kB;
   NodeT n0[K + 1], n1[K + 1];
   int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
-  for (int p = 0; p < NP; ++p) {
-    const PhiEntry3D e = tab[p];
-    const int ox = e.ox;
-    const int oy = (int)(short)(e.oy_near & 0xffff);
-    // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
-    // more either side when the fraction is near an integer)
-    const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
-    const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
-    if (!skip) {
-      // (a full tile, so that no lane past the grid edge reads outside it)
-      const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
-      const int i0 = ixb + ox, j = iy + oy;
-      if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
-        // clamped indices keep the loads of edge lanes inside the arrays
-        // (their samples are masked below); inside the grid they are exact
-        const int jj = min(max(j, 0), NY - 2);
+  // phi_p in pieces that end at the fold points of the two-level sum
+  for (int pc = 0; pc < NP;) {
+    const int pe = min(NP, (pc | (kPhiChunk - 1)) + 1);
+    for (int p = pc; p < pe; ++p) {
+      const PhiEntry3D e = tab[p];
+      const int ox = e.ox;
+      const int oy = (int)(short)(e.oy_near & 0xffff);
+      // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
+      // more either side when the fraction is near an integer)
+      const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
+      const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
+      if (!skip) {
+        // (a full tile, so that no lane past the grid edge reads outside it)
+        const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
+        const int i0 = ixb + ox, j = iy + oy;
+        if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+          // clamped indices keep the loads of edge lanes inside the arrays
+          // (their samples are masked below); inside the grid they are exact
+          const int jj = min(max(j, 0), NY - 2);
+#pragma unroll
+          for (int r = 0; r <= K; ++r) {
+            const int i = min(max(i0 + r, 0), NX - 1);
+            const NodeT* q = N + (size_t)i * NY + jj;
+            n0[r] = __ldg(q);
+            n1[r] = __ldg(q + 1);
+          }
+          pox = ox;
+          poy = oy;
+        }
+        const float uc = e.u + ey;
+        const float2 uc2 = make_float2(uc, uc);
+        float v[K], vb[K];
+        float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
 #pragma unroll
         for (int r = 0; r <= K; ++r) {
-          const int i = min(max(i0 + r, 0), NX - 1);
-          const NodeT* q = N + (size_t)i * NY + jj;
-          n0[r] = __ldg(q);
-          n1[r] = __ldg(q + 1);
+          // y interpolation of the row on both eta slices (packed pairs)
+          const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
+          float2 C = make_float2(0.f, 0.f);
+          if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
+          if (r > 0) {
+            const int q = r - 1;
+            const float tk = e.t + ex[q];
+            const float2 tk2 = make_float2(tk, tk);
+            // x interpolation, then the eta interpolation with the rapidity weights
+            const float2 L = __fmul2_rn(lerp2(tk2, Bp, B), rf);
+            v[q] = fmaf(omet, L.x, et * L.y);
+            vb[q] = 0.0f;
+            if (kB) {
+              const float2 M = __fmul2_rn(lerp2(tk2, Cp, C), rb);
+              vb[q] = fmaf(omet, M.x, et * M.y);
+            }
+          }
+          Bp = B;
+          Cp = C;
         }
-        pox = ox;
-        poy = oy;
-      }
-      const float uc = e.u + ey;
-      const float2 uc2 = make_float2(uc, uc);
-      float v[K], vb[K];
-      float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
+        const FSM_FLOAT2 cs = ev.cs[p];
+        if (!interior) {
+          const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
+          const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
 #pragma unroll
-      for (int r = 0; r <= K; ++r) {
-        // y interpolation of the row on both eta slices (packed pairs)
-        const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
-        float2 C = make_float2(0.f, 0.f);
-        if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
-        if (r > 0) {
-          const int q = r - 1;
-          const float tk = e.t + ex[q];
-          const float2 tk2 = make_float2(tk, tk);
-          // x interpolation, then the eta interpolation with the rapidity weights
-          const float2 L = __fmul2_rn(lerp2(tk2, Bp, B), rf);
-          v[q] = fmaf(omet, L.x, et * L.y);
-          vb[q] = 0.0f;
-          if (kB) {
-            const float2 M = __fmul2_rn(lerp2(tk2, Cp, C), rb);
-            vb[q] = fmaf(omet, M.x, et * M.y);
+          for (int k = 0; k < K; ++k) {
+            const int ik = i0 + k;
+            const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+            const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+            bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
+            if (act[k] && (ux || uy)) {
+              // the in-grid decision depends on the rounding: reference arithmetic
+              const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+              in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+            }
+            if (!in) {
+              v[k] = 0.0f;
+              vb[k] = 0.0f;
+            }
           }
         }
-        Bp = B;
-        Cp = C;
-      }
-      const FSM_FLOAT2 cs = ev.cs[p];
-      if (!interior) {
-        const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
-        const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+        const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+        const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const int ik = i0 + k;
-          const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-          const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-          bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
-          if (act[k] && (ux || uy)) {
-            // the in-grid decision depends on the rounding: reference arithmetic
-            const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-            in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
-          }
-          if (!in) {
-            v[k] = 0.0f;
-            vb[k] = 0.0f;
-          }
+          const float2 w = make_float2(v[k], vb[k]);
+          a01[k] = __fadd2_rn(a01[k], w);
+          a1c[k] = __ffma2_rn(w, c2, a1c[k]);
+          a1s[k] = __ffma2_rn(w, s2, a1s[k]);
+          a3[k] = fmaf(v[k], cc, a3[k]);
+          a4[k] = fmaf(v[k], csn, a4[k]);
+          a5[k] = fmaf(v[k], ss, a5[k]);
         }
       }
-      const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
-      const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const float2 w = make_float2(v[k], vb[k]);
-        a01[k] = __fadd2_rn(a01[k], w);
-        a1c[k] = __ffma2_rn(w, c2, a1c[k]);
-        a1s[k] = __ffma2_rn(w, s2, a1s[k]);
-        a3[k] = fmaf(v[k], cc, a3[k]);
-        a4[k] = fmaf(v[k], csn, a4[k]);
-        a5[k] = fmaf(v[k], ss, a5[k]);
-      }
     }
-    if ((p & (kPhiChunk - 1)) == kPhiChunk - 1 || p == NP - 1) {
+    {
       // second level of the two-level sum: per-rapidity sums in slots
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -969,6 +979,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
         a3[k] = a4[k] = a5[k] = 0.0f;
       }
     }
+    pc = pe;
   }
 }
 
