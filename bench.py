@@ -38,10 +38,10 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
 FLOPS_PER_SAMPLE_3D_BARYON = 75  # shift 5 + 2 trilinear x 21 + 14 moments x 2
-# DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.9 MB read +
-# 162.0 MB written) / 713.26 M samples in one ncu capture of the 128-event
+# DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.6 MB read +
+# 161.0 MB written) / 713.26 M samples in one ncu capture of the 128-event
 # batch (profiles/kernels_2d_uneven128_full.md)
-TRAFFIC_BYTES_PER_SAMPLE_2D = (88.902656e6 + 161.969152e6) / 713258674
+TRAFFIC_BYTES_PER_SAMPLE_2D = (88.60672e6 + 161.023744e6) / 713258674
 WORKLOAD = ("uneven_batch: 512 seeded lumpy 2D events, side {101,151,201,261,301}, DX U[0.05,0.1], "
             "DIM_PHIP {64,100,200} + arc-length rule, DTAU U[0.3,1.5], EOS 1/2 50:50, TAU0 0.2")
 
