@@ -258,12 +258,24 @@ void wave_retire(fsm_server* S, Wave* w) {
 // Builds and enqueues one wave from the head of the queue on stream `slot`
 // (mu held on entry and exit; released while planning).  Returns false when
 // nothing could be admitted for lack of memory.
+constexpr int kBacklogMix = 8;  // queued requests above which waves mix event kinds
+
 bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
   const int cap = S->opts.max_wave_events;
   std::vector<Request*> take;
-  while (!S->queue.empty() && (int)take.size() < cap) {
-    take.push_back(S->queue.front());
-    S->queue.pop_front();
+  // With a short queue a wave holds requests of one kind, that of the oldest
+  // one (boost-invariant or 3D), in arrival order: a 2D request then does not
+  // wait for the milliseconds of a 3D event sharing its wave.  Under a backlog
+  // waves take the queue in order, mixed, for throughput.
+  const bool kind3d = S->queue.front()->p.DIM_ETA > 1;
+  const bool mixed = (int)S->queue.size() > kBacklogMix;
+  for (auto it = S->queue.begin(); it != S->queue.end() && (int)take.size() < cap;) {
+    if (mixed || ((*it)->p.DIM_ETA > 1) == kind3d) {
+      take.push_back(*it);
+      it = S->queue.erase(it);
+    } else {
+      ++it;
+    }
   }
   cudaStream_t s = S->streams[slot];
   while (!take.empty()) {
