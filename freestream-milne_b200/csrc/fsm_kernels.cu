@@ -3,9 +3,10 @@
 //   fsm_prep2d_rows_kernel    F = e/(2 pi) and its natural-spline y-derivatives
 //   fsm_prep2d_cols_kernel    x- and mixed derivatives + float4 node packing
 //   fsm_prep2d_*_long_kernel  the same for grids whose lines exceed kMaxStrip
-//   fsm_prep3d_kernel         GeV/fm^3 -> fm^-4 conversion of 3D profiles
+//   fsm_prep3d_kernel         GeV/fm^3 -> fm^-4 conversion into eta-pair node arrays (3D)
 //   fsm_stream2d_kernel       fused free streaming + moment quadrature, 2D
 //   fsm_stream3d_kernel       fused free streaming + moment quadrature, 3D (+baryon)
+//   fsm_pack_kernel           gather of output fields for one-copy downloads
 //   fsm_landau_kernel         FP64 Landau matching + EoS + decomposition
 //
 // The stream kernels never store the momentum-resolved density F(x; phi_p, y):
