@@ -46,7 +46,21 @@ __device__ __forceinline__ float F_of(float e_gev) {
 __device__ __forceinline__ void stage_axis(AxisNode* dst, const AxisNode* __restrict__ src, int n) {
   const double* s = reinterpret_cast<const double*>(src - kPadLo);
   double* d = reinterpret_cast<double*>(dst);
-  for (int i = threadIdx.x; i < (n + kPadLo + kPadHi) * 4; i += blockDim.x) d[i] = __ldg(s + i);
+  const int total = (n + kPadLo + kPadHi) * 4;
+  constexpr int kB = 4;  // independent loads in flight per thread
+  for (int i0 = threadIdx.x; i0 < total; i0 += blockDim.x * kB) {
+    double v[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      v[u] = i < total ? __ldg(s + i) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < total) d[i] = v[u];
+    }
+  }
 }
 
 // y-lines (rows ix0 .. ix0+31, contiguous in memory): F = e/(2 pi) -> fa and
@@ -140,7 +154,7 @@ __global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_cols_kernel(
   float* Ys = Fs + 32 * np;
   stage_axis(tab, ev.ax, NX);
   {
-    constexpr int kB = 4;  // independent loads in flight per thread
+    constexpr int kB = 8;  // independent loads in flight per thread
     const float* __restrict__ fa = ev.fa;
     const float* __restrict__ sy = ev.sy;
     for (int i0 = warp; i0 < np; i0 += (kPrepThreads / 32) * kB) {
