@@ -1040,6 +1040,17 @@ extern "C" fsm_status fsm_batch_packed_offset(fsm_batch* b, unsigned mask, unsig
   return found ? FSM_OK : FSM_ERR_INVALID_ARG;
 }
 
+extern "C" fsm_status fsm_batch_packed_offsets(fsm_batch* b, unsigned mask, unsigned flags,
+                                               size_t* elems, size_t n) {
+  const size_t need = b ? b->plans.size() * kOutGroups * 10 : 0;
+  if (!b || !elems || !b->own_io || n < need) return FSM_ERR_INVALID_ARG;
+  for (size_t i = 0; i < need; ++i) elems[i] = (size_t)-1;
+  pack_walk(b, mask, flags, [&](int g, int c, int i, size_t, size_t dst, size_t) {
+    elems[((size_t)i * kOutGroups + g) * 10 + c] = dst;
+  });
+  return FSM_OK;
+}
+
 extern "C" fsm_status fsm_batch_download_packed(fsm_batch* b, unsigned mask, unsigned flags,
                                                 void* host_out, void* stream) {
   if (!b || !b->own_io || !host_out) return FSM_ERR_INVALID_ARG;

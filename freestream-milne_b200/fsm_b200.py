@@ -139,6 +139,7 @@ SIGNATURES = {
     "fsm_batch_packed_bytes": (ctypes.c_size_t, [_VP, ctypes.c_uint, ctypes.c_uint]),
     "fsm_batch_packed_offset": (_ST, [_VP, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "fsm_batch_packed_offsets": (_ST, [_VP, ctypes.c_uint, ctypes.c_uint, _VP, ctypes.c_size_t]),
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
@@ -425,11 +426,25 @@ class Batch:
                                            OUT_GROUPS.index(group), comp, ev, ctypes.byref(o))
         return o.value if st == 0 else None
 
+    def packed_offsets(self, groups, skip_eta=False):
+        """(events, 9 groups, 10 components) array of packed-buffer offsets,
+        -1 where a component is not in the packed buffer (cached)."""
+        key = (tuple(groups), bool(skip_eta))
+        cache = self.__dict__.setdefault("_pack_offsets", {})
+        if key not in cache:
+            a = np.empty(self.n * len(OUT_GROUPS) * 10, np.uint64)
+            check(lib().fsm_batch_packed_offsets(self.h, out_mask(groups),
+                                                 PACK_SKIP_ETA if skip_eta else 0,
+                                                 a.ctypes.data, a.size), "fsm_batch_packed_offsets")
+            cache[key] = a.astype(np.int64).reshape(self.n, len(OUT_GROUPS), 10)
+        return cache[key]
+
     def unpack_packed(self, packed, groups, ev, skip_eta=False):
         """Per-event dict of the `groups` arrays from a packed download; left-out
         components (zero by symmetry) come back as zeros."""
         p = self.params[ev]
         dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+        offs = self.packed_offsets(groups, skip_eta)[ev]
         res = {}
         for k in OUT_GROUPS:
             if k not in groups or (k in ("J", "nB", "V") and not p.BARYON):
@@ -437,8 +452,8 @@ class Batch:
             c = OUT_COMPS[k]
             a = np.zeros((c, dim), np.float32)
             for m in range(c):
-                off = self.packed_offset(groups, k, m, ev, skip_eta)
-                if off is not None:
+                off = int(offs[OUT_GROUPS.index(k), m])
+                if off >= 0:
                     a[m] = packed[off:off + dim]
             res[k] = a if c > 1 else a[0]
         return res

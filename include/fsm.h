@@ -218,6 +218,11 @@ fsm_status fsm_batch_download_packed(fsm_batch* b, unsigned mask, unsigned flags
 size_t fsm_batch_packed_bytes(fsm_batch* b, unsigned mask, unsigned flags);
 fsm_status fsm_batch_packed_offset(fsm_batch* b, unsigned mask, unsigned flags, int group, int comp,
                                    int ev, size_t* elem);
+/* All offsets at once: elems[(ev * 9 + g) * 10 + c] for event ev, group g
+ * (FSM_OUT_* == 1 << g) and component c, (size_t)-1 where the packed buffer
+ * has none; n >= n_events * 90. */
+fsm_status fsm_batch_packed_offsets(fsm_batch* b, unsigned mask, unsigned flags, size_t* elems,
+                                    size_t n);
 /* Waits for the stream the batch last used (upload, launch or download) and
  * checks the kernels' internal error counters. */
 fsm_status fsm_batch_check(fsm_batch* b);

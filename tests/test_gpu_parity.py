@@ -198,6 +198,13 @@ def test_packed_downloads(ctx, grouped):
                 assert sorted(got) == sorted(k for k in groups if k in w)
                 for k in got:
                     assert np.array_equal(got[k], w[k]), (grouped, skip, ev, k)
+    # the all-offsets call agrees with the one-component query
+    offs = b.packed_offsets(list(F.OUT_GROUPS), True)
+    for ev in range(b.n):
+        for g, k in enumerate(F.OUT_GROUPS):
+            for m in range(F.OUT_COMPS[k]):
+                one = b.packed_offset(list(F.OUT_GROUPS), k, m, ev, True)
+                assert (one if one is not None else -1) == offs[ev, g, m], (ev, k, m)
     full = b.packed_bytes(["u", "pi"])
     less = b.packed_bytes(["u", "pi"], True)
     n2d = sum(p.DIM_X * p.DIM_Y for p, _, _ in evs if p.DIM_ETA == 1)

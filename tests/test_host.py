@@ -87,6 +87,7 @@ def test_batch_download_entry_points_reject_null_batches():
     assert L.fsm_batch_download_groups(None, 1, None, None) == 1
     assert L.fsm_batch_download_packed(None, 1, F.PACK_SKIP_ETA, None, None) == 1
     assert L.fsm_batch_packed_offset(None, 1, 0, 0, 0, 0, None) == 1
+    assert L.fsm_batch_packed_offsets(None, 1, 0, None, 0) == 1
     assert L.fsm_batch_group_offset(None, 1, 0, 0, None) == 1
     assert L.fsm_batch_groups_bytes(None, 1) == 0 and L.fsm_batch_packed_bytes(None, 1, 0) == 0
 
