@@ -34,7 +34,7 @@ constexpr int kPhiTab2D = 6;         // float4 per phi_p entry of the 2D table
 constexpr int kMaxRunPhi2D = 64;     // phi_p per staged run (the run's table slice is staged with it)
 constexpr int kThreads3D = 256;
 constexpr int kThreadsLandau = 128;
-constexpr int kPhiChunk = 16;  // FP32 partial sums are folded into Kahan totals every 16 phi_p
+constexpr int kPhiChunk = 16;  // FP32 partial sums over 16 phi_p are added into FP32 totals (two-level sum)
 
 // Natural-spline axis data for the 2D prep kernels (host computed, double),
 // one entry per interval / unknown k of an axis with n nodes, on the float grid

@@ -529,7 +529,7 @@ extern "C" void fsm_params_derive(fsm_params* p) {
   p->TAU = p->TAU0 + p->DTAU;
 }
 
-// Positional parse with the reference's own format strings (src/FileIO.cpp:279-334).
+// Positional parse with the reference's own format strings (src/FileIO.cpp:166-245).
 extern "C" fsm_status fsm_params_read_file(const char* path, fsm_params* p) {
   if (!path || !p) return FSM_ERR_INVALID_ARG;
   FILE* fileIn = std::fopen(path, "r");

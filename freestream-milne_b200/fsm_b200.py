@@ -20,26 +20,9 @@ STATUS = {0: "FSM_OK", 1: "FSM_ERR_INVALID_ARG", 2: "FSM_ERR_SIZE_MISMATCH", 3: 
           7: "FSM_ERR_OUT_OF_MEMORY", 8: "FSM_ERR_FILE", 9: "FSM_ERR_BUSY", 10: "FSM_ERR_TIMEOUT",
           11: "FSM_ERR_PENDING", 12: "FSM_ERR_TOO_LARGE", 13: "FSM_ERR_CANCELLED"}
 
-# Field order of fsm_params == struct parameters (reference src/Parameter.h:2-33)
-PARAM_FIELDS = [
-    ("OUTPUTFORMAT", ctypes.c_int), ("BARYON", ctypes.c_int), ("IC_ENERGY", ctypes.c_int),
-    ("IC_BARYON", ctypes.c_int), ("ETA_WIDTH", ctypes.c_float), ("ETA_FLAT", ctypes.c_float),
-    ("SIGMA", ctypes.c_float), ("SIGMA_B", ctypes.c_float), ("DIM_X", ctypes.c_int),
-    ("DIM_Y", ctypes.c_int), ("DIM_ETA", ctypes.c_int), ("DIM_RAP", ctypes.c_int),
-    ("DIM_PHIP", ctypes.c_int), ("DX", ctypes.c_float), ("DY", ctypes.c_float),
-    ("DETA", ctypes.c_float), ("DRAP", ctypes.c_float), ("DTAU", ctypes.c_float),
-    ("TAU0", ctypes.c_float), ("EOS_TYPE", ctypes.c_int), ("E_FREEZE", ctypes.c_float),
-    ("VISCOUS_MATCHING", ctypes.c_int), ("E_DEP_FS", ctypes.c_int), ("E_R", ctypes.c_float),
-    ("TAU_R", ctypes.c_float), ("ALPHA", ctypes.c_float), ("DIM", ctypes.c_int),
-    ("TAU", ctypes.c_float),
-]
-
-
-class Params(ctypes.Structure):
-    _fields_ = PARAM_FIELDS
-
-    def as_dict(self):
-        return {k: getattr(self, k) for k, _ in PARAM_FIELDS}
+# fsm_params (field order of the reference's struct parameters,
+# src/Parameter.h:2-33), shared with the library-free workload generators
+from fsm_params import PARAM_FIELDS, Params  # noqa: E402,F401
 
 
 _FP = ctypes.POINTER(ctypes.c_float)

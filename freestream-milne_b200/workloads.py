@@ -24,7 +24,7 @@ x = ix*DX + xmin, xmin = -((DIM_X-1)/2)*DX (src/FreeStream.cpp:16-31).
 """
 import numpy as np
 
-import fsm_b200 as F
+from fsm_params import default_params, derive
 
 
 def axis(n, d):
@@ -54,12 +54,12 @@ def plateau(eta, flat, width):
 
 
 def gaussian2d(**over):
-    p = F.default_params(DIM_X=101, DIM_Y=101, DX=0.1, DY=0.1, DIM_ETA=1, DIM_RAP=1, DIM_PHIP=51,
-                         TAU0=0.1, DTAU=0.5, EOS_TYPE=1, BARYON=0, VISCOUS_MATCHING=1,
-                         E_DEP_FS=0, OUTPUTFORMAT=2)
+    p = default_params(DIM_X=101, DIM_Y=101, DX=0.1, DY=0.1, DIM_ETA=1, DIM_RAP=1, DIM_PHIP=51,
+                       TAU0=0.1, DTAU=0.5, EOS_TYPE=1, BARYON=0, VISCOUS_MATCHING=1,
+                       E_DEP_FS=0, OUTPUTFORMAT=2)
     for k, v in over.items():
         setattr(p, k, v)
-    F.lib().fsm_params_derive(p)
+    derive(p)
     x, y = axis(p.DIM_X, p.DX), axis(p.DIM_Y, p.DY)
     X, Y = np.meshgrid(x.astype(np.float64), y.astype(np.float64), indexing="ij")
     e = 10.0 * np.exp(-(X ** 2 + Y ** 2) / (2 * 1.5 ** 2))
@@ -68,12 +68,12 @@ def gaussian2d(**over):
 
 def lumpy2d(seed=1, side=261, dx=0.06, nphip=200, tau0=0.2, dtau=1.0, eos=2, radius=6.0, **over):
     rng = np.random.default_rng(seed)
-    p = F.default_params(DIM_X=side, DIM_Y=side, DX=dx, DY=dx, DIM_ETA=1, DIM_RAP=1,
-                         DIM_PHIP=nphip, TAU0=tau0, DTAU=dtau, EOS_TYPE=eos, BARYON=0,
-                         VISCOUS_MATCHING=1, E_DEP_FS=0, OUTPUTFORMAT=2)
+    p = default_params(DIM_X=side, DIM_Y=side, DX=dx, DY=dx, DIM_ETA=1, DIM_RAP=1,
+                       DIM_PHIP=nphip, TAU0=tau0, DTAU=dtau, EOS_TYPE=eos, BARYON=0,
+                       VISCOUS_MATCHING=1, E_DEP_FS=0, OUTPUTFORMAT=2)
     for k, v in over.items():
         setattr(p, k, v)
-    F.lib().fsm_params_derive(p)
+    derive(p)
     x, y = axis(p.DIM_X, p.DX), axis(p.DIM_Y, p.DY)
     e = hotspots(rng, x, y, radius=radius)
     return p, e.astype(np.float32).ravel(), None
@@ -92,14 +92,14 @@ def lumpy2d_baryon(seed=1, side=101, dx=0.08, nphip=64, dtau=0.8, nrap=5, drap=0
 def baryon3d(seed=2, side=131, dx=0.1, neta=51, deta=0.2, nrap=21, nphip=100, tau0=0.1,
              dtau=0.8, eta_flat=4.0, eta_width=1.0, **over):
     rng = np.random.default_rng(seed)
-    p = F.default_params(DIM_X=side, DIM_Y=side, DX=dx, DY=dx, DIM_ETA=neta, DETA=deta,
-                         DIM_RAP=nrap, DRAP=0.2, DIM_PHIP=nphip, TAU0=tau0, DTAU=dtau,
-                         EOS_TYPE=1, BARYON=1, IC_BARYON=3, SIGMA=1.0, SIGMA_B=1.0,
-                         ETA_FLAT=eta_flat, ETA_WIDTH=eta_width, VISCOUS_MATCHING=1,
-                         E_DEP_FS=0, OUTPUTFORMAT=2)
+    p = default_params(DIM_X=side, DIM_Y=side, DX=dx, DY=dx, DIM_ETA=neta, DETA=deta,
+                       DIM_RAP=nrap, DRAP=0.2, DIM_PHIP=nphip, TAU0=tau0, DTAU=dtau,
+                       EOS_TYPE=1, BARYON=1, IC_BARYON=3, SIGMA=1.0, SIGMA_B=1.0,
+                       ETA_FLAT=eta_flat, ETA_WIDTH=eta_width, VISCOUS_MATCHING=1,
+                       E_DEP_FS=0, OUTPUTFORMAT=2)
     for k, v in over.items():
         setattr(p, k, v)
-    F.lib().fsm_params_derive(p)
+    derive(p)
     x, y, eta = axis(p.DIM_X, p.DX), axis(p.DIM_Y, p.DY), axis(p.DIM_ETA, p.DETA)
     radius = min(6.0, 0.45 * side * dx)
     tp = hotspots(rng, x, y, radius=radius)

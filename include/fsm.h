@@ -14,7 +14,7 @@
  *   tt tx ty tn xx xy xn yy yn nn (src/LandauMatch.cpp:46-55), vectors t x y n.
  *   Units: inputs e in GeV/fm^3 as initialize_from_vector takes them
  *   (src/FreestreamMilne.cpp:43-46); nB as the IC_BARYON=3 file gives it
- *   (src/FileIO.cpp:227-258, no conversion); float outputs are in the
+ *   (read by src/FileIO.cpp:133-164, no conversion); float outputs are in the
  *   reference's internal units (fm^-4, fm^-3) -- the compat class applies the
  *   hbar*c factor of src/FreestreamMilne.cpp:700-716 when filling its vectors.
  */
@@ -38,7 +38,7 @@ typedef enum fsm_status {
   FSM_ERR_CUDA = 5,          /* a CUDA runtime call failed (see fsm_last_error)     */
   FSM_ERR_NO_DEVICE = 6,     /* no CUDA device: there is no CPU fallback            */
   FSM_ERR_OUT_OF_MEMORY = 7, /* device allocation failed                            */
-  FSM_ERR_FILE = 8,          /* params/IC file missing: FileIO.cpp:150-154,272-275  */
+  FSM_ERR_FILE = 8,          /* params/IC file missing: FileIO.cpp:150-154,178-181  */
   FSM_ERR_BUSY = 9,          /* server: request does not fit the HBM budget now     */
   FSM_ERR_TIMEOUT = 10,      /* a bounded wait ran out                              */
   FSM_ERR_PENDING = 11,      /* server: request admitted, result not ready yet      */
@@ -85,10 +85,10 @@ typedef struct fsm_params {
 
 /* Defaults of src/FreestreamMilne.cpp:149-171 (E_R, TAU_R, ALPHA: 1, 1, 0). */
 void fsm_params_default(fsm_params* p);
-/* Positional parse of a freestream_input file (src/FileIO.cpp:260-339): 26
+/* Positional parse of a freestream_input file (src/FileIO.cpp:166-245): 26
  * "KEY<ws>value" lines in fixed order, the key text is ignored.  A missing
  * file returns FSM_ERR_FILE and leaves *p untouched (the reference prints and
- * keeps its defaults, FileIO.cpp:272-275). */
+ * keeps its defaults, FileIO.cpp:178-181). */
 fsm_status fsm_params_read_file(const char* path, fsm_params* p);
 /* Fills DIM and TAU (FreestreamMilne.cpp:177-178). */
 void fsm_params_derive(fsm_params* p);

@@ -20,7 +20,9 @@ def _make(dirpath, *targets):
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (runs the sm_100a kernels)")
     # incremental builds of the oracle (test infrastructure) and the library
-    _make(ROOT / "oracle")
+    sys.path.insert(0, str(ROOT))
+    from __graft_entry__ import oracle_make_args
+    _make(ROOT / "oracle", *oracle_make_args())
     _make(PKG, "all", "hosttest")
 
 

@@ -45,8 +45,25 @@ def test_params_default_match_reference():
     assert p.DIM == 101 * 101 and p.TAU == pytest.approx(0.6)
 
 
+def test_python_params_match_library():
+    """The library-free parameter block (used by the workload generators, so
+    that the CPU reference timing never loads libfsm.so) has the library's
+    defaults and derives DIM and TAU bit for bit like fsm_params_derive."""
+    import fsm_params as FP
+    assert F.Params is FP.Params
+    a, b = F.default_params(), FP.default_params()
+    assert bytes(a) == bytes(b)
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        kw = dict(DIM_X=int(rng.integers(4, 400)), DIM_Y=int(rng.integers(4, 400)),
+                  DIM_ETA=int(rng.integers(1, 60)), TAU0=float(rng.uniform(0.01, 2.0)),
+                  DTAU=float(rng.uniform(0.0, 3.0)))
+        a, b = F.default_params(**kw), FP.default_params(**kw)
+        assert bytes(a) == bytes(b)
+
+
 def test_params_positional_file(tmp_path):
-    # keys are ignored: only the position of each value matters (src/FileIO.cpp:279-334)
+    # keys are ignored: only the position of each value matters (src/FileIO.cpp:166-245)
     vals = ["2", "1", "5", "3", "0.7", "2.5", "0.9", "1.1", "31", "29", "7", "5", "33", "0.12",
             "0.13", "0.2", "0.25", "0.75", "0.3", "2", "1.9", "0", "0", "3.0", "0.8", "0.5"]
     text = "".join(f"KEY{i}\t{v}\n" for i, v in enumerate(vals))
