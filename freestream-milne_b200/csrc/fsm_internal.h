@@ -34,6 +34,9 @@ constexpr int kPhiTab2D = 6;         // float4 per phi_p entry of the 2D table
 constexpr int kMaxRunPhi2D = 64;     // phi_p per staged run (the run's table slice is staged with it)
 constexpr int kThreads3D = 256;
 constexpr int kThreadsLandau = 128;
+// Polls of one bounded mbarrier wait of a staged copy (a context may lower it
+// to exercise the time-out path; the drain after a time-out always uses this).
+constexpr int kWaitPolls = 1 << 20;
 constexpr int kPhiChunk = 16;  // FP32 partial sums over 16 phi_p are added into FP32 totals (two-level sum)
 
 // Natural-spline axis data for the 2D prep kernels (host computed, double),

@@ -467,8 +467,6 @@ __device__ __forceinline__ void stage_window(float4* buf, const float4* __restri
   }
 }
 
-constexpr int kWaitLimit = 1 << 20;  // polls of one bounded mbarrier wait
-
 // One phi_p run of one 32 x 32 output tile, on a staged window `win`
 // (boxW columns per row) whose node (0, 0) is grid node (wx0, wy0).  Lane l of
 // warp w owns the cells (x0 + 4w + k, y0 + l), k = 0..3.  For each phi_p every
@@ -629,12 +627,14 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
 // window of each phi_p run are staged into shared memory by bulk copies
 // (cp.async.bulk, one per in-grid window row) completing on mbarriers,
 // double-buffered so the next run's window loads while the current one is
-// computed.  Every mbarrier wait is bounded; on time-out the CTA records an
-// error and leaves.
+// computed.  Every mbarrier wait gives up after wait_polls polls; on time-out
+// the CTA records an error, waits (bounded) until every copy it issued has
+// landed, and leaves.
 __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D* __restrict__ evs,
                                                                      const Tile2D* __restrict__ tiles,
                                                                      int ntiles, int box_cap,
-                                                                     Counters* ctr, int* err) {
+                                                                     Counters* ctr, int* err,
+                                                                     int wait_polls) {
   extern __shared__ __align__(128) float4 smem4[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ int s_tile;
@@ -706,14 +706,18 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
                      (uint32_t)(cn.p1 - cn.p0) * (uint32_t)sizeof(PhiEntry2D), &bars[b ^ 1]);
       }
       const uint32_t ph = b ? phase1 : phase0;
-      const bool ok = mbar_wait(&bars[b], ph, kWaitLimit);
+      const bool ok = mbar_wait(&bars[b], ph, wait_polls);
       if (b) phase1 ^= 1u;
       else phase0 ^= 1u;
       if (__syncthreads_or(!ok)) {
-        // a staged copy did not complete: record it, drain, and leave
+        // a staged copy did not complete in time: record it; before leaving,
+        // let both copies this CTA may have in flight land (run c's, and run
+        // c + 1's when it was issued) so that none writes into shared memory
+        // after the CTA has exited
         if (threadIdx.x == 0) {
           atomicAdd(err + 1, 1);
-          if (c + 1 < nch) mbar_wait(&bars[b ^ 1], b ? phase0 : phase1, kWaitLimit);
+          mbar_wait(&bars[b], ph, kWaitPolls);
+          if (c + 1 < nch) mbar_wait(&bars[b ^ 1], b ? phase0 : phase1, kWaitPolls);
         }
         return;
       }

@@ -21,13 +21,14 @@
 #include "../../include/fsm.h"
 #include "fsm_internal.h"
 #include "fsm_plan.h"
+#include "fsm_runtime.h"
 
 namespace fsm {
 __global__ void fsm_prep2d_rows_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
 __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
-__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*, int);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 }  // namespace fsm
 
@@ -38,6 +39,12 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB
 constexpr int kNoAllocMaxCells = 301 * 301;               // DIM_X * DIM_Y
 constexpr int kNoAllocMaxPhi = 1024;                      // DIM_PHIP after the arc-length rule
+// Fixed header of the scratch: the launch counters and the stream kernel's
+// error words sit at the same offsets for every event, so that
+// fsm_run_event_2d_noalloc_check can read them without knowing the event.
+constexpr size_t kHdrCtr = 0;
+constexpr size_t kHdrErr = 256;
+constexpr size_t kHdrBytes = 512;
 
 }  // namespace
 
@@ -74,27 +81,8 @@ fsm_status noalloc_scratch_address(char** out) {
   return FSM_OK;
 }
 
-// Raise (never lower) a kernel's dynamic shared-memory limit: the limit is a
-// process-wide attribute that other launches may rely on.
-fsm_status raise_dyn_smem(const void* fn, size_t bytes) {
-  cudaFuncAttributes a;
-  cudaError_t e = cudaFuncGetAttributes(&a, fn);
-  if (e != cudaSuccess) {
-    set_last_error(std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e));
-    return FSM_ERR_CUDA;
-  }
-  if ((int)bytes > a.maxDynamicSharedSizeBytes) {
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) {
-      set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-      return FSM_ERR_CUDA;
-    }
-  }
-  return FSM_OK;
-}
-
 struct Region {
-  size_t off = 0;
+  size_t off = kHdrBytes;
   size_t take(size_t bytes) {
     size_t o = off;
     off = (off + bytes + 255) / 256 * 256;
@@ -156,7 +144,8 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   std::vector<CellBlock> bl;
   for (int b = 0; b < DIM; b += kThreadsLandau) bl.push_back(CellBlock{0, b});
 
-  // scratch layout: uploaded part first, then device-written scratch
+  // scratch layout: the fixed header (counters, error words), the uploaded
+  // part, then the device-written scratch
   Region R;
   const size_t o_cs = R.take(P.cs.size() * sizeof(FSM_FLOAT2));
   const size_t o_tab = R.take(P.tab2.size() * sizeof(PhiEntry2D));
@@ -168,8 +157,8 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   const size_t o_rows = R.take(rows.size() * sizeof(LineBlock));
   const size_t o_cols = R.take(cols.size() * sizeof(LineBlock));
   const size_t o_bl = R.take(bl.size() * sizeof(CellBlock));
-  const size_t upload_bytes = R.off;
-  const size_t o_ctr = R.take(sizeof(Counters)), o_err = R.take(4 * sizeof(int));
+  const size_t o_up = kHdrBytes, upload_bytes = R.off - o_up;
+  const size_t o_ctr = kHdrCtr, o_err = kHdrErr;
   const size_t o_fa = R.take((size_t)DIM * 4), o_sy = R.take((size_t)DIM * 4);
   const size_t o_nodes = R.take((size_t)DIM * 16);
   const size_t o_T = R.take((size_t)DIM * 10 * 4);
@@ -224,7 +213,7 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   // host image of the uploaded part (ordinary host memory; no pinned staging)
   std::vector<char> H(upload_bytes, 0);
   auto put = [&](size_t off, const void* src, size_t n) {
-    if (n) std::memcpy(H.data() + off, src, n);
+    if (n) std::memcpy(H.data() + (off - o_up), src, n);
   };
   put(o_cs, P.cs.data(), P.cs.size() * sizeof(FSM_FLOAT2));
   put(o_tab, P.tab2.data(), P.tab2.size() * sizeof(PhiEntry2D));
@@ -238,32 +227,50 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   put(o_cols, cols.data(), cols.size() * sizeof(LineBlock));
   put(o_bl, bl.data(), bl.size() * sizeof(CellBlock));
 
-  // launch geometry of the stream kernel (as the batch path computes it)
-  const int box_cap = (P.box_elems + 7) & ~7;
-  const size_t smem2 = stream2d_smem(box_cap);
-  if ((st = raise_dyn_smem((const void*)fsm_stream2d_kernel, smem2)) != FSM_OK) return st;
-  const size_t smem_rows = strip ? prep_strip_smem(std::max(NX, NY)) : prep_rows_smem(NY);
-  if (strip) {
-    if ((st = raise_dyn_smem((const void*)fsm_prep2d_rows_kernel, smem_rows)) != FSM_OK) return st;
-    if ((st = raise_dyn_smem((const void*)fsm_prep2d_cols_kernel, smem_rows)) != FSM_OK) return st;
-  } else if ((st = raise_dyn_smem((const void*)fsm_prep2d_rows_long_kernel, smem_rows)) != FSM_OK) {
-    return st;
-  }
-  int dev = 0, sms = 0, occ = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream2d_kernel, kThreads2D, smem2);
-  const int ntiles = (int)tiles.size();
-  const int grid2 = std::max(1, std::min(ntiles, sms * std::max(occ, 1)));
-
-  // upload (pageable source: returns once the bytes are staged), reset the
-  // counters this call reads, then the same launch sequence as the batch path
+  // launch geometry of the stream kernel (as the batch path computes it); the
+  // dynamic shared-memory limits go through the library's one raise-only
+  // helper, so that no caller ever lowers a limit another launch relies on
   auto cu = [&](cudaError_t ce, const char* what) -> fsm_status {
     if (ce == cudaSuccess) return FSM_OK;
     set_last_error(std::string(what) + ": " + cudaGetErrorString(ce));
     return FSM_ERR_CUDA;
   };
-  if ((st = cu(cudaMemcpyAsync(D, H.data(), upload_bytes, cudaMemcpyHostToDevice, s), "upload")) != FSM_OK)
+  int dev = 0, sms = 0, occ = 0;
+  if ((st = cu(cudaGetDevice(&dev), "cudaGetDevice")) != FSM_OK) return st;
+  const int slot = dev & 63;
+  const int box_cap = (P.box_elems + 7) & ~7;
+  const size_t smem2 = stream2d_smem(box_cap);
+  if ((st = rt::ensure_dyn_smem((const void*)fsm_stream2d_kernel, dev, smem2, &rt::g_smem2[slot])) != FSM_OK)
+    return st;
+  const size_t smem_rows = strip ? prep_strip_smem(std::max(NX, NY)) : prep_rows_smem(NY);
+  if (strip) {
+    if ((st = rt::ensure_dyn_smem((const void*)fsm_prep2d_rows_kernel, dev, smem_rows,
+                                  &rt::g_smem_srows[slot])) != FSM_OK)
+      return st;
+    if ((st = rt::ensure_dyn_smem((const void*)fsm_prep2d_cols_kernel, dev, smem_rows,
+                                  &rt::g_smem_scols[slot])) != FSM_OK)
+      return st;
+  } else if ((st = rt::ensure_dyn_smem((const void*)fsm_prep2d_rows_long_kernel, dev, smem_rows,
+                                       &rt::g_smem_rows[slot])) != FSM_OK) {
+    return st;
+  }
+  if ((st = cu(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute")) !=
+      FSM_OK)
+    return st;
+  if ((st = cu(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream2d_kernel, kThreads2D, smem2),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor")) != FSM_OK)
+    return st;
+  if (sms <= 0 || occ <= 0) {
+    set_last_error("fsm_run_event_2d_noalloc: the stream kernel cannot be resident on this device");
+    return FSM_ERR_CUDA;
+  }
+  const int ntiles = (int)tiles.size();
+  const int grid2 = std::max(1, std::min(ntiles, sms * occ));
+
+  // upload (pageable source: returns once the bytes are staged), reset the
+  // counters this call reads, then the same launch sequence as the batch path
+  if ((st = cu(cudaMemcpyAsync(D + o_up, H.data(), upload_bytes, cudaMemcpyHostToDevice, s), "upload")) !=
+      FSM_OK)
     return st;
   if ((st = cu(cudaMemsetAsync(D + o_ctr, 0, sizeof(Counters), s), "memset")) != FSM_OK) return st;
   if ((st = cu(cudaMemsetAsync(D + o_err, 0, 4 * sizeof(int), s), "memset")) != FSM_OK) return st;
@@ -279,9 +286,38 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   }
   fsm_stream2d_kernel<<<grid2, kThreads2D, smem2, s>>>(d_ev2, reinterpret_cast<const Tile2D*>(D + o_tiles), ntiles,
                                                        box_cap, reinterpret_cast<Counters*>(D + o_ctr),
-                                                       reinterpret_cast<int*>(D + o_err));
+                                                       reinterpret_cast<int*>(D + o_err), kWaitPolls);
   fsm_landau_kernel<<<(int)bl.size(), kThreadsLandau, 0, s>>>(reinterpret_cast<const EvLandau*>(D + o_evl),
                                                             reinterpret_cast<const CellBlock*>(D + o_bl),
                                                             reinterpret_cast<Counters*>(D + o_ctr));
   return cu(cudaGetLastError(), "launch");
+}
+
+// Reads the error words the stream kernel of the last fsm_run_event_2d_noalloc
+// call on this device left in the scratch header, after waiting for `stream`
+// (the stream that call used).  The copy goes into a stack array: nothing is
+// allocated.  Samples outside the staged footprint -> FSM_ERR_CUDA; a staged
+// copy that did not land within the bounded wait -> FSM_ERR_TIMEOUT (the
+// affected tiles were not computed, so the outputs of that call are invalid).
+extern "C" fsm_status fsm_run_event_2d_noalloc_check(void* stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int err[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpyFromSymbolAsync(err, g_noalloc_scratch, sizeof(err), kHdrErr,
+                                            cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("fsm_run_event_2d_noalloc_check: ") + cudaGetErrorString(e));
+    return FSM_ERR_CUDA;
+  }
+  if (err[0]) {
+    set_last_error("fsm_run_event_2d_noalloc: " + std::to_string(err[0]) +
+                   " samples fell outside the staged footprint");
+    return FSM_ERR_CUDA;
+  }
+  if (err[1]) {
+    set_last_error("fsm_run_event_2d_noalloc: " + std::to_string(err[1]) +
+                   " staged copies did not complete within the bounded wait");
+    return FSM_ERR_TIMEOUT;
+  }
+  return FSM_OK;
 }

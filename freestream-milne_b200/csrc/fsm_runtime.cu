@@ -29,7 +29,7 @@ __global__ void fsm_prep2d_cols_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep2d_rows_long_kernel(const Ev2D*, const LineBlock*, int);
 __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
-__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*);
+__global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*, int);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
@@ -100,6 +100,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   if (n <= 0 || !params) return FSM_ERR_INVALID_ARG;
   std::unique_ptr<fsm_batch, void (*)(fsm_batch*)> b(new fsm_batch(), batch_free);
   b->ctx = ctx;
+  b->wait_polls = ctx->wait_polls;
   b->own_io = (ext_in_e == nullptr);
   b->plans.resize(n);
   {
@@ -631,7 +632,8 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
   if (timing) cudaEventRecord(ts.ev[1], s);
   if (b->ntiles)
     fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
-                                                               b->box_cap2, b->d_ctr, b->d_err);
+                                                               b->box_cap2, b->d_ctr, b->d_err,
+                                                               b->wait_polls);
   if (b->ntiles3)
     fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3, b->ntiles3,
                                                                b->d_ctr);
@@ -1254,6 +1256,18 @@ extern "C" fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t) {
   ctx->single_host = nullptr;
   batch_free(ctx->single_dev);
   ctx->single_dev = nullptr;
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_ctx_set_wait_limit(fsm_ctx* ctx, int polls) {
+  if (!ctx || polls < 0) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->wait_polls = polls;
+  // the cached one-event batches were built with the old bound
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  batch_free(ctx->single_host);
+  batch_free(ctx->single_dev);
+  ctx->single_host = ctx->single_dev = nullptr;
   return FSM_OK;
 }
 

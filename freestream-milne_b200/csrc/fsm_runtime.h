@@ -70,6 +70,7 @@ struct fsm_ctx {
   std::vector<cudaEvent_t> event_pool;
   std::mutex mu;
   int window_budget = fsm::kWindowBudget2D;  // staged window of a 2D phi_p run (autotuned)
+  int wait_polls = fsm::kWaitPolls;  // bounded waits of batches built from now on
   // energy-dependent DTAU of device profiles: sums on the device, read back
   float* d_sums = nullptr;
   float* h_sums = nullptr;
@@ -122,6 +123,7 @@ struct fsm_batch {
   int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
   size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
   int grid2 = 0, grid3 = 0;
+  int wait_polls = fsm::kWaitPolls;  // polls of one bounded wait in the stream kernel
   double samples = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -158,6 +160,12 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                        const float* const* ext_in_e, const float* const* ext_in_nB,
                        const fsm_outputs* ext_out, fsm_batch** out, const BatchMem* mem = nullptr);
 fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing);
+// Raises (never lowers) a kernel's dynamic shared-memory limit: the limit is a
+// process-wide attribute other launches (and captured graphs) rely on.
+// `slot` records the largest value set so far for that kernel on `device`;
+// every caller of the library uses the slots below, under one mutex.
+fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot);
+extern int g_smem2[64], g_smem3[64], g_smem_rows[64], g_smem_srows[64], g_smem_scols[64];
 fsm_status check_kernel_errors(fsm_batch* b);
 fsm_status fill_info(const EventPlan& P, fsm_run_info* info);
 

@@ -126,6 +126,8 @@ SIGNATURES = {
     "fsm_batch_check": (_ST, [_VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
+    "fsm_run_event_2d_noalloc_check": (_ST, [_VP]),
+    "fsm_ctx_set_wait_limit": (_ST, [_VP, ctypes.c_int]),
     "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
                               ctypes.c_int]),
     "fsm_diagnostics_device": (_ST, [ctypes.POINTER(Params), ctypes.POINTER(Outputs),
@@ -207,6 +209,12 @@ def run_event_2d_noalloc(params, d_e, dev_out, stream=None):
           "fsm_run_event_2d_noalloc")
 
 
+def run_event_2d_noalloc_check(stream=None):
+    """Waits for `stream` and raises if the last allocation-free call's
+    kernels reported an error."""
+    check(lib().fsm_run_event_2d_noalloc_check(stream), "fsm_run_event_2d_noalloc_check")
+
+
 def probe_fp32_tflops(device=0):
     v = ctypes.c_double()
     check(lib().fsm_probe_fp32_tflops(device, ctypes.byref(v)), "fsm_probe_fp32_tflops")
@@ -283,6 +291,10 @@ class Context:
         t = Tuning()
         check(lib().fsm_autotune(self.h, n, arr, pe, pn, ctypes.byref(t)), "fsm_autotune")
         return {"window_bytes": t.window_bytes, "ms": t.ms}
+
+    def set_wait_limit(self, polls):
+        """Polls of one bounded wait in batches built from now on (0: give up at once)."""
+        check(lib().fsm_ctx_set_wait_limit(self.h, int(polls)), "fsm_ctx_set_wait_limit")
 
     def set_tuning(self, window_bytes):
         t = Tuning(int(window_bytes), 0.0)

@@ -24,7 +24,7 @@ x = ix*DX + xmin, xmin = -((DIM_X-1)/2)*DX (src/FreeStream.cpp:16-31).
 """
 import numpy as np
 
-from fsm_params import default_params, derive
+from fsm_params import default_params, derive  # noqa: F401 (derive: re-exported)
 
 
 def axis(n, d):

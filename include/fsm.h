@@ -242,9 +242,17 @@ double fsm_batch_samples(fsm_batch* b);
  * events return FSM_ERR_TOO_LARGE.  The first call on each device looks up the
  * array's device address (make that first call before any stream capture).
  * All calls share the array, so calls that overlap on the GPU race: run them in
- * one stream or serialise them. */
+ * one stream or serialise them.  The call returns once its work is enqueued;
+ * the outputs are valid once fsm_run_event_2d_noalloc_check returns FSM_OK. */
 fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float* d_e_gev,
                                     const fsm_outputs* dev_out, void* stream);
+/* No counterpart in the reference.  Waits for `stream` and reports the
+ * kernel-side errors of the last fsm_run_event_2d_noalloc call on the current
+ * device, read from the fixed header of the same scratch array into host
+ * stack memory (no allocation): FSM_ERR_TIMEOUT when a staged copy did not
+ * land within its bounded wait (some tiles were not computed), FSM_ERR_CUDA
+ * when samples fell outside the staged footprint. */
+fsm_status fsm_run_event_2d_noalloc_check(void* stream);
 
 /* ------------------------------------------------------------- autotuning */
 /* Launch-shape tuning of a context (no counterpart in the reference).  The 2D
@@ -262,6 +270,15 @@ typedef struct fsm_tuning {
 fsm_status fsm_autotune(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
                         const float* const* host_nB, fsm_tuning* out);
 fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t);
+
+/* Polls of one bounded wait on a staged copy in the 2D stream kernel for the
+ * batches (and one-event batches) of ctx built after the call; default 1 << 20,
+ * 0 makes every such wait give up at once.  No counterpart in the reference,
+ * whose CPU loops have nothing to wait on: it exists so that the time-out path
+ * (FSM_ERR_TIMEOUT from fsm_batch_check, the context staying usable) can be
+ * exercised without a fault.  After a time-out the kernel always waits, with
+ * the default bound, for the copies it has in flight before it exits. */
+fsm_status fsm_ctx_set_wait_limit(fsm_ctx* ctx, int polls);
 
 /* ---------------------------------------------------------- request server */
 /* No counterpart in the reference, which computes one event per call.  A

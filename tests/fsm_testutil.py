@@ -144,12 +144,18 @@ def _per_cell_errors(got, ref, tau, m, ttt, baryon):
 
 
 def compare_parity(got, ref_float, ref64, tau, baryon=False):
-    """Parity with the reference's float output: per cell and quantity, the
-    GPU result is within the tolerance of the reference's value, or at least as
-    close to the FP64 precision oracle as the reference's own value is (the
-    reference's float path carries its own rounding noise, amplified by ~gamma^2
-    in the Landau-matched quantities of boosted cells).  Returns
-    ({name: worst error vs reference}, {name: cells decided by the FP64 rule})."""
+    """Parity with the reference's float output, per cell and quantity: the GPU
+    result is within the tolerance of the reference's value, or -- only in a
+    cell where the reference's own float value is more than a quarter of the
+    tolerance away from the FP64 precision oracle (its rounding noise,
+    amplified by ~gamma^2 in the Landau-matched quantities of boosted cells) --
+    within the tolerance of the FP64 value.  Such "rescued" cells are therefore
+    bounded in value by the tolerance against FP64 and confined to cells where
+    the reference itself is noisy; their count is returned (and printed by the
+    tests).  The strict contract, every masked cell within tolerance of FP64
+    (e relative to e), is compare(got, ref64, ...), run beside this check.
+    Returns ({name: worst error vs reference}, {name: rescued cells},
+    {name: masked cells})."""
     m = mask_of(ref64)
     ttt = np.asarray(ref64["T"], np.float64)[0][m]
     if baryon:
@@ -159,16 +165,17 @@ def compare_parity(got, ref_float, ref64, tau, baryon=False):
     g_64 = _per_cell_errors(got, ref64, tau, m, ttt, baryon)
     r_64 = _per_cell_errors(ref_float, ref64, tau, m, ttt, baryon)
     limits = dict(T=TOL_T, e=TOL_E, u=TOL_U, Pi=TOL_VISC, pi=TOL_VISC, J=TOL_T, nB=TOL_B, V=TOL_B)
-    worst, rescued, bad = {}, {}, {}
+    worst, rescued, cells, bad = {}, {}, {}, {}
     for k, a in g_ref.items():
         sel = keep if k in ("J", "nB", "V") else np.ones(a.size, bool)
         a, b, c = a[sel], g_64[k][sel], r_64[k][sel]
         over = a > limits[k]
-        ok_by_64 = b <= c * (1 + 1e-6) + 1e-9
+        ok_by_64 = (b <= limits[k]) & (c > 0.25 * limits[k])
         worst[k] = float(a.max()) if a.size else 0.0
         rescued[k] = int(np.count_nonzero(over & ok_by_64))
+        cells[k] = int(a.size)
         nbad = int(np.count_nonzero(over & ~ok_by_64))
         if nbad:
             bad[k] = (nbad, float(a[over & ~ok_by_64].max()))
     assert not bad, f"parity violated: {bad} (worst vs reference {worst})"
-    return worst, rescued
+    return worst, rescued, cells

@@ -27,10 +27,10 @@ def test_gpu_matches_reference_fixture(ctx, name):
     assert got["info"]["tau"] == pytest.approx(float(meta[2]))
     # the FP64 precision oracle (the reference's sample set, FP64 values)
     ref64 = O.run(oracle_params(d), e, nB=nB, fp64=2)
-    errs, rescued = compare_parity(got, ref, ref64, meta[2], baryon=bool(d["BARYON"]))
+    errs, rescued, cells = compare_parity(got, ref, ref64, meta[2], baryon=bool(d["BARYON"]))
     errs64 = compare(got, ref64, meta[2], baryon=bool(d["BARYON"]))
-    print(name, "vs reference float:", errs, "closer to FP64 than the reference:", rescued,
-          "vs FP64:", errs64)
+    print(name, "vs reference float:", errs, "rescued (within tolerance of FP64 where the "
+          "reference is noisy):", rescued, "of", cells, "vs FP64:", errs64)
 
 
 def test_gpu_gaussian_full_grid(ctx):
@@ -92,6 +92,59 @@ def test_gpu_2d_baryon(ctx):
     errs = compare_parity(got, ref, ref64, ref["tau"], baryon=True)
     errs64 = compare(got, ref64, ref["tau"], baryon=True)
     print("baryon2d vs float", errs, "vs FP64", errs64)
+
+
+def _report(name, got, ref, ref64, tau, baryon=False):
+    errs, rescued, cells = compare_parity(got, ref, ref64, tau, baryon=baryon)
+    errs64 = compare(got, ref64, tau, baryon=baryon)
+    print(f"{name}: vs reference float {errs}; rescued {rescued} of {cells}; vs FP64 {errs64}")
+    return errs64
+
+
+def test_gpu_3d_baryon_full_size(ctx):
+    """The 3D configuration with baryon charge at full size: 131 x 131 x 51
+    cells, 21 tan-map rapidities, DIM_PHIP 100, DTAU 0.8 (875,211 cells, 1.84 G
+    reference-equivalent samples), against the oracle's float run and its FP64
+    precision run."""
+    p, e, nB = W.baryon3d()
+    assert (p.DIM_X, p.DIM_Y, p.DIM_ETA, p.DIM_RAP, p.DIM_PHIP) == (131, 131, 51, 21, 100)
+    got = ctx.run_event(p, e, nB)
+    ref = _oracle(p, e, nB)
+    ref64 = _oracle(p, e, nB, fp64=2)
+    assert got["info"]["dim_phip"] == ref["dim_phip"] == 100
+    _report("baryon3d 131^2x51", got, ref, ref64, ref["tau"], baryon=True)
+
+
+def _extreme_events():
+    """The corners of the batched configuration's parameter ranges: the
+    largest grid at the finest spacing and longest DTAU (the arc-length rule
+    raises DIM_PHIP 64 -> 189; the widest staged windows), the smallest event,
+    a mid-size one, and the largest sample count (301^2, DIM_PHIP 200)."""
+    return [W.lumpy2d(seed=5, side=301, dx=0.05, nphip=64, dtau=1.5, eos=2, radius=6.0),
+            W.lumpy2d(seed=6, side=101, dx=0.1, nphip=64, dtau=0.3, eos=1, radius=3.0),
+            W.lumpy2d(seed=7, side=201, dx=0.075, nphip=100, dtau=0.9, eos=2, radius=5.0),
+            W.lumpy2d(seed=8, side=301, dx=0.05, nphip=200, dtau=1.5, eos=1, radius=6.0),
+            W.lumpy2d(seed=9, side=151, dx=0.1, nphip=64, dtau=1.5, eos=1, radius=4.0)]
+
+
+def test_gpu_batch_extreme_shapes(ctx):
+    """One batch holding the extreme shapes of the 512-event configuration:
+    every event against the oracle's float and FP64 runs, and bit for bit
+    against its own single-event result."""
+    evs = _extreme_events()
+    b = F.Batch(ctx, [p for p, _, _ in evs])
+    assert b.info(0)["dim_phip"] == 189
+    outs = b.run_host([(e, nB) for _, e, nB in evs])
+    b.close()
+    for (p, e, _), got in zip(evs, outs):
+        ref = _oracle(p, e)
+        ref64 = _oracle(p, e, fp64=2)
+        got["info"] = {"tau": ref["tau"]}
+        _report(f"{p.DIM_X}^2 dx {p.DX:.3f} dtau {p.DTAU:.2f} phi {ref['dim_phip']}", got, ref, ref64,
+                ref["tau"])
+        single = ctx.run_event(p, e)
+        for k in ("T", "e", "P", "Pi", "u", "pi"):
+            assert np.array_equal(got[k], single[k]), k
 
 
 def test_gpu_3d_baryon_reduced(ctx):

@@ -2,7 +2,8 @@
 memory when they run the free streaming (e.g. a framework that owns all device
 memory through its own pool).  It must give the results of the ordinary device
 entry point.  Kept in its own file, collected last, so a run that stops at its
-first failure has run every other test first; it also passes alone."""
+first failure has run every other test first; it also passes alone.  Its
+companion check reads the kernels' error words without allocating."""
 import numpy as np
 import pytest
 
@@ -24,10 +25,21 @@ def _host(outs, dim):
             for k, v in outs.items()}
 
 
+def _long_thin():
+    """100 x 900 cells: a line longer than the strip kernels stage, so the
+    long-line spline kernels run (within the entry point's cell limit)."""
+    p, _, _ = W.lumpy2d(seed=7, side=41, dx=0.08, nphip=64, dtau=0.6, eos=1, radius=1.2)
+    p.DIM_X, p.DIM_Y = 100, 900
+    W.derive(p)
+    rng = np.random.default_rng(8)
+    e = W.hotspots(rng, W.axis(100, p.DX), W.axis(900, p.DY), radius=3.0)
+    return p, e.astype(np.float32).ravel(), None
+
+
 def test_no_alloc_entry_matches_device_entry(ctx):
     import torch
     events = [W.lumpy2d(seed=21, side=151, dx=0.07, nphip=100, dtau=0.9, eos=2, radius=4.0),
-              W.gaussian2d()]
+              W.gaussian2d(), _long_thin()]
     stream = torch.cuda.current_stream().cuda_stream
     for p, e, _ in events:  # two calls in a row, each against the existing entry point
         dim = e.size
@@ -38,6 +50,7 @@ def test_no_alloc_entry_matches_device_entry(ctx):
         got = _dev_outputs(torch, dim)
         F.run_event_2d_noalloc(p, d_e.data_ptr(), {k: v.data_ptr() for k, v in got.items()},
                                stream=stream)
+        F.run_event_2d_noalloc_check(stream)  # waits; raises on a kernel-side error
         torch.cuda.synchronize()
         r, g = _host(ref, dim), _host(got, dim)
         compare(g, r, float(p.TAU0 + p.DTAU))
