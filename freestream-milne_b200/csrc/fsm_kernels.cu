@@ -294,15 +294,21 @@ __global__ void __launch_bounds__(128) fsm_prep2d_cols_long_kernel(
 // The reference's sums for the energy-dependent free-streaming time: float
 // running sums of eps^2 and eps over the converted profile, in cell order
 // (src/FreeStream.cpp:404-409).  The rounding of a running float sum depends
-// on its order, so one thread adds the cells in that order.
-__global__ void fsm_edep_sums_kernel(const float* __restrict__ e_gev, int n, float* sums) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// on its order, so one thread adds the cells of one event in that order (the
+// DTAU that follows is then bit-identical to the reference's); the events of
+// a batch run in parallel, one thread each, in one launch.
+__global__ void fsm_edep_sums_kernel(const float* const* __restrict__ e_gev, const int* __restrict__ cells,
+                                     int count, float* sums) {
+  const int ev = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ev >= count) return;
+  const float* __restrict__ e = e_gev[ev];
+  const int n = cells[ev];
   float num = 0.0f, den = 0.0f;
   int i = 0;
   for (; i + 8 <= n; i += 8) {
     float v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = to_fm4(__ldg(e_gev + i + k));
+    for (int k = 0; k < 8; ++k) v[k] = to_fm4(__ldg(e + i + k));
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       num = __fadd_rn(num, __fmul_rn(v[k], v[k]));
@@ -310,12 +316,12 @@ __global__ void fsm_edep_sums_kernel(const float* __restrict__ e_gev, int n, flo
     }
   }
   for (; i < n; ++i) {
-    const float v = to_fm4(__ldg(e_gev + i));
+    const float v = to_fm4(__ldg(e + i));
     num = __fadd_rn(num, __fmul_rn(v, v));
     den = __fadd_rn(den, v);
   }
-  sums[0] = num;
-  sums[1] = den;
+  sums[2 * ev] = num;
+  sums[2 * ev + 1] = den;
 }
 
 // ------------------------------------------------------------------ prep 3D

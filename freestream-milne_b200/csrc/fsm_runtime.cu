@@ -33,7 +33,7 @@ __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counte
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
-__global__ void fsm_edep_sums_kernel(const float*, int, float*);
+__global__ void fsm_edep_sums_kernel(const float* const*, const int*, int, float*);
 __global__ void fsm_diag_kernel(int, int, int, float, float, float, const float*, const float*,
                                 const float*, const float*, const float*, float*, float*, float*,
                                 float*, float*, float*);
@@ -66,6 +66,9 @@ bool has_device() {
 
 void batch_free(fsm_batch* b) {
   if (!b) return;
+  batch_free(b->inner);
+  if (b->d_edep) cudaFree(b->d_edep);
+  if (b->h_sums) cudaFreeHost(b->h_sums);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_segs) cudaFree(b->d_segs);
   if (b->d_pack) cudaFree(b->d_pack);
@@ -263,8 +266,9 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   size_t o_ctr = L.take(sizeof(Counters));
   size_t o_err = L.take(sizeof(int) * 4);
   const size_t upload_bytes = L.off;  // everything above comes from the host
-  // scratch and moments
-  for (int i = 0; i < n; ++i) {
+  // scratch and moments (none for a batch that only holds slabs)
+  const bool io_only = mem && mem->io_only;
+  for (int i = 0; i < n && !io_only; ++i) {
     const EventPlan& P = b->plans[i];
     EvOffs& o = eo[i];
     if (!P.is3d) {
@@ -648,9 +652,51 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
   return FSM_OK;
 }
 
+bool same_params(const fsm_params& a, const fsm_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+fsm_status launch(fsm_batch* b, cudaStream_t s);
+
+// A batch with E_DEP_FS events: the sums of every such event's converted
+// profile in one launch (one thread per event, the reference's order), one
+// sync, then DTAU per event and the inner batch planned with it (reused while
+// every DTAU stays the same), launched on the same stream.
+fsm_status launch_deferred(fsm_batch* b, cudaStream_t s) {
+  const int ne = (int)b->edep.size();
+  const float* const* d_ptr = reinterpret_cast<const float* const*>(b->d_edep);
+  const int* d_cells = reinterpret_cast<const int*>(b->d_edep + align_up(ne * sizeof(float*)));
+  float* d_sums = reinterpret_cast<float*>(b->d_edep + align_up(ne * sizeof(float*)) +
+                                           align_up(ne * sizeof(int)));
+  fsm_edep_sums_kernel<<<(ne + 127) / 128, 128, 0, s>>>(d_ptr, d_cells, ne, d_sums);
+  FSM_CUDA_TRY(cudaGetLastError());
+  FSM_CUDA_TRY(cudaMemcpyAsync(b->h_sums, d_sums, 2 * ne * sizeof(float), cudaMemcpyDeviceToHost, s));
+  FSM_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<fsm_params> res = b->raw;
+  for (int k = 0; k < ne; ++k) {
+    fsm_params& p = res[b->edep[k]];
+    p.DTAU = edep_dtau(p, b->h_sums[2 * k], b->h_sums[2 * k + 1]);
+    p.E_DEP_FS = 0;
+    fsm_params_derive(&p);
+  }
+  bool same = b->inner && res.size() == b->inner_params.size();
+  for (size_t i = 0; same && i < res.size(); ++i) same = same_params(res[i], b->inner_params[i]);
+  if (!same) {
+    batch_free(b->inner);
+    b->inner = nullptr;
+    const int n = (int)res.size();
+    std::vector<const float*> ie(b->d_in_e.begin(), b->d_in_e.end()),
+        inb(b->d_in_nB.begin(), b->d_in_nB.end());
+    fsm_status st = batch_build(b->ctx, n, res.data(), nullptr, ie.data(), inb.data(), b->d_out.data(),
+                                &b->inner);
+    if (st != FSM_OK) return st;
+    b->inner_params = res;
+  }
+  b->samples = b->inner->samples;
+  return launch(b->inner, s);
+}
+
 fsm_status launch(fsm_batch* b, cudaStream_t s) {
   fsm_ctx* ctx = b->ctx;
   b->last_stream = s;
+  if (!b->edep.empty()) return launch_deferred(b, s);
   if (ctx->timing) return enqueue(b, s, true);
   if (!b->graph || b->graph_stream != s) {
     if (b->graph) {
@@ -685,6 +731,10 @@ fsm_status launch(fsm_batch* b, cudaStream_t s) {
 // Reads the kernels' error counters in stream order on the batch's last
 // stream and waits for it, so every copy enqueued before has completed.
 fsm_status check_kernel_errors(fsm_batch* b) {
+  if (b->inner) {  // the launches of an E_DEP_FS batch ran its inner batch
+    b->inner->last_stream = b->last_stream ? b->last_stream : b->inner->last_stream;
+    return check_kernel_errors(b->inner);
+  }
   int err[4] = {0, 0, 0, 0};
   cudaStream_t s = b->last_stream ? b->last_stream : b->ctx->stream;
   FSM_CUDA_TRY(cudaMemcpyAsync(err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost, s));
@@ -702,7 +752,6 @@ fsm_status check_kernel_errors(fsm_batch* b) {
   return FSM_OK;
 }
 
-bool same_params(const fsm_params& a, const fsm_params& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
 fsm_status fill_info(const EventPlan& P, fsm_run_info* info) {
   if (!info) return FSM_OK;
@@ -861,14 +910,25 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
     // the device in the reference's order and read back before planning
     fsm_params_derive(&pe);
     if (pe.DIM <= 0) return FSM_ERR_INVALID_ARG;
+    // device block: [input pointer | cell count | sums]; pinned mirror
     if (!ctx->d_sums) {
-      FSM_CUDA_TRY(cudaMalloc(&ctx->d_sums, 2 * sizeof(float)));
-      FSM_CUDA_TRY(cudaMallocHost(&ctx->h_sums, 2 * sizeof(float)));
+      FSM_CUDA_TRY(cudaMalloc(&ctx->d_sums, 64));
+      FSM_CUDA_TRY(cudaMallocHost(&ctx->h_sums, 64));
     }
-    fsm_edep_sums_kernel<<<1, 32, 0, st>>>(d_e_gev, pe.DIM, ctx->d_sums);
-    FSM_CUDA_TRY(cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    char* hb = reinterpret_cast<char*>(ctx->h_sums);
+    char* db = reinterpret_cast<char*>(ctx->d_sums);
+    FSM_CUDA_TRY(cudaStreamSynchronize(st));  // the pinned block may be in use by a previous call
+    *reinterpret_cast<const float**>(hb) = d_e_gev;
+    *reinterpret_cast<int*>(hb + 16) = pe.DIM;
+    FSM_CUDA_TRY(cudaMemcpyAsync(db, hb, 32, cudaMemcpyHostToDevice, st));
+    fsm_edep_sums_kernel<<<1, 32, 0, st>>>(reinterpret_cast<const float* const*>(db),
+                                           reinterpret_cast<const int*>(db + 16), 1,
+                                           reinterpret_cast<float*>(db + 32));
+    FSM_CUDA_TRY(cudaGetLastError());
+    FSM_CUDA_TRY(cudaMemcpyAsync(hb + 32, db + 32, 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
     FSM_CUDA_TRY(cudaStreamSynchronize(st));
-    pe.DTAU = edep_dtau(pe, ctx->h_sums[0], ctx->h_sums[1]);
+    const float* sums = reinterpret_cast<const float*>(hb + 32);
+    pe.DTAU = edep_dtau(pe, sums[0], sums[1]);
     pe.E_DEP_FS = 0;
   }
   p = &pe;
@@ -909,7 +969,35 @@ extern "C" fsm_status fsm_batch_create_ex(fsm_ctx* ctx, int n, const fsm_params*
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
   BatchMem layout;  // no pools: only the output layout
   layout.grouped_out = grouped_outputs != 0;
-  return batch_build(ctx, n, params, nullptr, nullptr, nullptr, nullptr, out, &layout);
+  std::vector<int> edep;
+  for (int i = 0; i < n; ++i)
+    if (params[i].E_DEP_FS == 1) edep.push_back(i);
+  if (edep.empty()) return batch_build(ctx, n, params, nullptr, nullptr, nullptr, nullptr, out, &layout);
+  // E_DEP_FS events: this batch holds the slabs (laid out from provisional
+  // parameters, which fix only the event sizes); its launches run an inner
+  // batch planned with the DTAUs of the uploaded profiles
+  std::vector<fsm_params> prov(params, params + n);
+  for (int i : edep) prov[i].E_DEP_FS = 0;
+  layout.io_only = true;
+  fsm_batch* b = nullptr;
+  fsm_status st = batch_build(ctx, n, prov.data(), nullptr, nullptr, nullptr, nullptr, &b, &layout);
+  if (st != FSM_OK) return st;
+  std::unique_ptr<fsm_batch, void (*)(fsm_batch*)> hold(b, batch_free);
+  b->edep = edep;
+  b->raw.assign(params, params + n);
+  for (auto& p : b->raw) fsm_params_derive(&p);
+  const int ne = (int)edep.size();
+  const size_t o_cells = align_up(ne * sizeof(float*)), o_sums = o_cells + align_up(ne * sizeof(int));
+  FSM_CUDA_TRY(cudaMalloc(&b->d_edep, o_sums + 2 * ne * sizeof(float)));
+  FSM_CUDA_TRY(cudaMallocHost(&b->h_sums, 2 * ne * sizeof(float)));
+  std::vector<char> h(o_sums, 0);
+  for (int k = 0; k < ne; ++k) {
+    reinterpret_cast<const float**>(h.data())[k] = b->d_in_e[edep[k]];
+    reinterpret_cast<int*>(h.data() + o_cells)[k] = b->plans[edep[k]].DIM;
+  }
+  FSM_CUDA_TRY(cudaMemcpy(b->d_edep, h.data(), o_sums, cudaMemcpyHostToDevice));
+  *out = hold.release();
+  return FSM_OK;
 }
 
 extern "C" fsm_status fsm_batch_group_offset(fsm_batch* b, unsigned mask, int group, int ev,
@@ -1138,6 +1226,13 @@ extern "C" fsm_status fsm_batch_run_host(fsm_batch* b, const float* const* e_gev
 
 extern "C" fsm_status fsm_batch_info(fsm_batch* b, int ev, fsm_run_info* info) {
   if (!b || ev < 0 || ev >= (int)b->plans.size()) return FSM_ERR_INVALID_ARG;
+  if (!b->edep.empty()) {
+    if (!b->inner) {
+      set_last_error("E_DEP_FS batch: the run values are known after the first launch");
+      return FSM_ERR_PENDING;
+    }
+    return fill_info(b->inner->plans[ev], info);
+  }
   return fill_info(b->plans[ev], info);
 }
 

@@ -136,6 +136,18 @@ struct fsm_batch {
   size_t seg_cap = 0;
   float* d_pack = nullptr;
   size_t pack_elems = 0, pack_cap = 0;
+  // Events with E_DEP_FS = 1 (free-streaming time from the profile,
+  // src/FreeStream.cpp:389-417) cannot be planned before their inputs exist.
+  // Such a batch holds the slabs only; each launch takes every such event's
+  // profile sums on the device (one launch, one sync), resolves DTAU, and runs
+  // `inner`, a batch planned with the resolved parameters that reads and
+  // writes this batch's slabs (rebuilt only when a DTAU changes).
+  std::vector<int> edep;              // indices of the E_DEP_FS events
+  std::vector<fsm_params> raw;        // the caller's parameters
+  fsm_batch* inner = nullptr;
+  std::vector<fsm_params> inner_params;
+  char* d_edep = nullptr;             // device: input pointers, cell counts, sums
+  float* h_sums = nullptr;            // pinned: the sums read back
 };
 
 namespace fsm {
@@ -152,6 +164,9 @@ struct BatchMem {
   char* (*host)(void* user, size_t bytes) = nullptr;
   cudaStream_t stream = nullptr;
   bool grouped_out = false;  // output slab laid out group by group
+  // only the input/output slabs and the tables: no stream-kernel scratch (a
+  // batch whose launches run an inner batch planned later, see fsm_batch::inner)
+  bool io_only = false;
 };
 
 bool has_device();

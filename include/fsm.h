@@ -161,7 +161,15 @@ fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* 
 /* --------------------------------------------------------------- batches */
 /* Many 2D/3D events of uneven size in one persistent launch per kernel family,
  * captured into a CUDA graph on first launch.  The batch owns device input
- * and output slabs; per-event views come from fsm_batch_views. */
+ * and output slabs; per-event views come from fsm_batch_views.
+ * Events with E_DEP_FS = 1 (free-streaming time from the profile,
+ * src/FreeStream.cpp:389-417, src/FreestreamMilne.cpp:316-332) are planned at
+ * launch: each fsm_batch_launch of such a batch first sums every such event's
+ * uploaded profile on the device (one launch, in the reference's order, so
+ * DTAU is bit-identical to the reference's) and synchronises the stream once,
+ * then runs the batch planned with those DTAUs (re-planned only when one
+ * changes).  fsm_batch_info reports their run values after the first launch
+ * (FSM_ERR_PENDING before). */
 typedef struct fsm_batch fsm_batch;
 
 fsm_status fsm_batch_create(fsm_ctx* ctx, int n_events, const fsm_params* params,

@@ -162,9 +162,7 @@ def test_batch_equals_single_events(ctx):
     evs = []
     for name in golden_names():
         d, e, nB, _, _ = load_golden(name)
-        if d["E_DEP_FS"]:
-            continue  # batches take device-resident profiles: no host-side tau_fs
-        evs.append((fsm_params(d), e, nB))
+        evs.append((fsm_params(d), e, nB))  # E_DEP_FS events included
     b = F.Batch(ctx, [p for p, _, _ in evs])
     outs = b.run_host([(e, nB) for _, e, nB in evs])
     for (p, e, nB), o in zip(evs, outs):
@@ -187,8 +185,7 @@ def test_grouped_batch_downloads(ctx):
     evs = []
     for name in golden_names():
         d, e, nB, _, _ = load_golden(name)
-        if not d["E_DEP_FS"]:
-            evs.append((fsm_params(d), e, nB))
+        evs.append((fsm_params(d), e, nB))
     inputs = [(e, nB) for _, e, nB in evs]
     plain = F.Batch(ctx, [p for p, _, _ in evs])
     want = plain.run_host(inputs)
@@ -232,8 +229,7 @@ def test_packed_downloads(ctx, grouped):
     evs = []
     for name in golden_names():
         d, e, nB, _, _ = load_golden(name)
-        if not d["E_DEP_FS"]:
-            evs.append((fsm_params(d), e, nB))
+        evs.append((fsm_params(d), e, nB))
     inputs = [(e, nB) for _, e, nB in evs]
     b = F.Batch(ctx, [p for p, _, _ in evs], grouped=grouped)
     want = b.run_host(inputs)
@@ -286,6 +282,32 @@ def test_energy_dependent_tau(ctx):
     got = ctx.run_event(fsm_params(d), e)
     assert got["info"]["dtau"] == pytest.approx(float(meta[1]), rel=0, abs=0)
     compare_parity(got, ref, O.run(oracle_params(d), e, fp64=2), meta[2])
+
+
+def test_energy_dependent_tau_in_batches(ctx):
+    """E_DEP_FS events inside a batch built before its inputs exist: each
+    launch takes the profiles' sums on the device and plans with the resulting
+    DTAU, so the batch reproduces the reference's DTAU and outputs (parity with
+    the golden fixture), equals the one-event path bit for bit, and re-plans
+    when a new profile changes DTAU."""
+    d, e, nB, ref, meta = load_golden("edepfs2d_45")
+    p = fsm_params(d)
+    other = W.lumpy2d(seed=3, side=61, dx=0.08, nphip=48, dtau=0.6, eos=2, radius=2.0)
+    b = F.Batch(ctx, [p, other[0], p])
+    e2 = (e * np.float32(1.7)).astype(np.float32)  # a second profile: another DTAU
+    outs = b.run_host([(e, None), (other[1], None), (e2, None)])
+    assert b.info(0)["dtau"] == float(meta[1])
+    assert b.info(2)["dtau"] != b.info(0)["dtau"]
+    compare_parity(outs[0], ref, O.run(oracle_params(d), e, fp64=2), meta[2])
+    for got, (pp, ee) in zip(outs, [(p, e), (other[0], other[1]), (p, e2)]):
+        single = ctx.run_event(pp, ee)
+        for k in ("T", "e", "P", "Pi", "u", "pi"):
+            assert np.array_equal(got[k], single[k]), k
+    # a launch with the profiles swapped re-plans and still matches
+    outs2 = b.run_host([(e2, None), (other[1], None), (e, None)])
+    for k in ("T", "e", "u", "pi"):
+        assert np.array_equal(outs2[0][k], outs[2][k]) and np.array_equal(outs2[2][k], outs[0][k])
+    b.close()
 
 
 def test_energy_dependent_tau_device_entry(ctx):
