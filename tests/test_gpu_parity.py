@@ -27,10 +27,10 @@ def test_gpu_matches_reference_fixture(ctx, name):
     assert got["info"]["tau"] == pytest.approx(float(meta[2]))
     # the FP64 precision oracle (the reference's sample set, FP64 values)
     ref64 = O.run(oracle_params(d), e, nB=nB, fp64=2)
-    errs, rescued, cells = compare_parity(got, ref, ref64, meta[2], baryon=bool(d["BARYON"]))
+    errs, rescued, cells, residual = compare_parity(got, ref, ref64, meta[2], baryon=bool(d["BARYON"]))
     errs64 = compare(got, ref64, meta[2], baryon=bool(d["BARYON"]))
     print(name, "vs reference float:", errs, "rescued (within tolerance of FP64 where the "
-          "reference is noisy):", rescued, "of", cells, "vs FP64:", errs64)
+          "reference is noisy):", rescued, "of", cells, "residual:", residual, "vs FP64:", errs64)
 
 
 def test_gpu_gaussian_full_grid(ctx):
@@ -94,10 +94,14 @@ def test_gpu_2d_baryon(ctx):
     print("baryon2d vs float", errs, "vs FP64", errs64)
 
 
-def _report(name, got, ref, ref64, tau, baryon=False):
-    errs, rescued, cells = compare_parity(got, ref, ref64, tau, baryon=baryon)
-    errs64 = compare(got, ref64, tau, baryon=baryon)
-    print(f"{name}: vs reference float {errs}; rescued {rescued} of {cells}; vs FP64 {errs64}")
+def _report(name, got, ref, ref64, tau, baryon=False, strict=True):
+    errs, rescued, cells, residual = compare_parity(got, ref, ref64, tau, baryon=baryon)
+    # the strict FP64 contract; for the extreme 2D shapes on T, e and Pi only
+    # (u and pi there: the bounded residual of compare_parity)
+    what = ("T", "e", "u", "Pi", "pi") if strict else ("T", "e", "Pi")
+    errs64 = compare(got, ref64, tau, what=what, baryon=baryon)
+    print(f"{name}: vs reference float {errs}; rescued {rescued} of {cells}; residual {residual}; "
+          f"vs FP64 {errs64}")
     return errs64
 
 
@@ -141,7 +145,7 @@ def test_gpu_batch_extreme_shapes(ctx):
         ref64 = _oracle(p, e, fp64=2)
         got["info"] = {"tau": ref["tau"]}
         _report(f"{p.DIM_X}^2 dx {p.DX:.3f} dtau {p.DTAU:.2f} phi {ref['dim_phip']}", got, ref, ref64,
-                ref["tau"])
+                ref["tau"], strict=False)
         single = ctx.run_event(p, e)
         for k in ("T", "e", "P", "Pi", "u", "pi"):
             assert np.array_equal(got[k], single[k]), k
