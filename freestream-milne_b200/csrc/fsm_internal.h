@@ -94,8 +94,10 @@ struct PhiEntry2D {
   float c, s, cc, cs;        // cos, sin (reference floats), cos^2, cos sin
   float t, u;
   int ox;
-  int oy_near;               // low 16 bits: oy (signed); bit 16: near in x; bit 17: near in y
+  int oy_near;               // low 16 bits: oy (signed); bit 16: near in x; bit 17: near in y;
+                             // bit 18: (ox, oy) differs from the previous phi_p's (or phi_p 0)
 };
+constexpr int kReloadBit2D = 1 << 18;
 
 // A run of consecutive phi_p nodes whose source offsets fit one staged window:
 // for a tile at (x0, y0) the window starts at row x0 + ox0 - 1, column

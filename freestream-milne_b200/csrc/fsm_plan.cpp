@@ -269,6 +269,15 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       const int neary = (u < 1e-3 || u > 1.0 - 1e-3) ? 1 : 0;
       w.oy_near = ((int)oy & 0xffff) | (nearx << 16) | (neary << 17);
     }
+    // bit 18: the integer offset differs from the previous phi_p's (always at
+    // phi_p 0, where every tile starts), so the stream kernel reloads the
+    // nodes it keeps in registers exactly there
+    for (int k = 0; k < NP; ++k) {
+      PhiEntry2D& w = E.tab2[k];
+      const bool moved = (k == 0) || w.ox != E.tab2[k - 1].ox ||
+                         (w.oy_near & 0xffff) != (E.tab2[k - 1].oy_near & 0xffff);
+      if (moved) w.oy_near |= 1 << 18;
+    }
     // phi_p runs of at most kMaxRunPhi2D nodes whose staged window (tile +
     // offset spread + 1-node margins) fits the window budget; consecutive
     // nodes have neighbouring offsets.  A budget that cuts the circle into

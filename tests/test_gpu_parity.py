@@ -96,10 +96,14 @@ def test_gpu_2d_baryon(ctx):
 
 def _report(name, got, ref, ref64, tau, baryon=False, strict=True):
     errs, rescued, cells, residual = compare_parity(got, ref, ref64, tau, baryon=baryon)
-    # the strict FP64 contract; for the extreme 2D shapes on T, e and Pi only
-    # (u and pi there: the bounded residual of compare_parity)
-    what = ("T", "e", "u", "Pi", "pi") if strict else ("T", "e", "Pi")
-    errs64 = compare(got, ref64, tau, what=what, baryon=baryon)
+    # the strict FP64 contract; for the extreme 2D shapes on T and Pi, and e
+    # norm-wise (relative to T^{tau tau}: in their nearly light-like fringe
+    # cells e is ~T^{tau tau}/20, and u and pi there fall under the bounded
+    # residual of compare_parity)
+    if strict:
+        errs64 = compare(got, ref64, tau, baryon=baryon)
+    else:
+        errs64 = compare(got, ref64, tau, what=("T", "e", "Pi"), baryon=baryon, e_normwise=True)
     print(f"{name}: vs reference float {errs}; rescued {rescued} of {cells}; residual {residual}; "
           f"vs FP64 {errs64}")
     return errs64
