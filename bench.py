@@ -250,6 +250,47 @@ def event_3d(F, W, local, sp, stream, args):
     return out
 
 
+def output_files(F, W, ctx):
+    """Every output file of one event (the reference's post-matching file set,
+    47 files for a 2D event) from host arrays: fsm_write_outputs (files
+    formatted concurrently on all host threads) against the reference's own
+    writers (src/FileIO.cpp:11-131, one file after another, as its
+    run_freestream_milne calls them), on the outputs of the 261^2 lumpy event."""
+    import shutil
+    import numpy as np
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py as O
+    p, e, _ = W.lumpy2d(seed=1)
+    got = ctx.run_event(p, e)
+    dg = ctx.diagnostics(p, got)
+    p.TAU = got["info"]["tau"]
+    tmp = pathlib.Path(tempfile.mkdtemp(prefix="fsm_out_"))
+    try:
+        ours = []
+        (tmp / "ours").mkdir()
+        for _ in range(3):
+            t0 = time.perf_counter()
+            F.write_outputs(tmp / "ours", p, got, dg)
+            ours.append(time.perf_counter() - t0)
+        nbytes = sum(f.stat().st_size for f in (tmp / "ours").iterdir())
+        nfiles = len(list((tmp / "ours").iterdir()))
+        out = {"event": "261^2 lumpy, DIM_PHIP 200, WB EoS", "files": nfiles, "bytes": nbytes,
+               "ours_ms": 1e3 * min(ours), "threads": os.cpu_count()}
+        if O.ref_available():
+            (tmp / "ref" / "output").mkdir(parents=True)
+            d17 = np.concatenate([np.asarray(dg[k], np.float32).reshape(c, -1)
+                                  for k, c in F.DIAG_COMPS.items()])
+            t0 = time.perf_counter()
+            O.ref_write_outputs(tmp / "ref", O.Params(**p.as_dict()), got, d17)
+            out["reference_ms"] = 1e3 * (time.perf_counter() - t0)
+            out["reference"] = "the reference's writers, compiled from its sources (one thread)"
+            out["identical_bytes"] = all((tmp / "ours" / f.name).read_bytes() == f.read_bytes()
+                                         for f in (tmp / "ref" / "output").iterdir())
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def reference_arm(args):
     """The reference's CPU implementation on the same 512 events: the timed
     steps walk through the seeded event list in order, ceil(512 / steps)
@@ -447,6 +488,10 @@ def main():
     if not args.no_3d:
         ev3d = event_3d(F, W, local, sp, stream, args)
 
+    files = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        files = output_files(F, W, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
@@ -494,6 +539,7 @@ def main():
                                         "one device allocation, table upload), timed on the host; "
                                         "e2e above replays one planned batch"},
             "gpu_launches": launches_per_step * args.steps,
+            "output_files": files,
             "served": served,
             "event_3d": ev3d,
             "clocks": clocks,

@@ -250,56 +250,25 @@ inline int FREESTREAMMILNE::run_freestream_milne() {
   // hydro validity and thermal vorticity (src/FreestreamMilne.cpp:561-615),
   // computed on the GPU from the matched fields
   std::vector<float> dg(17 * n);
+  fsm_diagnostics hdg = {dg.data(), dg.data() + n, dg.data() + 2 * n, dg.data() + 6 * n,
+                         dg.data() + 7 * n, dg.data() + 11 * n};
   {
     fsm_outputs hin = {nullptr, nullptr, e.data(), P.data(), Pi.data(), u.data(), pi.data(),
                        nullptr, nullptr};
-    fsm_diagnostics hout = {dg.data(), dg.data() + n, dg.data() + 2 * n, dg.data() + 6 * n,
-                            dg.data() + 7 * n, dg.data() + 11 * n};
-    if (fsm_diagnostics_host(ctx_, &params, &hin, &hout) != FSM_OK) {
+    if (fsm_diagnostics_host(ctx_, &params, &hin, &hdg) != FSM_OK) {
       printf("freestream-milne: %s\n", fsm_last_error());
       return 1;
     }
-    write_field(dg, 0, "R_Pi_Inv_projection", params, true);
-    write_field(dg, n, "R_pimunu_Inv_projection", params, true);
     const int ctr = (params.DIM_Y * params.DIM_ETA * ((params.DIM_X - 1) / 2)) +
                     (params.DIM_ETA * ((params.DIM_Y - 1) / 2)) + ((params.DIM_ETA - 1) / 2);
     printf("R_Pi_Inv at center : %f \n", dg[ctr]);
     printf("R_pimunu_Inv at center : %f \n", dg[n + ctr]);
-    static const char* pu[4] = {"pi_dot_u_tau_projection", "pi_dot_u_x_projection",
-                                "pi_dot_u_y_projection", "pi_dot_u_eta_projection"};
-    for (int m = 0; m < 4; ++m) write_field(dg, (2 + m) * n, pu[m], params, true);
-    write_field(dg, 6 * n, "pi_mu_mu_projection", params, true);
   }
 
-  // hydro variables (src/FreestreamMilne.cpp:618-673)
-  write_field(e, 0, "e", params, false);
-  write_field(P, 0, "p", params, false);
-  write_field(Pi, 0, "bulk_PI", params, false);
-  write_field(e, 0, "e_projection", params, true);
-  write_field(P, 0, "p_projection", params, true);
-  write_field(Pi, 0, "bulk_PI_projection", params, true);
-  static const char* un[4] = {"ut", "ux", "uy", "un"};
-  for (int m = 0; m < 4; ++m) write_field(u, m * n, un[m], params, false);
-  for (int m = 0; m < 4; ++m)
-    write_field(u, m * n, (std::string(un[m]) + "_projection").c_str(), params, true);
-  static const char* pn[10] = {"pitt", "pitx", "pity", "pitn", "pixx",
-                               "pixy", "pixn", "piyy", "piyn", "pinn"};
-  for (int m = 0; m < 10; ++m) write_field(pi, m * n, pn[m], params, false);
-  for (int m = 0; m < 10; ++m)
-    write_field(pi, m * n, (std::string(pn[m]) + "_projection").c_str(), params, true);
-  write_field(dg, 8 * n, "beta_x_projection", params, true);
-  write_field(dg, 8 * n, "beta_x", params, false);
-  write_field(dg, 9 * n, "beta_y_projection", params, true);
-  write_field(dg, 9 * n, "beta_y", params, false);
-  write_field(dg, 14 * n, "w_xy_projection", params, true);
-  write_field(dg, 14 * n, "w_xy", params, false);
-  if (params.BARYON) {
-    write_field(nBo, 0, "nB", params, false);
-    write_field(nBo, 0, "nB_projection", params, true);
-    write_field(V, 1 * n, "V_x", params, false);
-    write_field(V, 2 * n, "V_y", params, false);
-    write_field(V, 3 * n, "V_eta", params, false);
-  }
+  // every output file of src/FreestreamMilne.cpp:561-673 in one call, the
+  // files formatted concurrently (the reference's ofstream fails silently when
+  // output/ is missing; so does this class)
+  fsm_write_outputs("output", &params, &out, &hdg, 0);
 
   // vectors for the caller, GeV / fm^3 (src/FreestreamMilne.cpp:677-718)
   std::vector<double>* vs[17] = {&final_energy_density, &final_pressure, &final_ut, &final_ux,

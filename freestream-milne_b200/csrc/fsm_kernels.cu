@@ -487,38 +487,31 @@ __device__ __forceinline__ void stage_window(float4* buf, const float4* __restri
 // is evaluated only in warps where some sample needs it.  Moments accumulate
 // in FP32 chunks of 16 phi_p folded into FP32 totals (two-level summation).
 //
-// kInterior: every sample of the run provably lands at least two nodes inside
-// the grid, so the in-grid test (src/FreeStream.cpp:213) is skipped.
-// Otherwise the test is made per phi_p for the warp as a whole first: a warp
-// whose cells all land two or more nodes inside takes the test-free path, and
-// only warps whose footprint reaches the boundary test their samples.
+// kInterior: every sample of the run provably lands inside the grid, so the
+// in-grid test (src/FreeStream.cpp:213) is skipped.
 //
 // Consecutive phi_p often share the integer offset (the source point moves by
 // at most about one cell per phi_p step): the thread keeps the 2 x (K + 1)
 // nodes of the last offset in registers (nd0/nd1, node values of the grid,
-// the same in every staged window) and reloads them only where the table
-// marks a new offset (kReloadBit2D; always at phi_p 0, where every tile
-// starts).  Out-of-grid window entries are never copied; samples that would
+// the same in every staged window) and reloads them only when the offset
+// changes.  Out-of-grid window entries are never copied; samples that would
 // read them are masked below, whatever the registers hold.
 //
-// `stab` holds the table entries of the run's phi_p p0 .. p1 - 1; [ty0, ty1]
-// is the tile's y range inside the grid.
+// `stab` holds the table entries of the run's phi_p p0 .. p1 - 1.
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
-                                             int p0, int p1, int ixb, int iy, int ty0, int ty1,
-                                             float ey, const float (&ex)[kCellsPerThread],
+                                             int p0, int p1, int ixb, int iy, float ey,
+                                             const float (&ex)[kCellsPerThread],
                                              float (&a0)[kCellsPerThread],
                                              float2 (&a12)[kCellsPerThread],
                                              float2 (&a34)[kCellsPerThread],
                                              float4 (&nd0)[kCellsPerThread + 1],
-                                             float4 (&nd1)[kCellsPerThread + 1],
-                                             float* __restrict__ stot, int* err) {
+                                             float4 (&nd1)[kCellsPerThread + 1], int& pox,
+                                             int& poy, float* __restrict__ stot, int* err) {
   constexpr int K = kCellsPerThread;
   const int NX = ev.NX, NY = ev.NY;
   const float2 ey2 = make_float2(ey, ey);
-  // this thread's window position relative to the node of offset (0, 0)
-  const float4* const tbase = win + (ixb - wx0) * boxW + (iy - wy0);
   // phi_p in pieces that end at the fold points of the two-level sum, so the
   // inner loop carries no fold test
   for (int pc = p0; pc < p1;) {
@@ -526,19 +519,22 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
     for (int p = pc; p < pe; ++p) {
       const float4* e = stab + kPhiTab2D * (p - p0);
       const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
-      const int oyn = __float_as_int(tu.w);
-      if (oyn & kReloadBit2D) {  // uniform over the block: the offset is per phi_p
-        const int ox = __float_as_int(tu.z), oy = (int)(short)(oyn & 0xffff);
-        const float4* rowp = tbase + ox * boxW + oy;
+      const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
+      const int oy = (int)(short)(oyn & 0xffff);
+      const int j = iy + oy, i0 = ixb + ox;
+      // y weights of this lane, first-order corrected for its own coordinate
+      const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
+      const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
+      const float4* rowp = win + (i0 - wx0) * boxW + (j - wy0);
+      if (ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
 #pragma unroll
         for (int r = 0; r <= K; ++r) {
           nd0[r] = rowp[r * boxW];
           nd1[r] = rowp[r * boxW + 1];
         }
+        pox = ox;
+        poy = oy;
       }
-      // y weights of this lane, first-order corrected for its own coordinate
-      const float2 Kp = __ffma2_rn(ey2, make_float2(dwy.x, dwy.y), make_float2(wy.x, wy.y));
-      const float2 Lp = __ffma2_rn(ey2, make_float2(dwy.z, dwy.w), make_float2(wy.z, wy.w));
       float cv[K];
       float2 VDp = make_float2(0.f, 0.f);
 #pragma unroll
@@ -578,38 +574,31 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       }
       const float4 mw = e[4];
       if (!kInterior) {
-        const int ox = __float_as_int(tu.z), oy = (int)(short)(oyn & 0xffff);
-        const int i0 = ixb + ox, j = iy + oy;
-        // every sample of this warp (x: i0 .. i0 + 3; y: the tile's lanes)
-        // lands two or more nodes inside the grid: no test needed (uniform)
-        const bool wfast = (i0 >= 2) && (i0 + K - 1 <= NX - 3) && (ty0 + oy >= 2) && (ty1 + oy <= NY - 3);
-        if (!wfast) {
-          const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
-          const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
-          if (!(nearx || neary)) {
+        const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
+        const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+        if (!(nearx || neary)) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
-              cv[k] = in ? cv[k] : 0.0f;
-            }
-          } else {
-            // the fraction lies within 1e-3 of an integer: a sample next to the
-            // grid boundary may fall in or out with the rounding of its float
-            // position, so those samples are decided and evaluated with the
-            // reference arithmetic
+          for (int k = 0; k < K; ++k) {
+            const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
+            cv[k] = in ? cv[k] : 0.0f;
+          }
+        } else {
+          // the fraction lies within 1e-3 of an integer: a sample next to the
+          // grid boundary may fall in or out with the rounding of its float
+          // position, so those samples are decided and evaluated with the
+          // reference arithmetic
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const int ik = i0 + k;
-              const bool cx = (ik >= 1) && (ik <= NX - 2);
-              const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-              const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-              if (ixb + k < NX && iy < NY && (ux || uy) && (ux || cx) && (uy || in_y)) {
-                const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-                const float y = __fadd_rn(__fmul_rn((float)iy, ev.DY), ev.ymin);
-                cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
-              } else {
-                cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
-              }
+          for (int k = 0; k < K; ++k) {
+            const int ik = i0 + k;
+            const bool cx = (ik >= 1) && (ik <= NX - 2);
+            const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+            const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+            if (ixb + k < NX && iy < NY && (ux || uy) && (ux || cx) && (uy || in_y)) {
+              const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+              const float y = __fadd_rn(__fmul_rn((float)iy, ev.DY), ev.ymin);
+              cv[k] = exact_sample(ev, win, true, wx0, wy0, boxW, 0, x, y, mw.x, mw.y, err);
+            } else {
+              cv[k] = (cx && in_y && !ux && !uy) ? cv[k] : 0.0f;
             }
           }
         }
@@ -709,7 +698,8 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     }
 #pragma unroll
     for (int m = 0; m < kTotSlots2D; ++m) stot[m * kThreads2D] = 0.0f;
-    float4 nd0[K + 1], nd1[K + 1];  // loaded at phi_p 0 (its table entry marks a reload)
+    float4 nd0[K + 1], nd1[K + 1];
+    int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
     // warps whose cells all lie past the grid's x edge skip the runs
     const bool live = ixb <= x_hi;
 
@@ -747,11 +737,11 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
                             (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
       if (!live) {
       } else if (interior) {
-        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, tl.y0, y_hi, ey, ex,
-                           a0, a12, a34, nd0, nd1, stot, err);
+        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
+                           a12, a34, nd0, nd1, pox, poy, stot, err);
       } else {
-        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, tl.y0, y_hi, ey, ex,
-                            a0, a12, a34, nd0, nd1, stot, err);
+        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
+                            a12, a34, nd0, nd1, pox, poy, stot, err);
       }
       __syncthreads();  // buffer b is free for the load of run c + 2
     }
@@ -914,7 +904,13 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
       // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
       // more either side when the fraction is near an integer)
       const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
-      const bool skip = (xb + 1 < 1) || (xa - 1 > NX - 2) || (yb + 1 < 1) || (ya - 1 > NY - 2);
+      // this warp's rows (ixb .. ixb + 3 inside the grid) shifted by ox: when
+      // they all land outside (a margin of one node for near-integer
+      // fractions), the warp has no sample here and skips the phi_p (uniform
+      // over the warp; the nodes it holds stay tagged with their own offset)
+      const int wa = ixb + ox, wb = min(ixb + K - 1, x_hi) + ox;
+      const bool skip = (yb + 1 < 1) || (ya - 1 > NY - 2) || (wb + 1 < 1) || (wa - 1 > NX - 2) ||
+                        (ixb > x_hi);
       if (!skip) {
         // (a full tile, so that no lane past the grid edge reads outside it)
         const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);

@@ -130,6 +130,8 @@ SIGNATURES = {
     "fsm_ctx_set_wait_limit": (_ST, [_VP, ctypes.c_int]),
     "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
                               ctypes.c_int]),
+    "fsm_write_outputs": (_ST, [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.POINTER(Outputs),
+                                ctypes.POINTER(Diagnostics), ctypes.c_int]),
     "fsm_diagnostics_device": (_ST, [ctypes.POINTER(Params), ctypes.POINTER(Outputs),
                                      ctypes.POINTER(Diagnostics), _VP]),
     "fsm_diagnostics_host": (_ST, [_VP, ctypes.POINTER(Params), ctypes.POINTER(Outputs),
@@ -517,6 +519,27 @@ def write_field(path, var, params, projection=False, nthreads=0):
         raise ValueError("field size does not match the grid")
     check(lib().fsm_write_field(str(path).encode(), v.ctypes.data, ctypes.byref(params),
                                 int(bool(projection)), int(nthreads)), "fsm_write_field")
+
+
+def write_outputs(dirpath, params, result, diag=None, nthreads=0):
+    """Every output file of one event (the reference's post-matching file set)
+    from host arrays: result as returned by Context.run_event, diag as by
+    Context.diagnostics (or None)."""
+    keep = []
+
+    def ptr(a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        keep.append(a)
+        return a.ctypes.data
+
+    o = Outputs(**{k: ptr(result[k]) for k in ("e", "P", "Pi", "u", "pi", "nB", "V")
+                   if result.get(k) is not None})
+    d = None
+    if diag is not None:
+        d = Diagnostics(**{k: ptr(diag[k]) for k in DIAG_COMPS if diag.get(k) is not None})
+    check(lib().fsm_write_outputs(str(dirpath).encode(), ctypes.byref(params), ctypes.byref(o),
+                                  ctypes.byref(d) if d is not None else None, int(nthreads)),
+          "fsm_write_outputs")
 
 
 def device_count():

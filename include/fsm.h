@@ -384,6 +384,18 @@ fsm_status fsm_diagnostics_host(fsm_ctx* ctx, const fsm_params* p, const fsm_out
  * which fails silently, an unwritable path returns FSM_ERR_FILE. */
 fsm_status fsm_write_field(const char* path, const float* var, const fsm_params* p, int projection,
                            int nthreads);
+/* Every per-cell file the reference writes after Landau matching
+ * (src/FreestreamMilne.cpp:561-673 via src/FileIO.cpp:11-131), byte-identical,
+ * into directory `dir` under the reference's file names (<dir>/e.dat,
+ * <dir>/e_projection.dat, ... the reference writes them into output/): from
+ * `diag` the hydro-validity projections (R_Pi_Inv, R_pimunu_Inv, pi_dot_u_*,
+ * pi_mu_mu) and beta_x, beta_y, w_xy (full and projection); from `out` e, p,
+ * bulk_PI, u^mu, pi^{mu nu} (full and projection) and with BARYON nB (both)
+ * and V_x, V_y, V_eta.  Host arrays; NULL fields (and a NULL diag) are
+ * skipped.  The files are formatted concurrently by nthreads host threads
+ * (0 = all hardware threads), largest first. */
+fsm_status fsm_write_outputs(const char* dir, const fsm_params* p, const fsm_outputs* out,
+                             const fsm_diagnostics* diag, int nthreads);
 
 /* ------------------------------------------------------------ diagnostics */
 /* Measured FP32 FMA throughput of `device` in TFLOP/s (a short FMA-chain

@@ -103,7 +103,28 @@ def ref():
         _ref.ref_run_full.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]
         _ref.ref_run_full.restype = ctypes.c_int
+        _ref.ref_write_outputs.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)] + [ctypes.c_void_p] * 8
+        _ref.ref_write_outputs.restype = ctypes.c_int
     return _ref
+
+
+def ref_write_outputs(workdir, params, res, diag17):
+    """The reference's own writers on host fields (float32 arrays) inside
+    workdir/output; diag17 as oracle_diagnostics lays it out."""
+    keep = []
+
+    def ptr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float32).ravel()
+        keep.append(a)
+        return a.ctypes.data
+
+    rc = ref().ref_write_outputs(str(workdir).encode(), ctypes.byref(params), ptr(res["e"]),
+                                 ptr(res["P"]), ptr(res["Pi"]), ptr(res["u"]), ptr(res["pi"]),
+                                 ptr(res.get("nB")), ptr(res.get("V")), ptr(diag17))
+    if rc != 0:
+        raise RuntimeError(f"ref_write_outputs failed with code {rc}")
 
 
 OUT_SHAPES = dict(T=10, J=4, e=1, P=1, Pi=1, u=4, pi=10, nB=1, V=4)

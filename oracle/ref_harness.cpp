@@ -198,3 +198,75 @@ extern "C" void ref_diagnostics(const oracle_params* pin, float tau, const float
   free2dArrayf(beta, 4);
   free2dArrayf(om, 6);
 }
+
+// The reference's own writers (src/FileIO.cpp:11-131) called in the order of
+// src/FreestreamMilne.cpp:561-673 on given host fields, inside `workdir`
+// (which must hold an output/ directory).  diag17: R_Pi_Inv, R_pimunu_Inv,
+// pi_dot_u (4), pi_mu_mu, beta (4), omega (6), each n floats.
+extern "C" int ref_write_outputs(const char* workdir, const oracle_params* pin, const float* e,
+                                 const float* P, const float* Pi, const float* u, const float* pi,
+                                 const float* nB, const float* V, const float* diag17) {
+  char old[4096];
+  if (!getcwd(old, sizeof(old))) return 1;
+  if (chdir(workdir) != 0) return 2;
+  parameters params;
+  std::memcpy(&params, pin, sizeof(params));
+  params.DIM = params.DIM_X * params.DIM_Y * params.DIM_ETA;
+  const int n = params.DIM;
+  auto vec2d = [&](const float* src, int comps) {
+    float** a = calloc2dArrayf(nullptr, comps, n);
+    for (int m = 0; m < comps; ++m) std::memcpy(a[m], src + (size_t)m * n, (size_t)n * 4);
+    return a;
+  };
+  std::vector<float> ev(e, e + n), Pv(P, P + n), Piv(Pi, Pi + n);
+  float** flow = vec2d(u, 4);
+  float** shear = vec2d(pi, 10);
+  float** beta = vec2d(diag17 + (size_t)7 * n, 4);
+  float** om = vec2d(diag17 + (size_t)11 * n, 6);
+  std::vector<float> d0(diag17, diag17 + n), d1(diag17 + n, diag17 + 2 * (size_t)n);
+  std::vector<float> pdu[4], pmm(diag17 + 6 * (size_t)n, diag17 + 7 * (size_t)n);
+  for (int m = 0; m < 4; ++m) pdu[m].assign(diag17 + (2 + m) * (size_t)n, diag17 + (3 + m) * (size_t)n);
+  writeScalarToFileProjection(d0.data(), (char*)"R_Pi_Inv_projection", params);
+  writeScalarToFileProjection(d1.data(), (char*)"R_pimunu_Inv_projection", params);
+  writeScalarToFileProjection(pdu[0].data(), (char*)"pi_dot_u_tau_projection", params);
+  writeScalarToFileProjection(pdu[1].data(), (char*)"pi_dot_u_x_projection", params);
+  writeScalarToFileProjection(pdu[2].data(), (char*)"pi_dot_u_y_projection", params);
+  writeScalarToFileProjection(pdu[3].data(), (char*)"pi_dot_u_eta_projection", params);
+  writeScalarToFileProjection(pmm.data(), (char*)"pi_mu_mu_projection", params);
+  writeScalarToFile(ev.data(), (char*)"e", params);
+  writeScalarToFile(Pv.data(), (char*)"p", params);
+  writeScalarToFile(Piv.data(), (char*)"bulk_PI", params);
+  writeScalarToFileProjection(ev.data(), (char*)"e_projection", params);
+  writeScalarToFileProjection(Pv.data(), (char*)"p_projection", params);
+  writeScalarToFileProjection(Piv.data(), (char*)"bulk_PI_projection", params);
+  static const char* un[4] = {"ut", "ux", "uy", "un"};
+  for (int m = 0; m < 4; ++m) writeVectorToFile(flow, (char*)un[m], m, params);
+  for (int m = 0; m < 4; ++m)
+    writeVectorToFileProjection(flow, (char*)(std::string(un[m]) + "_projection").c_str(), m, params);
+  static const char* pn[10] = {"pitt", "pitx", "pity", "pitn", "pixx", "pixy", "pixn", "piyy", "piyn", "pinn"};
+  for (int m = 0; m < 10; ++m) writeVectorToFile(shear, (char*)pn[m], m, params);
+  for (int m = 0; m < 10; ++m)
+    writeVectorToFileProjection(shear, (char*)(std::string(pn[m]) + "_projection").c_str(), m, params);
+  writeVectorToFileProjection(beta, (char*)"beta_x_projection", 1, params);
+  writeVectorToFile(beta, (char*)"beta_x", 1, params);
+  writeVectorToFileProjection(beta, (char*)"beta_y_projection", 2, params);
+  writeVectorToFile(beta, (char*)"beta_y", 2, params);
+  writeVectorToFileProjection(om, (char*)"w_xy_projection", 3, params);
+  writeVectorToFile(om, (char*)"w_xy", 3, params);
+  if (params.BARYON) {
+    std::vector<float> nb(nB, nB + n);
+    float** bd = vec2d(V, 4);
+    writeScalarToFile(nb.data(), (char*)"nB", params);
+    writeScalarToFileProjection(nb.data(), (char*)"nB_projection", params);
+    writeVectorToFile(bd, (char*)"V_x", 1, params);
+    writeVectorToFile(bd, (char*)"V_y", 2, params);
+    writeVectorToFile(bd, (char*)"V_eta", 3, params);
+    free2dArrayf(bd, 4);
+  }
+  free2dArrayf(flow, 4);
+  free2dArrayf(shear, 10);
+  free2dArrayf(beta, 4);
+  free2dArrayf(om, 6);
+  if (chdir(old) != 0) return 3;
+  return 0;
+}

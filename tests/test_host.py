@@ -247,3 +247,44 @@ def test_text_writer_matches_reference_format(tmp_path):
         out = tmp_path / (name + ".txt")
         F.write_field(out, var, p, projection=proj, nthreads=3)
         assert out.read_bytes() == want, name
+
+
+@pytest.mark.parametrize("case", ["lumpy2d", "baryon3d"])
+def test_all_output_files_match_reference_writers(tmp_path, case):
+    """fsm_write_outputs writes the reference's whole post-matching file set
+    (src/FreestreamMilne.cpp:561-673) byte for byte like the reference's own
+    writers (src/FileIO.cpp:11-131, compiled from the reference sources) on the
+    same float fields -- the Landau-matched outputs and diagnostics of an
+    oracle run -- with the files formatted concurrently."""
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    import workloads as W
+    if case == "lumpy2d":
+        p, e, nB = W.lumpy2d(seed=4, side=31, dx=0.1, nphip=24, dtau=0.6, eos=2, radius=1.2)
+        p.DIM_Y = 29
+        W.derive(p)
+        e = e.reshape(31, 31)[:, :29].ravel().copy()
+    else:
+        p, e, nB = W.baryon3d(seed=3, side=21, neta=9, nrap=7, nphip=16)
+    po = O.Params(**p.as_dict())
+    res = O.run(po, e, nB=nB)
+    f32 = {k: np.asarray(res[k], np.float32) for k in ("e", "P", "Pi", "u", "pi", "nB", "V") if k in res}
+    n = p.DIM_X * p.DIM_Y * p.DIM_ETA
+    d17 = np.asarray(O.diagnostics(po, res["tau"], f32["e"], f32["P"], f32["Pi"], f32["u"], f32["pi"]),
+                     np.float32).reshape(17, n)
+    diag, off = {}, 0
+    for k, c in F.DIAG_COMPS.items():
+        diag[k] = d17[off:off + c]
+        off += c
+    p.TAU = res["tau"]
+    mine = tmp_path / "mine"
+    mine.mkdir()
+    F.write_outputs(mine, p, f32, diag, nthreads=4)
+    theirs = tmp_path / "ref"
+    (theirs / "output").mkdir(parents=True)
+    O.ref_write_outputs(theirs, O.Params(**p.as_dict()), f32, d17)
+    a = sorted(x.name for x in mine.iterdir())
+    b = sorted(x.name for x in (theirs / "output").iterdir())
+    assert a == b and len(a) == (52 if p.BARYON else 47), (len(a), set(a) ^ set(b))
+    for name in a:
+        assert (mine / name).read_bytes() == (theirs / "output" / name).read_bytes(), name
