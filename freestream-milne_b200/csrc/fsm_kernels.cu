@@ -912,19 +912,33 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
       const bool skip = (yb + 1 < 1) || (ya - 1 > NY - 2) || (wb + 1 < 1) || (wa - 1 > NX - 2) ||
                         (ixb > x_hi);
       if (!skip) {
-        // (a full tile, so that no lane past the grid edge reads outside it)
-        const bool interior = full && (xa >= 2) && (xb <= NX - 3) && (ya >= 2) && (yb <= NY - 3);
         const int i0 = ixb + ox, j = iy + oy;
+        // every sample of this warp lands two or more nodes inside the grid:
+        // its rows i0 .. i0 + 3 and all 32 lanes' columns (lanes past the
+        // grid edge included, so that their loads stay inside the arrays);
+        // then no sample needs the in-grid test or its rounding (uniform)
+        const bool inside = (i0 >= 2) && (i0 + K - 1 <= NX - 3) && (tl.y0 + oy >= 2) &&
+                            (tl.y0 + kTileY - 1 + oy <= NY - 3);
         if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
-          // clamped indices keep the loads of edge lanes inside the arrays
-          // (their samples are masked below); inside the grid they are exact
-          const int jj = min(max(j, 0), NY - 2);
+          if (inside) {
+            // one base index, rows NY apart
+            const int q0 = i0 * NY + j;
 #pragma unroll
-          for (int r = 0; r <= K; ++r) {
-            const int i = min(max(i0 + r, 0), NX - 1);
-            const NodeT* q = N + (size_t)i * NY + jj;
-            n0[r] = __ldg(q);
-            n1[r] = __ldg(q + 1);
+            for (int r = 0; r <= K; ++r) {
+              n0[r] = __ldg(N + (q0 + r * NY));
+              n1[r] = __ldg(N + (q0 + r * NY + 1));
+            }
+          } else {
+            // clamped indices keep the loads of edge lanes inside the arrays
+            // (their samples are masked below); inside the grid they are exact
+            const int jj = min(max(j, 0), NY - 2);
+#pragma unroll
+            for (int r = 0; r <= K; ++r) {
+              const int i = min(max(i0 + r, 0), NX - 1);
+              const NodeT* q = N + (size_t)i * NY + jj;
+              n0[r] = __ldg(q);
+              n1[r] = __ldg(q + 1);
+            }
           }
           pox = ox;
           poy = oy;
@@ -956,23 +970,32 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
           Cp = C;
         }
         const FSM_FLOAT2 cs = ev.cs[p];
-        if (!interior) {
+        if (!inside) {
           const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
           const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+          if (!(nearx || neary)) {  // uniform: no decision depends on the rounding
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int ik = i0 + k;
-            const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-            const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-            bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
-            if (act[k] && (ux || uy)) {
-              // the in-grid decision depends on the rounding: reference arithmetic
-              const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-              in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+            for (int k = 0; k < K; ++k) {
+              const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
+              v[k] = in ? v[k] : 0.0f;
+              vb[k] = in ? vb[k] : 0.0f;
             }
-            if (!in) {
-              v[k] = 0.0f;
-              vb[k] = 0.0f;
+          } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              const int ik = i0 + k;
+              const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+              const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+              bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
+              if (act[k] && (ux || uy)) {
+                // the in-grid decision depends on the rounding: reference arithmetic
+                const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+                in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+              }
+              if (!in) {
+                v[k] = 0.0f;
+                vb[k] = 0.0f;
+              }
             }
           }
         }
