@@ -886,154 +886,173 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
     a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
     a3[k] = a4[k] = a5[k] = 0.0f;
   }
+  // eta interpolation with the rapidity weights in one pair per field:
+  // (1 - et) rf(slice) and et rf(slice + 1)
   const float omet = 1.0f - et;
-  const float2 rf = make_float2(rf0, rf1), rb = make_float2(rb0, rb1);
+  const float2 wE = make_float2(omet * rf0, et * rf1), wB = make_float2(omet * rb0, et * rb1);
   // float2 nodes of the last offset stay in registers; float4 nodes (with
   // baryons) are reloaded for every phi_p (kept, they would not fit the
   // registers of two CTAs per SM)
   constexpr bool kCache = !kB;
   NodeT n0[K + 1], n1[K + 1];
   int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
-  // phi_p in pieces that end at the fold points of the two-level sum
-  for (int pc = 0; pc < NP;) {
-    const int pe = min(NP, (pc | (kPhiChunk - 1)) + 1);
-    for (int p = pc; p < pe; ++p) {
-      const PhiEntry3D e = tab[p];
-      const int ox = e.ox;
-      const int oy = (int)(short)(e.oy_near & 0xffff);
-      // sample floor indices of the tile's cells: [x0 + ox, x_hi + ox] (one
-      // more either side when the fraction is near an integer)
-      const int xa = tl.x0 + ox, xb = x_hi + ox, ya = tl.y0 + oy, yb = y_hi + oy;
-      // this warp's rows (ixb .. ixb + 3 inside the grid) shifted by ox: when
-      // they all land outside (a margin of one node for near-integer
-      // fractions), the warp has no sample here and skips the phi_p (uniform
-      // over the warp; the nodes it holds stay tagged with their own offset)
-      const int wa = ixb + ox, wb = min(ixb + K - 1, x_hi) + ox;
-      const bool skip = (yb + 1 < 1) || (ya - 1 > NY - 2) || (wb + 1 < 1) || (wa - 1 > NX - 2) ||
-                        (ixb > x_hi);
-      if (!skip) {
-        const int i0 = ixb + ox, j = iy + oy;
+  // phi_p in blocks of 32: the warp's lanes test the 32 phi_p at once (does
+  // any sample of this warp reach the grid; does every sample land two or
+  // more nodes inside) and the warp then visits only the phi_p that reach it,
+  // in order, folding the partial sums at the same points (every kPhiChunk
+  // phi_p) as a visit of every phi_p would
+  static_assert(32 % kPhiChunk == 0, "fold points inside a 32-phi_p block");
+  const int lane = threadIdx.x & 31;
+  for (int pb = 0; pb < NP; pb += 32) {
+    unsigned vis_mask, in_mask;
+    {
+      const int p = pb + lane;
+      bool vis = false, ins = false;
+      if (p < NP && ixb <= x_hi) {
+        const PhiEntry3D e = tab[p];
+        const int ox = e.ox;
+        const int oy = (int)(short)(e.oy_near & 0xffff);
+        // sample floor indices of the tile's rows [x0 + ox, x_hi + ox] (one
+        // more either side when the fraction is near an integer); this
+        // warp's rows ixb .. min(ixb + 3, x_hi)
+        const int ya = tl.y0 + oy, yb = y_hi + oy;
+        const int wa = ixb + ox, wb = min(ixb + K - 1, x_hi) + ox;
+        vis = !((yb + 1 < 1) || (ya - 1 > NY - 2) || (wb + 1 < 1) || (wa - 1 > NX - 2));
         // every sample of this warp lands two or more nodes inside the grid:
-        // its rows i0 .. i0 + 3 and all 32 lanes' columns (lanes past the
-        // grid edge included, so that their loads stay inside the arrays);
-        // then no sample needs the in-grid test or its rounding (uniform)
-        const bool inside = (i0 >= 2) && (i0 + K - 1 <= NX - 3) && (tl.y0 + oy >= 2) &&
-                            (tl.y0 + kTileY - 1 + oy <= NY - 3);
-        if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
-          if (inside) {
-            // one base index, rows NY apart
-            const int q0 = i0 * NY + j;
+        // its rows wa .. wa + 3 and all 32 lanes' columns (lanes past the
+        // grid edge included, so that their loads stay inside the arrays)
+        ins = (wa >= 2) && (wa + K - 1 <= NX - 3) && (tl.y0 + oy >= 2) && (tl.y0 + kTileY - 1 + oy <= NY - 3);
+      }
+      vis_mask = __ballot_sync(0xffffffffu, vis);
+      in_mask = __ballot_sync(0xffffffffu, ins);
+    }
+    for (int pc = pb; pc < min(NP, pb + 32); pc += kPhiChunk) {
+      unsigned m = (vis_mask >> (pc - pb)) & ((1u << kPhiChunk) - 1u);
+      while (m) {
+        const int bit = __ffs(m) - 1;
+        m &= m - 1u;
+        const int p = pc + bit;
+        const PhiEntry3D e = tab[p];
+        const int ox = e.ox;
+        const int oy = (int)(short)(e.oy_near & 0xffff);
+        {
+          const int i0 = ixb + ox, j = iy + oy;
+          const bool inside = (in_mask >> (p - pb)) & 1u;
+          if (!kCache || ox != pox || oy != poy) {  // uniform over the block: the offset is per phi_p
+            if (inside) {
+              // one base index, rows NY apart
+              const int q0 = i0 * NY + j;
 #pragma unroll
-            for (int r = 0; r <= K; ++r) {
-              n0[r] = __ldg(N + (q0 + r * NY));
-              n1[r] = __ldg(N + (q0 + r * NY + 1));
-            }
-          } else {
-            // clamped indices keep the loads of edge lanes inside the arrays
-            // (their samples are masked below); inside the grid they are exact
-            const int jj = min(max(j, 0), NY - 2);
-#pragma unroll
-            for (int r = 0; r <= K; ++r) {
-              const int i = min(max(i0 + r, 0), NX - 1);
-              const NodeT* q = N + (size_t)i * NY + jj;
-              n0[r] = __ldg(q);
-              n1[r] = __ldg(q + 1);
-            }
-          }
-          pox = ox;
-          poy = oy;
-        }
-        const float uc = e.u + ey;
-        const float2 uc2 = make_float2(uc, uc);
-        float v[K], vb[K];
-        float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int r = 0; r <= K; ++r) {
-          // y interpolation of the row on both eta slices (packed pairs)
-          const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
-          float2 C = make_float2(0.f, 0.f);
-          if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
-          if (r > 0) {
-            const int q = r - 1;
-            const float tk = e.t + ex[q];
-            const float2 tk2 = make_float2(tk, tk);
-            // x interpolation, then the eta interpolation with the rapidity weights
-            const float2 L = __fmul2_rn(lerp2(tk2, Bp, B), rf);
-            v[q] = fmaf(omet, L.x, et * L.y);
-            vb[q] = 0.0f;
-            if (kB) {
-              const float2 M = __fmul2_rn(lerp2(tk2, Cp, C), rb);
-              vb[q] = fmaf(omet, M.x, et * M.y);
-            }
-          }
-          Bp = B;
-          Cp = C;
-        }
-        const FSM_FLOAT2 cs = ev.cs[p];
-        if (!inside) {
-          const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
-          const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
-          if (!(nearx || neary)) {  // uniform: no decision depends on the rounding
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
-              v[k] = in ? v[k] : 0.0f;
-              vb[k] = in ? vb[k] : 0.0f;
-            }
-          } else {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const int ik = i0 + k;
-              const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
-              const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
-              bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
-              if (act[k] && (ux || uy)) {
-                // the in-grid decision depends on the rounding: reference arithmetic
-                const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-                in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+              for (int r = 0; r <= K; ++r) {
+                n0[r] = __ldg(N + (q0 + r * NY));
+                n1[r] = __ldg(N + (q0 + r * NY + 1));
               }
-              if (!in) {
-                v[k] = 0.0f;
-                vb[k] = 0.0f;
+            } else {
+              // clamped indices keep the loads of edge lanes inside the arrays
+              // (their samples are masked below); inside the grid they are exact
+              const int jj = min(max(j, 0), NY - 2);
+#pragma unroll
+              for (int r = 0; r <= K; ++r) {
+                const int i = min(max(i0 + r, 0), NX - 1);
+                const NodeT* q = N + (size_t)i * NY + jj;
+                n0[r] = __ldg(q);
+                n1[r] = __ldg(q + 1);
               }
             }
+            pox = ox;
+            poy = oy;
+          }
+          const float uc = e.u + ey;
+          const float2 uc2 = make_float2(uc, uc);
+          float v[K], vb[K];
+          float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r <= K; ++r) {
+            // y interpolation of the row on both eta slices (packed pairs)
+            const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
+            float2 C = make_float2(0.f, 0.f);
+            if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
+            if (r > 0) {
+              const int q = r - 1;
+              const float tk = e.t + ex[q];
+              const float2 tk2 = make_float2(tk, tk);
+              // x interpolation, then the eta interpolation with the rapidity weights
+              const float2 L = lerp2(tk2, Bp, B);
+              v[q] = fmaf(wE.x, L.x, wE.y * L.y);
+              vb[q] = 0.0f;
+              if (kB) {
+                const float2 M = lerp2(tk2, Cp, C);
+                vb[q] = fmaf(wB.x, M.x, wB.y * M.y);
+              }
+            }
+            Bp = B;
+            Cp = C;
+          }
+          const FSM_FLOAT2 cs = ev.cs[p];
+          if (!inside) {
+            const bool nearx = (e.oy_near >> 16) & 1, neary = (e.oy_near >> 17) & 1;
+            const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
+            if (!(nearx || neary)) {  // uniform: no decision depends on the rounding
+#pragma unroll
+              for (int k = 0; k < K; ++k) {
+                const bool in = in_y && ((unsigned)(i0 + k - 1) <= (unsigned)(NX - 3));
+                v[k] = in ? v[k] : 0.0f;
+                vb[k] = in ? vb[k] : 0.0f;
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < K; ++k) {
+                const int ik = i0 + k;
+                const bool ux = nearx && (ik == 0 || ik == 1 || ik == NX - 2 || ik == NX - 1);
+                const bool uy = neary && (j == 0 || j == 1 || j == NY - 2 || j == NY - 1);
+                bool in = in_y && ((unsigned)(ik - 1) <= (unsigned)(NX - 3));
+                if (act[k] && (ux || uy)) {
+                  // the in-grid decision depends on the rounding: reference arithmetic
+                  const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
+                  in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+                }
+                if (!in) {
+                  v[k] = 0.0f;
+                  vb[k] = 0.0f;
+                }
+              }
+            }
+          }
+          const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+          const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const float2 w = make_float2(v[k], vb[k]);
+            a01[k] = __fadd2_rn(a01[k], w);
+            a1c[k] = __ffma2_rn(w, c2, a1c[k]);
+            a1s[k] = __ffma2_rn(w, s2, a1s[k]);
+            a3[k] = fmaf(v[k], cc, a3[k]);
+            a4[k] = fmaf(v[k], csn, a4[k]);
+            a5[k] = fmaf(v[k], ss, a5[k]);
           }
         }
-        const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
-        const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
+      }
+      {
+        // second level of the two-level sum: per-rapidity sums in slots
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const float2 w = make_float2(v[k], vb[k]);
-          a01[k] = __fadd2_rn(a01[k], w);
-          a1c[k] = __ffma2_rn(w, c2, a1c[k]);
-          a1s[k] = __ffma2_rn(w, s2, a1s[k]);
-          a3[k] = fmaf(v[k], cc, a3[k]);
-          a4[k] = fmaf(v[k], csn, a4[k]);
-          a5[k] = fmaf(v[k], ss, a5[k]);
+          float* q = sl + k * kSlotsPerCell3D * kThreads3D;
+          q[0 * kThreads3D] += a01[k].x;
+          q[1 * kThreads3D] += a1c[k].x;
+          q[2 * kThreads3D] += a1s[k].x;
+          q[3 * kThreads3D] += a3[k];
+          q[4 * kThreads3D] += a4[k];
+          q[5 * kThreads3D] += a5[k];
+          if (kB) {
+            q[16 * kThreads3D] += a01[k].y;
+            q[17 * kThreads3D] += a1c[k].y;
+            q[18 * kThreads3D] += a1s[k].y;
+          }
+          a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
+          a3[k] = a4[k] = a5[k] = 0.0f;
         }
       }
     }
-    {
-      // second level of the two-level sum: per-rapidity sums in slots
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        float* q = sl + k * kSlotsPerCell3D * kThreads3D;
-        q[0 * kThreads3D] += a01[k].x;
-        q[1 * kThreads3D] += a1c[k].x;
-        q[2 * kThreads3D] += a1s[k].x;
-        q[3 * kThreads3D] += a3[k];
-        q[4 * kThreads3D] += a4[k];
-        q[5 * kThreads3D] += a5[k];
-        if (kB) {
-          q[16 * kThreads3D] += a01[k].y;
-          q[17 * kThreads3D] += a1c[k].y;
-          q[18 * kThreads3D] += a1s[k].y;
-        }
-        a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
-        a3[k] = a4[k] = a5[k] = 0.0f;
-      }
-    }
-    pc = pe;
   }
 }
 
