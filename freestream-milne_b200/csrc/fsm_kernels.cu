@@ -501,8 +501,8 @@ __device__ __forceinline__ void stage_window(float4* buf, const float4* __restri
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
-                                             int p0, int p1, int ixb, int iy, float ey,
-                                             const float (&ex)[kCellsPerThread],
+                                             int p0, int p1, int ixb, int iy, int x_hi, int ty0,
+                                             int ty1, float ey, const float (&ex)[kCellsPerThread],
                                              float (&a0)[kCellsPerThread],
                                              float2 (&a12)[kCellsPerThread],
                                              float2 (&a34)[kCellsPerThread],
@@ -516,7 +516,28 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
   // inner loop carries no fold test
   for (int pc = p0; pc < p1;) {
     const int pe = min(p1, (pc | (kPhiChunk - 1)) + 1);
-    for (int p = pc; p < pe; ++p) {
+    // Runs near the boundary: the warp's lanes test the piece's phi_p at once
+    // (does any sample of this warp reach the grid; does every sample land two
+    // or more nodes inside, so that no in-grid test is needed), and the warp
+    // visits only the phi_p that reach it, in order.  A phi_p that reaches no
+    // sample of the warp adds nothing to its sums.
+    unsigned vis_mask = 0xffffffffu, in_mask = 0xffffffffu;
+    if (!kInterior) {
+      const int pl = pc + (threadIdx.x & 31);
+      bool vis = false, ins = false;
+      if (pl < pe) {
+        const float4 tl4 = stab[kPhiTab2D * (pl - p0) + 5];
+        const int lox = __float_as_int(tl4.z), loy = (int)(short)(__float_as_int(tl4.w) & 0xffff);
+        const int wa = ixb + lox, wb = min(ixb + K - 1, x_hi) + lox;
+        vis = (wb + 1 >= 1) && (wa - 1 <= NX - 2) && (ty1 + loy + 1 >= 1) && (ty0 + loy - 1 <= NY - 2);
+        ins = (wa >= 2) && (wa + K - 1 <= NX - 3) && (ty0 + loy >= 2) && (ty1 + loy <= NY - 3);
+      }
+      vis_mask = __ballot_sync(0xffffffffu, vis);
+      in_mask = __ballot_sync(0xffffffffu, ins);
+    }
+    for (unsigned m = kInterior ? (pe - pc == 32 ? 0xffffffffu : (1u << (pe - pc)) - 1u) : vis_mask; m;) {
+      const int p = pc + __ffs(m) - 1;
+      m &= m - 1u;
       const float4* e = stab + kPhiTab2D * (p - p0);
       const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
       const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
@@ -573,7 +594,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
         }
       }
       const float4 mw = e[4];
-      if (!kInterior) {
+      if (!kInterior && !((in_mask >> (p - pc)) & 1u)) {
         const bool nearx = (oyn >> 16) & 1, neary = (oyn >> 17) & 1;
         const bool in_y = (unsigned)(j - 1) <= (unsigned)(NY - 3);
         if (!(nearx || neary)) {
@@ -737,10 +758,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
                             (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
       if (!live) {
       } else if (interior) {
-        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
+        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, x_hi, tl.y0, y_hi, ey, ex, a0,
                            a12, a34, nd0, nd1, pox, poy, stot, err);
       } else {
-        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, ey, ex, a0,
+        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, x_hi, tl.y0, y_hi, ey, ex, a0,
                             a12, a34, nd0, nd1, pox, poy, stot, err);
       }
       __syncthreads();  // buffer b is free for the load of run c + 2
