@@ -186,6 +186,7 @@ def serve_stream(args, F, W, local, rank, ctx, reps):
                 time.sleep(1e-4)
         th.join()
         st = srv.stats()
+        st["breakdown"] = srv.breakdown()
         srv.stop()
         return st
 
@@ -208,6 +209,7 @@ def serve_stream(args, F, W, local, rank, ctx, reps):
             "events_per_s": reps.sum(st["events_per_s"]),
             "p50_ms": reps.max(st["p50_ms"]), "p99_ms": reps.max(st["p99_ms"]),
             "max_ms": reps.max(st["max_ms"]), "waves": st["waves"],
+            "burst_breakdown": burst["breakdown"], "load_breakdown": st["breakdown"],
             "plain_events_per_s": plain_all, "burst_over_plain": cap_all / plain_all,
             "outputs": hydro,
             "budget": {"hbm_bytes": budget["hbm_budget"], "pinned_host_bytes": budget["host_budget"]}}

@@ -99,6 +99,7 @@ struct OutBlock {
 struct Request {
   long long id = 0;
   fsm_params p{};
+  Clock::time_point t_wave;  // when a wave took it from the queue
   std::vector<float> e, nB;
   Clock::time_point t_submit, t_done;
   bool done = false;
@@ -122,6 +123,12 @@ struct Wave {
   size_t hgrp[kOutGroups];  // element offset of each kept output group in hout, or -1
   bool done = false;
   Clock::time_point t_done;
+  // breakdown: host time to plan (batch_build) and to stage the inputs into
+  // the pinned slab; CUDA events before the H2D copy, before the kernels,
+  // after the kernels and after the D2H copies (on the wave's stream)
+  Clock::time_point t_start;
+  double plan_ms = 0, stage_ms = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 }  // namespace
@@ -153,6 +160,10 @@ struct fsm_server {
   std::vector<double> lat_ms;
   Clock::time_point t_first{}, t_last{};
   bool have_first = false;
+  // per-wave breakdown sums (fsm_server_breakdown_get)
+  double sum_plan = 0, sum_stage = 0, sum_h2d = 0, sum_kernels = 0, sum_d2h = 0, sum_queue = 0;
+  long long sum_events = 0, timed_waves = 0, queued_reqs = 0;
+  std::vector<cudaEvent_t> event_pool;
 };
 
 namespace {
@@ -191,9 +202,28 @@ void CUDART_CB wave_done_cb(void* user) {
   delete W;
 }
 
+cudaEvent_t take_event(fsm_server* S) {
+  if (!S->event_pool.empty()) {
+    cudaEvent_t e = S->event_pool.back();
+    S->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+
 // Releases a wave's pool regions and batch (mu held); the output slab only
 // when keep_out is false.
 void wave_release(fsm_server* S, Wave* w, bool keep_out = false) {
+  for (auto& e : w->ev)
+    if (e) {
+      S->event_pool.push_back(e);
+      e = nullptr;
+    }
   if (w->b) batch_free(w->b);
   S->dpool.release(w->d, w->dbytes);
   S->hpool.release(w->hs, w->hsbytes);
@@ -231,6 +261,28 @@ void finish_request(fsm_server* S, Request* r, fsm_status st, Clock::time_point 
 
 // Outputs of a completed wave into its requests (mu held).
 void wave_retire(fsm_server* S, Wave* w) {
+  {
+    float t[3] = {0, 0, 0};
+    bool ok = true;
+    for (int k = 0; k < 3 && ok; ++k) {
+      ok = w->ev[k] && w->ev[k + 1] && cudaEventElapsedTime(&t[k], w->ev[k], w->ev[k + 1]) == cudaSuccess;
+    }
+    if (ok) {
+      S->sum_h2d += t[0];
+      S->sum_kernels += t[1];
+      S->sum_d2h += t[2];
+      S->sum_plan += w->plan_ms;
+      S->sum_stage += w->stage_ms;
+      S->sum_events += (long long)w->reqs.size();
+      ++S->timed_waves;
+    } else {
+      cudaGetLastError();
+    }
+    for (Request* r : w->reqs) {
+      S->sum_queue += std::chrono::duration<double, std::milli>(r->t_wave - r->t_submit).count();
+      ++S->queued_reqs;
+    }
+  }
   const int* err = reinterpret_cast<const int*>(w->hout + w->houtbytes - 16);
   fsm_status st = FSM_OK;
   if (err[1] != 0) st = FSM_ERR_TIMEOUT;
@@ -278,10 +330,13 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
     }
   }
   cudaStream_t s = S->streams[slot];
+  const Clock::time_point t_take = Clock::now();
+  for (Request* r : take) r->t_wave = t_take;
   while (!take.empty()) {
     auto* w = new Wave();
     w->slot = slot;
     w->reqs = take;
+    w->t_start = Clock::now();
     std::vector<fsm_params> ps(take.size());
     std::vector<const float*> he(take.size());
     for (size_t i = 0; i < take.size(); ++i) {
@@ -300,6 +355,8 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
     lk.unlock();
     fsm_status st = batch_build(S->ctx, (int)take.size(), ps.data(), he.data(), nullptr, nullptr,
                                 nullptr, &b, &mem);
+    const Clock::time_point t_planned = Clock::now();
+    w->plan_ms = std::chrono::duration<double, std::milli>(t_planned - w->t_start).count();
     lk.lock();
     if (st == FSM_OK) {
       w->b = b;
@@ -326,11 +383,16 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
         parallel_copy(dst, take[i]->e.data(), n * 4);
         if (b->plans[i].baryon) parallel_copy(dst + n, take[i]->nB.data(), n * 4);
       }
+      w->stage_ms = std::chrono::duration<double, std::milli>(Clock::now() - t_planned).count();
       lk.lock();
+      for (auto& e : w->ev) e = take_event(S);
+      if (w->ev[0]) cudaEventRecord(w->ev[0], s);
       cudaError_t ce = cudaMemcpyAsync(b->d_mem + b->in_slab_off, w->hin, b->in_slab_bytes,
                                        cudaMemcpyHostToDevice, s);
+      if (w->ev[1]) cudaEventRecord(w->ev[1], s);
       if (ce == cudaSuccess) st = enqueue(b, s, false);
       else st = FSM_ERR_CUDA;
+      if (w->ev[2]) cudaEventRecord(w->ev[2], s);
       if (st == FSM_OK) {
         // only the output groups the server keeps, one copy per group
         ce = cudaSuccess;
@@ -341,6 +403,7 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
         }
         if (ce == cudaSuccess)
           ce = cudaMemcpyAsync(w->hout + w->houtbytes - 16, b->d_err, 16, cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess && w->ev[3]) ce = cudaEventRecord(w->ev[3], s);
         if (ce == cudaSuccess) ce = cudaLaunchHostFunc(s, wave_done_cb, user);
         if (ce != cudaSuccess) {
           set_last_error(std::string("server wave: ") + cudaGetErrorString(ce));
@@ -606,6 +669,25 @@ extern "C" fsm_status fsm_server_stats_get(fsm_server* S, fsm_server_stats* st) 
   return FSM_OK;
 }
 
+extern "C" fsm_status fsm_server_breakdown_get(fsm_server* S, fsm_server_breakdown* bd) {
+  if (!S || !bd) return FSM_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(S->mu);
+  *bd = fsm_server_breakdown{};
+  const double n = (double)std::max<long long>(S->timed_waves, 1);
+  bd->waves = S->timed_waves;
+  bd->events_per_wave = (double)S->sum_events / n;
+  bd->plan_ms = S->sum_plan / n;
+  bd->stage_ms = S->sum_stage / n;
+  bd->h2d_ms = S->sum_h2d / n;
+  bd->kernels_ms = S->sum_kernels / n;
+  bd->d2h_ms = S->sum_d2h / n;
+  bd->queue_ms = S->queued_reqs ? S->sum_queue / (double)S->queued_reqs : 0.0;
+  const double span = std::chrono::duration<double, std::milli>(S->t_last - S->t_first).count();
+  bd->device_busy = span > 0 ? (S->sum_h2d + S->sum_kernels + S->sum_d2h) / span : 0.0;
+  bd->kernel_busy = span > 0 ? S->sum_kernels / span : 0.0;
+  return FSM_OK;
+}
+
 extern "C" fsm_status fsm_server_stop(fsm_server* S) {
   if (!S) return FSM_ERR_INVALID_ARG;
   {
@@ -624,6 +706,7 @@ extern "C" fsm_status fsm_server_stop(fsm_server* S) {
     delete kv.second;
   }
   for (auto& s : S->streams) cudaStreamDestroy(s);
+  for (auto e : S->event_pool) cudaEventDestroy(e);
   cudaFreeHost(S->h_pool);
   cudaFree(S->d_pool);
   fsm_ctx_destroy(S->ctx);

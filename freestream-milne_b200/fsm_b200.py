@@ -76,6 +76,14 @@ class ServerStats(ctypes.Structure):
                 ("max_ms", ctypes.c_double), ("events_per_s", ctypes.c_double)]
 
 
+class ServerBreakdown(ctypes.Structure):
+    _fields_ = [("waves", ctypes.c_longlong), ("events_per_wave", ctypes.c_double),
+                ("plan_ms", ctypes.c_double), ("stage_ms", ctypes.c_double),
+                ("h2d_ms", ctypes.c_double), ("kernels_ms", ctypes.c_double),
+                ("d2h_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("device_busy", ctypes.c_double), ("kernel_busy", ctypes.c_double)]
+
+
 class Diagnostics(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in
                 ("R_Pi_Inv", "R_pimunu_Inv", "pi_dot_u", "pi_mu_mu", "beta", "omega")]
@@ -150,6 +158,7 @@ SIGNATURES = {
     "fsm_server_release": (_ST, [_VP, ctypes.c_longlong]),
     "fsm_server_stats_get": (_ST, [_VP, ctypes.POINTER(ServerStats)]),
     "fsm_server_stop": (_ST, [_VP]),
+    "fsm_server_breakdown_get": (_ST, [_VP, ctypes.POINTER(ServerBreakdown)]),
 }
 
 _lib = None
@@ -628,6 +637,12 @@ class Server:
         st = ServerStats()
         check(lib().fsm_server_stats_get(self.h, ctypes.byref(st)), "fsm_server_stats_get")
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def breakdown(self):
+        """Per-wave means of where the server's time goes (fsm_server_breakdown_get)."""
+        bd = ServerBreakdown()
+        check(lib().fsm_server_breakdown_get(self.h, ctypes.byref(bd)), "fsm_server_breakdown_get")
+        return {k: getattr(bd, k) for k, _ in ServerBreakdown._fields_}
 
     def stop(self):
         if self.h:

@@ -349,6 +349,23 @@ fsm_status fsm_server_poll_view(fsm_server* s, long long id, fsm_outputs* views,
                                 fsm_run_info* info, double timeout_ms, int* done);
 fsm_status fsm_server_release(fsm_server* s, long long id);
 fsm_status fsm_server_stats_get(fsm_server* s, fsm_server_stats* st);
+/* Where a server's time goes, averaged over the waves retired so far (no
+ * counterpart in the reference): host time to plan a wave (tables, runs, work
+ * lists) and to stage its inputs into pinned memory; device time of its input
+ * copy, its kernels and its output copies (CUDA events on the wave's stream);
+ * the mean time a request waited in the queue before a wave took it; and the
+ * device time of all waves (copies + kernels, and kernels alone) per
+ * wall-clock time from the first submission to the last completion (above 1
+ * when waves on different streams overlap). */
+typedef struct fsm_server_breakdown {
+  long long waves;
+  double events_per_wave;
+  double plan_ms, stage_ms;          /* host, per wave                        */
+  double h2d_ms, kernels_ms, d2h_ms; /* device, per wave                      */
+  double queue_ms;                   /* per request: submit -> taken by a wave */
+  double device_busy, kernel_busy;   /* device time / wall time               */
+} fsm_server_breakdown;
+fsm_status fsm_server_breakdown_get(fsm_server* s, fsm_server_breakdown* bd);
 /* Finishes the waves in flight, cancels queued requests, frees everything. */
 fsm_status fsm_server_stop(fsm_server* s);
 
