@@ -362,8 +362,14 @@ def main():
     # the batch's one device allocation and the upload of its tables
     t0 = time.perf_counter()
     fresh = F.Batch(ctx, params)
+    create_cold_ms = 1e3 * (time.perf_counter() - t0)
+    fresh.close()  # its allocations stay with the context for the next batch
+    fresh_events = W.uneven_batch(n=args.events, seed=reps.seed(5))
+    t0 = time.perf_counter()
+    fresh = F.Batch(ctx, [p for p, _, _ in fresh_events])
     create_ms = 1e3 * (time.perf_counter() - t0)
     fresh.close()
+    del fresh_events
     h_in = torch.from_numpy(batch.pack_inputs([(e, nb) for _, e, nb in events])).pin_memory()
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
@@ -534,12 +540,13 @@ def main():
                                    "boost invariance)",
                     "pipeline": "2 batches on 2 streams, alternating steps; device gather "
                                 "+ one copy per step"},
-            "fresh_event_set": {"batch_create_ms": create_ms,
+            "fresh_event_set": {"batch_create_ms": create_ms, "first_batch_create_ms": create_cold_ms,
                                 "e2e_events_per_s_with_create": world * n / (
                                     e2e_ms / args.steps / 1e3 + create_ms / 1e3),
-                                "note": "fsm_batch_create on a new 512-event list (host planning, "
-                                        "one device allocation, table upload), timed on the host; "
-                                        "e2e above replays one planned batch"},
+                                "note": "fsm_batch_create on a new 512-event list (host planning on "
+                                        "the worker pool, table upload) after another batch was "
+                                        "destroyed (its allocations reused); first: with fresh "
+                                        "allocations; e2e above replays one planned batch"},
             "gpu_launches": launches_per_step * args.steps,
             "output_files": files,
             "served": served,

@@ -72,9 +72,29 @@ void batch_free(fsm_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_segs) cudaFree(b->d_segs);
   if (b->d_pack) cudaFree(b->d_pack);
-  if (!b->ext_mem) {
-    if (b->d_mem) cudaFree(b->d_mem);
-    if (b->h_stage) cudaFreeHost(b->h_stage);
+  if (!b->ext_mem && (b->d_mem || b->h_stage)) {
+    // the context keeps the larger allocations for its next batch; the work
+    // still using them ends first (as it would before a cudaFree)
+    fsm_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    char* free_dev = b->d_mem;
+    char* free_host = b->h_stage;
+    {
+      std::lock_guard<std::mutex> g(c->spare_mu);
+      if (b->d_mem && b->dev_cap > c->spare_dev_cap) {
+        free_dev = c->spare_dev;
+        c->spare_dev = b->d_mem;
+        c->spare_dev_cap = b->dev_cap;
+      }
+      if (b->h_stage && b->host_cap > c->spare_host_cap) {
+        free_host = c->spare_host;
+        c->spare_host = b->h_stage;
+        c->spare_host_cap = b->host_cap;
+      }
+    }
+    if (free_dev) cudaFree(free_dev);
+    if (free_host) cudaFreeHost(free_host);
   }
   delete b;
 }
@@ -306,14 +326,36 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       return FSM_ERR_OUT_OF_MEMORY;
     }
   } else {
-    cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
-    if (ce != cudaSuccess) {
-      cudaGetLastError();
-      set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
-                     cudaGetErrorString(ce));
-      return FSM_ERR_OUT_OF_MEMORY;
+    {  // the allocations of a destroyed batch, when they are large enough
+      std::lock_guard<std::mutex> g(ctx->spare_mu);
+      if (ctx->spare_dev && ctx->spare_dev_cap >= b->bytes) {
+        b->d_mem = ctx->spare_dev;
+        b->dev_cap = ctx->spare_dev_cap;
+        ctx->spare_dev = nullptr;
+        ctx->spare_dev_cap = 0;
+      }
+      if (ctx->spare_host && ctx->spare_host_cap >= b->stage_bytes) {
+        b->h_stage = ctx->spare_host;
+        b->host_cap = ctx->spare_host_cap;
+        ctx->spare_host = nullptr;
+        ctx->spare_host_cap = 0;
+      }
     }
-    FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
+    if (!b->d_mem) {
+      cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        b->d_mem = nullptr;
+        set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
+                       cudaGetErrorString(ce));
+        return FSM_ERR_OUT_OF_MEMORY;
+      }
+      b->dev_cap = b->bytes;
+    }
+    if (!b->h_stage) {
+      FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
+      b->host_cap = b->stage_bytes;
+    }
   }
   char* D = b->d_mem;
   char* H = b->h_stage;
@@ -814,6 +856,8 @@ extern "C" void fsm_ctx_destroy(fsm_ctx* ctx) {
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
+  if (ctx->spare_dev) cudaFree(ctx->spare_dev);
+  if (ctx->spare_host) cudaFreeHost(ctx->spare_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1357,7 +1401,6 @@ extern "C" fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t) {
 
 extern "C" fsm_status fsm_ctx_set_wait_limit(fsm_ctx* ctx, int polls) {
   if (!ctx || polls < 0) return FSM_ERR_INVALID_ARG;
-  std::lock_guard<std::mutex> g(ctx->mu);
   ctx->wait_polls = polls;
   // the cached one-event batches were built with the old bound
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);

@@ -78,6 +78,13 @@ struct fsm_ctx {
   fsm_batch* single_host = nullptr;
   fsm_batch* single_dev = nullptr;
   fsm_params single_host_raw{};
+  // the device and pinned allocations of the last batch destroyed, kept for
+  // the next batch that fits (a stream of event sets then allocates nothing)
+  std::mutex spare_mu;
+  char* spare_dev = nullptr;
+  size_t spare_dev_cap = 0;
+  char* spare_host = nullptr;
+  size_t spare_host_cap = 0;
 };
 
 struct fsm_batch {
@@ -88,6 +95,7 @@ struct fsm_batch {
   // device allocation
   char* d_mem = nullptr;
   size_t bytes = 0;
+  size_t dev_cap = 0, host_cap = 0;  // sizes of the own allocations (may exceed the need)
   // staging for descriptor uploads (pinned)
   char* h_stage = nullptr;
   size_t stage_bytes = 0;

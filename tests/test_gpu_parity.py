@@ -187,6 +187,30 @@ def test_batch_equals_single_events(ctx):
     b.close()
 
 
+def test_batches_on_recycled_allocations(ctx):
+    """A context keeps the allocations of a destroyed batch for its next one:
+    a batch built on that memory (after another batch wrote its own data into
+    it) gives the same results as one built on fresh memory."""
+    a = W.lumpy2d(seed=40, side=101, dx=0.08, nphip=64, dtau=0.7, eos=1, radius=3.0)
+    b = W.lumpy2d(seed=41, side=81, dx=0.07, nphip=100, dtau=1.1, eos=2, radius=2.5)
+    c = F.Context(0)
+    try:
+        fresh = F.Batch(c, [b[0], a[0]])
+        want = fresh.run_host([(b[1], None), (a[1], None)])
+        big = F.Batch(c, [a[0], a[0], b[0]])
+        big.run_host([(a[1], None), (a[1], None), (b[1], None)])
+        fresh.close()
+        big.close()  # the larger allocations go to the context
+        again = F.Batch(c, [b[0], a[0]])
+        got = again.run_host([(b[1], None), (a[1], None)])
+        again.close()
+        for w, g in zip(want, got):
+            for k in w:
+                assert np.array_equal(w[k], g[k]), k
+    finally:
+        c.close()
+
+
 def test_grouped_batch_downloads(ctx):
     """A batch with grouped outputs gives the same results as a per-event one,
     and download_groups copies back exactly the groups asked for."""
