@@ -356,6 +356,10 @@ def main():
     params = [p for p, _, _ in events]
     ctx = F.Context(local)
     tuning = ctx.autotune(params, [(e, nb) for _, e, nb in events])  # staged-window size
+    # per bucket (grid side x shift length): window and phi_p chunk
+    buckets = ctx.autotune_buckets(params, [(e, nb) for _, e, nb in events])
+    bucket_choice = {k: f"{t['window_bytes'] // 1024} KB / {t['phi_chunk']}"
+                     for k, t in enumerate(buckets) if t["window_bytes"]}
     batch = F.Batch(ctx, params)
     n = len(events)
     # host cost of a fresh event set: planning (tables, runs, work lists),
@@ -451,6 +455,7 @@ def main():
     # ---------------- kernel timing pass for the roofline (CUDA events per kernel family)
     tctx = F.Context(local, timing=True)
     tctx.set_tuning(tuning["window_bytes"])
+    tctx.set_tuning_buckets(buckets)
     tb = F.Batch(tctx, params)
     tb.upload(h_in.data_ptr(), sp)
     for _ in range(2):
@@ -517,7 +522,8 @@ def main():
             "config": config_of(args),
             "setup": {"events_per_step": n, "ranks": world, "parallelism": f"replicas{world}",
                       "cell_momentum_samples_per_step": samples,
-                      "autotuned_window_bytes": tuning["window_bytes"]},
+                      "autotuned_window_bytes": tuning["window_bytes"],
+                      "autotuned_buckets": bucket_choice},
             "p50_step_ms": sm[len(sm) // 2], "p99_step_ms": sm[min(len(sm) - 1, int(0.99 * len(sm)))],
             "plain_events_per_s": plain,
             "batched_over_plain": (value / plain) if plain else None,

@@ -133,6 +133,7 @@ struct Ev2D {
   const PhiEntry2D* tab; // [NPHI]
   const Chunk2D* chunks; // [nchunks]
   int nchunks;
+  int chunk;             // phi_p per FP32 partial sum of the two-level moment sum (16 or 32)
   // prep
   const float* e_gev;    // input
   const AxisNode* ax;   // [NX] x-axis spline data

@@ -485,7 +485,8 @@ __device__ __forceinline__ void stage_window(float4* buf, const float4* __restri
 // for its 4 samples.  Where the spline is not positive the reference falls back
 // to bilinear interpolation (src/FreeStream.cpp:245-246); that is rare, so it
 // is evaluated only in warps where some sample needs it.  Moments accumulate
-// in FP32 chunks of 16 phi_p folded into FP32 totals (two-level summation).
+// in FP32 chunks of ev.chunk (16 or 32, tuned) phi_p folded into FP32 totals
+// (two-level summation).
 //
 // kInterior: every sample of the run provably lands inside the grid, so the
 // in-grid test (src/FreeStream.cpp:213) is skipped.
@@ -515,7 +516,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
   // phi_p in pieces that end at the fold points of the two-level sum, so the
   // inner loop carries no fold test
   for (int pc = p0; pc < p1;) {
-    const int pe = min(p1, (pc | (kPhiChunk - 1)) + 1);
+    const int pe = min(p1, (pc | (ev.chunk - 1)) + 1);
     // Runs near the boundary: the warp's lanes test the piece's phi_p at once
     // (does any sample of this warp reach the grid; does every sample land two
     // or more nodes inside, so that no in-grid test is needed), and the warp
@@ -632,7 +633,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
         a34[k] = __ffma2_rn(v2, make_float2(mw.z, mw.w), a34[k]);
       }
     }
-    if ((pe & (kPhiChunk - 1)) == 0) {
+    if ((pe & (ev.chunk - 1)) == 0) {
       // second level of the two-level sum, thread-private slots in shared memory
 #pragma unroll
       for (int k = 0; k < K; ++k) {

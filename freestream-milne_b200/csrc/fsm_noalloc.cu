@@ -195,6 +195,7 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   e.T = dev_out->T ? dev_out->T : reinterpret_cast<float*>(D + o_T);
   e.charge = 0;
   e.fb_scale = 1.0f;
+  e.chunk = kPhiChunk;
   EvLandau l{};
   l.DIM = DIM;
   l.is3d = 0;

@@ -50,6 +50,7 @@ struct EventPlan {
   float norm = 0, normB = 0;
   // 2D with BARYON: fallback and output scales of the charge pass (Ev2D)
   float fb_scale2 = 1.0f, jscale2 = 0.0f;
+  int phi_chunk = kPhiChunk;  // 2D: phi_p per FP32 partial sum (tuning; 16 or 32)
   double samples = 0;  // cell x momentum samples the stream kernel evaluates
   double ref_samples = 0;  // DIM * DIM_RAP * DIM_PHIP, the reference's count
 };

@@ -115,6 +115,23 @@ fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot) 
 int g_smem2[64] = {0}, g_smem3[64] = {0}, g_smem_rows[64] = {0}, g_smem_srows[64] = {0},
     g_smem_scols[64] = {0};
 
+int tuning_bucket(const fsm_params& p) {
+  const int side = std::max(p.DIM_X, p.DIM_Y);
+  const int sc = side < 128 ? 0 : side < 192 ? 1 : side < 256 ? 2 : 3;
+  const float cells = p.DTAU / std::max(1e-30f, std::min(p.DX, p.DY));
+  const int hc = cells < 8.0f ? 0 : cells < 16.0f ? 1 : cells < 24.0f ? 2 : 3;
+  return sc * 4 + hc;
+}
+
+void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk) {
+  *window = ctx->window_budget;
+  *chunk = kPhiChunk;
+  if (p.DIM_ETA > 1) return;  // 3D events: the 3D kernel has no staged windows; chunk 16
+  const fsm_tuning_bucket& t = ctx->buckets[tuning_bucket(p)];
+  if (t.window_bytes > 0) *window = t.window_bytes;
+  if (t.phi_chunk == 16 || t.phi_chunk == 32) *chunk = t.phi_chunk;
+}
+
 // Builds descriptors and uploads everything.  ext_in / ext_out (one event)
 // select external device buffers instead of owned slabs.
 fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const float* const* host_e,
@@ -137,8 +154,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     std::vector<std::string> why(n);
     // (many small events also pay: ~35 us of host planning each)
     parallel_for(n, (work > 2.0e5 || n >= 16) ? host_threads() : 1, [&](int i) {
-      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i],
-                         ctx->window_budget);
+      int window = 0, chunk = 0;
+      event_tuning(ctx, params[i], &window, &chunk);
+      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window);
+      b->plans[i].phi_chunk = chunk;
     });
     for (int i = 0; i < n; ++i)
       if (st[i] != FSM_OK) {  // the first failing event, as a serial loop would report
@@ -493,6 +512,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.T = b->d_T[i];
       e.charge = 0;
       e.fb_scale = 1.0f;
+      e.chunk = P.phi_chunk;
       if (P.baryon) {  // charge pass: same geometry and tables, its own field and scratch
         Ev2D& q = b->ev2[b->evq_of[i]];
         q = e;
@@ -899,7 +919,9 @@ extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const flo
   if (!b || p->E_DEP_FS != 0 || !same_params(ctx->single_host_raw, *p)) {
     EventPlan P;
     std::string why;
-    s = plan_event(*p, e_gev, &P, &why, ctx->window_budget);
+    int window = 0, chunk = 0;
+    event_tuning(ctx, *p, &window, &chunk);
+    s = plan_event(*p, e_gev, &P, &why, window);
     if (s != FSM_OK) {
       set_last_error(why);
       return s;
@@ -979,7 +1001,9 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
   p = &pe;
   EventPlan P;
   std::string why;
-  fsm_status s = plan_event(*p, nullptr, &P, &why, ctx->window_budget);
+  int window = 0, chunk = 0;
+  event_tuning(ctx, *p, &window, &chunk);
+  fsm_status s = plan_event(*p, nullptr, &P, &why, window);
   if (s != FSM_OK) {
     set_last_error(why);
     return s;
@@ -1473,4 +1497,153 @@ extern "C" fsm_status fsm_autotune(fsm_ctx* ctx, int n, const fsm_params* params
   out->window_bytes = best;
   out->ms = best_ms;
   return fsm_ctx_set_tuning(ctx, out);
+}
+
+// ====================================================== per-bucket tuning
+namespace {
+void drop_single_batches(fsm_ctx* ctx) {  // they were planned with the old tuning
+  batch_free(ctx->single_host);
+  ctx->single_host = nullptr;
+  batch_free(ctx->single_dev);
+  ctx->single_dev = nullptr;
+}
+}  // namespace
+
+extern "C" fsm_status fsm_ctx_set_tuning_buckets(fsm_ctx* ctx, const fsm_tuning_bucket* table) {
+  if (!ctx || !table) return FSM_ERR_INVALID_ARG;
+  for (int k = 0; k < FSM_TUNING_BUCKETS; ++k) {
+    const fsm_tuning_bucket& t = table[k];
+    const bool ok = (t.window_bytes == 0 || (t.window_bytes >= (kTileX + 3) * (kTileY + 3) * 16 &&
+                                             t.window_bytes <= 96 * 1024)) &&
+                    (t.phi_chunk == 0 || t.phi_chunk == 16 || t.phi_chunk == 32);
+    if (!ok) {
+      set_last_error("fsm_ctx_set_tuning_buckets: bucket " + std::to_string(k) +
+                     " has a window outside [4900, 98304] bytes or a chunk other than 16 or 32");
+      return FSM_ERR_INVALID_ARG;
+    }
+  }
+  std::copy(table, table + FSM_TUNING_BUCKETS, ctx->buckets);
+  drop_single_batches(ctx);
+  return FSM_OK;
+}
+
+extern "C" fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params* params,
+                                           const float* const* host_e, const float* const* host_nB,
+                                           fsm_tuning_bucket* out) {
+  if (!ctx || n <= 0 || !params || !out) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(ctx->device));
+  constexpr int kPerBucket = 64;  // events timed per bucket at most
+  static const int cand_kb[] = {24, 32, 40, 48};
+  static const int cand_chunk[] = {16, 32};
+  std::vector<int> members[FSM_TUNING_BUCKETS];
+  for (int i = 0; i < n; ++i)
+    if (params[i].DIM_ETA == 1) {
+      auto& m = members[tuning_bucket(params[i])];
+      if ((int)m.size() < kPerBucket) m.push_back(i);
+    }
+  fsm_tuning_bucket saved[FSM_TUNING_BUCKETS], result[FSM_TUNING_BUCKETS] = {};
+  std::copy(ctx->buckets, ctx->buckets + FSM_TUNING_BUCKETS, saved);
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FSM_CUDA_TRY(cudaEventCreate(&e0));
+  FSM_CUDA_TRY(cudaEventCreate(&e1));
+  fsm_status status = FSM_OK;
+  for (int k = 0; k < FSM_TUNING_BUCKETS && status == FSM_OK; ++k) {
+    const int m = (int)members[k].size();
+    if (!m) continue;
+    std::vector<fsm_params> ps(m);
+    std::vector<const float*> he(m, nullptr), hb(m, nullptr);
+    for (int j = 0; j < m; ++j) {
+      ps[j] = params[members[k][j]];
+      if (host_e) he[j] = host_e[members[k][j]];
+      if (host_nB) hb[j] = host_nB[members[k][j]];
+    }
+    fsm_tuning_bucket best{};
+    for (int kb : cand_kb)
+      for (int chunk : cand_chunk) {
+        ctx->buckets[k] = fsm_tuning_bucket{kb * 1024, chunk, 0.0, 0};
+        fsm_batch* b = nullptr;
+        fsm_status s = batch_build(ctx, m, ps.data(), host_e ? he.data() : nullptr, nullptr, nullptr,
+                                   nullptr, &b);
+        if (s != FSM_OK) {
+          batch_free(b);
+          continue;  // e.g. too many runs for this window: not a candidate
+        }
+        for (int j = 0; j < m; ++j) {
+          const size_t dim = (size_t)b->plans[j].DIM;
+          if (host_e && he[j]) cudaMemcpyAsync(b->d_in_e[j], he[j], dim * 4, cudaMemcpyHostToDevice, st);
+          if (b->plans[j].baryon && hb[j])
+            cudaMemcpyAsync(b->d_in_nB[j], hb[j], dim * 4, cudaMemcpyHostToDevice, st);
+        }
+        if (!host_e) cudaMemsetAsync(b->d_mem + b->in_slab_off, 0, b->in_slab_bytes, st);
+        double ms = 0.0;
+        for (int rep = 0; rep < 4 && s == FSM_OK; ++rep) {
+          cudaEventRecord(e0, st);
+          s = enqueue(b, st, false);
+          cudaEventRecord(e1, st);
+          if (cudaEventSynchronize(e1) != cudaSuccess) s = FSM_ERR_CUDA;
+          float t = 0.f;
+          cudaEventElapsedTime(&t, e0, e1);
+          if (rep >= 1) ms += t;  // the first launch warms up
+        }
+        if (s == FSM_OK) s = check_kernel_errors(b);
+        batch_free(b);
+        if (s != FSM_OK) {
+          status = s;
+          break;
+        }
+        ms /= 3.0;
+        if (best.ms == 0.0 || ms < best.ms) best = fsm_tuning_bucket{kb * 1024, chunk, ms, m};
+      }
+    result[k] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::copy(saved, saved + FSM_TUNING_BUCKETS, ctx->buckets);
+  if (status != FSM_OK) return status;
+  std::copy(result, result + FSM_TUNING_BUCKETS, out);
+  return fsm_ctx_set_tuning_buckets(ctx, result);
+}
+
+extern "C" fsm_status fsm_tuning_save(fsm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return FSM_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "w");
+  if (!f) {
+    set_last_error(std::string("fsm_tuning_save: cannot open ") + path);
+    return FSM_ERR_FILE;
+  }
+  std::fprintf(f, "# bucket window_bytes phi_chunk ms events\n");
+  for (int k = 0; k < FSM_TUNING_BUCKETS; ++k) {
+    const fsm_tuning_bucket& t = ctx->buckets[k];
+    if (t.window_bytes > 0)
+      std::fprintf(f, "%d %d %d %.6f %d\n", k, t.window_bytes, t.phi_chunk, t.ms, t.events);
+  }
+  return std::fclose(f) == 0 ? FSM_OK : FSM_ERR_FILE;
+}
+
+extern "C" fsm_status fsm_tuning_load(fsm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return FSM_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "r");
+  if (!f) {
+    set_last_error(std::string("fsm_tuning_load: cannot open ") + path);
+    return FSM_ERR_FILE;
+  }
+  fsm_tuning_bucket table[FSM_TUNING_BUCKETS] = {};
+  char line[256];
+  fsm_status st = FSM_OK;
+  while (std::fgets(line, sizeof(line), f)) {
+    if (line[0] == '#' || line[0] == '\n') continue;
+    int k = -1, w = 0, c = 0, ev = 0;
+    double ms = 0.0;
+    if (std::sscanf(line, "%d %d %d %lf %d", &k, &w, &c, &ms, &ev) != 5 || k < 0 ||
+        k >= FSM_TUNING_BUCKETS) {
+      set_last_error(std::string("fsm_tuning_load: malformed line: ") + line);
+      st = FSM_ERR_INVALID_ARG;
+      break;
+    }
+    table[k] = fsm_tuning_bucket{w, c, ms, ev};
+  }
+  std::fclose(f);
+  if (st != FSM_OK) return st;
+  return fsm_ctx_set_tuning_buckets(ctx, table);
 }

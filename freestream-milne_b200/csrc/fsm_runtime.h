@@ -71,6 +71,8 @@ struct fsm_ctx {
   std::mutex mu;
   int window_budget = fsm::kWindowBudget2D;  // staged window of a 2D phi_p run (autotuned)
   int wait_polls = fsm::kWaitPolls;  // bounded waits of batches built from now on
+  // per-bucket tuning of 2D events (window_bytes 0: the context's window)
+  fsm_tuning_bucket buckets[FSM_TUNING_BUCKETS] = {};
   // energy-dependent DTAU of device profiles: sums on the device, read back
   float* d_sums = nullptr;
   float* h_sums = nullptr;
@@ -183,6 +185,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                        const float* const* ext_in_e, const float* const* ext_in_nB,
                        const fsm_outputs* ext_out, fsm_batch** out, const BatchMem* mem = nullptr);
 fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing);
+// Tuning bucket of a 2D event (grid side class x shift-length class) and the
+// staged-window bound / phi_p chunk the context's tuning gives an event.
+int tuning_bucket(const fsm_params& p);
+void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk);
 // Raises (never lowers) a kernel's dynamic shared-memory limit: the limit is a
 // process-wide attribute other launches (and captured graphs) rely on.
 // `slot` records the largest value set so far for that kernel on `device`;

@@ -58,6 +58,14 @@ class Tuning(ctypes.Structure):
     _fields_ = [("window_bytes", ctypes.c_int), ("ms", ctypes.c_double)]
 
 
+class TuningBucket(ctypes.Structure):
+    _fields_ = [("window_bytes", ctypes.c_int), ("phi_chunk", ctypes.c_int), ("ms", ctypes.c_double),
+                ("events", ctypes.c_int)]
+
+
+TUNING_BUCKETS = 16
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
                 ("host_budget_bytes", ctypes.c_size_t), ("max_wave_events", ctypes.c_int),
@@ -147,6 +155,11 @@ SIGNATURES = {
     "fsm_autotune": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(_VP),
                            ctypes.POINTER(_VP), ctypes.POINTER(Tuning)]),
     "fsm_ctx_set_tuning": (_ST, [_VP, ctypes.POINTER(Tuning)]),
+    "fsm_autotune_buckets": (_ST, [_VP, ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(_VP),
+                                   ctypes.POINTER(_VP), ctypes.POINTER(TuningBucket)]),
+    "fsm_ctx_set_tuning_buckets": (_ST, [_VP, ctypes.POINTER(TuningBucket)]),
+    "fsm_tuning_save": (_ST, [_VP, ctypes.c_char_p]),
+    "fsm_tuning_load": (_ST, [_VP, ctypes.c_char_p]),
     "fsm_server_start": (_ST, [ctypes.POINTER(_VP), ctypes.POINTER(ServerOpts)]),
     "fsm_server_submit": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP,
                                 ctypes.POINTER(ctypes.c_longlong)]),
@@ -306,6 +319,40 @@ class Context:
     def set_wait_limit(self, polls):
         """Polls of one bounded wait in batches built from now on (0: give up at once)."""
         check(lib().fsm_ctx_set_wait_limit(self.h, int(polls)), "fsm_ctx_set_wait_limit")
+
+    def autotune_buckets(self, params_list, inputs=None):
+        """Per-bucket tuning (window, phi_p chunk) on these events; returns the
+        16 bucket entries as dicts (window_bytes 0: bucket not tuned)."""
+        n = len(params_list)
+        arr = (Params * n)(*params_list)
+        keep = []
+        he = hb = None
+        if inputs is not None:
+            he = (_VP * n)()
+            hb = (_VP * n)()
+            for i, (e, nb) in enumerate(inputs):
+                e = np.ascontiguousarray(e, dtype=np.float32)
+                keep.append(e)
+                he[i] = e.ctypes.data
+                if nb is not None:
+                    nb = np.ascontiguousarray(nb, dtype=np.float32)
+                    keep.append(nb)
+                    hb[i] = nb.ctypes.data
+        out = (TuningBucket * TUNING_BUCKETS)()
+        check(lib().fsm_autotune_buckets(self.h, n, arr, he, hb, out), "fsm_autotune_buckets")
+        return [{k: getattr(t, k) for k, _ in TuningBucket._fields_} for t in out]
+
+    def set_tuning_buckets(self, table):
+        arr = (TuningBucket * TUNING_BUCKETS)(*[TuningBucket(t["window_bytes"], t["phi_chunk"],
+                                                             t.get("ms", 0.0), t.get("events", 0))
+                                                for t in table])
+        check(lib().fsm_ctx_set_tuning_buckets(self.h, arr), "fsm_ctx_set_tuning_buckets")
+
+    def save_tuning(self, path):
+        check(lib().fsm_tuning_save(self.h, str(path).encode()), "fsm_tuning_save")
+
+    def load_tuning(self, path):
+        check(lib().fsm_tuning_load(self.h, str(path).encode()), "fsm_tuning_load")
 
     def set_tuning(self, window_bytes):
         t = Tuning(int(window_bytes), 0.0)

@@ -279,6 +279,34 @@ fsm_status fsm_autotune(fsm_ctx* ctx, int n, const fsm_params* params, const flo
                         const float* const* host_nB, fsm_tuning* out);
 fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t);
 
+/* Per-bucket tuning of boost-invariant events.  An event's bucket is
+ * side_class * 4 + shift_class, side_class from max(DIM_X, DIM_Y) (0: < 128,
+ * 1: < 192, 2: < 256, 3: larger) and shift_class from the shift length in
+ * cells DTAU / min(DX, DY) (0: < 8, 1: < 16, 2: < 24, 3: larger).  Per bucket
+ * the 2D stream kernel's staged-window bound and its phi_p chunk (phi_p per
+ * FP32 partial sum of the two-level moment sum: 16 or 32; 32 folds less
+ * often, with a larger summation error still far inside the parity
+ * tolerance).  fsm_autotune_buckets times, for every bucket the given events
+ * fall in, the launch sequence of those events (at most 64 of them) for
+ * windows of 24-48 KB and both chunks, keeps the fastest per bucket for ctx
+ * and writes the FSM_TUNING_BUCKETS entries (window_bytes 0 for buckets
+ * without events: they keep the context's window and chunk 16).  The table
+ * can be stored and restored as text with fsm_tuning_save / fsm_tuning_load
+ * (one "bucket window_bytes phi_chunk ms events" line per tuned bucket). */
+#define FSM_TUNING_BUCKETS 16
+typedef struct fsm_tuning_bucket {
+  int window_bytes;  /* staged window bound (0: the context's)               */
+  int phi_chunk;     /* 16 or 32 (0: 16)                                       */
+  double ms;         /* measured launch-sequence time of the bucket's events   */
+  int events;        /* events the measurement used                            */
+} fsm_tuning_bucket;
+fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params* params,
+                                const float* const* host_e, const float* const* host_nB,
+                                fsm_tuning_bucket* out);
+fsm_status fsm_ctx_set_tuning_buckets(fsm_ctx* ctx, const fsm_tuning_bucket* table);
+fsm_status fsm_tuning_save(fsm_ctx* ctx, const char* path);
+fsm_status fsm_tuning_load(fsm_ctx* ctx, const char* path);
+
 /* Polls of one bounded wait on a staged copy in the 2D stream kernel for the
  * batches (and one-event batches) of ctx built after the call; default 1 << 20,
  * 0 makes every such wait give up at once.  No counterpart in the reference,

@@ -408,6 +408,48 @@ def test_autotune_keeps_results():
     c.close()
 
 
+def test_bucket_autotuner_choices_keep_results(tmp_path):
+    """Every choice the per-bucket autotuner can make: with the 16-phi_p chunk
+    the results equal the untuned ones bit for bit for every staged-window
+    size; with the 32-phi_p chunk (a different summation order) they pass the
+    parity checks against the oracle's float and FP64 runs.  The tuned table
+    survives a save / load round trip."""
+    evs = [W.lumpy2d(seed=50, side=101, dx=0.1, nphip=64, dtau=0.4, eos=1, radius=3.0),   # 0, 0
+           W.lumpy2d(seed=51, side=151, dx=0.08, nphip=100, dtau=1.0, eos=2, radius=4.0),  # 1, 1
+           W.lumpy2d(seed=52, side=201, dx=0.05, nphip=64, dtau=1.0, eos=1, radius=4.0)]   # 2, 2
+    base = F.Context(0)
+    ref = [base.run_event(p, e) for p, e, _ in evs]
+    base.close()
+    c = F.Context(0)
+    try:
+        table = c.autotune_buckets([p for p, _, _ in evs], [(e, nb) for _, e, nb in evs])
+        tuned = [k for k, t in enumerate(table) if t["window_bytes"]]
+        assert sorted(tuned) == [0, 5, 10], tuned
+        for t in table:
+            if t["window_bytes"]:
+                assert t["phi_chunk"] in (16, 32) and t["ms"] > 0 and t["events"] == 1
+        path = tmp_path / "tuning.txt"
+        c.save_tuning(path)
+        c2 = F.Context(0)
+        c2.load_tuning(path)
+        for window in (24 * 1024, 48 * 1024):
+            for chunk in (16, 32):
+                c2.set_tuning_buckets([{"window_bytes": window, "phi_chunk": chunk}] * 16)
+                for (p, e, _), r in zip(evs, ref):
+                    got = c2.run_event(p, e)
+                    if chunk == 16:
+                        for name in ("T", "e", "u", "pi"):
+                            np.testing.assert_array_equal(got[name], r[name], err_msg=f"{window} {name}")
+                    else:
+                        o = _oracle(p, e)
+                        o64 = _oracle(p, e, fp64=2)
+                        compare_parity(got, o, o64, o["tau"])
+                        compare(got, o64, o["tau"])
+        c2.close()
+    finally:
+        c.close()
+
+
 def test_invalid_inputs_are_rejected(ctx):
     p = F.default_params(DIM_X=3)
     with pytest.raises(F.FsmError):
