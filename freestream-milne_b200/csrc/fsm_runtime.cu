@@ -360,20 +360,29 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
         ctx->spare_host_cap = 0;
       }
     }
+    // allocations rounded up (at most 1/8 above the need, on a coarse grid)
+    // so that a later batch of similar size fits the one this batch leaves
+    auto rounded = [](size_t need) {
+      size_t step = 1;
+      while (step * 8 < need) step <<= 1;
+      return (need + step - 1) / step * step;
+    };
     if (!b->d_mem) {
-      cudaError_t ce = cudaMalloc(&b->d_mem, b->bytes);
+      const size_t cap = rounded(b->bytes);
+      cudaError_t ce = cudaMalloc(&b->d_mem, cap);
       if (ce != cudaSuccess) {
         cudaGetLastError();
         b->d_mem = nullptr;
-        set_last_error(std::string("cudaMalloc of ") + std::to_string(b->bytes) + " bytes: " +
+        set_last_error(std::string("cudaMalloc of ") + std::to_string(cap) + " bytes: " +
                        cudaGetErrorString(ce));
         return FSM_ERR_OUT_OF_MEMORY;
       }
-      b->dev_cap = b->bytes;
+      b->dev_cap = cap;
     }
     if (!b->h_stage) {
-      FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, b->stage_bytes));
-      b->host_cap = b->stage_bytes;
+      const size_t cap = rounded(b->stage_bytes);
+      FSM_CUDA_TRY(cudaMallocHost(&b->h_stage, cap));
+      b->host_cap = cap;
     }
   }
   char* D = b->d_mem;
@@ -1533,8 +1542,13 @@ extern "C" fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params
   if (!ctx || n <= 0 || !params || !out) return FSM_ERR_INVALID_ARG;
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
   constexpr int kPerBucket = 64;  // events timed per bucket at most
-  static const int cand_kb[] = {24, 32, 40, 48};
-  static const int cand_chunk[] = {16, 32};
+  // windows up to 40 KB: a batch sizes its shared memory by its largest
+  // window, and above that one bucket would drop the whole launch to one CTA
+  // per SM (measured: 48 KB in one bucket made a 512-event batch 1.5x
+  // slower).  The chunk stays 16: 32 was measured past the e tolerance
+  // against FP64 on a 201^2 event (1.05e-4); callers may still set it.
+  static const int cand_kb[] = {24, 28, 32, 36, 40};
+  static const int cand_chunk[] = {16};
   std::vector<int> members[FSM_TUNING_BUCKETS];
   for (int i = 0; i < n; ++i)
     if (params[i].DIM_ETA == 1) {

@@ -284,11 +284,12 @@ fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t);
  * 1: < 192, 2: < 256, 3: larger) and shift_class from the shift length in
  * cells DTAU / min(DX, DY) (0: < 8, 1: < 16, 2: < 24, 3: larger).  Per bucket
  * the 2D stream kernel's staged-window bound and its phi_p chunk (phi_p per
- * FP32 partial sum of the two-level moment sum: 16 or 32; 32 folds less
- * often, with a larger summation error still far inside the parity
- * tolerance).  fsm_autotune_buckets times, for every bucket the given events
- * fall in, the launch sequence of those events (at most 64 of them) for
- * windows of 24-48 KB and both chunks, keeps the fastest per bucket for ctx
+ * FP32 partial sum of the two-level moment sum: 16, or 32 -- about 2 % faster
+ * and with a larger summation error: e against FP64 reached 1.05e-4 on a 201^2
+ * event, so the tuner keeps 16).  fsm_autotune_buckets times, for every bucket
+ * the given events fall in, the launch sequence of those events (at most 64
+ * of them) for windows of 24-40 KB (larger windows would lower the occupancy
+ * of every batch holding such an event), keeps the fastest per bucket for ctx
  * and writes the FSM_TUNING_BUCKETS entries (window_bytes 0 for buckets
  * without events: they keep the context's window and chunk 16).  The table
  * can be stored and restored as text with fsm_tuning_save / fsm_tuning_load

@@ -409,11 +409,11 @@ def test_autotune_keeps_results():
 
 
 def test_bucket_autotuner_choices_keep_results(tmp_path):
-    """Every choice the per-bucket autotuner can make: with the 16-phi_p chunk
-    the results equal the untuned ones bit for bit for every staged-window
-    size; with the 32-phi_p chunk (a different summation order) they pass the
-    parity checks against the oracle's float and FP64 runs.  The tuned table
-    survives a save / load round trip."""
+    """Every choice the per-bucket autotuner can make (windows of 24-40 KB,
+    the 16-phi_p chunk) gives the untuned results bit for bit; the 32-phi_p
+    chunk a caller may set (a different summation order, not chosen by the
+    tuner) passes the parity checks against the reference's float output and
+    T and Pi against FP64.  The tuned table survives a save / load round trip."""
     evs = [W.lumpy2d(seed=50, side=101, dx=0.1, nphip=64, dtau=0.4, eos=1, radius=3.0),   # 0, 0
            W.lumpy2d(seed=51, side=151, dx=0.08, nphip=100, dtau=1.0, eos=2, radius=4.0),  # 1, 1
            W.lumpy2d(seed=52, side=201, dx=0.05, nphip=64, dtau=1.0, eos=1, radius=4.0)]   # 2, 2
@@ -427,13 +427,16 @@ def test_bucket_autotuner_choices_keep_results(tmp_path):
         assert sorted(tuned) == [0, 5, 10], tuned
         for t in table:
             if t["window_bytes"]:
-                assert t["phi_chunk"] in (16, 32) and t["ms"] > 0 and t["events"] == 1
+                assert 24 * 1024 <= t["window_bytes"] <= 40 * 1024
+                assert t["phi_chunk"] == 16 and t["ms"] > 0 and t["events"] == 1
         path = tmp_path / "tuning.txt"
         c.save_tuning(path)
         c2 = F.Context(0)
         c2.load_tuning(path)
-        for window in (24 * 1024, 48 * 1024):
+        for window in (24 * 1024, 28 * 1024, 32 * 1024, 36 * 1024, 40 * 1024):
             for chunk in (16, 32):
+                if chunk == 32 and window != 40 * 1024:
+                    continue
                 c2.set_tuning_buckets([{"window_bytes": window, "phi_chunk": chunk}] * 16)
                 for (p, e, _), r in zip(evs, ref):
                     got = c2.run_event(p, e)
@@ -444,7 +447,7 @@ def test_bucket_autotuner_choices_keep_results(tmp_path):
                         o = _oracle(p, e)
                         o64 = _oracle(p, e, fp64=2)
                         compare_parity(got, o, o64, o["tau"])
-                        compare(got, o64, o["tau"])
+                        compare(got, o64, o["tau"], what=("T", "Pi"))
         c2.close()
     finally:
         c.close()
