@@ -126,28 +126,6 @@ inline void FREESTREAMMILNE::output_to_vectors(
 
 namespace fsm_compat {
 
-// "x y eta value" profile in GeV/fm^3 (or baryon density), cells addressed by
-// their rounded coordinates (src/FileIO.cpp:133-164).  Missing file: message
-// and exit(1), as the reference.
-inline void read_density_file(std::vector<float>& density, const char* name, const fsm_params& p) {
-  const float xmin = (-1.0) * ((float)(p.DIM_X - 1) / 2.0) * p.DX;
-  const float ymin = (-1.0) * ((float)(p.DIM_Y - 1) / 2.0) * p.DY;
-  const float etamin = (-1.0) * ((float)(p.DIM_ETA - 1) / 2.0) * p.DETA;
-  std::ifstream in(std::string(name) + ".dat");
-  if (!in) {
-    printf("Couldn't open initial profile!\n");
-    exit(1);
-  }
-  float x, y, eta, value;
-  while (in >> x >> y >> eta >> value) {
-    const int ix = (int)std::round((x - xmin) / p.DX);
-    const int iy = (int)std::round((y - ymin) / p.DY);
-    const int ie = (int)std::round((eta - etamin) / p.DETA);
-    const long long is = (long long)(p.DIM_Y * p.DIM_ETA) * ix + (long long)p.DIM_ETA * iy + ie;
-    if (is >= 0 && is < (long long)density.size()) density[(size_t)is] = value;
-  }
-}
-
 inline void write_field(const std::vector<float>& v, size_t off, const char* name,
                         const fsm_params& p, bool projection) {
   const std::string path = std::string("output/") + name + ".dat";
@@ -169,36 +147,50 @@ inline int FREESTREAMMILNE::run_freestream_milne() {
   const int DIM = params.DIM;
   gridSize = DIM;
 
-  // initial energy density (GeV/fm^3) and baryon density
-  std::vector<float> e_gev((size_t)DIM, 0.0f), nB;
-  if (params.IC_ENERGY == 5) {
+  // initial energy density and baryon density (src/FreestreamMilne.cpp:225-306):
+  // the caller's vector in GeV/fm^3 (IC_ENERGY 5, converted by fsm_run_event),
+  // or one of the reference's initial conditions, already in fm^-4
+  std::vector<float> e_in((size_t)DIM, 0.0f), nB;
+  const bool from_vector = params.IC_ENERGY == 5;
+  if (from_vector) {
     if ((size_t)params.DIM != init_energy_density.size()) {
       printf("Grid dimension of input vector does not match freestream_input file! \n");
       printf("Vector size : %d , DIM = %d \n", (int)init_energy_density.size(), params.DIM);
       exit(-1);
     }
-    e_gev = init_energy_density;
-  } else if (params.IC_ENERGY == 3) {
-    read_density_file(e_gev, "initial_profiles/e", params);
+    e_in = init_energy_density;
   } else {
-    printf("Not a valid initial Condition... Goodbye\n");
-    return 0;
+    const fsm_status ic = fsm_initial_energy(&params, "initial_profiles", e_in.data());
+    if (ic == FSM_ERR_INVALID_IC) {
+      printf("Not a valid initial Condition... Goodbye\n");
+      return 0;
+    }
+    if (ic == FSM_ERR_FILE && params.IC_ENERGY == 3) {  // src/FileIO.cpp:150-154
+      printf("Couldn't open initial profile!\n");
+      exit(1);
+    }
+    if (ic == FSM_ERR_FILE)  // IC 4: the reference prints and goes on with zeros
+      printf("Could not find initial profile in initial_profiles!");
   }
   if (params.BARYON) {
     nB.assign((size_t)DIM, 0.0f);
-    if (params.IC_BARYON == 3) {
-      read_density_file(nB, "initial_profiles/nB", params);
-    } else {
+    const fsm_status ic = fsm_initial_baryon(&params, "initial_profiles", nB.data());
+    if (ic == FSM_ERR_INVALID_IC) {
       printf("Not a valid initial Condition... Goodbye\n");
       return 0;
+    }
+    if (ic == FSM_ERR_FILE) {
+      printf("Couldn't open initial profile!\n");
+      exit(1);
     }
   }
 
   // initial profiles in fm^-4 as the reference writes them
   // (src/FreestreamMilne.cpp:266-267, 310-313)
   {
-    std::vector<float> e0((size_t)DIM);
-    for (int i = 0; i < DIM; ++i) e0[i] = e_gev[i] * 1.0f / (float)hbarc + 1.0e-7f;
+    std::vector<float> e0(e_in);
+    if (from_vector)
+      for (int i = 0; i < DIM; ++i) e0[i] = e_in[i] * 1.0f / (float)hbarc + 1.0e-7f;
     write_field(e0, 0, "initial_e", params, false);
     if (params.BARYON) write_field(nB, 0, "initial_nB", params, false);
     write_field(e0, 0, "initial_e_projection", params, true);
@@ -220,8 +212,11 @@ inline int FREESTREAMMILNE::run_freestream_milne() {
                      u.data(), pi.data(), params.BARYON ? nBo.data() : nullptr,
                      params.BARYON ? V.data() : nullptr};
   fsm_run_info info;
-  const fsm_status st = fsm_run_event(ctx_, &params, e_gev.data(), params.BARYON ? nB.data() : nullptr,
-                                      &out, &info);
+  const fsm_status st = from_vector
+                            ? fsm_run_event(ctx_, &params, e_in.data(), params.BARYON ? nB.data() : nullptr,
+                                            &out, &info)
+                            : fsm_run_event_fm4(ctx_, &params, e_in.data(),
+                                                params.BARYON ? nB.data() : nullptr, &out, &info);
   if (st != FSM_OK) {
     printf("freestream-milne: %s: %s\n", fsm_status_str(st), fsm_last_error());
     return 1;

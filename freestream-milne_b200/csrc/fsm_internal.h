@@ -134,6 +134,7 @@ struct Ev2D {
   const Chunk2D* chunks; // [nchunks]
   int nchunks;
   int chunk;             // phi_p per FP32 partial sum of the two-level moment sum (16 or 32)
+  int raw;               // e_gev already holds fm^-4 (no GeV/fm^3 conversion)
   // prep
   const float* e_gev;    // input
   const AxisNode* ax;   // [NX] x-axis spline data
@@ -184,6 +185,7 @@ struct Ev3D {
   int NX, NY, NE, NR, NPHI;
   int r_lo, r_hi;  // live rapidity nodes [r_lo, r_hi)
   int baryon;
+  int raw;         // e_gev already holds fm^-4 (no GeV/fm^3 conversion)
   float DX, DY;
   float xmin, ymin;
   float norm, normB, d_phip, DRAP;

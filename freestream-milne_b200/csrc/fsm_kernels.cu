@@ -31,9 +31,9 @@ __device__ __forceinline__ float to_fm4(float e_gev) {
   return __fadd_rn(__fdiv_rn(__fmul_rn(e_gev, 1.0f), 0.197326938f), 1.0e-7f);
 }
 // 2D initial density F = e/(2 pi), double division rounded to float
-// (src/FreeStream.cpp:318).
-__device__ __forceinline__ float F_of(float e_gev) {
-  return (float)(__ddiv_rn((double)to_fm4(e_gev), 6.283185307179586));
+// (src/FreeStream.cpp:318), from GeV/fm^3 or (raw) from fm^-4.
+__device__ __forceinline__ float F_of(float e, int raw) {
+  return (float)(__ddiv_rn((double)(raw ? e : to_fm4(e)), 6.283185307179586));
 }
 
 
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kPrepThreads, 2) fsm_prep2d_rows_kernel(
         for (int u = 0; u < kB; ++u) {
           const int c = c0 + 32 * u;
           if (c < NY) {
-            const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u]);
+            const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u], ev.raw);
             fl[c] = f;
             fa[row + c] = f;
           }
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kPrepRows * 32) fsm_prep2d_rows_long_kernel(
       for (int u = 0; u < kB; ++u) {
         const int c = c0 + 32 * u;
         if (c < NY) {
-          const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u]);
+          const float f = ev.charge ? __fmul_rn(in[u], ev.qnorm) : F_of(in[u], ev.raw);
           fr[kPadLo + c] = f;
           fa[row + c] = f;
         }
@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict_
   const int e = q / plane, r = q - e * plane;
   const int ix = r / NY, iy = r - ix * NY;
   const size_t is = ((size_t)ix * NY + iy) * NE + e;  // the reference's cell order
-  const float E0 = to_fm4(__ldg(ev.e_gev + is)), E1 = to_fm4(__ldg(ev.e_gev + is + 1));
+  const float a0 = __ldg(ev.e_gev + is), a1 = __ldg(ev.e_gev + is + 1);
+  const float E0 = ev.raw ? a0 : to_fm4(a0), E1 = ev.raw ? a1 : to_fm4(a1);
   if (ev.baryon)
     reinterpret_cast<float4*>(ev.nodes3)[q] = make_float4(E0, E1, __ldg(ev.nB + is), __ldg(ev.nB + is + 1));
   else

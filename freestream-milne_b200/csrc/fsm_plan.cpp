@@ -161,9 +161,10 @@ float edep_dtau(const fsm_params& p, float numerator, float denominator) {
 }
 
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why, int window_budget) {
+                      std::string* why, int window_budget, bool input_fm4) {
   EventPlan& E = *out;
   E = EventPlan();
+  E.input_fm4 = input_fm4;
   fsm_params p = in;
   auto fail = [&](fsm_status s, const char* msg) {
     if (why) *why = msg;
@@ -198,7 +199,9 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     float numerator = 0.0, denominator = 0.0;
     float rescale = 1.0, lower_tolerance = 1.0e-7;
     for (int i = 0; i < p.DIM; i++) {
-      float eps = host_e_gev[i] * rescale / (float)hbarc + lower_tolerance;
+      // the sums run over the profile in fm^-4 (converted from GeV/fm^3 unless
+      // it already is, src/FreestreamMilne.cpp:266-267)
+      float eps = input_fm4 ? host_e_gev[i] : host_e_gev[i] * rescale / (float)hbarc + lower_tolerance;
       numerator += (eps * eps);
       denominator += eps;
     }

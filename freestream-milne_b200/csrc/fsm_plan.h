@@ -51,6 +51,7 @@ struct EventPlan {
   // 2D with BARYON: fallback and output scales of the charge pass (Ev2D)
   float fb_scale2 = 1.0f, jscale2 = 0.0f;
   int phi_chunk = kPhiChunk;  // 2D: phi_p per FP32 partial sum (tuning; 16 or 32)
+  bool input_fm4 = false;     // the profile is already in fm^-4 (no conversion)
   double samples = 0;  // cell x momentum samples the stream kernel evaluates
   double ref_samples = 0;  // DIM * DIM_RAP * DIM_PHIP, the reference's count
 };
@@ -61,7 +62,7 @@ struct EventPlan {
 // stays within window_budget bytes.  Returns FSM_OK or an error with a message
 // in *why.
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why, int window_budget = kWindowBudget2D);
+                      std::string* why, int window_budget = kWindowBudget2D, bool input_fm4 = false);
 
 // Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
 // reference's float sums of eps^2 and eps over the converted profile

@@ -156,7 +156,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     parallel_for(n, (work > 2.0e5 || n >= 16) ? host_threads() : 1, [&](int i) {
       int window = 0, chunk = 0;
       event_tuning(ctx, params[i], &window, &chunk);
-      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window);
+      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window,
+                         mem && mem->input_fm4);
       b->plans[i].phi_chunk = chunk;
     });
     for (int i = 0; i < n; ++i)
@@ -522,6 +523,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.charge = 0;
       e.fb_scale = 1.0f;
       e.chunk = P.phi_chunk;
+      e.raw = P.input_fm4 ? 1 : 0;
       if (P.baryon) {  // charge pass: same geometry and tables, its own field and scratch
         Ev2D& q = b->ev2[b->evq_of[i]];
         q = e;
@@ -548,6 +550,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.r_lo = P.r_lo;
       e.r_hi = P.r_hi;
       e.baryon = P.baryon ? 1 : 0;
+      e.raw = P.input_fm4 ? 1 : 0;
       e.DX = p.DX;
       e.DY = p.DY;
       e.xmin = P.xmin;
@@ -915,35 +918,41 @@ extern "C" fsm_status fsm_ctx_timing(fsm_ctx* ctx, fsm_timing* t, int reset) {
   return FSM_OK;
 }
 
-extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
-                                    const float* nB, const fsm_outputs* host_out,
-                                    fsm_run_info* info) {
+namespace {
+// One event, host buffers in and out; fm4: the energy profile is already in
+// fm^-4 (otherwise GeV/fm^3, converted as src/FreestreamMilne.cpp:266-267).
+fsm_status run_event_host(fsm_ctx* ctx, const fsm_params* p, const float* e_gev, const float* nB,
+                          const fsm_outputs* host_out, fsm_run_info* info, bool fm4) {
   if (!ctx || !p || !e_gev || !host_out) return FSM_ERR_INVALID_ARG;
   if (p->BARYON && !nB) return FSM_ERR_INVALID_ARG;
   FSM_CUDA_TRY(cudaSetDevice(ctx->device));
   fsm_status s;
   fsm_batch* b = ctx->single_host;
-  // the cached batch serves the same parameters again without planning (an
-  // energy-dependent DTAU depends on the profile, so those events re-plan)
-  if (!b || p->E_DEP_FS != 0 || !same_params(ctx->single_host_raw, *p)) {
+  // the cached batch serves the same parameters (and input units) again
+  // without planning (an energy-dependent DTAU depends on the profile, so
+  // those events re-plan)
+  if (!b || p->E_DEP_FS != 0 || !same_params(ctx->single_host_raw, *p) || ctx->single_host_fm4 != fm4) {
     EventPlan P;
     std::string why;
     int window = 0, chunk = 0;
     event_tuning(ctx, *p, &window, &chunk);
-    s = plan_event(*p, e_gev, &P, &why, window);
+    s = plan_event(*p, e_gev, &P, &why, window, fm4);
     if (s != FSM_OK) {
       set_last_error(why);
       return s;
     }
-    if (!b || !same_params(b->plans[0].p, P.p)) {
+    if (!b || !same_params(b->plans[0].p, P.p) || ctx->single_host_fm4 != fm4) {
       batch_free(ctx->single_host);
       ctx->single_host = nullptr;
       const float* he[1] = {e_gev};
-      s = batch_build(ctx, 1, p, he, nullptr, nullptr, nullptr, &ctx->single_host);
+      BatchMem units;
+      units.input_fm4 = fm4;
+      s = batch_build(ctx, 1, p, he, nullptr, nullptr, nullptr, &ctx->single_host, &units);
       if (s != FSM_OK) return s;
       b = ctx->single_host;
     }
     ctx->single_host_raw = *p;
+    ctx->single_host_fm4 = fm4;
   }
   const EventPlan& P = b->plans[0];
   cudaStream_t st = ctx->stream;
@@ -971,6 +980,19 @@ extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const flo
   FSM_CUDA_TRY(cudaStreamSynchronize(st));
   if ((s = check_kernel_errors(b)) != FSM_OK) return s;
   return fill_info(P, info);
+}
+}  // namespace
+
+extern "C" fsm_status fsm_run_event(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
+                                    const float* nB, const fsm_outputs* host_out,
+                                    fsm_run_info* info) {
+  return run_event_host(ctx, p, e_gev, nB, host_out, info, false);
+}
+
+extern "C" fsm_status fsm_run_event_fm4(fsm_ctx* ctx, const fsm_params* p, const float* e_fm4,
+                                        const float* nB, const fsm_outputs* host_out,
+                                        fsm_run_info* info) {
+  return run_event_host(ctx, p, e_fm4, nB, host_out, info, true);
 }
 
 extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, const float* d_e_gev,

@@ -80,6 +80,7 @@ struct fsm_ctx {
   fsm_batch* single_host = nullptr;
   fsm_batch* single_dev = nullptr;
   fsm_params single_host_raw{};
+  bool single_host_fm4 = false;  // units the cached one-event host batch was built for
   // the device and pinned allocations of the last batch destroyed, kept for
   // the next batch that fits (a stream of event sets then allocates nothing)
   std::mutex spare_mu;
@@ -177,6 +178,8 @@ struct BatchMem {
   // only the input/output slabs and the tables: no stream-kernel scratch (a
   // batch whose launches run an inner batch planned later, see fsm_batch::inner)
   bool io_only = false;
+  // the energy profiles are already in fm^-4 (fsm_run_event_fm4)
+  bool input_fm4 = false;
 };
 
 bool has_device();

@@ -146,6 +146,11 @@ SIGNATURES = {
     "fsm_ctx_set_wait_limit": (_ST, [_VP, ctypes.c_int]),
     "fsm_write_field": (_ST, [ctypes.c_char_p, _VP, ctypes.POINTER(Params), ctypes.c_int,
                               ctypes.c_int]),
+    "fsm_initial_energy": (_ST, [ctypes.POINTER(Params), ctypes.c_char_p, _VP]),
+    "fsm_initial_baryon": (_ST, [ctypes.POINTER(Params), ctypes.c_char_p, _VP]),
+    "fsm_read_profile": (_ST, [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int, _VP]),
+    "fsm_run_event_fm4": (_ST, [_VP, ctypes.POINTER(Params), _VP, _VP, ctypes.POINTER(Outputs),
+                                ctypes.POINTER(RunInfo)]),
     "fsm_write_outputs": (_ST, [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.POINTER(Outputs),
                                 ctypes.POINTER(Diagnostics), ctypes.c_int]),
     "fsm_diagnostics_device": (_ST, [ctypes.POINTER(Params), ctypes.POINTER(Outputs),
@@ -267,10 +272,12 @@ class Context:
         check(lib().fsm_ctx_timing(self.h, ctypes.byref(t), int(reset)), "fsm_ctx_timing")
         return {k: getattr(t, k) for k, _ in Timing._fields_}
 
-    def run_event(self, params, e_gev, nB=None, outputs=None, into=None):
+    def run_event(self, params, e_gev, nB=None, outputs=None, into=None, fm4=False):
         """Plain per-event path with host buffers; returns {name: ndarray}
         (written into the arrays of `into`, a previous result of the same
-        shape, when given)."""
+        shape, when given).  fm4: the profile is already in fm^-4
+        (fsm_run_event_fm4, the reference's initial conditions other than the
+        vector); otherwise in GeV/fm^3."""
         e_gev = np.ascontiguousarray(e_gev, dtype=np.float32).ravel()
         dim = params.DIM_X * params.DIM_Y * params.DIM_ETA
         if e_gev.size != dim:
@@ -291,8 +298,9 @@ class Context:
             nB = np.ascontiguousarray(nB, dtype=np.float32).ravel()
             nb_ptr = nB.ctypes.data
         info = RunInfo()
-        check(lib().fsm_run_event(self.h, ctypes.byref(params), e_gev.ctypes.data, nb_ptr,
-                                  ctypes.byref(o), ctypes.byref(info)), "fsm_run_event")
+        fn = lib().fsm_run_event_fm4 if fm4 else lib().fsm_run_event
+        check(fn(self.h, ctypes.byref(params), e_gev.ctypes.data, nb_ptr, ctypes.byref(o),
+                 ctypes.byref(info)), "fsm_run_event_fm4" if fm4 else "fsm_run_event")
         arrs["info"] = {k: getattr(info, k) for k, _ in RunInfo._fields_}
         return arrs
 
@@ -596,6 +604,26 @@ def write_outputs(dirpath, params, result, diag=None, nthreads=0):
     check(lib().fsm_write_outputs(str(dirpath).encode(), ctypes.byref(params), ctypes.byref(o),
                                   ctypes.byref(d) if d is not None else None, int(nthreads)),
           "fsm_write_outputs")
+
+
+PROFILE_FORMATS = {"xyev": 0, "cpuvh": 1, "supermc_block": 2, "trento_block": 3, "trento3d_block": 4}
+
+
+def initial_profile(params, kind="energy", directory=None):
+    """The reference's initial condition params.IC_ENERGY (or IC_BARYON) as a
+    float32 profile in fm^-4 (fsm_initial_energy / fsm_initial_baryon)."""
+    out = np.zeros(params.DIM_X * params.DIM_Y * params.DIM_ETA, np.float32)
+    fn = lib().fsm_initial_energy if kind == "energy" else lib().fsm_initial_baryon
+    check(fn(ctypes.byref(params), None if directory is None else str(directory).encode(),
+             out.ctypes.data), "fsm_initial_" + kind)
+    return out
+
+
+def read_profile(path, params, fmt):
+    out = np.zeros(params.DIM_X * params.DIM_Y * params.DIM_ETA, np.float32)
+    check(lib().fsm_read_profile(str(path).encode(), ctypes.byref(params), PROFILE_FORMATS[fmt],
+                                 out.ctypes.data), "fsm_read_profile")
+    return out
 
 
 def device_count():

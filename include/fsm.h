@@ -443,6 +443,42 @@ fsm_status fsm_write_field(const char* path, const float* var, const fsm_params*
 fsm_status fsm_write_outputs(const char* dir, const fsm_params* p, const fsm_outputs* out,
                              const fsm_diagnostics* diag, int nthreads);
 
+/* ------------------------------------------------------ initial conditions */
+/* The reference's initial conditions other than the caller's vector
+ * (src/FreestreamMilne.cpp:225-306), as host profiles in fm^-4 -- the units
+ * the reference computes with; pass them to fsm_run_event_fm4.  IC_ENERGY: 1
+ * smooth elliptical Gaussian, 2 the same times a rand() draw per cell, 3 an
+ * "x y eta value" file <dir>/e.dat, 4 a CPU-VH file <dir>/e.dat, 6 two
+ * Gaussians times rand() draws (the reference's norm is 0: a zero profile);
+ * IC_BARYON: 1, 2 as energy 1, 2 with the baryon widths, 3 <dir>/nB.dat.  dir
+ * NULL: "initial_profiles" (the reference's directory).  The Monte-Carlo
+ * profiles draw from the C library's rand() in the reference's order.
+ * Missing files return FSM_ERR_FILE (the reference exits for IC 3 and prints
+ * for IC 4); IC_ENERGY 5 and unknown values FSM_ERR_INVALID_IC. */
+fsm_status fsm_initial_energy(const fsm_params* p, const char* dir, float* e_fm4);
+fsm_status fsm_initial_baryon(const fsm_params* p, const char* dir, float* nB);
+/* One profile file of DIM floats in fm^-4 in one of the reference's formats:
+ * "x y eta value" lines (src/FileIO.cpp:133-164), CPU-VH "d d d value" lines in
+ * eta, y, x order plus 1e-7 (src/InitialConditions.cpp:316-355), superMC and
+ * TRENTO transverse blocks times the reference's eta plateau plus 1e-3
+ * (:127-236; TRENTO skips a 12-line header, rows are y), and TRENTO 3D blocks
+ * plus 1e-3 (:274-314).  The reference has these block readers but does not
+ * reach them from run_freestream_milne; they are here for callers that read
+ * such files. */
+enum {
+  FSM_PROFILE_XYEV = 0,
+  FSM_PROFILE_CPUVH = 1,
+  FSM_PROFILE_SUPERMC_BLOCK = 2,
+  FSM_PROFILE_TRENTO_BLOCK = 3,
+  FSM_PROFILE_TRENTO3D_BLOCK = 4
+};
+fsm_status fsm_read_profile(const char* path, const fsm_params* p, int format, float* out);
+/* fsm_run_event for a profile already in fm^-4 (IC_ENERGY other than 5: the
+ * reference then uses the profile as it is, src/FreestreamMilne.cpp:231-281,
+ * and takes the E_DEP_FS sums over it, src/FreeStream.cpp:389-417). */
+fsm_status fsm_run_event_fm4(fsm_ctx* ctx, const fsm_params* p, const float* e_fm4, const float* nB,
+                             const fsm_outputs* host_out, fsm_run_info* info);
+
 /* ------------------------------------------------------------ diagnostics */
 /* Measured FP32 FMA throughput of `device` in TFLOP/s (a short FMA-chain
  * kernel timed with CUDA events): the peak the stream kernels' roofline

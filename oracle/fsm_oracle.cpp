@@ -34,6 +34,9 @@
 
 namespace {
 
+// The profile passed to oracle_run is already in fm^-4 (oracle_run_fm4).
+static thread_local bool g_raw_input = false;
+
 // hbar*c as the reference stores it: `float hbarc = 0.197326938;`
 // (src/FreestreamMilne.cpp:141)
 const float kHbarcF = 0.197326938f;
@@ -179,11 +182,15 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
   p.TAU = p.TAU0 + p.DTAU;
   const int DIM = p.DIM;
 
-  // initial energy density in fm^-4 (src/FreestreamMilne.cpp:266-267)
+  // initial energy density in fm^-4 (src/FreestreamMilne.cpp:266-267), or
+  // as given when the profile already is in fm^-4 (the reference's other
+  // initial conditions, :231-281)
   std::vector<R> e0(DIM);
   const R lower_tolerance = 1.0e-7;
   for (int i = 0; i < DIM; ++i) {
-    if (sizeof(R) == 4) {
+    if (g_raw_input) {
+      e0[i] = (R)e_gev[i];
+    } else if (sizeof(R) == 4) {
       float rescale = 1.0f;
       e0[i] = (R)(e_gev[i] * rescale / (float)kHbarcF + (float)lower_tolerance);
     } else {
@@ -195,8 +202,9 @@ int run(const oracle_params& pin, const float* e_gev, const float* nB_in, oracle
   if (p.E_DEP_FS == 1) {  // the free-streaming time is geometry: G arithmetic
     G num = 0.0, den = 0.0;
     for (int i = 0; i < DIM; ++i) {
-      G eps = (sizeof(G) == 4) ? (G)(e_gev[i] * 1.0f / kHbarcF + 1.0e-7f)
-                               : (G)((double)e_gev[i] / 0.197326938 + 1.0e-7);
+      G eps = g_raw_input ? (G)e_gev[i]
+              : (sizeof(G) == 4) ? (G)(e_gev[i] * 1.0f / kHbarcF + 1.0e-7f)
+                                 : (G)((double)e_gev[i] / 0.197326938 + 1.0e-7);
       num += (eps * eps);
       den += eps;
     }
@@ -488,6 +496,15 @@ extern "C" int oracle_run(const oracle_params* p, int fp64, const float* e_gev, 
   if (fp64 == 1) return run<double, false>(*p, e_gev, nB, out);
   if (fp64 == 2) return run<double, true>(*p, e_gev, nB, out);
   return run<float, true>(*p, e_gev, nB, out);
+}
+
+// oracle_run for a profile already in fm^-4 (no GeV/fm^3 conversion).
+extern "C" int oracle_run_fm4(const oracle_params* p, int fp64, const float* e_fm4, const float* nB,
+                              oracle_out* out, int nthreads) {
+  g_raw_input = true;
+  const int rc = oracle_run(p, fp64, e_fm4, nB, out, nthreads);
+  g_raw_input = false;
+  return rc;
 }
 
 extern "C" void oracle_spline_derivs(const double* x, const double* y, int n, double* d) {

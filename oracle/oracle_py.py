@@ -76,6 +76,8 @@ def lib():
         _lib.oracle_run.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.POINTER(Out), ctypes.c_int]
         _lib.oracle_run.restype = ctypes.c_int
+        _lib.oracle_run_fm4.argtypes = _lib.oracle_run.argtypes
+        _lib.oracle_run_fm4.restype = ctypes.c_int
         _lib.oracle_spline_derivs.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int, ctypes.c_void_p]
         _lib.oracle_bicubic_eval.argtypes = ([ctypes.c_void_p] * 3 + [ctypes.c_int] * 2 +
                                              [ctypes.c_void_p] * 2 + [ctypes.c_int, ctypes.c_void_p])
@@ -100,12 +102,26 @@ def ref():
         _ref.ref_run.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p,
                                  ctypes.POINTER(Out)]
         _ref.ref_run.restype = ctypes.c_int
+        _ref.ref_run_fm4.argtypes = _ref.ref_run.argtypes
+        _ref.ref_run_fm4.restype = ctypes.c_int
         _ref.ref_run_full.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]
         _ref.ref_run_full.restype = ctypes.c_int
         _ref.ref_write_outputs.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params)] + [ctypes.c_void_p] * 8
         _ref.ref_write_outputs.restype = ctypes.c_int
+        _ref.ref_initial.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_int, ctypes.c_void_p]
+        _ref.ref_initial.restype = ctypes.c_int
     return _ref
+
+
+def ref_initial(workdir, params, which):
+    """The reference's own initial-condition function `which` (see
+    ref_harness.cpp) run inside workdir; returns the float32 profile."""
+    out = np.zeros(params.DIM_X * params.DIM_Y * params.DIM_ETA, np.float32)
+    rc = ref().ref_initial(str(workdir).encode(), ctypes.byref(params), int(which), out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ref_initial failed with code {rc}")
+    return out
 
 
 def ref_write_outputs(workdir, params, res, diag17):
@@ -143,9 +159,11 @@ def _alloc_out(dim, baryon):
     return o, arrs
 
 
-def run(params, e_gev, nB=None, fp64=False, impl="oracle", nthreads=0):
+def run(params, e_gev, nB=None, fp64=False, impl="oracle", nthreads=0, fm4=False):
     """Run the hot path on the CPU.  impl: 'oracle' (restatement) or 'ref'
-    (reference sources).  Returns a dict of float64 arrays plus metadata."""
+    (reference sources); fm4: the profile is already in fm^-4 (the reference's
+    initial conditions other than the vector).  Returns a dict of float64
+    arrays plus metadata."""
     e_gev = np.ascontiguousarray(e_gev, dtype=np.float32).ravel()
     dim = params.DIM_X * params.DIM_Y * params.DIM_ETA
     if e_gev.size != dim:
@@ -159,14 +177,15 @@ def run(params, e_gev, nB=None, fp64=False, impl="oracle", nthreads=0):
         nb_ptr = nB.ctypes.data
     o, arrs = _alloc_out(dim, baryon)
     if impl == "oracle":
-        rc = lib().oracle_run(ctypes.byref(params), int(fp64), e_gev.ctypes.data, nb_ptr,
-                              ctypes.byref(o), int(nthreads))
+        fn = lib().oracle_run_fm4 if fm4 else lib().oracle_run
+        rc = fn(ctypes.byref(params), int(fp64), e_gev.ctypes.data, nb_ptr, ctypes.byref(o), int(nthreads))
     elif impl == "ref":
         if fp64:
             raise ValueError("the reference build is float only")
         if nthreads:
             os.environ["OMP_NUM_THREADS"] = str(nthreads)
-        rc = ref().ref_run(ctypes.byref(params), e_gev.ctypes.data, nb_ptr, ctypes.byref(o))
+        fn = ref().ref_run_fm4 if fm4 else ref().ref_run
+        rc = fn(ctypes.byref(params), e_gev.ctypes.data, nb_ptr, ctypes.byref(o))
     else:
         raise ValueError(impl)
     if rc != 0:

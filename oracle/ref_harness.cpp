@@ -17,6 +17,10 @@
 
 static_assert(sizeof(oracle_params) == sizeof(parameters), "parameter layout must match");
 
+// ref_run_fm4 passes a profile already in fm^-4 (used as is, as the
+// reference uses its own initial conditions, src/FreestreamMilne.cpp:231-281).
+static bool g_ref_raw_input = false;
+
 // Runs the pipeline of src/FreestreamMilne.cpp:251-506 on the given inputs by
 // calling the reference's own functions in the reference's order.
 extern "C" int ref_run(const oracle_params* pin, const float* e_gev, const float* nB_in,
@@ -32,7 +36,8 @@ extern "C" int ref_run(const oracle_params* pin, const float* e_gev, const float
 
   float* initialEnergyDensity = (float*)calloc(params.DIM, sizeof(float));
   for (int i = 0; i < DIM; i++)
-    initialEnergyDensity[i] = e_gev[i] * rescale / (float)hbarc + lower_tolerance;
+    initialEnergyDensity[i] =
+        g_ref_raw_input ? e_gev[i] : e_gev[i] * rescale / (float)hbarc + lower_tolerance;
   float* initialChargeDensity = NULL;
   if (params.BARYON) {
     initialChargeDensity = (float*)calloc(params.DIM, sizeof(float));
@@ -167,6 +172,14 @@ extern "C" int ref_run_full(const char* workdir, const float* e_gev, int n, doub
   return rc;
 }
 
+extern "C" int ref_run_fm4(const oracle_params* pin, const float* e_fm4, const float* nB_in,
+                           oracle_out* out) {
+  g_ref_raw_input = true;
+  const int rc = ref_run(pin, e_fm4, nB_in, out);
+  g_ref_raw_input = false;
+  return rc;
+}
+
 // The reference's own diagnostic functions (src/HydroValidity.cpp:8-101,
 // src/LandauMatch.cpp:395-489) on given Landau-matched fields; out as
 // oracle_diagnostics.
@@ -269,4 +282,36 @@ extern "C" int ref_write_outputs(const char* workdir, const oracle_params* pin, 
   free2dArrayf(om, 6);
   if (chdir(old) != 0) return 3;
   return 0;
+}
+
+// The reference's own initial conditions (src/InitialConditions.cpp,
+// src/FileIO.cpp:133-164) inside `workdir` (whose initial_profiles/ holds the
+// files the readers open).  which: 1 / 2 smooth / rand() elliptical Gaussian
+// with the energy widths (15, 15, 15), 11 / 12 the same with the baryon
+// widths (2, 3, 1), 3 readDensityFile of initial_profiles/e, 4 the CPU-VH
+// reader, 6 the two-Gaussian profile, 21 / 22 / 23 the superMC, TRENTO and
+// TRENTO 3D block readers.
+extern "C" int ref_initial(const char* workdir, const oracle_params* pin, int which, float* out) {
+  char old[4096];
+  if (!getcwd(old, sizeof(old))) return 1;
+  if (chdir(workdir) != 0) return 2;
+  parameters params;
+  std::memcpy(&params, pin, sizeof(params));
+  params.DIM = params.DIM_X * params.DIM_Y * params.DIM_ETA;
+  int rc = 0;
+  switch (which) {
+    case 1: initializeEllipticalGauss(out, 15.0, 15.0, 15.0, params); break;
+    case 2: initializeEllipticalMCGauss(out, 15.0, 15.0, 15.0, params); break;
+    case 11: initializeEllipticalGauss(out, 2.0, 3.0, 1.0, params); break;
+    case 12: initializeEllipticalMCGauss(out, 2.0, 3.0, 1.0, params); break;
+    case 3: readDensityFile(out, (char*)"initial_profiles/e", params); break;
+    case 4: readEnergyDensityCPUVH(out, params); break;
+    case 6: initialize2Gaussians(out, 1.0, 1.0, 1.0, params); break;
+    case 21: readEnergyDensitySuperMCBlock(out, params); break;
+    case 22: readEnergyDensityTRENTOBlock(out, params); break;
+    case 23: readEnergyDensityTRENTO3DBlock(out, params); break;
+    default: rc = 4;
+  }
+  if (chdir(old) != 0) return 3;
+  return rc;
 }

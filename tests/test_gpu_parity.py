@@ -453,6 +453,34 @@ def test_bucket_autotuner_choices_keep_results(tmp_path):
         c.close()
 
 
+@pytest.mark.parametrize("case", ["ic1_2d", "ic1_3d_baryon", "ic1_2d_edepfs"])
+def test_initial_conditions_in_fm4(ctx, case):
+    """The reference's own initial conditions (here the smooth elliptical
+    Gaussian, IC_ENERGY = 1) are in fm^-4 and used as they are: through
+    fsm_run_event_fm4 against the oracle fed the same profile (its fm^-4 mode
+    is bit-exact with the reference's sources), float and FP64 runs; with
+    E_DEP_FS the free-streaming time comes from the raw profile as well."""
+    if case == "ic1_2d":
+        p = F.default_params(DIM_X=61, DIM_Y=55, DX=0.4, DY=0.4, DIM_PHIP=48, DTAU=1.5, TAU0=0.5,
+                             IC_ENERGY=1, EOS_TYPE=2)
+    elif case == "ic1_3d_baryon":
+        p = F.default_params(DIM_X=31, DIM_Y=29, DIM_ETA=11, DX=0.4, DY=0.4, DETA=0.4, DIM_RAP=9,
+                             DIM_PHIP=24, DTAU=1.0, TAU0=0.5, IC_ENERGY=1, BARYON=1, IC_BARYON=1)
+    else:
+        p = F.default_params(DIM_X=61, DIM_Y=55, DX=0.4, DY=0.4, DIM_PHIP=48, DTAU=1.5, TAU0=0.5,
+                             IC_ENERGY=1, E_DEP_FS=1, TAU_R=0.8, E_R=4.0, ALPHA=0.25)
+    e = F.initial_profile(p, "energy")
+    nB = F.initial_profile(p, "baryon") if p.BARYON else None
+    got = ctx.run_event(p, e, nB, fm4=True)
+    po = O.Params(**p.as_dict())
+    ref = O.run(po, e, nB=nB, fm4=True)
+    ref64 = O.run(po, e, nB=nB, fm4=True, fp64=2)
+    assert got["info"]["dim_phip"] == ref["dim_phip"]
+    assert got["info"]["dtau"] == pytest.approx(ref["dtau"], rel=0, abs=0)
+    compare_parity(got, ref, ref64, ref["tau"], baryon=bool(p.BARYON))
+    compare(got, ref64, ref["tau"], baryon=bool(p.BARYON))
+
+
 def test_invalid_inputs_are_rejected(ctx):
     p = F.default_params(DIM_X=3)
     with pytest.raises(F.FsmError):

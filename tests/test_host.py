@@ -288,3 +288,84 @@ def test_all_output_files_match_reference_writers(tmp_path, case):
     assert a == b and len(a) == (52 if p.BARYON else 47), (len(a), set(a) ^ set(b))
     for name in a:
         assert (mine / name).read_bytes() == (theirs / "output" / name).read_bytes(), name
+
+
+def _ic_files(run, p, rng):
+    """Writes the reference's input files for the readers into run/initial_profiles."""
+    d = run / "initial_profiles"
+    d.mkdir(parents=True)
+    NX, NY, NE = p.DIM_X, p.DIM_Y, p.DIM_ETA
+    vals = rng.gamma(1.0, 5.0, NX * NY * NE).astype(np.float32)
+    xmin = np.float32(-1.0 * (np.float32(NX - 1) / 2.0) * np.float32(p.DX))
+    ymin = np.float32(-1.0 * (np.float32(NY - 1) / 2.0) * np.float32(p.DY))
+    emin = np.float32(-1.0 * (np.float32(NE - 1) / 2.0) * np.float32(p.DETA))
+    lines = []
+    for ix in range(NX):
+        for iy in range(NY):
+            for ie in range(NE):
+                v = vals[(ix * NY + iy) * NE + ie]
+                lines.append(f"{ix * p.DX + xmin:.6g} {iy * p.DY + ymin:.6g} {ie * p.DETA + emin:.6g} {v:.7g}")
+    (d / "e.dat").write_text("\n".join(lines) + "\n")
+    return d, vals
+
+
+@pytest.mark.parametrize("case", ["2d", "3d"])
+def test_initial_conditions_match_reference(tmp_path, case):
+    """The reference's initial conditions (analytic, Monte-Carlo with the C
+    library's rand(), and every file reader) bit for bit against its own
+    functions compiled from its sources, on the same inputs and rand() seed."""
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    libc = ctypes.CDLL(None)
+    ne = 1 if case == "2d" else 9
+    p = F.default_params(DIM_X=23, DIM_Y=19, DIM_ETA=ne, DX=0.13, DY=0.11, DETA=0.3,
+                         ETA_FLAT=0.6, ETA_WIDTH=0.45)
+    po = O.Params(**p.as_dict())
+    rng = np.random.default_rng(3)
+    d, vals = _ic_files(tmp_path, p, rng)
+    n = p.DIM_X * p.DIM_Y * p.DIM_ETA
+
+    def ours(ic, kind="energy"):
+        q = F.Params(**p.as_dict())
+        if kind == "energy":
+            q.IC_ENERGY = ic
+        else:
+            q.IC_BARYON = ic
+        return F.initial_profile(q, kind, d)
+
+    for ic, which in ((1, 1), (3, 3), (2, 2), (6, 6)):
+        libc.srand(777)
+        a = ours(ic)
+        libc.srand(777)
+        b = O.ref_initial(tmp_path, po, which)
+        assert np.array_equal(a, b), ic
+    for ic, which in ((1, 11), (2, 12)):
+        libc.srand(99)
+        a = ours(ic, "baryon")
+        libc.srand(99)
+        b = O.ref_initial(tmp_path, po, which)
+        assert np.array_equal(a, b), ("baryon", ic)
+    # CPU-VH ("d d d value" lines in eta, y, x order)
+    lines = [f"0 0 0 {v:.7g}" for v in vals]
+    (d / "e.dat").write_text("\n".join(lines) + "\n")
+    assert np.array_equal(ours(4), O.ref_initial(tmp_path, po, 4))
+    # block formats: superMC (ed.dat, x-major), TRENTO (12 header lines,
+    # y-major), TRENTO 3D (one value per cell)
+    t = vals[:p.DIM_X * p.DIM_Y]
+    (d / "ed.dat").write_text(" ".join(f"{v:.7g}" for v in t) + "\n")
+    assert np.array_equal(F.read_profile(d / "ed.dat", p, "supermc_block"), O.ref_initial(tmp_path, po, 21))
+    (d / "e.dat").write_text("# header\n" * 12 + " ".join(f"{v:.7g}" for v in t) + "\n")
+    assert np.array_equal(F.read_profile(d / "e.dat", p, "trento_block"), O.ref_initial(tmp_path, po, 22))
+    (d / "e.dat").write_text(" ".join(f"{v:.7g}" for v in vals) + "\n")
+    assert np.array_equal(F.read_profile(d / "e.dat", p, "trento3d_block"), O.ref_initial(tmp_path, po, 23))
+    assert n == vals.size
+    # missing files and unknown initial conditions are errors, not exits
+    q = F.Params(**p.as_dict())
+    q.IC_ENERGY = 3
+    with pytest.raises(F.FsmError) as ei:
+        F.initial_profile(q, "energy", tmp_path / "nowhere")
+    assert ei.value.status == 8
+    q.IC_ENERGY = 5
+    with pytest.raises(F.FsmError) as ei:
+        F.initial_profile(q, "energy", d)
+    assert ei.value.status == 3
