@@ -197,6 +197,17 @@ inline int FREESTREAMMILNE::run_freestream_milne() {
     if (params.BARYON) write_field(nB, 0, "initial_nB_projection", params, true);
   }
 
+  // total energy before streaming (src/FreestreamMilne.cpp:349-354): float
+  // running sum of the profile in fm^-4, in cell order
+  {
+    float totalEnergy = 0.0;
+    for (int is = 0; is < DIM; is++)
+      totalEnergy += from_vector ? e_in[is] * 1.0f / (float)hbarc + 1.0e-7f : e_in[is];
+    if (params.DIM_ETA > 1) totalEnergy *= (params.TAU0 * params.DX * params.DY * params.DETA);
+    else totalEnergy *= (params.DX * params.DY);
+    printf("Total energy on grid before streaming : %f \n", totalEnergy);
+  }
+
   if (!ctx_ && fsm_ctx_create(&ctx_, nullptr) != FSM_OK) {
     printf("freestream-milne: %s\n", fsm_last_error());
     return 1;

@@ -241,6 +241,15 @@ struct Tile2D {
   int ev, x0, y0, interior;
 };
 
+// Inputs of the energy bookkeeping of one event (fsm_batch_energy).
+struct EvEnergy {
+  const float* e_in;  // input profile (GeV/fm^3, or fm^-4 with raw)
+  const float* T00;   // T^{tau tau} after streaming
+  const float* e;     // Landau-matched energy density (fm^-4)
+  int n, raw;
+  float e_freeze;     // GeV/fm^3
+};
+
 // Counters reset before each launch sequence.
 struct Counters {
   int tile2d;

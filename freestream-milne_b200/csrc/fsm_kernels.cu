@@ -324,6 +324,30 @@ __global__ void fsm_edep_sums_kernel(const float* const* __restrict__ e_gev, con
   sums[2 * ev + 1] = den;
 }
 
+// ------------------------------------------------------- energy bookkeeping
+// The reference's convergence and freeze-out sums (src/FreestreamMilne.cpp:
+// 349-354, 531-545): float running sums in cell order of the initial profile
+// in fm^-4, of T^{tau tau}, and of T^{tau tau} where e hbar*c > E_FREEZE.  One
+// thread per event, in that order, so the sums equal the reference's bit for
+// bit; the events of a batch run in parallel.
+__global__ void fsm_energy_sums_kernel(const EvEnergy* __restrict__ evs, int count, float* sums) {
+  const int ev = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ev >= count) return;
+  const EvEnergy E = evs[ev];
+  const float hbarc = 0.197326938f;
+  float before = 0.0f, after = 0.0f, inside = 0.0f;
+  for (int is = 0; is < E.n; ++is) {
+    const float a = __ldg(E.e_in + is);
+    before = __fadd_rn(before, E.raw ? a : to_fm4(a));
+    const float t = __ldg(E.T00 + is);
+    after = __fadd_rn(after, t);
+    if (__fmul_rn(__ldg(E.e + is), hbarc) > E.e_freeze) inside = __fadd_rn(inside, t);
+  }
+  sums[3 * ev] = before;
+  sums[3 * ev + 1] = after;
+  sums[3 * ev + 2] = inside;
+}
+
 // ------------------------------------------------------------------ prep 3D
 // Eta-pair node arrays of a 3D event: node (e, ix, iy) holds the converted
 // energy density of slices e and e+1 at (ix, iy) (and the baryon density of

@@ -34,6 +34,7 @@ __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
 __global__ void fsm_edep_sums_kernel(const float* const*, const int*, int, float*);
+__global__ void fsm_energy_sums_kernel(const EvEnergy*, int, float*);
 __global__ void fsm_diag_kernel(int, int, int, float, float, float, const float*, const float*,
                                 const float*, const float*, const float*, float*, float*, float*,
                                 float*, float*, float*);
@@ -69,6 +70,8 @@ void batch_free(fsm_batch* b) {
   batch_free(b->inner);
   if (b->d_edep) cudaFree(b->d_edep);
   if (b->h_sums) cudaFreeHost(b->h_sums);
+  if (b->d_energy) cudaFree(b->d_energy);
+  if (b->h_energy) cudaFreeHost(b->h_energy);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_segs) cudaFree(b->d_segs);
   if (b->d_pack) cudaFree(b->d_pack);
@@ -1682,4 +1685,54 @@ extern "C" fsm_status fsm_tuning_load(fsm_ctx* ctx, const char* path) {
   std::fclose(f);
   if (st != FSM_OK) return st;
   return fsm_ctx_set_tuning_buckets(ctx, table);
+}
+
+// ==================================================== energy bookkeeping
+extern "C" fsm_status fsm_batch_energy(fsm_batch* b, fsm_energy* out, void* stream) {
+  if (!b || !out) return FSM_ERR_INVALID_ARG;
+  FSM_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  // an E_DEP_FS batch ran its inner batch: its plans hold the run values
+  const fsm_batch* pb = b->inner ? b->inner : b;
+  if (!b->edep.empty() && !b->inner) {
+    set_last_error("fsm_batch_energy: the batch has not been launched");
+    return FSM_ERR_PENDING;
+  }
+  const int n = (int)b->plans.size();
+  const size_t o_sums = align_up((size_t)n * sizeof(fsm::EvEnergy));
+  if (!b->d_energy) {
+    FSM_CUDA_TRY(cudaMalloc(&b->d_energy, o_sums + (size_t)n * 3 * sizeof(float)));
+    FSM_CUDA_TRY(cudaMallocHost(&b->h_energy, (size_t)n * 3 * sizeof(float)));
+  }
+  std::vector<fsm::EvEnergy> ev(n);
+  for (int i = 0; i < n; ++i) {
+    const EventPlan& P = pb->plans[i];
+    ev[i] = fsm::EvEnergy{b->d_in_e[i], b->d_out[i].T ? b->d_out[i].T : b->d_T[i], b->d_out[i].e, P.DIM,
+                          P.input_fm4 ? 1 : 0, P.p.E_FREEZE};
+    if (!ev[i].T00 || !ev[i].e) {
+      set_last_error("fsm_batch_energy: the batch has no T or e output for event " + std::to_string(i));
+      return FSM_ERR_INVALID_ARG;
+    }
+  }
+  cudaStream_t s = pick_stream(b->ctx, stream);
+  FSM_CUDA_TRY(cudaMemcpyAsync(b->d_energy, ev.data(), (size_t)n * sizeof(fsm::EvEnergy),
+                               cudaMemcpyHostToDevice, s));
+  fsm_energy_sums_kernel<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const fsm::EvEnergy*>(b->d_energy),
+                                                         n, reinterpret_cast<float*>(b->d_energy + o_sums));
+  FSM_CUDA_TRY(cudaGetLastError());
+  FSM_CUDA_TRY(cudaMemcpyAsync(b->h_energy, b->d_energy + o_sums, (size_t)n * 3 * sizeof(float),
+                               cudaMemcpyDeviceToHost, s));
+  FSM_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int i = 0; i < n; ++i) {
+    const fsm_params& p = pb->plans[i].p;
+    float before = b->h_energy[3 * i], after = b->h_energy[3 * i + 1], inside = b->h_energy[3 * i + 2];
+    // volume factors as src/FreestreamMilne.cpp:351-353, 533-544
+    if (p.DIM_ETA > 1) before *= (p.TAU0 * p.DX * p.DY * p.DETA);
+    else before *= (p.DX * p.DY);
+    if (p.DIM_ETA > 1) after *= (p.TAU * p.DX * p.DY * p.DETA);
+    else after *= (p.TAU * p.DX * p.DY);
+    if (p.DIM_ETA > 1) inside *= (p.TAU * p.DX * p.DY * p.DETA);
+    else inside *= (p.TAU * p.DX * p.DY);
+    out[i] = fsm_energy{before, after, inside, inside / after};
+  }
+  return FSM_OK;
 }

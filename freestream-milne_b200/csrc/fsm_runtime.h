@@ -159,6 +159,8 @@ struct fsm_batch {
   std::vector<fsm_params> inner_params;
   char* d_edep = nullptr;             // device: input pointers, cell counts, sums
   float* h_sums = nullptr;            // pinned: the sums read back
+  char* d_energy = nullptr;           // device: energy-bookkeeping descriptors and sums
+  float* h_energy = nullptr;          // pinned: those sums read back
 };
 
 namespace fsm {

@@ -58,6 +58,11 @@ class Tuning(ctypes.Structure):
     _fields_ = [("window_bytes", ctypes.c_int), ("ms", ctypes.c_double)]
 
 
+class Energy(ctypes.Structure):
+    _fields_ = [("before", ctypes.c_float), ("after", ctypes.c_float), ("inside", ctypes.c_float),
+                ("fraction", ctypes.c_float)]
+
+
 class TuningBucket(ctypes.Structure):
     _fields_ = [("window_bytes", ctypes.c_int), ("phi_chunk", ctypes.c_int), ("ms", ctypes.c_double),
                 ("events", ctypes.c_int)]
@@ -140,6 +145,7 @@ SIGNATURES = {
                                       ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "fsm_batch_packed_offsets": (_ST, [_VP, ctypes.c_uint, ctypes.c_uint, _VP, ctypes.c_size_t]),
     "fsm_batch_check": (_ST, [_VP]),
+    "fsm_batch_energy": (_ST, [_VP, ctypes.POINTER(Energy), _VP]),
     "fsm_probe_fp32_tflops": (_ST, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "fsm_run_event_2d_noalloc": (_ST, [ctypes.POINTER(Params), _VP, ctypes.POINTER(Outputs), _VP]),
     "fsm_run_event_2d_noalloc_check": (_ST, [_VP]),
@@ -535,6 +541,13 @@ class Batch:
 
     def check_errors(self):
         check(lib().fsm_batch_check(self.h), "fsm_batch_check")
+
+    def energy(self, stream=None):
+        """Per event: total energy before / after streaming, the part inside
+        E_FREEZE and its fraction (fsm_batch_energy)."""
+        out = (Energy * self.n)()
+        check(lib().fsm_batch_energy(self.h, out, stream), "fsm_batch_energy")
+        return [{k: getattr(x, k) for k, _ in Energy._fields_} for x in out]
 
     def pack_inputs(self, inputs):
         """inputs: list of (e_gev, nB or None) -> float32 host slab."""

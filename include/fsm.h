@@ -234,6 +234,18 @@ fsm_status fsm_batch_packed_offsets(fsm_batch* b, unsigned mask, unsigned flags,
 /* Waits for the stream the batch last used (upload, launch or download) and
  * checks the kernels' internal error counters. */
 fsm_status fsm_batch_check(fsm_batch* b);
+/* The reference's energy bookkeeping per event of the last launch
+ * (src/FreestreamMilne.cpp:349-354, 531-545): total energy on the grid before
+ * streaming (the initial profile in fm^-4 times DX DY, times TAU0 DETA in 3D),
+ * after streaming (T^{tau tau} times TAU DX DY [DETA]), the part of it in
+ * cells with e hbar*c > E_FREEZE, and that fraction; the running float sums
+ * are taken on the device in the reference's cell order (one thread per
+ * event, all events in one launch), so they equal the reference's.  Enqueued
+ * on `stream` after the launch and waited for; out has one entry per event. */
+typedef struct fsm_energy {
+  float before, after, inside, fraction;
+} fsm_energy;
+fsm_status fsm_batch_energy(fsm_batch* b, fsm_energy* out, void* stream);
 /* Total cell x momentum samples of one launch of the batch. */
 double fsm_batch_samples(fsm_batch* b);
 

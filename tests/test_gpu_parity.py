@@ -211,6 +211,42 @@ def test_batches_on_recycled_allocations(ctx):
         c.close()
 
 
+def test_energy_bookkeeping_on_device(ctx):
+    """The reference's total energies before and after streaming and the part
+    inside E_FREEZE (src/FreestreamMilne.cpp:349-354, 531-545), summed on the
+    device per event in the reference's cell order: equal bit for bit to
+    sequential float32 sums of the same fields with the reference's volume
+    factors (2D and 3D events, an E_DEP_FS event among them)."""
+    evs = []
+    for name in golden_names():
+        d, e, nB, _, _ = load_golden(name)
+        evs.append((fsm_params(d), e, nB))
+    b = F.Batch(ctx, [p for p, _, _ in evs])
+    outs = b.run_host([(e, nB) for _, e, nB in evs])
+    got = b.energy()
+    f32 = np.float32
+    hbarc = f32(0.197326938)
+    for i, ((p, e, _), o, g) in enumerate(zip(evs, outs, got)):
+        info = b.info(i)
+        tau = f32(info["tau"])
+        e_fm4 = (np.asarray(e, f32) * f32(1.0) / hbarc + f32(1e-7)).astype(f32)
+        t00 = np.asarray(o["T"], f32)[0]
+        inside = np.where(np.asarray(o["e"], f32) * hbarc > f32(p.E_FREEZE), t00, f32(0))
+        seq = lambda a: np.cumsum(a.astype(f32), dtype=f32)[-1]
+        dx, dy, de = f32(p.DX), f32(p.DY), f32(p.DETA)
+        if p.DIM_ETA > 1:
+            vb = f32(f32(f32(f32(p.TAU0) * dx) * dy) * de)
+            va = f32(f32(f32(tau * dx) * dy) * de)
+        else:
+            vb = f32(dx * dy)
+            va = f32(f32(tau * dx) * dy)
+        want = dict(before=f32(seq(e_fm4) * vb), after=f32(seq(t00) * va), inside=f32(seq(inside) * va))
+        for k, v in want.items():
+            assert f32(g[k]) == v, (i, k, g[k], v)
+        assert f32(g["fraction"]) == f32(want["inside"] / want["after"])
+    b.close()
+
+
 def test_grouped_batch_downloads(ctx):
     """A batch with grouped outputs gives the same results as a per-event one,
     and download_groups copies back exactly the groups asked for."""
