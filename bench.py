@@ -38,11 +38,11 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
 FLOPS_PER_SAMPLE_3D_BARYON = 75  # shift 5 + 2 trilinear x 21 + 14 moments x 2
-# DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.6 MB read +
-# 161.0 MB written) / 713.26 M samples, from one ncu capture of the launch on
+# DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.9 MB read +
+# 167.7 MB written) / 713.26 M samples, from one ncu capture of the launch on
 # the first 128 events of this workload (a full 512-event launch is above the
 # capture size rule), scaled by samples
-TRAFFIC_BYTES_PER_SAMPLE_2D = (88.60672e6 + 161.023744e6) / 713258674
+TRAFFIC_BYTES_PER_SAMPLE_2D = (88.878592e6 + 167.744512e6) / 713258674
 WORKLOAD = ("uneven_batch: 512 seeded lumpy 2D events, side {101,151,201,261,301}, DX U[0.05,0.1], "
             "DIM_PHIP {64,100,200} + arc-length rule, DTAU U[0.3,1.5], EOS 1/2 50:50, TAU0 0.2")
 L2_NOTE = ("no explicit flush: each step streams ~2 GB (inputs 86 MB, spline scratch, 1.6 GB "
@@ -146,14 +146,14 @@ def cpu_baseline(events, nthreads, budget_s=20.0):
     return done / dt, kind, f"first {done} events of the workload, {nthreads} OpenMP threads, {dt:.1f} s"
 
 
-def serve_stream(args, F, W, local, rank, ctx, reps):
-    """Mixed request stream (80 % 2D of sides 101-301, 20 % 3D of 131^2 x
-    {25, 51} with 21/31/41 rapidities) through the continuous-batching server:
-    a burst measures capacity, then Poisson arrivals at serve_load x capacity
-    give p50/p99 latency; the same requests one by one through fsm_run_event
-    give the plain path."""
+def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2):
+    """Request stream (by default 80 % 2D of sides 101-301, 20 % 3D of 131^2 x
+    {25, 51} with 21/31/41 rapidities; frac3d=0: boost-invariant requests only)
+    through the continuous-batching server: a burst measures capacity, then
+    Poisson arrivals at serve_load x capacity give p50/p99 latency; the same
+    requests one by one through fsm_run_event give the plain path."""
     import threading
-    reqs = W.stream_requests(args.serve_requests, rate_hz=1.0, seed=reps.seed(4))
+    reqs = W.stream_requests(args.serve_requests, rate_hz=1.0, seed=reps.seed(4), frac3d=frac3d)
     gaps = [reqs[0][0]] + [reqs[k][0] - reqs[k - 1][0] for k in range(1, len(reqs))]
     events = [ev for _, ev in reqs]
     hydro = ["e", "P", "Pi", "u", "pi", "nB", "V"]  # the fields the reference hands to hydro
@@ -492,9 +492,10 @@ def main():
             s.close()
 
     # ---------------- served: Poisson stream of mixed 2D/3D requests through the server
-    served = None
+    served = served_2d = None
     if not args.no_serve:
         served = serve_stream(args, F, W, local, rank, ctx, reps)
+        served_2d = serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.0)
 
     # ---------------- one 3D event with baryon charge (131^2 x 51, 21 rapidities, 100 phi_p)
     ev3d = None
@@ -556,6 +557,7 @@ def main():
             "gpu_launches": launches_per_step * args.steps,
             "output_files": files,
             "served": served,
+            "served_2d": served_2d,
             "event_3d": ev3d,
             "clocks": clocks,
         }
