@@ -215,6 +215,14 @@ def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2):
             "budget": {"hbm_bytes": budget["hbm_budget"], "pinned_host_bytes": budget["host_budget"]}}
 
 
+def issue_peak(torch, device, clocks):
+    """FP32 FMA issue peak in TFLOP/s: SMs x 128 FP32 lanes x 2 FLOP x the
+    maximum SM clock seen (nominal 148 x 128 x 2 x 1.965 GHz = 74.4)."""
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
+    return sms * 128 * 2 * mhz * 1e6 / 1e12
+
+
 def event_3d(F, W, local, sp, stream, args):
     """The 3D configuration with baryon charge, one event device-resident:
     131 x 131 x 51 cells, 21 rapidities (tan map), 100 phi_p, DTAU 0.8."""
@@ -501,6 +509,11 @@ def main():
     ev3d = None
     if not args.no_3d:
         ev3d = event_3d(F, W, local, sp, stream, args)
+        ev3d["roofline"] = {"bound": "fp32", "kernel": "fsm_stream3d_baryon_kernel",
+                            "achieved": ev3d["stream_tflops"], "peak": peak, "unit": "TFLOP/s",
+                            "frac": ev3d["stream_tflops"] / peak,
+                            "peak_source": "measured FP32 FMA probe on this GPU",
+                            "frac_of_issue_peak": ev3d["stream_tflops"] / issue_peak(torch, local, clocks)}
 
     files = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -532,6 +545,8 @@ def main():
             "roofline": {"bound": "fp32", "kernel": "fsm_stream2d_kernel", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "measured FP32 FMA probe on this GPU (fsm_probe_fp32_tflops)",
+                         "issue_peak": issue_peak(torch, local, clocks),
+                         "frac_of_issue_peak": achieved / issue_peak(torch, local, clocks),
                          "flops_per_sample": FLOPS_PER_SAMPLE_2D, "samples_per_launch": samples,
                          "launch_ms": stream_ms,
                          "traffic": TRAFFIC_BYTES_PER_SAMPLE_2D * samples,

@@ -253,9 +253,9 @@ struct EvEnergy {
 // Counters reset before each launch sequence.
 struct Counters {
   int tile2d;
-  int block3d;
+  int block3d;    // 3D tiles without baryon charge
   int fallback;
-  int pad;
+  int block3d_b;  // 3D tiles with baryon charge
 };
 
 }  // namespace fsm

@@ -1103,9 +1103,13 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
   }
 }
 
-__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
-                                                                     const Tile3D* __restrict__ tiles,
-                                                                     int ntiles, Counters* ctr) {
+// The tile loop of the 3D kernels; kB: the tiles' events carry baryon charge
+// (one kind per launch, so that each kernel is register-allocated for its own
+// path: compiled together, the two paths spilled).
+template <bool kB>
+__device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
+                                               const Tile3D* __restrict__ tiles, int ntiles,
+                                               int* counter) {
   extern __shared__ float slots3[];  // thread-private slots, [slot][thread]
   __shared__ int s_tile;
   constexpr int K = kCellsPerThread;
@@ -1113,7 +1117,7 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
   float* const sl = slots3 + threadIdx.x;
   auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->block3d, 1);
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
     const int tix = s_tile;
     if (tix >= ntiles) return;
@@ -1121,7 +1125,7 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
     const Ev3D& ev = evs[tl.ev];
     const int NX = ev.NX, NY = ev.NY, NE = ev.NE, NR = ev.NR, NP = ev.NPHI;
     const int ieta = tl.ieta;
-    const bool baryon = ev.baryon != 0;
+    constexpr bool baryon = kB;
     const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
     const int x_hi = min(tl.x0 + kTileX, NX) - 1, y_hi = min(tl.y0 + kTileY, NY) - 1;
     const bool full = (tl.x0 + kTileX <= NX) && (tl.y0 + kTileY <= NY);
@@ -1146,7 +1150,7 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
       const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
       const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
       const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
-      if (baryon) {
+      if constexpr (kB) {
         const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
         const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
         const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
@@ -1201,6 +1205,19 @@ __global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D*
     }
     __syncthreads();
   }
+}
+
+// 3D events without baryon charge (float2 eta-pair nodes).
+__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
+                                                                     const Tile3D* __restrict__ tiles,
+                                                                     int ntiles, Counters* ctr) {
+  stream3d_tiles<false>(evs, tiles, ntiles, &ctr->block3d);
+}
+
+// 3D events with baryon charge (float4 eta-pair nodes of energy and charge).
+__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_baryon_kernel(
+    const Ev3D* __restrict__ evs, const Tile3D* __restrict__ tiles, int ntiles, Counters* ctr) {
+  stream3d_tiles<true>(evs, tiles, ntiles, &ctr->block3d_b);
 }
 
 // ------------------------------------------------------------- packing

@@ -116,9 +116,22 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
                    " above its fixed scratch limit of " + std::to_string(kNoAllocMaxPhi));
     return FSM_ERR_TOO_LARGE;
   }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  {
+    // the call uploads its tables from host memory that is gone when it
+    // returns, so a graph replaying the upload would read freed memory
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+      set_last_error("fsm_run_event_2d_noalloc: cudaStreamIsCapturing failed");
+      return FSM_ERR_CUDA;
+    }
+    if (cap != cudaStreamCaptureStatusNone) {
+      set_last_error("fsm_run_event_2d_noalloc cannot be captured into a CUDA graph");
+      return FSM_ERR_UNSUPPORTED;
+    }
+  }
   char* D = nullptr;
   if ((st = noalloc_scratch_address(&D)) != FSM_OK) return st;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int NX = P.p.DIM_X, NY = P.p.DIM_Y, DIM = P.DIM;
 
   // work lists (as the batch path builds them for one event)

@@ -31,6 +31,7 @@ __global__ void fsm_prep2d_cols_long_kernel(const Ev2D*, const LineBlock*);
 __global__ void fsm_prep3d_kernel(const Ev3D*, const CellBlock*);
 __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counters*, int*, int);
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
+__global__ void fsm_stream3d_baryon_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
 __global__ void fsm_edep_sums_kernel(const float* const*, const int*, int, float*);
@@ -115,8 +116,8 @@ fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot) 
   }
   return FSM_OK;
 }
-int g_smem2[64] = {0}, g_smem3[64] = {0}, g_smem_rows[64] = {0}, g_smem_srows[64] = {0},
-    g_smem_scols[64] = {0};
+int g_smem2[64] = {0}, g_smem3[64] = {0}, g_smem3b[64] = {0}, g_smem_rows[64] = {0},
+    g_smem_srows[64] = {0}, g_smem_scols[64] = {0};
 
 int tuning_bucket(const fsm_params& p) {
   const int side = std::max(p.DIM_X, p.DIM_Y);
@@ -269,9 +270,15 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       const EventPlan &A = b->plans[a], &C = b->plans[c];
       return A.samples / std::max(1, A.DIM) > C.samples / std::max(1, C.DIM);
     });
-    // 3D tiles: 32 x 32 cells of one eta slice, slices with the most live
-    // rapidity nodes first
-    std::vector<std::pair<int, Tile3D>> t3;
+    // 3D tiles: 32 x 32 cells of one eta slice; the tiles of events with
+    // baryon charge first (their own kernel), then the others, each group
+    // with the slices of most live rapidity nodes first
+    struct T3 {
+      int work;
+      bool baryon;
+      Tile3D t;
+    };
+    std::vector<T3> t3;
     for (int i : order3) {
       const EventPlan& P = b->plans[i];
       const int NX = P.p.DIM_X, NY = P.p.DIM_Y, NE = P.p.DIM_ETA;
@@ -279,14 +286,16 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
         // slices without a live rapidity node still get tiles: they write zeros
         for (int x0 = 0; x0 < NX; x0 += kTileX)
           for (int y0 = 0; y0 < NY; y0 += kTileY)
-            t3.push_back({P.live_eta[ie] * P.p.DIM_PHIP, Tile3D{b->ev3_of[i], x0, y0, ie}});
+            t3.push_back({P.live_eta[ie] * P.p.DIM_PHIP, P.p.BARYON != 0, Tile3D{b->ev3_of[i], x0, y0, ie}});
       }
     }
-    std::stable_sort(t3.begin(), t3.end(),
-                     [](const std::pair<int, Tile3D>& a, const std::pair<int, Tile3D>& c) {
-                       return a.first > c.first;
-                     });
-    for (auto& t : t3) tiles3.push_back(t.second);
+    std::stable_sort(t3.begin(), t3.end(), [](const T3& a, const T3& c) {
+      return a.baryon != c.baryon ? a.baryon : a.work > c.work;
+    });
+    for (auto& t : t3) {
+      tiles3.push_back(t.t);
+      b->ntiles3b += t.baryon ? 1 : 0;
+    }
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
       if (P.is3d)
@@ -665,14 +674,23 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
                                                                b->smem2));
     b->grid2 = std::max(1, std::min(b->ntiles, ctx->num_sms * std::max(occ, 1)));
   }
-  if (b->ntiles3) {
+  if (b->ntiles3 > b->ntiles3b) {
     fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_kernel, ctx->device, b->smem3,
                                     &g_smem3[ctx->device & 63]);
     if (ss != FSM_OK) return ss;
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_kernel, kThreads3D,
                                                                b->smem3));
-    b->grid3 = std::max(1, std::min(b->ntiles3, ctx->num_sms * std::max(occ, 1)));
+    b->grid3 = std::max(1, std::min(b->ntiles3 - b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
+  }
+  if (b->ntiles3b) {
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_baryon_kernel, ctx->device, b->smem3,
+                                    &g_smem3b[ctx->device & 63]);
+    if (ss != FSM_OK) return ss;
+    int occ = 0;
+    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_baryon_kernel,
+                                                               kThreads3D, b->smem3));
+    b->grid3b = std::max(1, std::min(b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
   }
   if (mem && mem->dev)
     FSM_CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int) * 4, mem->stream));
@@ -716,9 +734,12 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
     fsm_stream2d_kernel<<<b->grid2, kThreads2D, b->smem2, s>>>(b->d_ev2, b->d_tiles, b->ntiles,
                                                                b->box_cap2, b->d_ctr, b->d_err,
                                                                b->wait_polls);
-  if (b->ntiles3)
-    fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3, b->ntiles3,
-                                                               b->d_ctr);
+  if (b->ntiles3b)
+    fsm_stream3d_baryon_kernel<<<b->grid3b, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3,
+                                                                       b->ntiles3b, b->d_ctr);
+  if (b->ntiles3 > b->ntiles3b)
+    fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(
+        b->d_ev3, b->d_tiles3 + b->ntiles3b, b->ntiles3 - b->ntiles3b, b->d_ctr);
   if (timing) cudaEventRecord(ts.ev[2], s);
   if (b->nbl) fsm_landau_kernel<<<b->nbl, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl, b->d_ctr);
   if (timing) {

@@ -131,9 +131,10 @@ struct fsm_batch {
   Counters* d_ctr = nullptr;
   int* d_err = nullptr;
   int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, ntiles3 = 0, nbl = 0;
+  int ntiles3b = 0;  // the first ntiles3b 3D tiles belong to events with baryon charge
   int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
   size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
-  int grid2 = 0, grid3 = 0;
+  int grid2 = 0, grid3 = 0, grid3b = 0;
   int wait_polls = fsm::kWaitPolls;  // polls of one bounded wait in the stream kernel
   double samples = 0;
   cudaGraphExec_t graph = nullptr;
@@ -199,7 +200,7 @@ void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chu
 // `slot` records the largest value set so far for that kernel on `device`;
 // every caller of the library uses the slots below, under one mutex.
 fsm_status ensure_dyn_smem(const void* fn, int device, size_t bytes, int* slot);
-extern int g_smem2[64], g_smem3[64], g_smem_rows[64], g_smem_srows[64], g_smem_scols[64];
+extern int g_smem2[64], g_smem3[64], g_smem3b[64], g_smem_rows[64], g_smem_srows[64], g_smem_scols[64];
 fsm_status check_kernel_errors(fsm_batch* b);
 fsm_status fill_info(const EventPlan& P, fsm_run_info* info);
 

@@ -259,8 +259,9 @@ double fsm_batch_samples(fsm_batch* b);
  * scratch lives in one fixed 8 MiB file-scope device array that every GPU
  * loading the library holds until the process exits; limits: DIM_X*DIM_Y <=
  * 90601 (e.g. 301 x 301) and DIM_PHIP <= 1024 after the arc-length rule, larger
- * events return FSM_ERR_TOO_LARGE.  The first call on each device looks up the
- * array's device address (make that first call before any stream capture).
+ * events return FSM_ERR_TOO_LARGE.  The call cannot be captured into a CUDA
+ * graph (it uploads its tables from host memory that is released when it
+ * returns): on a capturing stream it returns FSM_ERR_UNSUPPORTED.
  * All calls share the array, so calls that overlap on the GPU race: run them in
  * one stream or serialise them.  The call returns once its work is enqueued;
  * the outputs are valid once fsm_run_event_2d_noalloc_check returns FSM_OK. */

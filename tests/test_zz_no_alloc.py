@@ -65,3 +65,22 @@ def test_no_alloc_rejects_oversized_events(ctx):
     with pytest.raises(F.FsmError) as ei:
         F.run_event_2d_noalloc(p, d_e.data_ptr(), {k: v.data_ptr() for k, v in out.items()})
     assert ei.value.status == 12  # FSM_ERR_TOO_LARGE
+
+
+def test_no_alloc_rejects_stream_capture(ctx):
+    """Its table upload reads host memory released when the call returns, so
+    a call on a capturing stream is refused before it enqueues anything."""
+    import torch
+    p = F.default_params(DIM_X=41, DIM_Y=41)
+    d_e = torch.ones(41 * 41, dtype=torch.float32, device="cuda")
+    out = _dev_outputs(torch, 41 * 41)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        d_e.mul_(1.0)  # the graph holds one node of its own
+        with pytest.raises(F.FsmError) as ei:
+            F.run_event_2d_noalloc(p, d_e.data_ptr(), {k: v.data_ptr() for k, v in out.items()},
+                                   stream=s.cuda_stream)
+    assert ei.value.status == 4  # FSM_ERR_UNSUPPORTED
+    g.replay()
+    torch.cuda.synchronize()
