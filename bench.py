@@ -364,9 +364,12 @@ def main():
     params = [p for p, _, _ in events]
     ctx = F.Context(local)
     tuning = ctx.autotune(params, [(e, nb) for _, e, nb in events])  # staged-window size
-    # per bucket (grid side x shift length): window and phi_p chunk
+    # per bucket (grid side x shift length): window, phi_p chunk, tile shapes
     buckets = ctx.autotune_buckets(params, [(e, nb) for _, e, nb in events])
-    bucket_choice = {k: f"{t['window_bytes'] // 1024} KB / {t['phi_chunk']}"
+    tiles_name = {F.TILES_DEFAULT: "tail tiles", F.TILES_TAIL: "tail tiles",
+                  F.TILES_SQUARE: "32x32 tiles"}
+    bucket_choice = {k: f"{t['window_bytes'] // 1024} KB / {t['phi_chunk']} / "
+                        f"{tiles_name[t['tile_shapes']]}"
                      for k, t in enumerate(buckets) if t["window_bytes"]}
     batch = F.Batch(ctx, params)
     n = len(events)

@@ -70,3 +70,25 @@ extern "C" int fsm_hosttest_plan_digest(const fsm_params* p, int serial, unsigne
   *digest = h;
   return (int)s;
 }
+
+// The 2D output tiles of one event as (x0, y0, shape, x1, y1), with the runs
+// planned per shape (nch[5]) and the largest staged window in nodes; returns
+// the number of tiles (at most cap written) or -1 when planning fails.
+extern "C" int fsm_hosttest_tiles(const fsm_params* p, int tail_tiles, int window_budget, int* out,
+                                  int cap, int* nch, int* box_elems) {
+  fsm::EventPlan E;
+  std::string why;
+  if (fsm::plan_event(*p, nullptr, &E, &why, window_budget, false, tail_tiles != 0) != FSM_OK) return -1;
+  std::vector<fsm::Tile2D> t;
+  fsm::tiles_2d(E, 0, t);
+  for (int k = 0; k < (int)t.size() && k < cap; ++k) {
+    out[5 * k + 0] = t[k].x0;
+    out[5 * k + 1] = t[k].y0;
+    out[5 * k + 2] = t[k].shape;
+    out[5 * k + 3] = t[k].x1;
+    out[5 * k + 4] = t[k].y1;
+  }
+  for (int s = 0; s < fsm::kShapes2D; ++s) nch[s] = E.nch[s];
+  *box_elems = E.box_elems;
+  return (int)t.size();
+}

@@ -112,8 +112,22 @@ struct Chunk2D {
 #else
 #define FSM_HDI inline
 #endif
-FSM_HDI int win_h(const Chunk2D& c) { return kTileX + (c.ox1 - c.ox0) + 3; }
-FSM_HDI int win_w(const Chunk2D& c) { return kTileY + (c.oy1 - c.oy0) + 3; }
+// 2D output tile shapes.  A warp's lanes run along y in groups of Ly
+// consecutive cells (32 / Ly groups of 4 x cells side by side), and Wy warps
+// are stacked along y: TX = 4 * (32 / Ly) * (8 / Wy) x cells by TY = Ly * Wy
+// y cells, always 256 threads and 1024 cells.  Shape 0 (32 x 32) tiles an
+// event; the narrow shapes cover its partial last strips, so that fewer lanes
+// and warps run past the grid edge: 1 (64 x 16) and 2 (128 x 8) for a last
+// y strip of at most 16 / 8 cells, 3 (16 x 64) and 4 (8 x 128) for a last x
+// strip of at most 16 / 8 cells.
+constexpr int kShapes2D = 5;
+FSM_HDI int shape_ly(int s) { return s == 1 ? 16 : s == 2 ? 8 : 32; }
+FSM_HDI int shape_wy(int s) { return s == 3 ? 2 : s == 4 ? 4 : 1; }
+FSM_HDI int shape_tx(int s) { return kCellsPerThread * (32 / shape_ly(s)) * (kWarps2D / shape_wy(s)); }
+FSM_HDI int shape_ty(int s) { return shape_ly(s) * shape_wy(s); }
+// Staged window of a run for a tile of shape s: rows (x) and row length (y).
+FSM_HDI int win_h(const Chunk2D& c, int s) { return shape_tx(s) + (c.ox1 - c.ox0) + 3; }
+FSM_HDI int win_w(const Chunk2D& c, int s) { return shape_ty(s) + (c.oy1 - c.oy0) + 3; }
 constexpr int kMaxChunks2D = 64;
 constexpr int kWindowBudget2D = 32 * 1024;  // bytes of one staged window (default)
 constexpr int kMaxWindow2D = 64 * 1024;     // largest staged window the planner raises to
@@ -131,8 +145,9 @@ struct Ev2D {
   float xmin, ymin, xmax_i, ymax_i;  // grid origin and spline domain (src/FreeStream.cpp:113,142-146)
   float d_phip;
   const PhiEntry2D* tab; // [NPHI]
-  const Chunk2D* chunks; // [nchunks]
-  int nchunks;
+  const Chunk2D* chunks; // the runs of every tile shape the event uses
+  int choff[kShapes2D];  // first run of shape s in chunks
+  int nch[kShapes2D];    // runs of shape s (0: shape unused)
   int chunk;             // phi_p per FP32 partial sum of the two-level moment sum (16 or 32)
   int raw;               // e_gev already holds fm^-4 (no GeV/fm^3 conversion)
   // prep
@@ -154,6 +169,11 @@ struct Ev2D {
 
 // Per-(ieta, irap) quantities of the 3D path, computed on the host with the
 // reference's float arithmetic (src/FreeStream.cpp:174-201, LandauMatch.cpp:36-55).
+// Thread-private shared-memory slots per cell of the 3D stream kernels:
+// T^{mu nu} (10), with baryon charge also J^mu (4).
+constexpr int kSlots3D = 10;
+constexpr int kSlots3DBaryon = 14;
+
 struct RapEta {
   float D;      // TAU*cosh(rap-eta_new) - TAU0*cosh(rap-eta): transverse shift length
   float efrac;  // fractional part of the shifted eta index
@@ -237,8 +257,10 @@ constexpr int kMaxCopySeg = 1 << 16;  // floats per segment (one block each)
 
 // One 2D output tile of one event; interior = 1 when every sample of every
 // cell of the tile provably lands inside the grid (no bounds logic needed).
+// A 2D output tile: shape `shape` from (x0, y0), storing the cells below
+// (x1, y1) (the grid, or the end of the strip the tile belongs to).
 struct Tile2D {
-  int ev, x0, y0, interior;
+  int ev, x0, y0, shape, x1, y1;
 };
 
 // Inputs of the energy bookkeeping of one event (fsm_batch_energy).

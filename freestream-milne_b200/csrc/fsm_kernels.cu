@@ -527,8 +527,9 @@ __device__ __forceinline__ void stage_window(float4* buf, const float4* __restri
 template <bool kInterior>
 __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __restrict__ win, int wx0,
                                              int wy0, int boxW, const float4* __restrict__ stab,
-                                             int p0, int p1, int ixb, int iy, int x_hi, int ty0,
-                                             int ty1, float ey, const float (&ex)[kCellsPerThread],
+                                             int p0, int p1, int ixb, int iy, int wxa, int wxb,
+                                             int wya, int wyb, int wxn, float ey,
+                                             const float (&ex)[kCellsPerThread],
                                              float (&a0)[kCellsPerThread],
                                              float2 (&a12)[kCellsPerThread],
                                              float2 (&a34)[kCellsPerThread],
@@ -554,9 +555,11 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       if (pl < pe) {
         const float4 tl4 = stab[kPhiTab2D * (pl - p0) + 5];
         const int lox = __float_as_int(tl4.z), loy = (int)(short)(__float_as_int(tl4.w) & 0xffff);
-        const int wa = ixb + lox, wb = min(ixb + K - 1, x_hi) + lox;
-        vis = (wb + 1 >= 1) && (wa - 1 <= NX - 2) && (ty1 + loy + 1 >= 1) && (ty0 + loy - 1 <= NY - 2);
-        ins = (wa >= 2) && (wa + K - 1 <= NX - 3) && (ty0 + loy >= 2) && (ty1 + loy <= NY - 3);
+        // the warp's cells: x wxa .. wxb inside the grid (wxa .. wxa + wxn - 1
+        // computed), y wya .. wyb inside the grid
+        const int wa = wxa + lox, wb = wxb + lox;
+        vis = (wb + 1 >= 1) && (wa - 1 <= NX - 2) && (wyb + loy + 1 >= 1) && (wya + loy - 1 <= NY - 2);
+        ins = (wa >= 2) && (wa + wxn - 1 <= NX - 3) && (wya + loy >= 2) && (wyb + loy <= NY - 3);
       }
       vis_mask = __ballot_sync(0xffffffffu, vis);
       in_mask = __ballot_sync(0xffffffffu, ins);
@@ -714,18 +717,31 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     if (t >= ntiles) return;
     const Tile2D tl = tiles[t];
     const Ev2D& ev = evs[tl.ev];
-    const int nch = ev.nchunks;
-    const Chunk2D* __restrict__ chunks = ev.chunks;
+    const int sh = tl.shape;
+    const int nch = ev.nch[sh];
+    const Chunk2D* __restrict__ chunks = ev.chunks + ev.choff[sh];
     const float4* __restrict__ gnodes = reinterpret_cast<const float4*>(ev.nodes);
     if (warp == 0) {
       const Chunk2D c0 = chunks[0];
-      stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, win_w(c0),
-                   win_h(c0), tab0, ev.tab + c0.p0,
+      stage_window(buf0, gnodes, ev.NX, ev.NY, tl.x0 + c0.ox0 - 1, tl.y0 + c0.oy0 - 1, win_w(c0, sh),
+                   win_h(c0, sh), tab0, ev.tab + c0.p0,
                    (uint32_t)(c0.p1 - c0.p0) * (uint32_t)sizeof(PhiEntry2D), &bars[0]);
     }
+    // the tile's shape: lanes run along y in groups of ly cells (32 / ly
+    // groups of K x cells side by side), wy warps stacked along y
+    const int ly = shape_ly(sh), wy = shape_wy(sh);
+    const int gx = 32 / ly, wxcount = kWarps2D / wy;
+    const int wxi = warp % wxcount, wyi = warp / wxcount;
+    const int TX = K * gx * wxcount, TY = ly * wy;
     // per-thread cell constants
-    const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
-    const int x_hi = min(tl.x0 + kTileX, ev.NX) - 1, y_hi = min(tl.y0 + kTileY, ev.NY) - 1;
+    const int iy = tl.y0 + wyi * ly + (lane & (ly - 1));
+    const int ixb = tl.x0 + K * (wxi * gx + lane / ly);
+    // the last cell the tile stores (x1, y1 <= the grid's size)
+    const int x_hi = min(tl.x0 + TX, tl.x1) - 1, y_hi = min(tl.y0 + TY, tl.y1) - 1;
+    // this warp's cells
+    const int wxa = tl.x0 + K * wxi * gx, wxn = K * gx;
+    const int wxb = min(wxa + wxn - 1, x_hi);
+    const int wya = tl.y0 + wyi * ly, wyb = min(wya + ly - 1, y_hi);
     const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
     const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
@@ -747,15 +763,15 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     for (int m = 0; m < kTotSlots2D; ++m) stot[m * kThreads2D] = 0.0f;
     float4 nd0[K + 1], nd1[K + 1];
     int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
-    // warps whose cells all lie past the grid's x edge skip the runs
-    const bool live = ixb <= x_hi;
+    // warps whose cells all lie past the grid's edge skip the runs
+    const bool live = wxa <= x_hi && wya <= y_hi;
 
     for (int c = 0; c < nch; ++c) {
       const int b = c & 1;
       if (warp == 0 && c + 1 < nch) {
         const Chunk2D cn = chunks[c + 1];
         stage_window(b ? buf0 : buf1, gnodes, ev.NX, ev.NY, tl.x0 + cn.ox0 - 1, tl.y0 + cn.oy0 - 1,
-                     win_w(cn), win_h(cn), b ? tab0 : tab1, ev.tab + cn.p0,
+                     win_w(cn, sh), win_h(cn, sh), b ? tab0 : tab1, ev.tab + cn.p0,
                      (uint32_t)(cn.p1 - cn.p0) * (uint32_t)sizeof(PhiEntry2D), &bars[b ^ 1]);
       }
       const uint32_t ph = b ? phase1 : phase0;
@@ -775,7 +791,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
         return;
       }
       const Chunk2D ch = chunks[c];
-      const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1, boxW = win_w(ch);
+      const int wx0 = tl.x0 + ch.ox0 - 1, wy0 = tl.y0 + ch.oy0 - 1, boxW = win_w(ch, sh);
       const float4* win = b ? buf1 : buf0;
       const float4* stab = b ? tab1 : tab0;
       // every sample of this run lands at least one node inside the grid
@@ -784,11 +800,11 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
                             (tl.y0 + ch.oy0 >= 2) && (y_hi + ch.oy1 <= ev.NY - 3);
       if (!live) {
       } else if (interior) {
-        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, x_hi, tl.y0, y_hi, ey, ex, a0,
-                           a12, a34, nd0, nd1, pox, poy, stot, err);
+        stream2d_run<true>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, wxa, wxb, wya, wyb, wxn,
+                           ey, ex, a0, a12, a34, nd0, nd1, pox, poy, stot, err);
       } else {
-        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, x_hi, tl.y0, y_hi, ey, ex, a0,
-                            a12, a34, nd0, nd1, pox, poy, stot, err);
+        stream2d_run<false>(ev, win, wx0, wy0, boxW, stab, ch.p0, ch.p1, ixb, iy, wxa, wxb, wya, wyb, wxn,
+                            ey, ex, a0, a12, a34, nd0, nd1, pox, poy, stot, err);
       }
       __syncthreads();  // buffer b is free for the load of run c + 2
     }
@@ -802,7 +818,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       // in 2D the hypertrig rows are (1, cos, sin, 0)
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        if (ixb + k >= ev.NX || iy >= ev.NY) continue;
+        if (ixb + k > x_hi || iy > y_hi) continue;
         const size_t is = (size_t)(ixb + k) * ev.NY + iy;
         const float s0 = stot[(5 * k + 0) * kThreads2D] + a0[k];
         const float s1 = stot[(5 * k + 1) * kThreads2D] + a12[k].x;
@@ -816,7 +832,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      if (ixb + k >= ev.NX || iy >= ev.NY) continue;
+      if (ixb + k > x_hi || iy > y_hi) continue;
       const float tot[5] = {stot[(5 * k + 0) * kThreads2D] + a0[k],
                             stot[(5 * k + 1) * kThreads2D] + a12[k].x,
                             stot[(5 * k + 2) * kThreads2D] + a12[k].y,
@@ -906,10 +922,14 @@ __device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const typename No
 // its 4 samples and, without baryons, keeps those 2 x 5 nodes in registers
 // while consecutive phi_p share the offset.  phi_p whose whole tile lands outside the grid are
 // skipped; runs inside it skip the in-grid test.  Moments: FP32 partial sums
-// over 16 phi_p folded into per-rapidity sums, then into T^{mu nu} / J^mu
-// with the rapidity factors (src/LandauMatch.cpp:76-143), all in
-// thread-private shared-memory slots.
-constexpr int kSlotsPerCell3D = 23;  // per cell: Q 0..5, T 6..15, Qb 16..18, J 19..22
+// over 16 phi_p folded, with the rapidity factors (src/LandauMatch.cpp:76-143),
+// straight into T^{mu nu} / J^mu in thread-private shared-memory slots (per
+// cell T 0..9, J 10..13): no per-rapidity slots, so that the shared memory
+// of two CTAs leaves L1 room for the tiles' node footprints.
+template <bool kB>
+constexpr int slots3d() {
+  return kB ? kSlots3DBaryon : kSlots3D;
+}
 
 // The phi_p loop of one rapidity node for one tile (nodes of eta pair efl).
 template <bool kB>
@@ -920,9 +940,11 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
                                              const typename Node3D<kB>::T* __restrict__ N,
                                              const PhiEntry3D* __restrict__ tab, float D, float et,
                                              float rf0, float rf1, float rb0, float rb1,
+                                             const RapEta* __restrict__ rp, float jw,
                                              float* __restrict__ sl) {
   using NodeT = typename Node3D<kB>::T;
   constexpr int K = kCellsPerThread;
+  constexpr int kS = slots3d<kB>();
   const int NX = ev.NX, NY = ev.NY, NP = ev.NPHI;
   // moment partial sums: (energy, baryon) pairs of the weights 1, cos, sin
   // and the energy-only cos^2, cos sin, sin^2
@@ -1080,20 +1102,31 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
         }
       }
       {
-        // second level of the two-level sum: per-rapidity sums in slots
+        // second level of the two-level sum: the partial sums times the rows
+        // of the hypertrig table (src/LandauMatch.cpp:46-55), the rapidity
+        // Jacobian and the profile norm (:101), into T^{mu nu} (and J^mu with
+        // the charge norm, :120-139)
+        const RapEta r = *rp;
+        const float cA = jw * r.A, cB = jw * r.B, cC = jw * r.C, cD = jw * r.Dt, cE = jw * r.E;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          float* q = sl + k * kSlotsPerCell3D * kThreads3D;
-          q[0 * kThreads3D] += a01[k].x;
-          q[1 * kThreads3D] += a1c[k].x;
-          q[2 * kThreads3D] += a1s[k].x;
-          q[3 * kThreads3D] += a3[k];
-          q[4 * kThreads3D] += a4[k];
-          q[5 * kThreads3D] += a5[k];
+          float* q = sl + k * kS * kThreads3D;
+          q[0 * kThreads3D] += a01[k].x * jw;
+          q[1 * kThreads3D] += a1c[k].x * cA;
+          q[2 * kThreads3D] += a1s[k].x * cA;
+          q[3 * kThreads3D] += a01[k].x * cD;
+          q[4 * kThreads3D] += a3[k] * cB;
+          q[5 * kThreads3D] += a4[k] * cB;
+          q[6 * kThreads3D] += a1c[k].x * cC;
+          q[7 * kThreads3D] += a5[k] * cB;
+          q[8 * kThreads3D] += a1s[k].x * cC;
+          q[9 * kThreads3D] += a01[k].x * cE;
           if (kB) {
-            q[16 * kThreads3D] += a01[k].y;
-            q[17 * kThreads3D] += a1c[k].y;
-            q[18 * kThreads3D] += a1s[k].y;
+            const float nb = ev.normB, bA = nb * r.A, bD = nb * r.Dt;
+            q[10 * kThreads3D] += a01[k].y * nb;
+            q[11 * kThreads3D] += a1c[k].y * bA;
+            q[12 * kThreads3D] += a1s[k].y * bA;
+            q[13 * kThreads3D] += a01[k].y * bD;
           }
           a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
           a3[k] = a4[k] = a5[k] = 0.0f;
@@ -1113,6 +1146,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
   extern __shared__ float slots3[];  // thread-private slots, [slot][thread]
   __shared__ int s_tile;
   constexpr int K = kCellsPerThread;
+  constexpr int kS = slots3d<kB>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* const sl = slots3 + threadIdx.x;
   auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
@@ -1142,7 +1176,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
       act[k] = (ix < NX) && (iy < NY);
     }
 #pragma unroll
-    for (int m = 0; m < K * kSlotsPerCell3D; ++m) S(m) = 0.0f;
+    for (int m = 0; m < K * kS; ++m) S(m) = 0.0f;
     const size_t plane = (size_t)NX * NY;
     for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
       const RapEta re = ev.re[ieta * NR + irap];
@@ -1150,44 +1184,19 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
       const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
       const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
       const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
+      // rapidity Jacobian (src/LandauMatch.cpp:101) times the profile norm
+      const float jw = ev.jac[irap] * ev.norm;
+      const RapEta* rp = ev.re + ieta * NR + irap;
       if constexpr (kB) {
         const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
         const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
         const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
         stream3d_rap<true>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
-                           re.efrac, rf0, rf1, rb0, rb1, sl);
+                           re.efrac, rf0, rf1, rb0, rb1, rp, jw, sl);
       } else {
         const float2* N = reinterpret_cast<const float2*>(ev.nodes3) + (size_t)re.efl * plane;
         stream3d_rap<false>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
-                            re.efrac, rf0, rf1, 0.f, 0.f, sl);
-      }
-      // rows of the hypertrig table (src/LandauMatch.cpp:46-55) times the
-      // rapidity Jacobian (src/LandauMatch.cpp:101) and the profile norm
-      const float jw = ev.jac[irap] * ev.norm;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int b = k * kSlotsPerCell3D;
-        const float S1 = S(b + 0) * jw, Sc = S(b + 1) * jw, Ss = S(b + 2) * jw;
-        const float Scc = S(b + 3) * jw, Scs = S(b + 4) * jw, Sss = S(b + 5) * jw;
-        S(b + 6) += S1;
-        S(b + 7) += Sc * re.A;
-        S(b + 8) += Ss * re.A;
-        S(b + 9) += S1 * re.Dt;
-        S(b + 10) += Scc * re.B;
-        S(b + 11) += Scs * re.B;
-        S(b + 12) += Sc * re.C;
-        S(b + 13) += Sss * re.B;
-        S(b + 14) += Ss * re.C;
-        S(b + 15) += S1 * re.E;
-        for (int m = 0; m < 6; ++m) S(b + m) = 0.0f;
-        if (baryon) {
-          const float B1 = S(b + 16) * ev.normB, Bc = S(b + 17) * ev.normB, Bs = S(b + 18) * ev.normB;
-          S(b + 19) += B1;
-          S(b + 20) += Bc * re.A;
-          S(b + 21) += Bs * re.A;
-          S(b + 22) += B1 * re.Dt;
-          for (int m = 16; m < 19; ++m) S(b + m) = 0.0f;
-        }
+                            re.efrac, rf0, rf1, 0.f, 0.f, rp, jw, sl);
       }
     }
     const float dphi = ev.d_phip;
@@ -1196,11 +1205,11 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     for (int k = 0; k < K; ++k) {
       if (!act[k]) continue;
       const size_t is = ((size_t)(ixb + k) * NY + iy) * NE + ieta;
-      const int b = k * kSlotsPerCell3D;
-      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = S(b + 6 + m) * dphi;  // (LandauMatch.cpp:105)
+      const int b = k * kS;
+      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = S(b + m) * dphi;  // (LandauMatch.cpp:105)
       if (baryon) {
         const float jf = ev.DRAP * dphi;  // (LandauMatch.cpp:140)
-        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = S(b + 19 + m) * jf;
+        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = S(b + 10 + m) * jf;
       }
     }
     __syncthreads();

@@ -136,14 +136,7 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
 
   // work lists (as the batch path builds them for one event)
   std::vector<Tile2D> tiles;
-  for (int a = 0; a < (NX + kTileX - 1) / kTileX; ++a)
-    for (int c = 0; c < (NY + kTileY - 1) / kTileY; ++c) {
-      const int x0 = a * kTileX, y0 = c * kTileY;
-      const int interior = (x0 + kTileX <= NX) && (y0 + kTileY <= NY) && (x0 + P.ox_min >= 2) &&
-                           (x0 + kTileX - 1 + P.ox_max <= NX - 3) && (y0 + P.oy_min >= 2) &&
-                           (y0 + kTileY - 1 + P.oy_max <= NY - 3);
-      tiles.push_back(Tile2D{0, x0, y0, interior});
-    }
+  tiles_2d(P, 0, tiles);
   std::vector<LineBlock> rows, cols;
   const bool strip = NX <= kMaxStrip && NY <= kMaxStrip;
   if (strip) {
@@ -198,7 +191,10 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   e.d_phip = P.d_phip;
   e.tab = reinterpret_cast<const PhiEntry2D*>(D + o_tab);
   e.chunks = reinterpret_cast<const Chunk2D*>(D + o_chunks);
-  e.nchunks = (int)P.chunks2.size();
+  for (int sh = 0; sh < kShapes2D; ++sh) {
+    e.choff[sh] = P.choff[sh];
+    e.nch[sh] = P.nch[sh];
+  }
   e.e_gev = d_e_gev;
   e.ax = reinterpret_cast<const AxisNode*>(D + o_axx) + kPadLo;
   e.ay = reinterpret_cast<const AxisNode*>(D + o_axy) + kPadLo;

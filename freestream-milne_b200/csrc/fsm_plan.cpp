@@ -160,8 +160,37 @@ float edep_dtau(const fsm_params& p, float numerator, float denominator) {
   return p.TAU_R * std::pow((e_T / p.E_R), p.ALPHA);
 }
 
+int y_tail_shape(int NY) {
+  const int r = NY % kTileY;
+  return r == 0 ? -1 : r <= 8 ? 2 : r <= 16 ? 1 : -1;
+}
+
+int x_tail_shape(int NX) {
+  const int r = NX % kTileX;
+  return r == 0 ? -1 : r <= 8 ? 4 : r <= 16 ? 3 : -1;
+}
+
+void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out) {
+  const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
+  const int ys = P.y_shape, xs = P.x_shape;
+  // the 32 x 32 region: whole tiles up to the narrow last strips, or over the
+  // whole grid (rounded up) where a last strip keeps 32 x 32 tiles
+  const int NXm = xs >= 0 ? NX - NX % kTileX : (NX + kTileX - 1) / kTileX * kTileX;
+  const int NYm = ys >= 0 ? NY - NY % kTileY : (NY + kTileY - 1) / kTileY * kTileY;
+  for (int x0 = 0; x0 < NXm; x0 += kTileX)
+    for (int y0 = 0; y0 < NYm; y0 += kTileY) out.push_back(Tile2D{ev, x0, y0, 0, NX, NY});
+  // the last y strip, x < NXr (up to the last x strip, when that has its own
+  // tiles): its last tile stores no cell of the x strip
+  const int NXr = xs >= 0 ? NXm : NX;
+  if (ys >= 0)
+    for (int x0 = 0; x0 < NXr; x0 += shape_tx(ys)) out.push_back(Tile2D{ev, x0, NYm, ys, NXr, NY});
+  // the last x strip over the whole y range (its corner with the y strip included)
+  if (xs >= 0)
+    for (int y0 = 0; y0 < NY; y0 += shape_ty(xs)) out.push_back(Tile2D{ev, NXm, y0, xs, NX, NY});
+}
+
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why, int window_budget, bool input_fm4) {
+                      std::string* why, int window_budget, bool input_fm4, bool tail_tiles) {
   EventPlan& E = *out;
   E = EventPlan();
   E.input_fm4 = input_fm4;
@@ -281,52 +310,69 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
                          (w.oy_near & 0xffff) != (E.tab2[k - 1].oy_near & 0xffff);
       if (moved) w.oy_near |= 1 << 18;
     }
-    // phi_p runs of at most kMaxRunPhi2D nodes whose staged window (tile +
-    // offset spread + 1-node margins) fits the window budget; consecutive
-    // nodes have neighbouring offsets.  A budget that cuts the circle into
-    // more than kMaxChunks2D runs is raised up to kMaxWindow2D (fewer, larger
-    // windows for long free-streaming distances).
+    // offset range over all phi_p
+    auto oy_of = [&](int k) { return (int)(short)(E.tab2[k].oy_near & 0xffff); };
+    E.ox_min = E.ox_max = E.tab2[0].ox;
+    E.oy_min = E.oy_max = oy_of(0);
+    for (int k = 1; k < NP; ++k) {
+      E.ox_min = std::min(E.ox_min, E.tab2[k].ox);
+      E.ox_max = std::max(E.ox_max, E.tab2[k].ox);
+      E.oy_min = std::min(E.oy_min, oy_of(k));
+      E.oy_max = std::max(E.oy_max, oy_of(k));
+    }
+    // phi_p runs, per tile shape the event uses, of at most kMaxRunPhi2D
+    // nodes whose staged window (tile + offset spread + 1-node margins) fits
+    // the window budget; consecutive nodes have neighbouring offsets.  A
+    // budget that cuts the circle into more than kMaxChunks2D runs is raised
+    // up to kMaxWindow2D (fewer, larger windows for long free-streaming
+    // distances).
     const int min_runs = (NP + kMaxRunPhi2D - 1) / kMaxRunPhi2D;
-    for (int budget = window_budget;; budget = budget * 3 / 2) {
-      auto win_bytes = [](int dox, int doy) {
-        return (size_t)(kTileX + dox + 3) * (size_t)(kTileY + doy + 3) * 16;
-      };
-      E.chunks2.clear();
-      E.box_elems = 0;
-      int p0 = 0;
-      auto oy_of = [&](int k) { return (int)(short)(E.tab2[k].oy_near & 0xffff); };
-      int lo_x = E.tab2[0].ox, hi_x = lo_x, lo_y = oy_of(0), hi_y = lo_y;
-      E.ox_min = E.ox_max = lo_x;
-      E.oy_min = E.oy_max = lo_y;
-      for (int k = 1; k <= NP; ++k) {
-        bool flush = (k == NP) || (k - p0 == kMaxRunPhi2D);
-        if (!flush) {
-          int nlx = std::min(lo_x, E.tab2[k].ox), nhx = std::max(hi_x, E.tab2[k].ox);
-          int nly = std::min(lo_y, oy_of(k)), nhy = std::max(hi_y, oy_of(k));
-          if (win_bytes(nhx - nlx, nhy - nly) > (size_t)budget) {
-            flush = true;
-          } else {
-            lo_x = nlx; hi_x = nhx; lo_y = nly; hi_y = nhy;
+    E.y_shape = tail_tiles ? y_tail_shape(E.p.DIM_Y) : -1;
+    E.x_shape = tail_tiles ? x_tail_shape(E.p.DIM_X) : -1;
+    E.chunks2.clear();
+    E.box_elems = 0;
+    for (int sh = 0; sh < kShapes2D; ++sh) {
+      E.choff[sh] = (int)E.chunks2.size();
+      E.nch[sh] = 0;
+      if (sh != 0 && sh != E.y_shape && sh != E.x_shape) continue;
+      const int TX = shape_tx(sh), TY = shape_ty(sh);
+      std::vector<Chunk2D> runs;
+      int box = 0;
+      for (int budget = window_budget;; budget = budget * 3 / 2) {
+        auto win_bytes = [&](int dox, int doy) {
+          return (size_t)(TX + dox + 3) * (size_t)(TY + doy + 3) * 16;
+        };
+        runs.clear();
+        box = 0;
+        int p0 = 0;
+        int lo_x = E.tab2[0].ox, hi_x = lo_x, lo_y = oy_of(0), hi_y = lo_y;
+        for (int k = 1; k <= NP; ++k) {
+          bool flush = (k == NP) || (k - p0 == kMaxRunPhi2D);
+          if (!flush) {
+            int nlx = std::min(lo_x, E.tab2[k].ox), nhx = std::max(hi_x, E.tab2[k].ox);
+            int nly = std::min(lo_y, oy_of(k)), nhy = std::max(hi_y, oy_of(k));
+            if (win_bytes(nhx - nlx, nhy - nly) > (size_t)budget) {
+              flush = true;
+            } else {
+              lo_x = nlx; hi_x = nhx; lo_y = nly; hi_y = nhy;
+            }
+          }
+          if (flush) {
+            runs.push_back(Chunk2D{p0, k, lo_x, lo_y, hi_x, hi_y});
+            box = std::max(box, (TX + (hi_x - lo_x) + 3) * (TY + (hi_y - lo_y) + 3));
+            if (k < NP) {
+              p0 = k;
+              lo_x = hi_x = E.tab2[k].ox;
+              lo_y = hi_y = oy_of(k);
+            }
           }
         }
-        if (flush) {
-          E.chunks2.push_back(Chunk2D{p0, k, lo_x, lo_y, hi_x, hi_y});
-          E.box_elems = std::max(E.box_elems, (kTileX + (hi_x - lo_x) + 3) * (kTileY + (hi_y - lo_y) + 3));
-          if (k < NP) {
-            p0 = k;
-            lo_x = hi_x = E.tab2[k].ox;
-            lo_y = hi_y = oy_of(k);
-          }
-        }
-        if (k < NP) {
-          E.ox_min = std::min(E.ox_min, E.tab2[k].ox);
-          E.ox_max = std::max(E.ox_max, E.tab2[k].ox);
-          E.oy_min = std::min(E.oy_min, oy_of(k));
-          E.oy_max = std::max(E.oy_max, oy_of(k));
-        }
+        const bool few = (int)runs.size() <= std::max(kMaxChunks2D, 2 * min_runs);
+        if (few || budget * 3 / 2 > kMaxWindow2D) break;
       }
-      const bool few = (int)E.chunks2.size() <= std::max(kMaxChunks2D, 2 * min_runs);
-      if (few || budget * 3 / 2 > kMaxWindow2D) break;
+      E.chunks2.insert(E.chunks2.end(), runs.begin(), runs.end());
+      E.nch[sh] = (int)runs.size();
+      E.box_elems = std::max(E.box_elems, box);
     }
     E.samples = (double)p.DIM * NP;
     E.ref_samples = (double)p.DIM * NR * NP;

@@ -36,7 +36,9 @@ struct EventPlan {
   float xmin = 0, ymin = 0, etamin = 0, xmax_i = 0, ymax_i = 0, d_phip = 0;
   std::vector<FSM_FLOAT2> cs;  // (cos, sin) of phi_p
   std::vector<PhiEntry2D> tab2;  // 2D stream table
-  std::vector<Chunk2D> chunks2;  // phi_p runs staged as one window each
+  std::vector<Chunk2D> chunks2;  // phi_p runs staged as one window each, shape by shape
+  int choff[kShapes2D] = {}, nch[kShapes2D] = {};  // runs of tile shape s: chunks2[choff[s]..]
+  int y_shape = -1, x_shape = -1;  // narrow tile shapes of the last y / x strip (-1: 32 x 32)
   int box_elems = 0;             // largest staged window (nodes) of one run
   int ox_min = 0, ox_max = 0, oy_min = 0, oy_max = 0;  // offset range over all phi_p
   // 2D spline axes
@@ -62,7 +64,18 @@ struct EventPlan {
 // stays within window_budget bytes.  Returns FSM_OK or an error with a message
 // in *why.
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,
-                      std::string* why, int window_budget = kWindowBudget2D, bool input_fm4 = false);
+                      std::string* why, int window_budget = kWindowBudget2D, bool input_fm4 = false,
+                      bool tail_tiles = true);
+
+// Narrow tile shape for the last, partial strip of a 2D grid along y (x):
+// 2 (1) when at most 8 (16) cells are left over, else -1 (32 x 32 tiles).
+int y_tail_shape(int NY);
+int x_tail_shape(int NX);
+// The output tiles of 2D event `ev` (of plan P): 32 x 32 tiles over the grid
+// minus its narrow last strips, tiles of the planned narrow shapes over those
+// strips (the x strip's including the corner).  Every cell is stored by one
+// tile.
+void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out);
 
 // Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
 // reference's float sums of eps^2 and eps over the converted profile

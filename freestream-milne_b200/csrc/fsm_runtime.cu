@@ -127,13 +127,15 @@ int tuning_bucket(const fsm_params& p) {
   return sc * 4 + hc;
 }
 
-void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk) {
+void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk, bool* tail) {
   *window = ctx->window_budget;
   *chunk = kPhiChunk;
+  *tail = true;
   if (p.DIM_ETA > 1) return;  // 3D events: the 3D kernel has no staged windows; chunk 16
   const fsm_tuning_bucket& t = ctx->buckets[tuning_bucket(p)];
   if (t.window_bytes > 0) *window = t.window_bytes;
   if (t.phi_chunk == 16 || t.phi_chunk == 32) *chunk = t.phi_chunk;
+  if (t.tile_shapes == FSM_TILES_SQUARE) *tail = false;
 }
 
 // Builds descriptors and uploads everything.  ext_in / ext_out (one event)
@@ -159,9 +161,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     // (many small events also pay: ~35 us of host planning each)
     parallel_for(n, (work > 2.0e5 || n >= 16) ? host_threads() : 1, [&](int i) {
       int window = 0, chunk = 0;
-      event_tuning(ctx, params[i], &window, &chunk);
+      bool tail = true;
+      event_tuning(ctx, params[i], &window, &chunk, &tail);
       st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window,
-                         mem && mem->input_fm4);
+                         mem && mem->input_fm4, tail);
       b->plans[i].phi_chunk = chunk;
     });
     for (int i = 0; i < n; ++i)
@@ -228,21 +231,15 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     std::stable_sort(order2.begin(), order2.end(), [&](int a, int c) {
       return b->plans[a].p.DIM_PHIP > b->plans[c].p.DIM_PHIP;
     });
+    std::vector<Tile2D> tt;
     for (int i : order2) {
-      const EventPlan& P = b->plans[i];
-      const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
-      int tx = (NX + kTileX - 1) / kTileX, ty = (NY + kTileY - 1) / kTileY;
-      for (int a = 0; a < tx; ++a)
-        for (int c = 0; c < ty; ++c) {
-          const int x0 = a * kTileX, y0 = c * kTileY;
-          // every sample of every cell lands at least one node inside the grid
-          // boundary, so neither the in-grid test nor its rounding matters
-          const int interior = (x0 + kTileX <= NX) && (y0 + kTileY <= NY) && (x0 + P.ox_min >= 2) &&
-                               (x0 + kTileX - 1 + P.ox_max <= NX - 3) && (y0 + P.oy_min >= 2) &&
-                               (y0 + kTileY - 1 + P.oy_max <= NY - 3);
-          tiles.push_back(Tile2D{b->ev2_of[i], x0, y0, interior});
-          if (b->evq_of[i] >= 0) tiles.push_back(Tile2D{b->evq_of[i], x0, y0, interior});
-        }
+      tt.clear();
+      tiles_2d(b->plans[i], b->ev2_of[i], tt);
+      for (const Tile2D& t : tt) {
+        tiles.push_back(t);
+        // the charge pass of a 2D baryon event: the same tiles
+        if (b->evq_of[i] >= 0) tiles.push_back(Tile2D{b->evq_of[i], t.x0, t.y0, t.shape, t.x1, t.y1});
+      }
     }
     for (int i = 0; i < n; ++i) {
       const EventPlan& P = b->plans[i];
@@ -523,7 +520,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.d_phip = P.d_phip;
       e.tab = reinterpret_cast<const PhiEntry2D*>(D + o.tab2);
       e.chunks = reinterpret_cast<const Chunk2D*>(D + o.chunks);
-      e.nchunks = (int)P.chunks2.size();
+      for (int sh = 0; sh < kShapes2D; ++sh) {
+        e.choff[sh] = P.choff[sh];
+        e.nch[sh] = P.nch[sh];
+      }
       b->box_cap2 = std::max(b->box_cap2, P.box_elems);
       e.e_gev = b->d_in_e[i];
       e.ax = reinterpret_cast<const AxisNode*>(D + o.axx) + kPadLo;
@@ -607,7 +607,9 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   b->cs_cap3 = (max_np3 + 1) & ~1;
   b->box_cap2 = (b->box_cap2 + 7) & ~7;  // float4 units, 128-byte multiple
   b->smem2 = stream2d_smem(b->box_cap2);
-  b->smem3 = (size_t)kThreads3D * kCellsPerThread * 23 * 4;  // thread-private moment slots
+  // thread-private moment slots of the two 3D kernels
+  b->smem3 = (size_t)kThreads3D * kCellsPerThread * kSlots3D * 4;
+  b->smem3b = (size_t)kThreads3D * kCellsPerThread * kSlots3DBaryon * 4;
   b->smem_rows = prep_rows_smem(b->ny_cap2);
   b->smem_strip = prep_strip_smem(b->strip_cap2);
   // the kernels index their dynamic shared memory by these capacities
@@ -684,12 +686,12 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     b->grid3 = std::max(1, std::min(b->ntiles3 - b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
   }
   if (b->ntiles3b) {
-    fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_baryon_kernel, ctx->device, b->smem3,
+    fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_baryon_kernel, ctx->device, b->smem3b,
                                     &g_smem3b[ctx->device & 63]);
     if (ss != FSM_OK) return ss;
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_baryon_kernel,
-                                                               kThreads3D, b->smem3));
+                                                               kThreads3D, b->smem3b));
     b->grid3b = std::max(1, std::min(b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
   }
   if (mem && mem->dev)
@@ -735,7 +737,7 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
                                                                b->box_cap2, b->d_ctr, b->d_err,
                                                                b->wait_polls);
   if (b->ntiles3b)
-    fsm_stream3d_baryon_kernel<<<b->grid3b, kThreads3D, b->smem3, s>>>(b->d_ev3, b->d_tiles3,
+    fsm_stream3d_baryon_kernel<<<b->grid3b, kThreads3D, b->smem3b, s>>>(b->d_ev3, b->d_tiles3,
                                                                        b->ntiles3b, b->d_ctr);
   if (b->ntiles3 > b->ntiles3b)
     fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(
@@ -959,8 +961,9 @@ fsm_status run_event_host(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
     EventPlan P;
     std::string why;
     int window = 0, chunk = 0;
-    event_tuning(ctx, *p, &window, &chunk);
-    s = plan_event(*p, e_gev, &P, &why, window, fm4);
+    bool tail = true;
+    event_tuning(ctx, *p, &window, &chunk, &tail);
+    s = plan_event(*p, e_gev, &P, &why, window, fm4, tail);
     if (s != FSM_OK) {
       set_last_error(why);
       return s;
@@ -1057,8 +1060,9 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
   EventPlan P;
   std::string why;
   int window = 0, chunk = 0;
-  event_tuning(ctx, *p, &window, &chunk);
-  fsm_status s = plan_event(*p, nullptr, &P, &why, window);
+  bool tail = true;
+  event_tuning(ctx, *p, &window, &chunk, &tail);
+  fsm_status s = plan_event(*p, nullptr, &P, &why, window, false, tail);
   if (s != FSM_OK) {
     set_last_error(why);
     return s;
@@ -1570,10 +1574,12 @@ extern "C" fsm_status fsm_ctx_set_tuning_buckets(fsm_ctx* ctx, const fsm_tuning_
     const fsm_tuning_bucket& t = table[k];
     const bool ok = (t.window_bytes == 0 || (t.window_bytes >= (kTileX + 3) * (kTileY + 3) * 16 &&
                                              t.window_bytes <= 96 * 1024)) &&
-                    (t.phi_chunk == 0 || t.phi_chunk == 16 || t.phi_chunk == 32);
+                    (t.phi_chunk == 0 || t.phi_chunk == 16 || t.phi_chunk == 32) &&
+                    (t.tile_shapes >= FSM_TILES_DEFAULT && t.tile_shapes <= FSM_TILES_SQUARE);
     if (!ok) {
       set_last_error("fsm_ctx_set_tuning_buckets: bucket " + std::to_string(k) +
-                     " has a window outside [4900, 98304] bytes or a chunk other than 16 or 32");
+                     " has a window outside [4900, 98304] bytes, a chunk other than 16 or 32"
+                     " or an unknown tile_shapes value");
       return FSM_ERR_INVALID_ARG;
     }
   }
@@ -1595,6 +1601,7 @@ extern "C" fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params
   // against FP64 on a 201^2 event (1.05e-4); callers may still set it.
   static const int cand_kb[] = {24, 28, 32, 36, 40};
   static const int cand_chunk[] = {16};
+  static const int cand_tiles[] = {FSM_TILES_TAIL, FSM_TILES_SQUARE};
   std::vector<int> members[FSM_TUNING_BUCKETS];
   for (int i = 0; i < n; ++i)
     if (params[i].DIM_ETA == 1) {
@@ -1618,10 +1625,17 @@ extern "C" fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params
       if (host_e) he[j] = host_e[members[k][j]];
       if (host_nB) hb[j] = host_nB[members[k][j]];
     }
+    // narrow tail tiles are a candidate only where some event has a partial
+    // last strip they would cover
+    bool any_tail = false;
+    for (int j = 0; j < m; ++j)
+      any_tail = any_tail || y_tail_shape(ps[j].DIM_Y) >= 0 || x_tail_shape(ps[j].DIM_X) >= 0;
     fsm_tuning_bucket best{};
     for (int kb : cand_kb)
-      for (int chunk : cand_chunk) {
-        ctx->buckets[k] = fsm_tuning_bucket{kb * 1024, chunk, 0.0, 0};
+      for (int chunk : cand_chunk)
+        for (int tiles : cand_tiles) {
+        if (tiles == FSM_TILES_SQUARE && !any_tail) continue;
+        ctx->buckets[k] = fsm_tuning_bucket{kb * 1024, chunk, 0.0, 0, tiles};
         fsm_batch* b = nullptr;
         fsm_status s = batch_build(ctx, m, ps.data(), host_e ? he.data() : nullptr, nullptr, nullptr,
                                    nullptr, &b);
@@ -1653,8 +1667,8 @@ extern "C" fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params
           break;
         }
         ms /= 3.0;
-        if (best.ms == 0.0 || ms < best.ms) best = fsm_tuning_bucket{kb * 1024, chunk, ms, m};
-      }
+        if (best.ms == 0.0 || ms < best.ms) best = fsm_tuning_bucket{kb * 1024, chunk, ms, m, tiles};
+        }
     result[k] = best;
   }
   cudaEventDestroy(e0);
@@ -1672,11 +1686,12 @@ extern "C" fsm_status fsm_tuning_save(fsm_ctx* ctx, const char* path) {
     set_last_error(std::string("fsm_tuning_save: cannot open ") + path);
     return FSM_ERR_FILE;
   }
-  std::fprintf(f, "# bucket window_bytes phi_chunk ms events\n");
+  std::fprintf(f, "# bucket window_bytes phi_chunk ms events tile_shapes\n");
   for (int k = 0; k < FSM_TUNING_BUCKETS; ++k) {
     const fsm_tuning_bucket& t = ctx->buckets[k];
     if (t.window_bytes > 0)
-      std::fprintf(f, "%d %d %d %.6f %d\n", k, t.window_bytes, t.phi_chunk, t.ms, t.events);
+      std::fprintf(f, "%d %d %d %.6f %d %d\n", k, t.window_bytes, t.phi_chunk, t.ms, t.events,
+                   t.tile_shapes);
   }
   return std::fclose(f) == 0 ? FSM_OK : FSM_ERR_FILE;
 }
@@ -1693,15 +1708,16 @@ extern "C" fsm_status fsm_tuning_load(fsm_ctx* ctx, const char* path) {
   fsm_status st = FSM_OK;
   while (std::fgets(line, sizeof(line), f)) {
     if (line[0] == '#' || line[0] == '\n') continue;
-    int k = -1, w = 0, c = 0, ev = 0;
+    int k = -1, w = 0, c = 0, ev = 0, tiles = FSM_TILES_DEFAULT;
     double ms = 0.0;
-    if (std::sscanf(line, "%d %d %d %lf %d", &k, &w, &c, &ms, &ev) != 5 || k < 0 ||
-        k >= FSM_TUNING_BUCKETS) {
+    // tables written before the tile_shapes column read as the default shapes
+    const int got = std::sscanf(line, "%d %d %d %lf %d %d", &k, &w, &c, &ms, &ev, &tiles);
+    if (got < 5 || k < 0 || k >= FSM_TUNING_BUCKETS) {
       set_last_error(std::string("fsm_tuning_load: malformed line: ") + line);
       st = FSM_ERR_INVALID_ARG;
       break;
     }
-    table[k] = fsm_tuning_bucket{w, c, ms, ev};
+    table[k] = fsm_tuning_bucket{w, c, ms, ev, tiles};
   }
   std::fclose(f);
   if (st != FSM_OK) return st;

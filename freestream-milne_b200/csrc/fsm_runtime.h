@@ -133,7 +133,7 @@ struct fsm_batch {
   int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, ntiles3 = 0, nbl = 0;
   int ntiles3b = 0;  // the first ntiles3b 3D tiles belong to events with baryon charge
   int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
-  size_t smem2 = 0, smem3 = 0, smem_rows = 0, smem_strip = 0;
+  size_t smem2 = 0, smem3 = 0, smem3b = 0, smem_rows = 0, smem_strip = 0;
   int grid2 = 0, grid3 = 0, grid3b = 0;
   int wait_polls = fsm::kWaitPolls;  // polls of one bounded wait in the stream kernel
   double samples = 0;
@@ -194,7 +194,7 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing);
 // Tuning bucket of a 2D event (grid side class x shift-length class) and the
 // staged-window bound / phi_p chunk the context's tuning gives an event.
 int tuning_bucket(const fsm_params& p);
-void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk);
+void event_tuning(const fsm_ctx* ctx, const fsm_params& p, int* window, int* chunk, bool* tail);
 // Raises (never lowers) a kernel's dynamic shared-memory limit: the limit is a
 // process-wide attribute other launches (and captured graphs) rely on.
 // `slot` records the largest value set so far for that kernel on `device`;

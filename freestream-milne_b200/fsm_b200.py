@@ -65,10 +65,11 @@ class Energy(ctypes.Structure):
 
 class TuningBucket(ctypes.Structure):
     _fields_ = [("window_bytes", ctypes.c_int), ("phi_chunk", ctypes.c_int), ("ms", ctypes.c_double),
-                ("events", ctypes.c_int)]
+                ("events", ctypes.c_int), ("tile_shapes", ctypes.c_int)]
 
 
 TUNING_BUCKETS = 16
+TILES_DEFAULT, TILES_TAIL, TILES_SQUARE = 0, 1, 2  # FSM_TILES_*
 
 
 class ServerOpts(ctypes.Structure):
@@ -335,8 +336,9 @@ class Context:
         check(lib().fsm_ctx_set_wait_limit(self.h, int(polls)), "fsm_ctx_set_wait_limit")
 
     def autotune_buckets(self, params_list, inputs=None):
-        """Per-bucket tuning (window, phi_p chunk) on these events; returns the
-        16 bucket entries as dicts (window_bytes 0: bucket not tuned)."""
+        """Per-bucket tuning (window, phi_p chunk, tile shapes) on these events;
+        returns the 16 bucket entries as dicts (window_bytes 0: bucket not
+        tuned)."""
         n = len(params_list)
         arr = (Params * n)(*params_list)
         keep = []
@@ -358,7 +360,8 @@ class Context:
 
     def set_tuning_buckets(self, table):
         arr = (TuningBucket * TUNING_BUCKETS)(*[TuningBucket(t["window_bytes"], t["phi_chunk"],
-                                                             t.get("ms", 0.0), t.get("events", 0))
+                                                             t.get("ms", 0.0), t.get("events", 0),
+                                                             t.get("tile_shapes", TILES_DEFAULT))
                                                 for t in table])
         check(lib().fsm_ctx_set_tuning_buckets(self.h, arr), "fsm_ctx_set_tuning_buckets")
 

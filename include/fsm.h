@@ -296,23 +296,34 @@ fsm_status fsm_ctx_set_tuning(fsm_ctx* ctx, const fsm_tuning* t);
  * side_class * 4 + shift_class, side_class from max(DIM_X, DIM_Y) (0: < 128,
  * 1: < 192, 2: < 256, 3: larger) and shift_class from the shift length in
  * cells DTAU / min(DX, DY) (0: < 8, 1: < 16, 2: < 24, 3: larger).  Per bucket
- * the 2D stream kernel's staged-window bound and its phi_p chunk (phi_p per
+ * the 2D stream kernel's staged-window bound, its phi_p chunk (phi_p per
  * FP32 partial sum of the two-level moment sum: 16, or 32 -- about 2 % faster
  * and with a larger summation error: e against FP64 reached 1.05e-4 on a 201^2
- * event, so the tuner keeps 16).  fsm_autotune_buckets times, for every bucket
- * the given events fall in, the launch sequence of those events (at most 64
- * of them) for windows of 24-40 KB (larger windows would lower the occupancy
- * of every batch holding such an event), keeps the fastest per bucket for ctx
- * and writes the FSM_TUNING_BUCKETS entries (window_bytes 0 for buckets
- * without events: they keep the context's window and chunk 16).  The table
- * can be stored and restored as text with fsm_tuning_save / fsm_tuning_load
- * (one "bucket window_bytes phi_chunk ms events" line per tuned bucket). */
+ * event, so the tuner keeps 16) and its output tile shapes: 32 x 32 tiles
+ * everywhere, or narrow tiles (64 x 16, 128 x 8 along a last partial y strip
+ * of at most 16 / 8 cells; 16 x 64, 8 x 128 along such an x strip) so that
+ * fewer lanes and warps run past the grid edge.  fsm_autotune_buckets times,
+ * for every bucket the given events fall in, the launch sequence of those
+ * events (at most 64 of them) for windows of 24-40 KB (larger windows would
+ * lower the occupancy of every batch holding such an event) with and without
+ * the narrow tiles, keeps the fastest per bucket for ctx and writes the
+ * FSM_TUNING_BUCKETS entries (window_bytes 0 for buckets without events: they
+ * keep the context's window, chunk 16 and narrow tail tiles).  The table can
+ * be stored and restored as text with fsm_tuning_save / fsm_tuning_load (one
+ * "bucket window_bytes phi_chunk ms events tile_shapes" line per tuned
+ * bucket).  Results do not depend on the window or the tile shapes. */
 #define FSM_TUNING_BUCKETS 16
+enum {
+  FSM_TILES_DEFAULT = 0, /* narrow tiles on partial last strips              */
+  FSM_TILES_TAIL = 1,    /* the same, chosen by the tuner                    */
+  FSM_TILES_SQUARE = 2   /* 32 x 32 tiles only                               */
+};
 typedef struct fsm_tuning_bucket {
   int window_bytes;  /* staged window bound (0: the context's)               */
   int phi_chunk;     /* 16 or 32 (0: 16)                                       */
   double ms;         /* measured launch-sequence time of the bucket's events   */
   int events;        /* events the measurement used                            */
+  int tile_shapes;   /* FSM_TILES_*                                            */
 } fsm_tuning_bucket;
 fsm_status fsm_autotune_buckets(fsm_ctx* ctx, int n, const fsm_params* params,
                                 const float* const* host_e, const float* const* host_nB,

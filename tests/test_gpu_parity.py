@@ -446,10 +446,11 @@ def test_autotune_keeps_results():
 
 def test_bucket_autotuner_choices_keep_results(tmp_path):
     """Every choice the per-bucket autotuner can make (windows of 24-40 KB,
-    the 16-phi_p chunk) gives the untuned results bit for bit; the 32-phi_p
-    chunk a caller may set (a different summation order, not chosen by the
-    tuner) passes the parity checks against the reference's float output and
-    T and Pi against FP64.  The tuned table survives a save / load round trip."""
+    the 16-phi_p chunk, narrow tail tiles or 32 x 32 tiles only) gives the
+    untuned results bit for bit; the 32-phi_p chunk a caller may set (a
+    different summation order, not chosen by the tuner) passes the parity
+    checks against the reference's float output and T and Pi against FP64.
+    The tuned table survives a save / load round trip."""
     evs = [W.lumpy2d(seed=50, side=101, dx=0.1, nphip=64, dtau=0.4, eos=1, radius=3.0),   # 0, 0
            W.lumpy2d(seed=51, side=151, dx=0.08, nphip=100, dtau=1.0, eos=2, radius=4.0),  # 1, 1
            W.lumpy2d(seed=52, side=201, dx=0.05, nphip=64, dtau=1.0, eos=1, radius=4.0)]   # 2, 2
@@ -465,20 +466,23 @@ def test_bucket_autotuner_choices_keep_results(tmp_path):
             if t["window_bytes"]:
                 assert 24 * 1024 <= t["window_bytes"] <= 40 * 1024
                 assert t["phi_chunk"] == 16 and t["ms"] > 0 and t["events"] == 1
+                assert t["tile_shapes"] in (F.TILES_TAIL, F.TILES_SQUARE)
         path = tmp_path / "tuning.txt"
         c.save_tuning(path)
         c2 = F.Context(0)
         c2.load_tuning(path)
         for window in (24 * 1024, 28 * 1024, 32 * 1024, 36 * 1024, 40 * 1024):
-            for chunk in (16, 32):
+            for chunk, tiles in ((16, F.TILES_TAIL), (16, F.TILES_SQUARE), (32, F.TILES_TAIL)):
                 if chunk == 32 and window != 40 * 1024:
                     continue
-                c2.set_tuning_buckets([{"window_bytes": window, "phi_chunk": chunk}] * 16)
+                c2.set_tuning_buckets([{"window_bytes": window, "phi_chunk": chunk,
+                                        "tile_shapes": tiles}] * 16)
                 for (p, e, _), r in zip(evs, ref):
                     got = c2.run_event(p, e)
                     if chunk == 16:
                         for name in ("T", "e", "u", "pi"):
-                            np.testing.assert_array_equal(got[name], r[name], err_msg=f"{window} {name}")
+                            np.testing.assert_array_equal(got[name], r[name],
+                                                          err_msg=f"{window} {tiles} {name}")
                     else:
                         o = _oracle(p, e)
                         o64 = _oracle(p, e, fp64=2)

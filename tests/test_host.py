@@ -128,6 +128,50 @@ def test_parallel_planning_matches_serial():
         assert d[0] == d[1] == d[2], (p.DIM_ETA, p.DIM_RAP, d)
 
 
+SHAPE_TX = {0: 32, 1: 64, 2: 128, 3: 16, 4: 8}
+SHAPE_TY = {0: 32, 1: 16, 2: 8, 3: 64, 4: 128}
+
+
+def test_tiles_cover_every_cell_once():
+    """The 2D tiling -- 32 x 32 tiles plus the narrow shapes over partial last
+    strips -- covers every cell of the grid exactly once, plans runs for every
+    shape it uses, keeps each run's staged window inside the kernel's largest,
+    and needs no more tiles (each 1024 cells of work) than 32 x 32 tiles alone."""
+    import numpy as np
+    import workloads as W
+    L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
+    L.fsm_hosttest_tiles.argtypes = [ctypes.POINTER(F.Params), ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    cap = 4096
+    buf = np.zeros(5 * cap, np.int32)
+    nch = np.zeros(5, np.int32)
+    box = ctypes.c_int()
+    sides = [(5, 7), (9, 40), (31, 33), (32, 32), (41, 41), (45, 41), (101, 101),
+             (151, 151), (201, 261), (301, 301), (100, 900), (263, 17), (8, 300)]
+    for nx, ny in sides:
+        p, _, _ = W.lumpy2d(seed=3, side=41, dx=0.08, nphip=64, dtau=0.9, eos=1, radius=1.0)
+        p.DIM_X, p.DIM_Y = nx, ny
+        W.derive(p)
+        slots = {}
+        for tail in (1, 0):
+            n = L.fsm_hosttest_tiles(ctypes.byref(p), tail, 32768, buf.ctypes.data, cap,
+                                     nch.ctypes.data, ctypes.byref(box))
+            assert 0 < n <= cap, (nx, ny, n)
+            cover = np.zeros((nx, ny), np.int32)
+            t = buf[:5 * n].reshape(n, 5)
+            for x0, y0, sh, x1, y1 in t:
+                tx, ty = SHAPE_TX[int(sh)], SHAPE_TY[int(sh)]
+                assert x0 < x1 <= nx and y0 < y1 <= ny, (nx, ny, x0, y0, sh, x1, y1)
+                cover[x0:min(x0 + tx, x1), y0:min(y0 + ty, y1)] += 1  # the cells the tile stores
+                assert nch[sh] > 0, (nx, ny, sh)
+            assert (cover == 1).all(), (nx, ny, tail, int(cover.min()), int(cover.max()))
+            if not tail:
+                assert set(t[:, 2].tolist()) == {0}
+            assert box.value * 16 <= 96 * 1024
+            slots[tail] = n * 1024
+        assert slots[1] <= slots[0], (nx, ny, slots)
+
+
 def _host_landau():
     L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
     L.fsm_hosttest_landau_cell.argtypes = ([ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 +
