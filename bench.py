@@ -38,6 +38,24 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
 FLOPS_PER_SAMPLE_3D_BARYON = 75  # shift 5 + 2 trilinear x 21 + 14 moments x 2
+# algorithmic DRAM bytes per cell of the 2D prep and Landau kernels: prep reads
+# the profile (4 B), writes and re-reads F and its y-slopes (8 + 8 B) and
+# writes the node array (16 B); Landau reads the 6 non-zero T components of a
+# boost-invariant event (24 B) and writes e, P, Pi, u, pi (68 B)
+PREP_BYTES_PER_CELL_2D = 36
+LANDAU_BYTES_PER_CELL_2D = 92
+
+
+def _hbm_gbs():
+    """Measured copy bandwidth of this pool's B200s (GB/s), else the earlier
+    measurement of 6650 GB/s."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
+HBM_GBS = _hbm_gbs()
 # DRAM bytes per cell x phi_p sample of fsm_stream2d_kernel: (88.9 MB read +
 # 167.7 MB written) / 713.26 M samples, from one ncu capture of the launch on
 # the first 128 events of this workload (a full 512-event launch is above the
@@ -215,6 +233,20 @@ def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2):
             "budget": {"hbm_bytes": budget["hbm_budget"], "pinned_host_bytes": budget["host_budget"]}}
 
 
+def other_kernels(tm, steps, cells):
+    """The prep and Landau kernels against the measured HBM copy bandwidth
+    (their algorithmic bytes per cell over their CUDA-event time); both are
+    bound by FP64 latency, not by DRAM, so the fractions stay well below 1."""
+    out = {}
+    for name, per_cell in (("prep", PREP_BYTES_PER_CELL_2D), ("landau", LANDAU_BYTES_PER_CELL_2D)):
+        ms = tm[f"{name}_ms"] / steps
+        gbs = cells * per_cell / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "cells": cells, "bytes_per_cell": per_cell, "achieved_gbs": gbs,
+                     "peak_gbs": HBM_GBS, "frac": gbs / HBM_GBS, "bound": "fp64 latency",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy)"}
+    return out
+
+
 def issue_peak(torch, device, clocks):
     """FP32 FMA issue peak in TFLOP/s: SMs x 128 FP32 lanes x 2 FLOP x the
     maximum SM clock seen (nominal 148 x 128 x 2 x 1.965 GHz = 74.4)."""
@@ -372,6 +404,7 @@ def main():
                         f"{tiles_name[t['tile_shapes']]}"
                      for k, t in enumerate(buckets) if t["window_bytes"]}
     batch = F.Batch(ctx, params)
+    cells_per_step = sum(p.DIM_X * p.DIM_Y for p in params)
     n = len(events)
     # host cost of a fresh event set: planning (tables, runs, work lists),
     # the batch's one device allocation and the upload of its tables
@@ -558,6 +591,7 @@ def main():
             "kernel_ms_per_step": {"prep": tm["prep_ms"] / args.steps,
                                    "stream": tm["stream_ms"] / args.steps,
                                    "landau": tm["landau_ms"] / args.steps},
+            "other_kernels": other_kernels(tm, args.steps, cells_per_step),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "events/s", "h2d_bytes_per_step": batch.in_bytes,
                     "d2h_bytes_per_step": d2h_bytes, "d2h_fields": e2e_groups,

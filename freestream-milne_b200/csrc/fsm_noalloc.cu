@@ -135,8 +135,10 @@ extern "C" fsm_status fsm_run_event_2d_noalloc(const fsm_params* p, const float*
   const int NX = P.p.DIM_X, NY = P.p.DIM_Y, DIM = P.DIM;
 
   // work lists (as the batch path builds them for one event)
+  // one event of at most kNoAllocMaxCells cells has fewer 32 x 32 tiles than
+  // the GPU has SMs: square tiles (see tiles_2d)
   std::vector<Tile2D> tiles;
-  tiles_2d(P, 0, tiles);
+  tiles_2d(P, 0, tiles, true);
   std::vector<LineBlock> rows, cols;
   const bool strip = NX <= kMaxStrip && NY <= kMaxStrip;
   if (strip) {

@@ -170,9 +170,9 @@ int x_tail_shape(int NX) {
   return r == 0 ? -1 : r <= 8 ? 4 : r <= 16 ? 3 : -1;
 }
 
-void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out) {
+void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out, bool square) {
   const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
-  const int ys = P.y_shape, xs = P.x_shape;
+  const int ys = square ? -1 : P.y_shape, xs = square ? -1 : P.x_shape;
   // the 32 x 32 region: whole tiles up to the narrow last strips, or over the
   // whole grid (rounded up) where a last strip keeps 32 x 32 tiles
   const int NXm = xs >= 0 ? NX - NX % kTileX : (NX + kTileX - 1) / kTileX * kTileX;

@@ -75,7 +75,9 @@ int x_tail_shape(int NX);
 // minus its narrow last strips, tiles of the planned narrow shapes over those
 // strips (the x strip's including the corner).  Every cell is stored by one
 // tile.
-void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out);
+// square: 32 x 32 tiles only (for launches too small to fill the GPU, where
+// the narrow tiles' longer staging would lengthen the slowest tile).
+void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out, bool square = false);
 
 // Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
 // reference's float sums of eps^2 and eps over the converted profile

@@ -231,10 +231,21 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     std::stable_sort(order2.begin(), order2.end(), [&](int a, int c) {
       return b->plans[a].p.DIM_PHIP > b->plans[c].p.DIM_PHIP;
     });
+    // narrow tiles on the partial last strips pay where the launch has work
+    // for every SM; a launch with fewer 32 x 32 tiles than two per SM (one
+    // small event) is bound by its slowest tile, which narrow tiles (taller
+    // staged windows, more runs) would lengthen
+    long long sq = 0;
+    for (int i : order2) {
+      const EventPlan& P = b->plans[i];
+      sq += (long long)((P.p.DIM_X + kTileX - 1) / kTileX) * ((P.p.DIM_Y + kTileY - 1) / kTileY) *
+            (b->evq_of[i] >= 0 ? 2 : 1);
+    }
+    const bool square = sq < 2LL * ctx->num_sms;
     std::vector<Tile2D> tt;
     for (int i : order2) {
       tt.clear();
-      tiles_2d(b->plans[i], b->ev2_of[i], tt);
+      tiles_2d(b->plans[i], b->ev2_of[i], tt, square);
       for (const Tile2D& t : tt) {
         tiles.push_back(t);
         // the charge pass of a 2D baryon event: the same tiles
