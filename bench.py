@@ -164,7 +164,7 @@ def cpu_baseline(events, nthreads, budget_s=20.0):
     return done / dt, kind, f"first {done} events of the workload, {nthreads} OpenMP threads, {dt:.1f} s"
 
 
-def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2):
+def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2, opts=None):
     """Request stream (by default 80 % 2D of sides 101-301, 20 % 3D of 131^2 x
     {25, 51} with 21/31/41 rapidities; frac3d=0: boost-invariant requests only)
     through the continuous-batching server: a burst measures capacity, then
@@ -175,7 +175,11 @@ def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2):
     gaps = [reqs[0][0]] + [reqs[k][0] - reqs[k - 1][0] for k in range(1, len(reqs))]
     events = [ev for _, ev in reqs]
     hydro = ["e", "P", "Pi", "u", "pi", "nB", "V"]  # the fields the reference hands to hydro
-    budget = dict(hbm_budget=48 << 30, host_budget=8 << 30, streams=2, outputs=hydro)
+    # 4 streams (waves overlap host planning, copies and kernels; measured
+    # burst capacity 916 / 1180 / 1400 events/s with 2 / 3 / 4) and one more
+    # reserved for boost-invariant waves
+    budget = dict(hbm_budget=48 << 30, host_budget=8 << 30, streams=4, stream_2d=True, outputs=hydro)
+    budget.update(opts or {})
 
     def run(rate_hz):
         srv = F.Server(local, **budget)

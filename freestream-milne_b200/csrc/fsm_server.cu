@@ -141,6 +141,7 @@ struct fsm_server {
   Pool dpool, hpool;
   std::vector<cudaStream_t> streams;
   std::vector<Wave*> slot_wave;  // wave in flight per stream, or nullptr
+  int slot_2d = -1;              // the stream reserved for boost-invariant waves, or -1
   std::mutex mu;
   std::condition_variable cv;       // scheduler wake-ups
   std::condition_variable cv_done;  // pollers
@@ -311,6 +312,16 @@ void wave_retire(fsm_server* S, Wave* w) {
 // (mu held on entry and exit; released while planning).  Returns false when
 // nothing could be admitted for lack of memory.
 constexpr int kBacklogMix = 8;  // queued requests above which waves mix event kinds
+// 3D events per wave at most: one 131^2 x 51 event already fills the GPU, so
+// batching more of them gains no kernel efficiency, while every one added
+// delays the results of the others by its kernels and its output copy
+constexpr int kMax3DPerWave = 2;
+
+bool queue_has_2d(const fsm_server* S) {
+  for (const Request* r : S->queue)
+    if (r->p.DIM_ETA == 1) return true;
+  return false;
+}
 
 bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
   const int cap = S->opts.max_wave_events;
@@ -318,11 +329,16 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
   // With a short queue a wave holds requests of one kind, that of the oldest
   // one (boost-invariant or 3D), in arrival order: a 2D request then does not
   // wait for the milliseconds of a 3D event sharing its wave.  Under a backlog
-  // waves take the queue in order, mixed, for throughput.
-  const bool kind3d = S->queue.front()->p.DIM_ETA > 1;
-  const bool mixed = (int)S->queue.size() > kBacklogMix;
+  // waves take the queue in order, mixed, for throughput.  The stream reserved
+  // for boost-invariant waves takes 2D requests only.
+  const bool only2d = slot == S->slot_2d;
+  const bool kind3d = !only2d && S->queue.front()->p.DIM_ETA > 1;
+  const bool mixed = !only2d && (int)S->queue.size() > kBacklogMix;
+  int n3d = 0;
   for (auto it = S->queue.begin(); it != S->queue.end() && (int)take.size() < cap;) {
-    if (mixed || ((*it)->p.DIM_ETA > 1) == kind3d) {
+    const bool is3d = (*it)->p.DIM_ETA > 1;
+    if ((mixed || is3d == kind3d) && !(is3d && n3d >= kMax3DPerWave)) {
+      n3d += is3d ? 1 : 0;
       take.push_back(*it);
       it = S->queue.erase(it);
     } else {
@@ -484,6 +500,7 @@ void scheduler(fsm_server* S) {
     if (!S->mem_wait) {
       for (size_t k = 0; k < S->slot_wave.size() && !S->queue.empty(); ++k) {
         if (S->slot_wave[k]) continue;
+        if ((int)k == S->slot_2d && !queue_has_2d(S)) continue;
         const unsigned long long g0 = S->wake_gen;
         if (!wave_launch(S, lk, (int)k)) {
           // wait for memory only if none was freed while the wave was planned
@@ -509,7 +526,7 @@ extern "C" fsm_status fsm_server_start(fsm_server** out, const fsm_server_opts* 
   if (S->opts.hbm_budget_bytes == 0) S->opts.hbm_budget_bytes = (size_t)8 << 30;
   if (S->opts.host_budget_bytes == 0) S->opts.host_budget_bytes = (size_t)2 << 30;
   if (S->opts.max_wave_events <= 0) S->opts.max_wave_events = 512;
-  if (S->opts.streams <= 0) S->opts.streams = 2;
+  if (S->opts.streams <= 0) S->opts.streams = 4;
   if (S->opts.output_mask == 0) S->opts.output_mask = FSM_OUT_ALL;
   fsm_ctx_opts co{S->opts.device, 0};
   fsm_status st = fsm_ctx_create(&S->ctx, &co);
@@ -525,9 +542,10 @@ extern "C" fsm_status fsm_server_start(fsm_server** out, const fsm_server_opts* 
   }
   S->dpool.reset(S->d_pool, S->opts.hbm_budget_bytes);
   S->hpool.reset(S->h_pool, S->opts.host_budget_bytes);
-  S->streams.resize(S->opts.streams);
+  S->streams.resize(S->opts.streams + (S->opts.stream_2d ? 1 : 0));
+  if (S->opts.stream_2d) S->slot_2d = S->opts.streams;
   for (auto& s : S->streams) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-  S->slot_wave.assign(S->opts.streams, nullptr);
+  S->slot_wave.assign(S->streams.size(), nullptr);
   fsm_server* raw = S.get();
   S->th = std::thread(scheduler, raw);
   *out = S.release();

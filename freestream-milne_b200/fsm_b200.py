@@ -75,7 +75,7 @@ TILES_DEFAULT, TILES_TAIL, TILES_SQUARE = 0, 1, 2  # FSM_TILES_*
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
                 ("host_budget_bytes", ctypes.c_size_t), ("max_wave_events", ctypes.c_int),
-                ("streams", ctypes.c_int), ("output_mask", ctypes.c_uint)]
+                ("streams", ctypes.c_int), ("output_mask", ctypes.c_uint), ("stream_2d", ctypes.c_int)]
 
 
 # output groups of the server (FSM_OUT_* in fsm.h), in slab order
@@ -654,12 +654,12 @@ class Server:
     arrive, poll for their outputs; results equal Context.run_event's."""
 
     def __init__(self, device=0, hbm_budget=0, host_budget=0, max_wave_events=0, streams=0,
-                 outputs=None):
+                 outputs=None, stream_2d=False):
         self.h = ctypes.c_void_p()
         self.outputs = list(outputs) if outputs else list(OUT_GROUPS)
         mask = out_mask(self.outputs)
         opts = ServerOpts(device, int(hbm_budget), int(host_budget), int(max_wave_events),
-                          int(streams), mask)
+                          int(streams), mask, int(bool(stream_2d)))
         check(lib().fsm_server_start(ctypes.byref(self.h), ctypes.byref(opts)), "fsm_server_start")
         self._pending = {}
 

@@ -372,10 +372,13 @@ typedef struct fsm_server_opts {
   size_t hbm_budget_bytes;   /* device memory held for waves in flight (0: 8 GiB)   */
   size_t host_budget_bytes;  /* pinned host memory for inputs/outputs (0: 2 GiB)    */
   int max_wave_events;       /* events per launch wave (0: 512)                     */
-  int streams;               /* waves in flight (0: 2)                              */
+  int streams;               /* waves in flight (0: 4)                              */
   unsigned output_mask;      /* FSM_OUT_* groups copied back (0: all); fields of
                                 fsm_server_poll's host_out outside it are left as
                                 they are                                            */
+  int stream_2d;             /* 1: one more stream whose waves hold boost-invariant
+                                requests only, so that they never queue behind 3D
+                                waves (0: none)                                     */
 } fsm_server_opts;
 
 typedef struct fsm_server_stats {

@@ -67,6 +67,26 @@ def test_server_results_alone_in_mix_and_plain(ctx):
 
 
 @pytest.mark.gpu
+def test_server_reserved_2d_stream(ctx):
+    """With a stream reserved for boost-invariant waves (and 3D events capped
+    per wave), a burst of mixed requests -- several 3D ones among them --
+    gives every request the plain entry point's outputs."""
+    reqs = _mixed_requests()
+    p3, e3, nb3 = W.baryon3d(seed=7, side=31, neta=15, nrap=11, nphip=24)
+    reqs += [(p3, e3, nb3)] * 3
+    srv = F.Server(streams=2, stream_2d=True)
+    try:
+        ids = [srv.submit(p, e, nb) for p, e, nb in reqs * 2]
+        got = [srv.poll(i) for i in ids]
+        st = srv.stats()
+    finally:
+        srv.stop()
+    for k, (p, e, nb) in enumerate(reqs * 2):
+        _same(got[k], ctx.run_event(p, e, nb))
+    assert st["completed"] == 2 * len(reqs) and st["failed"] == 0
+
+
+@pytest.mark.gpu
 def test_server_budget_splits_waves_and_rejects_oversize():
     small = [W.lumpy2d(seed=10 + k, side=61, dx=0.1, nphip=64, dtau=0.5, eos=1, radius=2.0)
              for k in range(12)]
