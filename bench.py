@@ -108,6 +108,16 @@ class Clocks:
         except Exception:
             self.p = None
 
+    def wait_first(self, timeout_s=5.0):
+        """Waits until nvidia-smi has written its first sample (it takes a
+        while to start), so that the timed region that follows is sampled."""
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < timeout_s:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                return
+            time.sleep(0.02)
+
     def stop(self):
         if self.p is None:
             return None
@@ -437,6 +447,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
+    clk.wait_first()
     with torch.cuda.stream(stream):
         step_ev[0].record(stream)
         for k in range(args.steps):

@@ -381,9 +381,11 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
         ctx->spare_host_cap = 0;
       }
     }
-    // allocations rounded up (at most 1/8 above the need, on a coarse grid)
-    // so that a later batch of similar size fits the one this batch leaves
+    // allocations with 1/8 of headroom, rounded up on a coarse grid (at most
+    // another 1/8), so that a later batch of similar size -- a new event set
+    // of the same mix -- fits the one this batch leaves
     auto rounded = [](size_t need) {
+      need += need / 8;
       size_t step = 1;
       while (step * 8 < need) step <<= 1;
       return (need + step - 1) / step * step;
