@@ -197,8 +197,10 @@ struct PhiEntry3D {
 };
 
 // A 3D output tile: 32 x 32 cells of one eta slice of one event.
+// A 3D output tile of eta slice ieta: shape `shape` (as the 2D shapes) from
+// (x0, y0), storing the cells below (x1, y1).
 struct Tile3D {
-  int ev, x0, y0, ieta;
+  int ev, x0, y0, ieta, shape, x1, y1;
 };
 
 struct Ev3D {

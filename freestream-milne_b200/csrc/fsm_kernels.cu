@@ -933,8 +933,8 @@ constexpr int slots3d() {
 
 // The phi_p loop of one rapidity node for one tile (nodes of eta pair efl).
 template <bool kB>
-__device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, int ixb, int iy,
-                                             int x_hi, int y_hi, bool full, float y, float ey,
+__device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, int wxa, int wxb,
+                                             int wxn, int wya, int wyb, int wyn, float y, float ey,
                                              const float (&ex)[kCellsPerThread],
                                              const bool (&act)[kCellsPerThread],
                                              const typename Node3D<kB>::T* __restrict__ N,
@@ -977,20 +977,21 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, const Tile3D& tl, i
     {
       const int p = pb + lane;
       bool vis = false, ins = false;
-      if (p < NP && ixb <= x_hi) {
+      if (p < NP && wxa <= wxb && wya <= wyb) {
         const PhiEntry3D e = tab[p];
         const int ox = e.ox;
         const int oy = (int)(short)(e.oy_near & 0xffff);
-        // sample floor indices of the tile's rows [x0 + ox, x_hi + ox] (one
-        // more either side when the fraction is near an integer); this
-        // warp's rows ixb .. min(ixb + 3, x_hi)
-        const int ya = tl.y0 + oy, yb = y_hi + oy;
-        const int wa = ixb + ox, wb = min(ixb + K - 1, x_hi) + ox;
+        // sample floor indices of this warp's stored cells, rows wxa .. wxb
+        // and columns wya .. wyb, shifted (one more either side when the
+        // fraction is near an integer)
+        const int ya = wya + oy, yb = wyb + oy;
+        const int wa = wxa + ox, wb = wxb + ox;
         vis = !((yb + 1 < 1) || (ya - 1 > NY - 2) || (wb + 1 < 1) || (wa - 1 > NX - 2));
         // every sample of this warp lands two or more nodes inside the grid:
-        // its rows wa .. wa + 3 and all 32 lanes' columns (lanes past the
-        // grid edge included, so that their loads stay inside the arrays)
-        ins = (wa >= 2) && (wa + K - 1 <= NX - 3) && (tl.y0 + oy >= 2) && (tl.y0 + kTileY - 1 + oy <= NY - 3);
+        // all its lanes' rows wxa .. wxa + wxn - 1 and columns wya .. wya +
+        // wyn - 1 (cells past the grid edge included, so that their loads
+        // stay inside the arrays)
+        ins = (wa >= 2) && (wxa + wxn - 1 + ox <= NX - 3) && (ya >= 2) && (wya + wyn - 1 + oy <= NY - 3);
       }
       vis_mask = __ballot_sync(0xffffffffu, vis);
       in_mask = __ballot_sync(0xffffffffu, ins);
@@ -1147,6 +1148,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
   __shared__ int s_tile;
   constexpr int K = kCellsPerThread;
   constexpr int kS = slots3d<kB>();
+  static_assert(kThreads3D == kWarps2D * 32, "the tile shapes are laid out for 8 warps");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* const sl = slots3 + threadIdx.x;
   auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
@@ -1160,9 +1162,19 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     const int NX = ev.NX, NY = ev.NY, NE = ev.NE, NR = ev.NR, NP = ev.NPHI;
     const int ieta = tl.ieta;
     constexpr bool baryon = kB;
-    const int iy = tl.y0 + lane, ixb = tl.x0 + warp * K;
-    const int x_hi = min(tl.x0 + kTileX, NX) - 1, y_hi = min(tl.y0 + kTileY, NY) - 1;
-    const bool full = (tl.x0 + kTileX <= NX) && (tl.y0 + kTileY <= NY);
+    // the tile's shape (as in 2D): lanes along y in groups of ly cells, wy
+    // warps stacked along y
+    const int sh = tl.shape;
+    const int ly = shape_ly(sh), wy = shape_wy(sh);
+    const int gx = 32 / ly, wxcount = kWarps2D / wy;
+    const int wxi = warp % wxcount, wyi = warp / wxcount;
+    const int iy = tl.y0 + wyi * ly + (lane & (ly - 1));
+    const int ixb = tl.x0 + K * (wxi * gx + lane / ly);
+    // the last cell the tile stores (x1, y1 <= the grid's size)
+    const int x_hi = min(tl.x0 + K * gx * wxcount, tl.x1) - 1, y_hi = min(tl.y0 + ly * wy, tl.y1) - 1;
+    // this warp's cells: all of them, and those the tile stores
+    const int wxa = tl.x0 + K * wxi * gx, wxn = K * gx, wxb = min(wxa + wxn - 1, x_hi);
+    const int wya = tl.y0 + wyi * ly, wyb = min(wya + ly - 1, y_hi);
     const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
     const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
@@ -1173,7 +1185,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
       const int ix = ixb + k;
       const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
       ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
-      act[k] = (ix < NX) && (iy < NY);
+      act[k] = (ix <= x_hi) && (iy <= y_hi);
     }
 #pragma unroll
     for (int m = 0; m < K * kS; ++m) S(m) = 0.0f;
@@ -1191,11 +1203,11 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
         const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
         const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
         const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
-        stream3d_rap<true>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
+        stream3d_rap<true>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, tab, re.D,
                            re.efrac, rf0, rf1, rb0, rb1, rp, jw, sl);
       } else {
         const float2* N = reinterpret_cast<const float2*>(ev.nodes3) + (size_t)re.efl * plane;
-        stream3d_rap<false>(ev, tl, ixb, iy, x_hi, y_hi, full, y, ey, ex, act, N, tab, re.D,
+        stream3d_rap<false>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, tab, re.D,
                             re.efrac, rf0, rf1, 0.f, 0.f, rp, jw, sl);
       }
     }

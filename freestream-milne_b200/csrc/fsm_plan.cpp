@@ -170,23 +170,27 @@ int x_tail_shape(int NX) {
   return r == 0 ? -1 : r <= 8 ? 4 : r <= 16 ? 3 : -1;
 }
 
-void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out, bool square) {
-  const int NX = P.p.DIM_X, NY = P.p.DIM_Y;
-  const int ys = square ? -1 : P.y_shape, xs = square ? -1 : P.x_shape;
+void grid_tiles(int NX, int NY, int ys, int xs, std::vector<TileXY>& out) {
   // the 32 x 32 region: whole tiles up to the narrow last strips, or over the
   // whole grid (rounded up) where a last strip keeps 32 x 32 tiles
   const int NXm = xs >= 0 ? NX - NX % kTileX : (NX + kTileX - 1) / kTileX * kTileX;
   const int NYm = ys >= 0 ? NY - NY % kTileY : (NY + kTileY - 1) / kTileY * kTileY;
   for (int x0 = 0; x0 < NXm; x0 += kTileX)
-    for (int y0 = 0; y0 < NYm; y0 += kTileY) out.push_back(Tile2D{ev, x0, y0, 0, NX, NY});
+    for (int y0 = 0; y0 < NYm; y0 += kTileY) out.push_back(TileXY{x0, y0, 0, NX, NY});
   // the last y strip, x < NXr (up to the last x strip, when that has its own
   // tiles): its last tile stores no cell of the x strip
   const int NXr = xs >= 0 ? NXm : NX;
   if (ys >= 0)
-    for (int x0 = 0; x0 < NXr; x0 += shape_tx(ys)) out.push_back(Tile2D{ev, x0, NYm, ys, NXr, NY});
+    for (int x0 = 0; x0 < NXr; x0 += shape_tx(ys)) out.push_back(TileXY{x0, NYm, ys, NXr, NY});
   // the last x strip over the whole y range (its corner with the y strip included)
   if (xs >= 0)
-    for (int y0 = 0; y0 < NY; y0 += shape_ty(xs)) out.push_back(Tile2D{ev, NXm, y0, xs, NX, NY});
+    for (int y0 = 0; y0 < NY; y0 += shape_ty(xs)) out.push_back(TileXY{NXm, y0, xs, NX, NY});
+}
+
+void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out, bool square) {
+  std::vector<TileXY> t;
+  grid_tiles(P.p.DIM_X, P.p.DIM_Y, square ? -1 : P.y_shape, square ? -1 : P.x_shape, t);
+  for (const TileXY& q : t) out.push_back(Tile2D{ev, q.x0, q.y0, q.shape, q.x1, q.y1});
 }
 
 fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* out,

@@ -78,6 +78,12 @@ int x_tail_shape(int NX);
 // square: 32 x 32 tiles only (for launches too small to fill the GPU, where
 // the narrow tiles' longer staging would lengthen the slowest tile).
 void tiles_2d(const EventPlan& P, int ev, std::vector<Tile2D>& out, bool square = false);
+// The same tiling of an NX x NY grid with narrow shapes ys / xs (-1: none),
+// as (x0, y0, shape, x1, y1) entries; the 3D tiles of each eta slice use it.
+struct TileXY {
+  int x0, y0, shape, x1, y1;
+};
+void grid_tiles(int NX, int NY, int ys, int xs, std::vector<TileXY>& out);
 
 // Energy-dependent free-streaming time tau_R (e_T / e_R)^alpha from the
 // reference's float sums of eps^2 and eps over the converted profile

@@ -287,14 +287,19 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       Tile3D t;
     };
     std::vector<T3> t3;
+    std::vector<TileXY> txy;
     for (int i : order3) {
       const EventPlan& P = b->plans[i];
       const int NX = P.p.DIM_X, NY = P.p.DIM_Y, NE = P.p.DIM_ETA;
+      // the 2D tiling of a slice, narrow tiles on partial last strips (a 3D
+      // event has tiles for every SM)
+      txy.clear();
+      grid_tiles(NX, NY, y_tail_shape(NY), x_tail_shape(NX), txy);
       for (int ie = 0; ie < NE; ++ie) {
         // slices without a live rapidity node still get tiles: they write zeros
-        for (int x0 = 0; x0 < NX; x0 += kTileX)
-          for (int y0 = 0; y0 < NY; y0 += kTileY)
-            t3.push_back({P.live_eta[ie] * P.p.DIM_PHIP, P.p.BARYON != 0, Tile3D{b->ev3_of[i], x0, y0, ie}});
+        for (const TileXY& q : txy)
+          t3.push_back({P.live_eta[ie] * P.p.DIM_PHIP, P.p.BARYON != 0,
+                        Tile3D{b->ev3_of[i], q.x0, q.y0, ie, q.shape, q.x1, q.y1}});
       }
     }
     std::stable_sort(t3.begin(), t3.end(), [](const T3& a, const T3& c) {
