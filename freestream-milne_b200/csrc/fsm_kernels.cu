@@ -5,9 +5,11 @@
 //   fsm_prep2d_*_long_kernel  the same for grids whose lines exceed kMaxStrip
 //   fsm_prep3d_kernel         GeV/fm^3 -> fm^-4 conversion into eta-pair node arrays (3D)
 //   fsm_stream2d_kernel       fused free streaming + moment quadrature, 2D
-//   fsm_stream3d_kernel       fused free streaming + moment quadrature, 3D (+baryon)
+//   fsm_stream3d_kernel       fused free streaming + moment quadrature, 3D
+//   fsm_stream3d_baryon_kernel  the same with baryon charge
 //   fsm_pack_kernel           gather of output fields for one-copy downloads
-//   fsm_landau_kernel         FP64 Landau matching + EoS + decomposition
+//   fsm_landau_kernel         FP64 Landau matching + EoS + decomposition, 2D
+//   fsm_landau3d_kernel       the same for 3D events
 //
 // The stream kernels never store the momentum-resolved density F(x; phi_p, y):
 // each thread evaluates the shifted profile for its cell and reduces it into
@@ -1257,9 +1259,12 @@ __global__ void __launch_bounds__(256) fsm_pack_kernel(const float* __restrict__
 // Eight 128-thread blocks per SM (64 registers, some spilled to L1): the
 // solver is latency-bound, and the extra warps gain more than the spills cost
 // (measured against 4 to 7 blocks, and 64- and 256-thread blocks).
-__global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvLandau* __restrict__ evs,
-                                                                    const CellBlock* __restrict__ blocks,
-                                                                    Counters* ctr) {
+// Boost-invariant and 3D events run in separate instantiations (the union of
+// the 3x3 and 4x4 eigenproblems spilled 492 bytes per thread, the 3x3 path
+// alone 156).
+template <bool k3D>
+__device__ __forceinline__ void landau_block(const EvLandau* __restrict__ evs,
+                                             const CellBlock* __restrict__ blocks, Counters* ctr) {
   const CellBlock b = blocks[blockIdx.x];
   const EvLandau& ev = evs[b.ev];
   const int DIM = ev.DIM;
@@ -1267,7 +1272,7 @@ __global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvL
   int fb = 0;
   if (is < DIM) {
     float T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}, J[4] = {0, 0, 0, 0};
-    if (ev.is3d) {
+    if constexpr (k3D) {
 #pragma unroll
       for (int m = 0; m < 10; ++m) T[m] = __ldg(ev.T + (size_t)m * DIM + is);
     } else {  // boost-invariant: the stream kernel wrote T^{tau eta} = T^{x eta} = T^{y eta} = T^{eta eta} = 0
@@ -1280,7 +1285,7 @@ __global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvL
       for (int m = 0; m < 4; ++m) J[m] = __ldg(ev.J + (size_t)m * DIM + is);
     }
     CellOut o;
-    landau_cell(T, J, ev.is3d, ev.baryon, ev.eos, ev.viscous, ev.TAU, &o);
+    landau_cell_t<k3D>(T, J, ev.baryon, ev.eos, ev.viscous, ev.TAU, &o);
     fb = o.fallback;
     if (ev.e) ev.e[is] = o.e;
     if (ev.P) ev.P[is] = o.P;
@@ -1303,6 +1308,20 @@ __global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvL
   }
   const unsigned mask = __ballot_sync(0xffffffffu, fb);
   if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&ctr->fallback, __popc(mask));
+}
+
+// Boost-invariant events (3x3 eigenproblem).
+__global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau_kernel(const EvLandau* __restrict__ evs,
+                                                                    const CellBlock* __restrict__ blocks,
+                                                                    Counters* ctr) {
+  landau_block<false>(evs, blocks, ctr);
+}
+
+// 3D events (4x4 eigenproblem).
+__global__ void __launch_bounds__(kThreadsLandau, 8) fsm_landau3d_kernel(const EvLandau* __restrict__ evs,
+                                                                      const CellBlock* __restrict__ blocks,
+                                                                      Counters* ctr) {
+  landau_block<true>(evs, blocks, ctr);
 }
 
 // ------------------------------------------------------------- diagnostics

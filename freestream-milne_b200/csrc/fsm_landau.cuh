@@ -342,12 +342,13 @@ struct CellOut {
 // One cell: eigen-solve, EoS, bulk/shear (src/LandauMatch.cpp:332-367) and
 // baryon density/diffusion (src/LandauMatch.cpp:370-392).  T components in
 // the reference's row order; decomposition in FP64 from the float e, P, u.
-FSM_HD void landau_cell(const float T[10], const float J[4], int is3d, int baryon, int eos,
-                        int viscous, float TAU, CellOut* o) {
+template <bool k3D>
+FSM_HD void landau_cell_t(const float T[10], const float J[4], int baryon, int eos, int viscous,
+                          float TAU, CellOut* o) {
   double tau2 = (double)TAU * (double)TAU;
   double e = 0.0, u[4] = {0.0, 0.0, 0.0, 0.0};
   int ok;
-  if (is3d) {
+  if constexpr (k3D) {
     double M[4][4];
     const int idx[4][4] = {{0, 1, 2, 3}, {1, 4, 5, 6}, {2, 5, 7, 8}, {3, 6, 8, 9}};
 #pragma unroll
@@ -417,6 +418,16 @@ FSM_HD void landau_cell(const float T[10], const float J[4], int is3d, int baryo
 #pragma unroll
     for (int r = 0; r < 4; ++r) o->V[r] = 0.0f;
   }
+}
+
+// Either dimension (the device kernels instantiate each separately, so that
+// each is register-allocated for its own eigenproblem).
+FSM_HD void landau_cell(const float T[10], const float J[4], int is3d, int baryon, int eos,
+                        int viscous, float TAU, CellOut* o) {
+  if (is3d)
+    landau_cell_t<true>(T, J, baryon, eos, viscous, TAU, o);
+  else
+    landau_cell_t<false>(T, J, baryon, eos, viscous, TAU, o);
 }
 
 }  // namespace fsm

@@ -33,6 +33,7 @@ __global__ void fsm_stream2d_kernel(const Ev2D*, const Tile2D*, int, int, Counte
 __global__ void fsm_stream3d_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_stream3d_baryon_kernel(const Ev3D*, const Tile3D*, int, Counters*);
 __global__ void fsm_landau_kernel(const EvLandau*, const CellBlock*, Counters*);
+__global__ void fsm_landau3d_kernel(const EvLandau*, const CellBlock*, Counters*);
 __global__ void fsm_pack_kernel(const float*, float*, const CopySeg*);
 __global__ void fsm_edep_sums_kernel(const float* const*, const int*, int, float*);
 __global__ void fsm_energy_sums_kernel(const EvEnergy*, int, float*);
@@ -314,8 +315,16 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       if (P.is3d)
         for (int s = 0; s < (P.p.DIM_ETA - 1) * P.p.DIM_X * P.p.DIM_Y; s += 256)
           prep3.push_back(CellBlock{b->ev3_of[i], s});
-      for (int s = 0; s < P.DIM; s += kThreadsLandau) bl.push_back(CellBlock{i, s});
     }
+    // Landau blocks: the boost-invariant events' first (their kernel), then
+    // the 3D events'
+    for (int pass = 0; pass < 2; ++pass)
+      for (int i = 0; i < n; ++i) {
+        const EventPlan& P = b->plans[i];
+        if ((int)P.is3d != pass) continue;
+        for (int s = 0; s < P.DIM; s += kThreadsLandau) bl.push_back(CellBlock{i, s});
+        if (!P.is3d) b->nbl2 = (int)bl.size();
+      }
   }
   // descriptors + work lists
   size_t o_ev2 = L.take(std::max(n2, 1) * sizeof(Ev2D));
@@ -761,7 +770,10 @@ fsm_status enqueue(fsm_batch* b, cudaStream_t s, bool timing) {
     fsm_stream3d_kernel<<<b->grid3, kThreads3D, b->smem3, s>>>(
         b->d_ev3, b->d_tiles3 + b->ntiles3b, b->ntiles3 - b->ntiles3b, b->d_ctr);
   if (timing) cudaEventRecord(ts.ev[2], s);
-  if (b->nbl) fsm_landau_kernel<<<b->nbl, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl, b->d_ctr);
+  if (b->nbl2) fsm_landau_kernel<<<b->nbl2, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl, b->d_ctr);
+  if (b->nbl > b->nbl2)
+    fsm_landau3d_kernel<<<b->nbl - b->nbl2, kThreadsLandau, 0, s>>>(b->d_evl, b->d_bl + b->nbl2,
+                                                                    b->d_ctr);
   if (timing) {
     cudaEventRecord(ts.ev[3], s);
     std::lock_guard<std::mutex> g(ctx->mu);

@@ -132,6 +132,7 @@ struct fsm_batch {
   int* d_err = nullptr;
   int ntiles = 0, nrows = 0, ncols = 0, nrows_l = 0, ncols_l = 0, nprep3 = 0, ntiles3 = 0, nbl = 0;
   int ntiles3b = 0;  // the first ntiles3b 3D tiles belong to events with baryon charge
+  int nbl2 = 0;      // the first nbl2 Landau blocks belong to boost-invariant events
   int cs_cap2 = 0, cs_cap3 = 0, box_cap2 = 0, ny_cap2 = 0, strip_cap2 = 0;
   size_t smem2 = 0, smem3 = 0, smem3b = 0, smem_rows = 0, smem_strip = 0;
   int grid2 = 0, grid3 = 0, grid3b = 0;
