@@ -72,7 +72,7 @@ extern "C" int fsm_hosttest_plan_digest(const fsm_params* p, int serial, unsigne
 }
 
 // The 2D output tiles of one event as (x0, y0, shape, x1, y1), with the runs
-// planned per shape (nch[5]) and the largest staged window in nodes; returns
+// planned per shape (nch[7]) and the largest staged window in nodes; returns
 // the number of tiles (at most cap written) or -1 when planning fails.
 extern "C" int fsm_hosttest_tiles(const fsm_params* p, int tail_tiles, int window_budget, int* out,
                                   int cap, int* nch, int* box_elems) {

@@ -117,12 +117,17 @@ struct Chunk2D {
 // are stacked along y: TX = 4 * (32 / Ly) * (8 / Wy) x cells by TY = Ly * Wy
 // y cells, always 256 threads and 1024 cells.  Shape 0 (32 x 32) tiles an
 // event; the narrow shapes cover its partial last strips, so that fewer lanes
-// and warps run past the grid edge: 1 (64 x 16) and 2 (128 x 8) for a last
-// y strip of at most 16 / 8 cells, 3 (16 x 64) and 4 (8 x 128) for a last x
-// strip of at most 16 / 8 cells.
-constexpr int kShapes2D = 5;
-FSM_HDI int shape_ly(int s) { return s == 1 ? 16 : s == 2 ? 8 : 32; }
-FSM_HDI int shape_wy(int s) { return s == 3 ? 2 : s == 4 ? 4 : 1; }
+// and warps run past the grid edge: 1 (64 x 16), 2 (128 x 8) and 6 (256 x 4)
+// for a last y strip of at most 16 / 8 / 4 cells, 3 (16 x 64), 4 (8 x 128)
+// and 5 (4 x 256) for a last x strip of at most 16 / 8 / 4 cells.
+constexpr int kShapes2D = 7;
+// log2(32 / Ly) and log2(Wy) of shapes 0..6, 3 bits per shape
+constexpr int kShapeLyLog = (1 << 3) | (2 << 6) | (3 << 18);
+constexpr int kShapeWyLog = (1 << 9) | (2 << 12) | (3 << 15);
+FSM_HDI int shape_ly_log(int s) { return (kShapeLyLog >> (3 * s)) & 7; }
+FSM_HDI int shape_wy_log(int s) { return (kShapeWyLog >> (3 * s)) & 7; }
+FSM_HDI int shape_ly(int s) { return 32 >> shape_ly_log(s); }
+FSM_HDI int shape_wy(int s) { return 1 << shape_wy_log(s); }
 FSM_HDI int shape_tx(int s) { return kCellsPerThread * (32 / shape_ly(s)) * (kWarps2D / shape_wy(s)); }
 FSM_HDI int shape_ty(int s) { return shape_ly(s) * shape_wy(s); }
 // Staged window of a run for a tile of shape s: rows (x) and row length (y).

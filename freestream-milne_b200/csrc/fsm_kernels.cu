@@ -731,13 +731,13 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     }
     // the tile's shape: lanes run along y in groups of ly cells (32 / ly
     // groups of K x cells side by side), wy warps stacked along y
-    const int ly = shape_ly(sh), wy = shape_wy(sh);
-    const int gx = 32 / ly, wxcount = kWarps2D / wy;
-    const int wxi = warp % wxcount, wyi = warp / wxcount;
-    const int TX = K * gx * wxcount, TY = ly * wy;
+    const int lyl = shape_ly_log(sh), wyl = shape_wy_log(sh);
+    const int ly = 32 >> lyl, gx = 1 << lyl, wxcount = kWarps2D >> wyl;
+    const int wxi = warp & (wxcount - 1), wyi = warp >> (3 - wyl);
+    const int TX = K * gx * wxcount, TY = ly << wyl;
     // per-thread cell constants
     const int iy = tl.y0 + wyi * ly + (lane & (ly - 1));
-    const int ixb = tl.x0 + K * (wxi * gx + lane / ly);
+    const int ixb = tl.x0 + K * (wxi * gx + (lane >> (5 - lyl)));
     // the last cell the tile stores (x1, y1 <= the grid's size)
     const int x_hi = min(tl.x0 + TX, tl.x1) - 1, y_hi = min(tl.y0 + TY, tl.y1) - 1;
     // this warp's cells
@@ -1150,7 +1150,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
   __shared__ int s_tile;
   constexpr int K = kCellsPerThread;
   constexpr int kS = slots3d<kB>();
-  static_assert(kThreads3D == kWarps2D * 32, "the tile shapes are laid out for 8 warps");
+  static_assert(kThreads3D == kWarps2D * 32 && kWarps2D == 8, "the tile shapes are laid out for 8 warps");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* const sl = slots3 + threadIdx.x;
   auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
@@ -1167,13 +1167,13 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     // the tile's shape (as in 2D): lanes along y in groups of ly cells, wy
     // warps stacked along y
     const int sh = tl.shape;
-    const int ly = shape_ly(sh), wy = shape_wy(sh);
-    const int gx = 32 / ly, wxcount = kWarps2D / wy;
-    const int wxi = warp % wxcount, wyi = warp / wxcount;
+    const int lyl = shape_ly_log(sh), wyl = shape_wy_log(sh);
+    const int ly = 32 >> lyl, gx = 1 << lyl, wxcount = kWarps2D >> wyl;
+    const int wxi = warp & (wxcount - 1), wyi = warp >> (3 - wyl);
     const int iy = tl.y0 + wyi * ly + (lane & (ly - 1));
-    const int ixb = tl.x0 + K * (wxi * gx + lane / ly);
+    const int ixb = tl.x0 + K * (wxi * gx + (lane >> (5 - lyl)));
     // the last cell the tile stores (x1, y1 <= the grid's size)
-    const int x_hi = min(tl.x0 + K * gx * wxcount, tl.x1) - 1, y_hi = min(tl.y0 + ly * wy, tl.y1) - 1;
+    const int x_hi = min(tl.x0 + K * gx * wxcount, tl.x1) - 1, y_hi = min(tl.y0 + (ly << wyl), tl.y1) - 1;
     // this warp's cells: all of them, and those the tile stores
     const int wxa = tl.x0 + K * wxi * gx, wxn = K * gx, wxb = min(wxa + wxn - 1, x_hi);
     const int wya = tl.y0 + wyi * ly, wyb = min(wya + ly - 1, y_hi);

@@ -162,12 +162,12 @@ float edep_dtau(const fsm_params& p, float numerator, float denominator) {
 
 int y_tail_shape(int NY) {
   const int r = NY % kTileY;
-  return r == 0 ? -1 : r <= 8 ? 2 : r <= 16 ? 1 : -1;
+  return r == 0 ? -1 : r <= 4 ? 6 : r <= 8 ? 2 : r <= 16 ? 1 : -1;
 }
 
 int x_tail_shape(int NX) {
   const int r = NX % kTileX;
-  return r == 0 ? -1 : r <= 8 ? 4 : r <= 16 ? 3 : -1;
+  return r == 0 ? -1 : r <= 4 ? 5 : r <= 8 ? 4 : r <= 16 ? 3 : -1;
 }
 
 void grid_tiles(int NX, int NY, int ys, int xs, std::vector<TileXY>& out) {
@@ -335,6 +335,10 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
     E.x_shape = tail_tiles ? x_tail_shape(E.p.DIM_X) : -1;
     E.chunks2.clear();
     E.box_elems = 0;
+    // the narrow shapes plan at the budget the 32 x 32 shape ended with and
+    // never raise it: a batch sizes its shared memory by its largest window,
+    // so a narrow tile must not push every CTA of the launch past two per SM
+    int budget0 = window_budget;
     for (int sh = 0; sh < kShapes2D; ++sh) {
       E.choff[sh] = (int)E.chunks2.size();
       E.nch[sh] = 0;
@@ -342,7 +346,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       const int TX = shape_tx(sh), TY = shape_ty(sh);
       std::vector<Chunk2D> runs;
       int box = 0;
-      for (int budget = window_budget;; budget = budget * 3 / 2) {
+      for (int budget = sh == 0 ? window_budget : budget0;; budget = budget * 3 / 2) {
+        if (sh == 0) budget0 = budget;
         auto win_bytes = [&](int dox, int doy) {
           return (size_t)(TX + dox + 3) * (size_t)(TY + doy + 3) * 16;
         };
@@ -372,7 +377,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
           }
         }
         const bool few = (int)runs.size() <= std::max(kMaxChunks2D, 2 * min_runs);
-        if (few || budget * 3 / 2 > kMaxWindow2D) break;
+        if (sh != 0 || few || budget * 3 / 2 > kMaxWindow2D) break;
       }
       E.chunks2.insert(E.chunks2.end(), runs.begin(), runs.end());
       E.nch[sh] = (int)runs.size();

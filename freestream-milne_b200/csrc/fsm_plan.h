@@ -68,7 +68,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
                       bool tail_tiles = true);
 
 // Narrow tile shape for the last, partial strip of a 2D grid along y (x):
-// 2 (1) when at most 8 (16) cells are left over, else -1 (32 x 32 tiles).
+// 6, 2, 1 (5, 4, 3) when at most 4, 8, 16 cells are left over, else -1
+// (32 x 32 tiles).
 int y_tail_shape(int NY);
 int x_tail_shape(int NX);
 // The output tiles of 2D event `ev` (of plan P): 32 x 32 tiles over the grid

@@ -128,8 +128,8 @@ def test_parallel_planning_matches_serial():
         assert d[0] == d[1] == d[2], (p.DIM_ETA, p.DIM_RAP, d)
 
 
-SHAPE_TX = {0: 32, 1: 64, 2: 128, 3: 16, 4: 8}
-SHAPE_TY = {0: 32, 1: 16, 2: 8, 3: 64, 4: 128}
+SHAPE_TX = {0: 32, 1: 64, 2: 128, 3: 16, 4: 8, 5: 4, 6: 256}
+SHAPE_TY = {0: 32, 1: 16, 2: 8, 3: 64, 4: 128, 5: 256, 6: 4}
 
 
 def test_tiles_cover_every_cell_once():
@@ -144,10 +144,11 @@ def test_tiles_cover_every_cell_once():
                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     cap = 4096
     buf = np.zeros(5 * cap, np.int32)
-    nch = np.zeros(5, np.int32)
+    nch = np.zeros(7, np.int32)
     box = ctypes.c_int()
     sides = [(5, 7), (9, 40), (31, 33), (32, 32), (41, 41), (45, 41), (101, 101),
-             (151, 151), (201, 261), (301, 301), (100, 900), (263, 17), (8, 300)]
+             (151, 151), (201, 261), (301, 301), (100, 900), (263, 17), (8, 300), (131, 131),
+             (36, 260), (260, 36), (68, 100)]
     for nx, ny in sides:
         p, _, _ = W.lumpy2d(seed=3, side=41, dx=0.08, nphip=64, dtau=0.9, eos=1, radius=1.0)
         p.DIM_X, p.DIM_Y = nx, ny
