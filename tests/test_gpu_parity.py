@@ -533,13 +533,14 @@ def test_invalid_inputs_are_rejected(ctx):
 
 def test_narrow_tail_tiles_keep_results():
     """A batch large enough for the narrow tail tiles (64 x 16, 128 x 8,
-    16 x 64, 8 x 128 over partial last strips) gives, bit for bit, the results
-    of 32 x 32 tiles only; every grid side's remainder shape is covered."""
+    256 x 4, 16 x 64, 8 x 128, 4 x 256 over partial last strips) gives, bit for
+    bit, the results of 32 x 32 tiles only; every remainder shape is covered."""
     evs = [W.lumpy2d(seed=60, side=301, dx=0.05, nphip=64, dtau=1.2, eos=1, radius=5.0),   # 13: 64x16, 16x64
            W.lumpy2d(seed=61, side=261, dx=0.06, nphip=100, dtau=0.8, eos=2, radius=5.0),  # 5: 128x8, 8x128
            W.lumpy2d(seed=62, side=301, dx=0.1, nphip=64, dtau=0.5, eos=2, radius=6.0),
            W.lumpy2d(seed=63, side=201, dx=0.075, nphip=64, dtau=1.0, eos=1, radius=5.0),  # 9: 64x16, 16x64
-           W.lumpy2d(seed=64, side=261, dx=0.05, nphip=64, dtau=0.4, eos=1, radius=4.0)]
+           W.lumpy2d(seed=64, side=261, dx=0.05, nphip=64, dtau=0.4, eos=1, radius=4.0),
+           W.lumpy2d(seed=65, side=260, dx=0.06, nphip=64, dtau=0.9, eos=2, radius=5.0)]   # 4: 256x4, 4x256
     outs = {}
     for tiles in (F.TILES_TAIL, F.TILES_SQUARE):
         c = F.Context(0)
