@@ -946,6 +946,9 @@ extern "C" void fsm_ctx_destroy(fsm_ctx* ctx) {
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
   if (ctx->spare_dev) cudaFree(ctx->spare_dev);
   if (ctx->spare_host) cudaFreeHost(ctx->spare_host);
+  if (ctx->pin_stage) cudaFreeHost(ctx->pin_stage);
+  for (auto e : ctx->pin_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -975,6 +978,90 @@ extern "C" fsm_status fsm_ctx_timing(fsm_ctx* ctx, fsm_timing* t, int reset) {
 }
 
 namespace {
+// Copies between caller host buffers and the device on the context's stream.
+// Pinned caller buffers are copied directly.  Pageable ones go through the
+// context's two pinned chunks: a pageable cudaMemcpy is staged by the driver
+// one bounce buffer at a time on one thread (~15 GB/s); here the host copy of
+// one chunk (several threads) overlaps the device copy of the next.  Returns
+// once every copy has completed.
+struct HostSeg {
+  char* h;        // caller host memory
+  char* d;        // device memory
+  size_t bytes;
+};
+constexpr size_t kPinChunk = size_t(8) << 20;
+
+bool is_pinned(const void* h) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+fsm_status ensure_pin_stage(fsm_ctx* ctx) {
+  if (ctx->pin_stage) return FSM_OK;
+  FSM_CUDA_TRY(cudaMallocHost(&ctx->pin_stage, 2 * kPinChunk));
+  for (auto& e : ctx->pin_ev) FSM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return FSM_OK;
+}
+
+fsm_status copy_staged(fsm_ctx* ctx, cudaStream_t st, const std::vector<HostSeg>& segs, bool to_device) {
+  const cudaMemcpyKind kind = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  struct Piece {
+    char* h;
+    char* d;
+    size_t n;
+  };
+  std::vector<Piece> pieces;
+  for (const HostSeg& g : segs) {
+    if (!g.h || !g.d || !g.bytes) continue;
+    if (is_pinned(g.h)) {
+      FSM_CUDA_TRY(cudaMemcpyAsync(to_device ? g.d : g.h, to_device ? g.h : g.d, g.bytes, kind, st));
+      continue;
+    }
+    for (size_t o = 0; o < g.bytes; o += kPinChunk)
+      pieces.push_back(Piece{g.h + o, g.d + o, std::min(kPinChunk, g.bytes - o)});
+  }
+  if (!pieces.empty()) {
+    fsm_status s = ensure_pin_stage(ctx);
+    if (s != FSM_OK) return s;
+  }
+  const int np = (int)pieces.size();
+  if (to_device) {
+    // host copy of piece i into chunk i % 2 once that chunk's previous upload
+    // has left it, then its upload
+    for (int i = 0; i < np; ++i) {
+      char* buf = ctx->pin_stage + (i & 1) * kPinChunk;
+      if (i >= 2) FSM_CUDA_TRY(cudaEventSynchronize(ctx->pin_ev[i & 1]));
+      parallel_copy(buf, pieces[i].h, pieces[i].n);
+      FSM_CUDA_TRY(cudaMemcpyAsync(pieces[i].d, buf, pieces[i].n, kind, st));
+      FSM_CUDA_TRY(cudaEventRecord(ctx->pin_ev[i & 1], st));
+    }
+  } else {
+    // download of piece i into chunk i % 2 once the host has copied piece
+    // i - 2 out of it; the host copies piece i - 1 while piece i downloads
+    for (int i = 0; i <= np; ++i) {
+      if (i >= 1) {
+        const int j = i - 1;  // download issued last round: copy it out
+        FSM_CUDA_TRY(cudaEventSynchronize(ctx->pin_ev[j & 1]));
+        if (i < np) {
+          char* buf = ctx->pin_stage + (i & 1) * kPinChunk;
+          FSM_CUDA_TRY(cudaMemcpyAsync(buf, pieces[i].d, pieces[i].n, kind, st));
+          FSM_CUDA_TRY(cudaEventRecord(ctx->pin_ev[i & 1], st));
+        }
+        parallel_copy(pieces[j].h, ctx->pin_stage + (j & 1) * kPinChunk, pieces[j].n);
+      } else if (np > 0) {
+        FSM_CUDA_TRY(cudaMemcpyAsync(ctx->pin_stage, pieces[0].d, pieces[0].n, kind, st));
+        FSM_CUDA_TRY(cudaEventRecord(ctx->pin_ev[0], st));
+      }
+    }
+  }
+  FSM_CUDA_TRY(cudaStreamSynchronize(st));
+  return FSM_OK;
+}
+
 // One event, host buffers in and out; fm4: the energy profile is already in
 // fm^-4 (otherwise GeV/fm^3, converted as src/FreestreamMilne.cpp:266-267).
 fsm_status run_event_host(fsm_ctx* ctx, const fsm_params* p, const float* e_gev, const float* nB,
@@ -1014,27 +1101,24 @@ fsm_status run_event_host(fsm_ctx* ctx, const fsm_params* p, const float* e_gev,
   const EventPlan& P = b->plans[0];
   cudaStream_t st = ctx->stream;
   const size_t DIM = P.DIM;
-  FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_e[0], e_gev, DIM * 4, cudaMemcpyHostToDevice, st));
-  if (P.baryon) FSM_CUDA_TRY(cudaMemcpyAsync(b->d_in_nB[0], nB, DIM * 4, cudaMemcpyHostToDevice, st));
+  auto seg = [&](const float* h, const float* dv, size_t comps) {
+    return HostSeg{const_cast<char*>(reinterpret_cast<const char*>(h)),
+                   const_cast<char*>(reinterpret_cast<const char*>(dv)), comps * DIM * 4};
+  };
+  std::vector<HostSeg> up{seg(e_gev, b->d_in_e[0], 1)};
+  if (P.baryon) up.push_back(seg(nB, b->d_in_nB[0], 1));
+  if ((s = copy_staged(ctx, st, up, true)) != FSM_OK) return s;
   s = launch(b, st);
   if (s != FSM_OK) return s;
   const fsm_outputs& d = b->d_out[0];
-  auto dl = [&](float* h, const float* dv, size_t comps) -> fsm_status {
-    if (h && dv) FSM_CUDA_TRY(cudaMemcpyAsync(h, dv, comps * DIM * 4, cudaMemcpyDeviceToHost, st));
-    return FSM_OK;
-  };
-  if ((s = dl(host_out->T, d.T, 10)) != FSM_OK) return s;
-  if ((s = dl(host_out->e, d.e, 1)) != FSM_OK) return s;
-  if ((s = dl(host_out->P, d.P, 1)) != FSM_OK) return s;
-  if ((s = dl(host_out->Pi, d.Pi, 1)) != FSM_OK) return s;
-  if ((s = dl(host_out->u, d.u, 4)) != FSM_OK) return s;
-  if ((s = dl(host_out->pi, d.pi, 10)) != FSM_OK) return s;
+  std::vector<HostSeg> down{seg(host_out->T, d.T, 10), seg(host_out->e, d.e, 1), seg(host_out->P, d.P, 1),
+                            seg(host_out->Pi, d.Pi, 1), seg(host_out->u, d.u, 4), seg(host_out->pi, d.pi, 10)};
   if (P.baryon) {
-    if ((s = dl(host_out->J, d.J, 4)) != FSM_OK) return s;
-    if ((s = dl(host_out->nB, d.nB, 1)) != FSM_OK) return s;
-    if ((s = dl(host_out->V, d.V, 4)) != FSM_OK) return s;
+    down.push_back(seg(host_out->J, d.J, 4));
+    down.push_back(seg(host_out->nB, d.nB, 1));
+    down.push_back(seg(host_out->V, d.V, 4));
   }
-  FSM_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((s = copy_staged(ctx, st, down, false)) != FSM_OK) return s;
   if ((s = check_kernel_errors(b)) != FSM_OK) return s;
   return fill_info(P, info);
 }

@@ -88,6 +88,11 @@ struct fsm_ctx {
   size_t spare_dev_cap = 0;
   char* spare_host = nullptr;
   size_t spare_host_cap = 0;
+  // two pinned chunks and their events: copies between pageable caller
+  // buffers and the device go through them, chunk by chunk, the host copy
+  // of one chunk overlapping the device copy of the next
+  char* pin_stage = nullptr;
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
 struct fsm_batch {
