@@ -296,34 +296,61 @@ __global__ void __launch_bounds__(128) fsm_prep2d_cols_long_kernel(
 // The reference's sums for the energy-dependent free-streaming time: float
 // running sums of eps^2 and eps over the converted profile, in cell order
 // (src/FreeStream.cpp:404-409).  The rounding of a running float sum depends
-// on its order, so one thread adds the cells of one event in that order (the
-// DTAU that follows is then bit-identical to the reference's); the events of
-// a batch run in parallel, one thread each, in one launch.
-__global__ void fsm_edep_sums_kernel(const float* const* __restrict__ e_gev, const int* __restrict__ cells,
-                                     int count, float* sums) {
-  const int ev = blockIdx.x * blockDim.x + threadIdx.x;
+// on its order, so one thread adds the cells of an event in that order (the
+// DTAU that follows is then bit-identical to the reference's: a reordered sum
+// of ~1e6 cells moves it by up to ~1e-4, beyond the tolerance of the moments).
+// One block per event: while thread 0 adds a chunk from shared memory (two
+// dependent float adds per cell, the sum's floor), the other threads load and
+// convert the next chunk, so the one summing thread never waits on memory.
+constexpr int kEdepChunk = 4096;
+constexpr int kEdepThreads = 256;
+
+__global__ void __launch_bounds__(kEdepThreads) fsm_edep_sums_kernel(const float* const* __restrict__ e_gev,
+                                                                    const int* __restrict__ cells, int count,
+                                                                    float* sums) {
+  __shared__ __align__(16) float buf[2][kEdepChunk];
+  const int ev = blockIdx.x;
   if (ev >= count) return;
   const float* __restrict__ e = e_gev[ev];
   const int n = cells[ev];
+  const int nch = (n + kEdepChunk - 1) / kEdepChunk;
+  const int tid = threadIdx.x;
+  // chunk 0: every thread loads
+  for (int i = tid; i < kEdepChunk && i < n; i += kEdepThreads) buf[0][i] = to_fm4(__ldg(e + i));
+  __syncthreads();
   float num = 0.0f, den = 0.0f;
-  int i = 0;
-  for (; i + 8 <= n; i += 8) {
-    float v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = to_fm4(__ldg(e + i + k));
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      num = __fadd_rn(num, __fmul_rn(v[k], v[k]));
-      den = __fadd_rn(den, v[k]);
+  for (int c = 0; c < nch; ++c) {
+    const int base = c * kEdepChunk, len = min(kEdepChunk, n - base);
+    if (tid == 0) {
+      const float* __restrict__ b = buf[c & 1];
+      int i = 0;
+      for (; i + 4 <= len; i += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(b + i);
+        num = __fadd_rn(num, __fmul_rn(v.x, v.x));
+        den = __fadd_rn(den, v.x);
+        num = __fadd_rn(num, __fmul_rn(v.y, v.y));
+        den = __fadd_rn(den, v.y);
+        num = __fadd_rn(num, __fmul_rn(v.z, v.z));
+        den = __fadd_rn(den, v.z);
+        num = __fadd_rn(num, __fmul_rn(v.w, v.w));
+        den = __fadd_rn(den, v.w);
+      }
+      for (; i < len; ++i) {
+        const float v = b[i];
+        num = __fadd_rn(num, __fmul_rn(v, v));
+        den = __fadd_rn(den, v);
+      }
+    } else if (c + 1 < nch) {
+      const int nb = (c + 1) * kEdepChunk, nlen = min(kEdepChunk, n - nb);
+      float* __restrict__ d = buf[(c + 1) & 1];
+      for (int i = tid - 1; i < nlen; i += kEdepThreads - 1) d[i] = to_fm4(__ldg(e + nb + i));
     }
+    __syncthreads();
   }
-  for (; i < n; ++i) {
-    const float v = to_fm4(__ldg(e + i));
-    num = __fadd_rn(num, __fmul_rn(v, v));
-    den = __fadd_rn(den, v);
+  if (tid == 0) {
+    sums[2 * ev] = num;
+    sums[2 * ev + 1] = den;
   }
-  sums[2 * ev] = num;
-  sums[2 * ev + 1] = den;
 }
 
 // ------------------------------------------------------- energy bookkeeping

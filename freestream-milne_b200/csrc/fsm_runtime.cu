@@ -796,7 +796,7 @@ fsm_status launch_deferred(fsm_batch* b, cudaStream_t s) {
   const int* d_cells = reinterpret_cast<const int*>(b->d_edep + align_up(ne * sizeof(float*)));
   float* d_sums = reinterpret_cast<float*>(b->d_edep + align_up(ne * sizeof(float*)) +
                                            align_up(ne * sizeof(int)));
-  fsm_edep_sums_kernel<<<(ne + 127) / 128, 128, 0, s>>>(d_ptr, d_cells, ne, d_sums);
+  fsm_edep_sums_kernel<<<ne, 256, 0, s>>>(d_ptr, d_cells, ne, d_sums);  // a block per event
   FSM_CUDA_TRY(cudaGetLastError());
   FSM_CUDA_TRY(cudaMemcpyAsync(b->h_sums, d_sums, 2 * ne * sizeof(float), cudaMemcpyDeviceToHost, s));
   FSM_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1160,7 +1160,7 @@ extern "C" fsm_status fsm_run_event_device(fsm_ctx* ctx, const fsm_params* p, co
     *reinterpret_cast<const float**>(hb) = d_e_gev;
     *reinterpret_cast<int*>(hb + 16) = pe.DIM;
     FSM_CUDA_TRY(cudaMemcpyAsync(db, hb, 32, cudaMemcpyHostToDevice, st));
-    fsm_edep_sums_kernel<<<1, 32, 0, st>>>(reinterpret_cast<const float* const*>(db),
+    fsm_edep_sums_kernel<<<1, 256, 0, st>>>(reinterpret_cast<const float* const*>(db),
                                            reinterpret_cast<const int*>(db + 16), 1,
                                            reinterpret_cast<float*>(db + 32));
     FSM_CUDA_TRY(cudaGetLastError());
