@@ -357,24 +357,56 @@ __global__ void __launch_bounds__(kEdepThreads) fsm_edep_sums_kernel(const float
 // The reference's convergence and freeze-out sums (src/FreestreamMilne.cpp:
 // 349-354, 531-545): float running sums in cell order of the initial profile
 // in fm^-4, of T^{tau tau}, and of T^{tau tau} where e hbar*c > E_FREEZE.  One
-// thread per event, in that order, so the sums equal the reference's bit for
-// bit; the events of a batch run in parallel.
-__global__ void fsm_energy_sums_kernel(const EvEnergy* __restrict__ evs, int count, float* sums) {
-  const int ev = blockIdx.x * blockDim.x + threadIdx.x;
+// thread adds them in that order, so the sums equal the reference's bit for
+// bit; a block per event stages the next chunk of the three arrays into
+// shared memory meanwhile (as the E_DEP_FS sums).  A cell outside E_FREEZE
+// is staged as +0 and added: inside starts at +0 and x + 0 = x for every
+// float the sum can reach, so the result is that of the reference's skip.
+constexpr int kEnergyChunk = 1536;
+
+__global__ void __launch_bounds__(kEdepThreads) fsm_energy_sums_kernel(const EvEnergy* __restrict__ evs,
+                                                                      int count, float* sums) {
+  __shared__ __align__(16) float sb[2][3][kEnergyChunk];
+  const int ev = blockIdx.x;
   if (ev >= count) return;
   const EvEnergy E = evs[ev];
   const float hbarc = 0.197326938f;
+  const int n = E.n;
+  const int nch = (n + kEnergyChunk - 1) / kEnergyChunk;
+  const int tid = threadIdx.x;
+  auto stage = [&](int c, int t0, int step) {
+    const int base = c * kEnergyChunk, len = min(kEnergyChunk, n - base);
+    float(*d)[kEnergyChunk] = sb[c & 1];
+    for (int i = t0; i < len; i += step) {
+      const float a = __ldg(E.e_in + base + i);
+      const float t = __ldg(E.T00 + base + i);
+      d[0][i] = E.raw ? a : to_fm4(a);
+      d[1][i] = t;
+      d[2][i] = (__fmul_rn(__ldg(E.e + base + i), hbarc) > E.e_freeze) ? t : 0.0f;
+    }
+  };
+  if (nch > 0) stage(0, tid, kEdepThreads);
+  __syncthreads();
   float before = 0.0f, after = 0.0f, inside = 0.0f;
-  for (int is = 0; is < E.n; ++is) {
-    const float a = __ldg(E.e_in + is);
-    before = __fadd_rn(before, E.raw ? a : to_fm4(a));
-    const float t = __ldg(E.T00 + is);
-    after = __fadd_rn(after, t);
-    if (__fmul_rn(__ldg(E.e + is), hbarc) > E.e_freeze) inside = __fadd_rn(inside, t);
+  for (int c = 0; c < nch; ++c) {
+    const int len = min(kEnergyChunk, n - c * kEnergyChunk);
+    if (tid == 0) {
+      const float(*b)[kEnergyChunk] = sb[c & 1];
+      for (int i = 0; i < len; ++i) {
+        before = __fadd_rn(before, b[0][i]);
+        after = __fadd_rn(after, b[1][i]);
+        inside = __fadd_rn(inside, b[2][i]);
+      }
+    } else if (c + 1 < nch) {
+      stage(c + 1, tid - 1, kEdepThreads - 1);
+    }
+    __syncthreads();
   }
-  sums[3 * ev] = before;
-  sums[3 * ev + 1] = after;
-  sums[3 * ev + 2] = inside;
+  if (tid == 0) {
+    sums[3 * ev] = before;
+    sums[3 * ev + 1] = after;
+    sums[3 * ev + 2] = inside;
+  }
 }
 
 // ------------------------------------------------------------------ prep 3D

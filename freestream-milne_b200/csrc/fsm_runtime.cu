@@ -1867,7 +1867,7 @@ extern "C" fsm_status fsm_batch_energy(fsm_batch* b, fsm_energy* out, void* stre
   cudaStream_t s = pick_stream(b->ctx, stream);
   FSM_CUDA_TRY(cudaMemcpyAsync(b->d_energy, ev.data(), (size_t)n * sizeof(fsm::EvEnergy),
                                cudaMemcpyHostToDevice, s));
-  fsm_energy_sums_kernel<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const fsm::EvEnergy*>(b->d_energy),
+  fsm_energy_sums_kernel<<<n, 256, 0, s>>>(reinterpret_cast<const fsm::EvEnergy*>(b->d_energy),
                                                          n, reinterpret_cast<float*>(b->d_energy + o_sums));
   FSM_CUDA_TRY(cudaGetLastError());
   FSM_CUDA_TRY(cudaMemcpyAsync(b->h_energy, b->d_energy + o_sums, (size_t)n * 3 * sizeof(float),
