@@ -261,6 +261,19 @@ def other_kernels(tm, steps, cells):
     return out
 
 
+def cpu_model():
+    """The host CPU's model name and logical core count."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name} ({os.cpu_count()} logical cores)"
+
+
 def issue_peak(torch, device, clocks):
     """FP32 FMA issue peak in TFLOP/s: SMs x 128 FP32 lanes x 2 FLOP x the
     maximum SM clock seen (nominal 148 x 128 x 2 x 1.965 GHz = 74.4)."""
@@ -574,7 +587,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
         rate, kind, sample = cpu_baseline(events, nthreads, budget_s=40.0)
-        cpu = {"value": rate, "unit": "events/s", "cores": nthreads, "kind": kind, "sample": sample}
+        # the same on one thread, on the first events for about 10 s
+        rate1, _, sample1 = cpu_baseline(events, 1, budget_s=10.0)
+        cpu = {"value": rate, "unit": "events/s", "cores": nthreads, "kind": kind, "sample": sample,
+               "single_thread": {"value": rate1, "sample": sample1}, "cpu_model": cpu_model()}
 
     launches_per_step = 4  # prep lines, prep pack, stream2d, landau (2D-only batch)
     if rank == 0:
