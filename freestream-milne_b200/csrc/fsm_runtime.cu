@@ -1027,6 +1027,8 @@ fsm_status copy_staged(fsm_ctx* ctx, cudaStream_t st, const std::vector<HostSeg>
   if (!pieces.empty()) {
     fsm_status s = ensure_pin_stage(ctx);
     if (s != FSM_OK) return s;
+    // a call that failed half-way may have left a copy into a chunk in flight
+    FSM_CUDA_TRY(cudaStreamSynchronize(st));
   }
   const int np = (int)pieces.size();
   if (to_device) {
