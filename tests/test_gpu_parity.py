@@ -554,3 +554,28 @@ def test_narrow_tail_tiles_keep_results():
     for o, q in zip(outs[F.TILES_TAIL], outs[F.TILES_SQUARE]):
         for k in ("T", "e", "P", "Pi", "u", "pi"):
             assert np.array_equal(o[k], q[k]), k
+
+
+def test_host_path_pinned_and_pageable_buffers(ctx):
+    """The one-event host path copies pageable caller buffers through pinned
+    chunks (several chunks for a 3D event's outputs) and pinned ones
+    directly: both give the device entry point's results bit for bit."""
+    import torch
+    p, e, nb = W.baryon3d(seed=11, side=101, neta=21, nrap=11, nphip=32)
+    pageable = ctx.run_event(p, e, nb)
+    dim = p.DIM_X * p.DIM_Y * p.DIM_ETA
+    assert 10 * dim * 4 > 8 << 20  # T alone spans several 8 MiB chunks
+    pinned = {k: torch.zeros((F.OUT_COMPS[k], dim) if F.OUT_COMPS[k] > 1 else (dim,),
+                             dtype=torch.float32).pin_memory().numpy() for k in F.OUT_COMPS}
+    e_pin = torch.from_numpy(np.ascontiguousarray(e, dtype=np.float32)).pin_memory().numpy()
+    nb_pin = torch.from_numpy(np.ascontiguousarray(nb, dtype=np.float32)).pin_memory().numpy()
+    got = ctx.run_event(p, e_pin, nb_pin, into=pinned)
+    d_e = torch.from_numpy(np.ascontiguousarray(e, dtype=np.float32)).cuda()
+    d_nb = torch.from_numpy(np.ascontiguousarray(nb, dtype=np.float32)).cuda()
+    dev = {k: torch.zeros(F.OUT_COMPS[k] * dim, dtype=torch.float32, device="cuda") for k in F.OUT_COMPS}
+    ctx.run_event_device(p, d_e.data_ptr(), d_nb.data_ptr(), {k: v.data_ptr() for k, v in dev.items()})
+    torch.cuda.synchronize()
+    for k in F.OUT_COMPS:
+        ref = dev[k].cpu().numpy().reshape(pageable[k].shape)
+        assert np.array_equal(pageable[k], ref), k
+        assert np.array_equal(got[k], ref), k
