@@ -870,8 +870,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       __syncthreads();  // buffer b is free for the load of run c + 2
     }
     // T = (sum over DIM_RAP identical rapidity copies) * d_phip / TAU
-    // (src/LandauMatch.cpp:104); T^yy = sum v sin^2 = S1 - S_cc.
+    // (src/LandauMatch.cpp:104), one scale per tile; T^yy = sum v sin^2 =
+    // S1 - S_cc.
     const float R = (float)ev.NR, dphi = ev.d_phip, TAU = ev.TAU;
+    const float tscale = __fdiv_rn(__fmul_rn(R, dphi), TAU);
     const size_t DIM = (size_t)ev.NX * ev.NY;
     float* T = ev.T;
     if (ev.charge) {
@@ -901,7 +903,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
                             stot[(5 * k + 4) * kThreads2D] + a34[k].y};
       float S[5];
 #pragma unroll
-      for (int m = 0; m < 5; ++m) S[m] = __fdiv_rn(__fmul_rn(__fmul_rn(tot[m], R), dphi), TAU);
+      for (int m = 0; m < 5; ++m) S[m] = __fmul_rn(tot[m], tscale);
       const size_t is = (size_t)(ixb + k) * ev.NY + iy;
       T[0 * DIM + is] = S[0];
       T[1 * DIM + is] = S[1];
