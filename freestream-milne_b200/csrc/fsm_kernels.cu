@@ -805,13 +805,16 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
     const int wya = tl.y0 + wyi * ly, wyb = min(wya + ly - 1, y_hi);
     const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
-    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
+    // the cells' rounding offsets in cells (a first-order correction, so one
+    // reciprocal per tile instead of a division per cell)
+    const double rdx = 1.0 / (double)DX, rdy = 1.0 / (double)DY;
+    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) * rdy);
     float ex[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int ix = ixb + k;
       const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
-      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
+      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) * rdx);
     }
     float a0[K];
     float2 a12[K], a34[K];
@@ -1240,14 +1243,17 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     const int wya = tl.y0 + wyi * ly, wyb = min(wya + ly - 1, y_hi);
     const float DX = ev.DX, DY = ev.DY, xmin = ev.xmin, ymin = ev.ymin;
     const float y = __fadd_rn(__fmul_rn((float)iy, DY), ymin);  // src/FreeStream.cpp:164
-    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) / (double)DY);
+    // the cells' rounding offsets in cells (a first-order correction, so one
+    // reciprocal per tile instead of a division per cell)
+    const double rdx = 1.0 / (double)DX, rdy = 1.0 / (double)DY;
+    const float ey = (float)(((double)y - ((double)ymin + (double)iy * (double)DY)) * rdy);
     float ex[K];
     bool act[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int ix = ixb + k;
       const float x = __fadd_rn(__fmul_rn((float)ix, DX), xmin);
-      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) / (double)DX);
+      ex[k] = (float)(((double)x - ((double)xmin + (double)ix * (double)DX)) * rdx);
       act[k] = (ix <= x_hi) && (iy <= y_hi);
     }
 #pragma unroll
