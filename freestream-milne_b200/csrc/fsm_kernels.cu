@@ -596,7 +596,7 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
                                              float2 (&a34)[kCellsPerThread],
                                              float4 (&nd0)[kCellsPerThread + 1],
                                              float4 (&nd1)[kCellsPerThread + 1], int& pox,
-                                             int& poy, float* __restrict__ stot, int* err) {
+                                             int& poy, float2* __restrict__ stot, int* err) {
   constexpr int K = kCellsPerThread;
   const int NX = ev.NX, NY = ev.NY;
   const float2 ey2 = make_float2(ey, ey);
@@ -726,11 +726,11 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       // second level of the two-level sum, thread-private slots in shared memory
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        stot[(5 * k + 0) * kThreads2D] += a0[k];
-        stot[(5 * k + 1) * kThreads2D] += a12[k].x;
-        stot[(5 * k + 2) * kThreads2D] += a12[k].y;
-        stot[(5 * k + 3) * kThreads2D] += a34[k].x;
-        stot[(5 * k + 4) * kThreads2D] += a34[k].y;
+        // packed slots: a0 of cells (0, 1) and (2, 3), then a12[k], a34[k]
+        if ((k & 1) == 1)
+          stot[(k >> 1) * kThreads2D] = __fadd2_rn(stot[(k >> 1) * kThreads2D], make_float2(a0[k - 1], a0[k]));
+        stot[(2 + k) * kThreads2D] = __fadd2_rn(stot[(2 + k) * kThreads2D], a12[k]);
+        stot[(6 + k) * kThreads2D] = __fadd2_rn(stot[(6 + k) * kThreads2D], a34[k]);
         a0[k] = 0.0f;
         a12[k] = a34[k] = make_float2(0.f, 0.f);
       }
@@ -761,7 +761,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
   float4* const tab1 = smem4 + kTabF4;
   float4* const buf0 = smem4 + 2 * kTabF4;
   float4* const buf1 = buf0 + box_cap;
-  float* const stot = reinterpret_cast<float*>(buf1 + box_cap) + threadIdx.x;
+  // per-thread moment totals, packed pairs: [a0 of cells 0,1], [a0 of 2,3],
+  // a12[0..3], a34[0..3]
+  static_assert(kCellsPerThread == 4 && kTotSlots2D == 20, "packed moment totals of 4 cells");
+  float2* const stot = reinterpret_cast<float2*>(buf1 + box_cap) + threadIdx.x;
   if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -824,7 +827,7 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       a12[k] = a34[k] = make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int m = 0; m < kTotSlots2D; ++m) stot[m * kThreads2D] = 0.0f;
+    for (int m = 0; m < kTotSlots2D / 2; ++m) stot[m * kThreads2D] = make_float2(0.f, 0.f);
     float4 nd0[K + 1], nd1[K + 1];
     int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
     // warps whose cells all lie past the grid's edge skip the runs
@@ -886,9 +889,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
       for (int k = 0; k < K; ++k) {
         if (ixb + k > x_hi || iy > y_hi) continue;
         const size_t is = (size_t)(ixb + k) * ev.NY + iy;
-        const float s0 = stot[(5 * k + 0) * kThreads2D] + a0[k];
-        const float s1 = stot[(5 * k + 1) * kThreads2D] + a12[k].x;
-        const float s2 = stot[(5 * k + 2) * kThreads2D] + a12[k].y;
+        const float2 p0 = stot[(k >> 1) * kThreads2D], p12 = stot[(2 + k) * kThreads2D];
+        const float s0 = ((k & 1) ? p0.y : p0.x) + a0[k];
+        const float s1 = p12.x + a12[k].x;
+        const float s2 = p12.y + a12[k].y;
         ev.J[0 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s0, ev.jscale), ev.DRAP), dphi);
         ev.J[1 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s1, ev.jscale), ev.DRAP), dphi);
         ev.J[2 * DIM + is] = __fmul_rn(__fmul_rn(__fmul_rn(s2, ev.jscale), ev.DRAP), dphi);
@@ -899,11 +903,10 @@ __global__ void __launch_bounds__(kThreads2D, 2) fsm_stream2d_kernel(const Ev2D*
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (ixb + k > x_hi || iy > y_hi) continue;
-      const float tot[5] = {stot[(5 * k + 0) * kThreads2D] + a0[k],
-                            stot[(5 * k + 1) * kThreads2D] + a12[k].x,
-                            stot[(5 * k + 2) * kThreads2D] + a12[k].y,
-                            stot[(5 * k + 3) * kThreads2D] + a34[k].x,
-                            stot[(5 * k + 4) * kThreads2D] + a34[k].y};
+      const float2 p0 = stot[(k >> 1) * kThreads2D], p12 = stot[(2 + k) * kThreads2D],
+                   p34 = stot[(6 + k) * kThreads2D];
+      const float tot[5] = {((k & 1) ? p0.y : p0.x) + a0[k], p12.x + a12[k].x, p12.y + a12[k].y,
+                            p34.x + a34[k].x, p34.y + a34[k].y};
       float S[5];
 #pragma unroll
       for (int m = 0; m < 5; ++m) S[m] = __fmul_rn(tot[m], tscale);
