@@ -724,11 +724,12 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
     }
     if ((pe & (ev.chunk - 1)) == 0) {
       // second level of the two-level sum, thread-private slots in shared memory
+      // packed slots: a0 of cells (0, 1) and (2, 3), then a12[k], a34[k]
+#pragma unroll
+      for (int k = 0; k < K; k += 2)
+        stot[(k >> 1) * kThreads2D] = __fadd2_rn(stot[(k >> 1) * kThreads2D], make_float2(a0[k], a0[k + 1]));
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        // packed slots: a0 of cells (0, 1) and (2, 3), then a12[k], a34[k]
-        if ((k & 1) == 1)
-          stot[(k >> 1) * kThreads2D] = __fadd2_rn(stot[(k >> 1) * kThreads2D], make_float2(a0[k - 1], a0[k]));
         stot[(2 + k) * kThreads2D] = __fadd2_rn(stot[(2 + k) * kThreads2D], a12[k]);
         stot[(6 + k) * kThreads2D] = __fadd2_rn(stot[(6 + k) * kThreads2D], a34[k]);
         a0[k] = 0.0f;
@@ -1010,7 +1011,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
                                              const PhiEntry3D* __restrict__ tab, float D, float et,
                                              float rf0, float rf1, float rb0, float rb1,
                                              const RapEta* __restrict__ rp, float jw,
-                                             float* __restrict__ sl) {
+                                             float2* __restrict__ sl) {
   using NodeT = typename Node3D<kB>::T;
   constexpr int K = kCellsPerThread;
   constexpr int kS = slots3d<kB>();
@@ -1066,7 +1067,8 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
       in_mask = __ballot_sync(0xffffffffu, ins);
     }
     for (int pc = pb; pc < min(NP, pb + 32); pc += kPhiChunk) {
-      unsigned m = (vis_mask >> (pc - pb)) & ((1u << kPhiChunk) - 1u);
+      const unsigned cm = (vis_mask >> (pc - pb)) & ((1u << kPhiChunk) - 1u);
+      unsigned m = cm;
       while (m) {
         const int bit = __ffs(m) - 1;
         m &= m - 1u;
@@ -1176,27 +1178,26 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
         // of the hypertrig table (src/LandauMatch.cpp:46-55), the rapidity
         // Jacobian and the profile norm (:101), into T^{mu nu} (and J^mu with
         // the charge norm, :120-139)
+        // (a chunk none of whose phi_p reached this warp left its partial
+        // sums at zero: nothing to fold)
+        if (!cm) continue;
         const RapEta r = *rp;
         const float cA = jw * r.A, cB = jw * r.B, cC = jw * r.C, cD = jw * r.Dt, cE = jw * r.E;
+        // packed slot pairs: (T0, T3), (T1, T2), (T4, T5), (T6, T8), (T7, T9)
+        // [, (J0, J3), (J1, J2)], each component a fused multiply-add
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          float* q = sl + k * kS * kThreads3D;
-          q[0 * kThreads3D] += a01[k].x * jw;
-          q[1 * kThreads3D] += a1c[k].x * cA;
-          q[2 * kThreads3D] += a1s[k].x * cA;
-          q[3 * kThreads3D] += a01[k].x * cD;
-          q[4 * kThreads3D] += a3[k] * cB;
-          q[5 * kThreads3D] += a4[k] * cB;
-          q[6 * kThreads3D] += a1c[k].x * cC;
-          q[7 * kThreads3D] += a5[k] * cB;
-          q[8 * kThreads3D] += a1s[k].x * cC;
-          q[9 * kThreads3D] += a01[k].x * cE;
+          float2* q = sl + k * (kS / 2) * kThreads3D;
+          auto acc = [&](int j, float2 a, float2 c) { q[j * kThreads3D] = __ffma2_rn(a, c, q[j * kThreads3D]); };
+          acc(0, make_float2(a01[k].x, a01[k].x), make_float2(jw, cD));
+          acc(1, make_float2(a1c[k].x, a1s[k].x), make_float2(cA, cA));
+          acc(2, make_float2(a3[k], a4[k]), make_float2(cB, cB));
+          acc(3, make_float2(a1c[k].x, a1s[k].x), make_float2(cC, cC));
+          acc(4, make_float2(a5[k], a01[k].x), make_float2(cB, cE));
           if (kB) {
             const float nb = ev.normB, bA = nb * r.A, bD = nb * r.Dt;
-            q[10 * kThreads3D] += a01[k].y * nb;
-            q[11 * kThreads3D] += a1c[k].y * bA;
-            q[12 * kThreads3D] += a1s[k].y * bA;
-            q[13 * kThreads3D] += a01[k].y * bD;
+            acc(5, make_float2(a01[k].y, a01[k].y), make_float2(nb, bD));
+            acc(6, make_float2(a1c[k].y, a1s[k].y), make_float2(bA, bA));
           }
           a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
           a3[k] = a4[k] = a5[k] = 0.0f;
@@ -1219,8 +1220,8 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
   constexpr int kS = slots3d<kB>();
   static_assert(kThreads3D == kWarps2D * 32 && kWarps2D == 8, "the tile shapes are laid out for 8 warps");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* const sl = slots3 + threadIdx.x;
-  auto S = [&](int m) -> float& { return sl[m * kThreads3D]; };
+  static_assert(kSlots3D % 2 == 0 && kSlots3DBaryon % 2 == 0, "slots in pairs");
+  float2* const sl = reinterpret_cast<float2*>(slots3) + threadIdx.x;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
@@ -1260,7 +1261,7 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
       act[k] = (ix <= x_hi) && (iy <= y_hi);
     }
 #pragma unroll
-    for (int m = 0; m < K * kS; ++m) S(m) = 0.0f;
+    for (int m = 0; m < K * kS / 2; ++m) sl[m * kThreads3D] = make_float2(0.f, 0.f);
     const size_t plane = (size_t)NX * NY;
     for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
       const RapEta re = ev.re[ieta * NR + irap];
@@ -1289,11 +1290,16 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     for (int k = 0; k < K; ++k) {
       if (!act[k]) continue;
       const size_t is = ((size_t)(ixb + k) * NY + iy) * NE + ieta;
-      const int b = k * kS;
-      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = S(b + m) * dphi;  // (LandauMatch.cpp:105)
+      const float2* q = sl + k * (kS / 2) * kThreads3D;
+      auto P = [&](int j) { return q[j * kThreads3D]; };
+      const float2 p0 = P(0), p1 = P(1), p2 = P(2), p3 = P(3), p4 = P(4);
+      const float t[10] = {p0.x, p1.x, p1.y, p0.y, p2.x, p2.y, p3.x, p4.x, p3.y, p4.y};
+      for (int m = 0; m < 10; ++m) ev.T[(size_t)m * DIM + is] = t[m] * dphi;  // (LandauMatch.cpp:105)
       if (baryon) {
         const float jf = ev.DRAP * dphi;  // (LandauMatch.cpp:140)
-        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = S(b + 10 + m) * jf;
+        const float2 p5 = P(5), p6 = P(6);
+        const float jv[4] = {p5.x, p6.x, p6.y, p5.y};
+        for (int m = 0; m < 4; ++m) ev.J[(size_t)m * DIM + is] = jv[m] * jf;
       }
     }
     __syncthreads();
