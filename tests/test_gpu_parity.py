@@ -79,7 +79,8 @@ def test_gpu_many_phi_nodes(ctx):
     ref = _oracle(p, e)
     ref64 = _oracle(p, e, fp64=2)
     compare_parity(got, ref, ref64, ref["tau"])
-    compare(got, ref64, ref["tau"])
+    errs = compare(got, ref64, ref["tau"])
+    print(f"2000 phi_p vs FP64: {errs}")
 
 
 def test_gpu_2d_baryon(ctx):
