@@ -625,9 +625,12 @@ __device__ __forceinline__ void stream2d_run(const Ev2D& ev, const float4* __res
       vis_mask = __ballot_sync(0xffffffffu, vis);
       in_mask = __ballot_sync(0xffffffffu, ins);
     }
-    for (unsigned m = kInterior ? (pe - pc == 32 ? 0xffffffffu : (1u << (pe - pc)) - 1u) : vis_mask; m;) {
-      const int p = pc + __ffs(m) - 1;
-      m &= m - 1u;
+    unsigned m = kInterior ? 0u : vis_mask;
+    for (int p = pc; kInterior ? (p < pe) : (m != 0u); ++p) {
+      if (!kInterior) {
+        p = pc + __ffs(m) - 1;
+        m &= m - 1u;
+      }
       const float4* e = stab + kPhiTab2D * (p - p0);
       const float4 wx = e[0], dwx = e[1], wy = e[2], dwy = e[3], tu = e[5];
       const int ox = __float_as_int(tu.z), oyn = __float_as_int(tu.w);
