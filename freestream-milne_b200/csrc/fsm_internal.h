@@ -201,6 +201,18 @@ struct PhiEntry3D {
   int oy_near;  // low 16 bits: oy (signed); bit 16: near in x; bit 17: near in y
 };
 
+// Weights of one combined node plane of a 3D event: the plane of pair (ieta,
+// irap) holds, per transverse node, the eta interpolation of the pair's two
+// source slices efl, efl+1 with the rapidity weights of that pair,
+// w0 E[efl] + w1 E[efl+1] (and b0 B[efl] + b1 B[efl+1]), w0 = (1 - efrac)
+// rf(efl), w1 = efrac rf(efl+1) (src/FreeStream.cpp:264-266 with the
+// rapidity factors of :345, 381-382).  Grouped by efl, so that the prep
+// kernel's thread of source node (efl, ix, iy) writes every plane that reads it.
+struct CombW {
+  int plane;
+  float w0, w1, b0, b1;
+};
+
 // A 3D output tile: 32 x 32 cells of one eta slice of one event.
 // A 3D output tile of eta slice ieta: shape `shape` (as the 2D shapes) from
 // (x0, y0), storing the cells below (x1, y1).
@@ -227,6 +239,14 @@ struct Ev3D {
   // eta-pair nodes [NE-1][NX][NY]: (E[e], E[e+1], B[e], B[e+1]) float4 with
   // BARYON, (E[e], E[e+1]) float2 without; E in fm^-4
   void* nodes3;
+  // combined node planes [nplanes][NX][NY]: (E, B) float2 with BARYON, E
+  // float without; plane_of[ieta * NR + irap] is the pair's plane (-1: the
+  // pair is never sampled); cw[cw_start[e] .. cw_start[e+1]) the planes that
+  // read source eta pair e
+  void* nodesc;
+  const int* plane_of;    // [NE*NR]
+  const int* cw_start;    // [NE]
+  const CombW* cw;        // [nplanes]
   float* T;               // [10][DIM]
   float* J;               // [4][DIM]
   long long cell_begin;   // first global cell index of this event in the 3D work list

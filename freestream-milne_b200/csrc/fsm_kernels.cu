@@ -412,9 +412,10 @@ __global__ void __launch_bounds__(kEdepThreads) fsm_energy_sums_kernel(const EvE
 // ------------------------------------------------------------------ prep 3D
 // Eta-pair node arrays of a 3D event: node (e, ix, iy) holds the converted
 // energy density of slices e and e+1 at (ix, iy) (and the baryon density of
-// both with BARYON), [NE-1][NX][NY], so that the stream kernel reads both
-// slices of a sample with one vector load and its lanes (consecutive y) read
-// consecutive nodes.  Thread per node.
+// both with BARYON), [NE-1][NX][NY], read by the rounding-sensitive exact
+// samples of the stream kernel; and the combined planes of every sampled
+// (slice, rapidity) pair that reads this eta pair (Ev3D::nodesc), in which the
+// stream kernel's lanes (consecutive y) read consecutive nodes.  Thread per node.
 __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict__ evs,
                                                          const CellBlock* __restrict__ blocks) {
   const CellBlock b = blocks[blockIdx.x];
@@ -428,10 +429,25 @@ __global__ void __launch_bounds__(256) fsm_prep3d_kernel(const Ev3D* __restrict_
   const size_t is = ((size_t)ix * NY + iy) * NE + e;  // the reference's cell order
   const float a0 = __ldg(ev.e_gev + is), a1 = __ldg(ev.e_gev + is + 1);
   const float E0 = ev.raw ? a0 : to_fm4(a0), E1 = ev.raw ? a1 : to_fm4(a1);
-  if (ev.baryon)
-    reinterpret_cast<float4*>(ev.nodes3)[q] = make_float4(E0, E1, __ldg(ev.nB + is), __ldg(ev.nB + is + 1));
-  else
+  // the combined planes that read this eta pair (weights uniform over the
+  // block's threads of one pair: broadcast loads), written plane by plane
+  const int c0 = __ldg(ev.cw_start + e), c1 = __ldg(ev.cw_start + e + 1);
+  if (ev.baryon) {
+    const float B0 = __ldg(ev.nB + is), B1 = __ldg(ev.nB + is + 1);
+    reinterpret_cast<float4*>(ev.nodes3)[q] = make_float4(E0, E1, B0, B1);
+    float2* C = reinterpret_cast<float2*>(ev.nodesc);
+    for (int c = c0; c < c1; ++c) {
+      const CombW w = ev.cw[c];
+      C[(size_t)w.plane * plane + r] = make_float2(fmaf(w.w0, E0, w.w1 * E1), fmaf(w.b0, B0, w.b1 * B1));
+    }
+  } else {
     reinterpret_cast<float2*>(ev.nodes3)[q] = make_float2(E0, E1);
+    float* C = reinterpret_cast<float*>(ev.nodesc);
+    for (int c = c0; c < c1; ++c) {
+      const CombW w = ev.cw[c];
+      C[(size_t)w.plane * plane + r] = fmaf(w.w0, E0, w.w1 * E1);
+    }
+  }
 }
 
 // ---------------------------------------------------------------- stream 2D
@@ -939,11 +955,6 @@ __device__ __forceinline__ float node_b0(const float4& n) { return n.z; }
 __device__ __forceinline__ float node_b1(const float4& n) { return n.w; }
 __device__ __forceinline__ float node_b0(const float2&) { return 0.0f; }
 __device__ __forceinline__ float node_b1(const float2&) { return 0.0f; }
-// (energy slice e, slice e+1) and (baryon slice e, slice e+1) pairs of a node
-__device__ __forceinline__ float2 node_e(const float4& n) { return make_float2(n.x, n.y); }
-__device__ __forceinline__ float2 node_e(const float2& n) { return n; }
-__device__ __forceinline__ float2 node_b(const float4& n) { return make_float2(n.z, n.w); }
-__device__ __forceinline__ float2 node_b(const float2&) { return make_float2(0.f, 0.f); }
 // Linear interpolation a + w (b - a) of both components, with b - a rounded
 // once (b + (-1) a is exact before the rounding) as the scalar fmaf(w, b - a, a).
 __device__ __forceinline__ float2 lerp2(float2 w, float2 a, float2 b) {
@@ -989,16 +1000,29 @@ __device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const typename No
 // D is the same for every cell, so for each phi_p the whole tile shifts by one
 // vector: the host table gives the integer offset and the fractions once, each
 // cell corrects the fraction for its own float-rounded coordinate, and the
-// lanes (consecutive y) read consecutive nodes of the eta-pair array, one
-// vector load per node for both eta slices (and both fields).  Lane l of warp
+// lanes (consecutive y) read consecutive nodes of the (slice, rapidity) pair's
+// combined plane, in which the prep kernel has already interpolated the two
+// source eta slices with their rapidity weights: one load per node for both
+// fields, a bilinear interpolation per sample.  Lane l of warp
 // w owns the cells (x0 + 4w + k, y0 + l); a thread interpolates 5 x rows for
-// its 4 samples and, without baryons, keeps those 2 x 5 nodes in registers
+// its 4 samples and keeps those 2 x 5 nodes in registers
 // while consecutive phi_p share the offset.  phi_p whose whole tile lands outside the grid are
 // skipped; runs inside it skip the in-grid test.  Moments: FP32 partial sums
 // over 16 phi_p folded, with the rapidity factors (src/LandauMatch.cpp:76-143),
 // straight into T^{mu nu} / J^mu in thread-private shared-memory slots (per
 // cell T 0..9, J 10..13): no per-rapidity slots, so that the shared memory
 // of two CTAs leaves L1 room for the tiles' node footprints.
+// Combined-plane nodes (Ev3D::nodesc): (E, B) with baryon charge, E without.
+template <bool kB> struct NodeC;
+template <> struct NodeC<true> { using T = float2; };
+template <> struct NodeC<false> { using T = float; };
+__device__ __forceinline__ float2 lerpc(float w, float2 a, float2 b) { return lerp2(make_float2(w, w), a, b); }
+__device__ __forceinline__ float lerpc(float w, float a, float b) { return fmaf(w, fmaf(a, -1.0f, b), a); }
+__device__ __forceinline__ float comb_e(float2 n) { return n.x; }
+__device__ __forceinline__ float comb_e(float n) { return n; }
+__device__ __forceinline__ float comb_b(float2 n) { return n.y; }
+__device__ __forceinline__ float comb_b(float) { return 0.0f; }
+
 template <bool kB>
 constexpr int slots3d() {
   return kB ? kSlots3DBaryon : kSlots3D;
@@ -1011,11 +1035,12 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
                                              const float (&ex)[kCellsPerThread],
                                              const bool (&act)[kCellsPerThread],
                                              const typename Node3D<kB>::T* __restrict__ N,
+                                             const typename NodeC<kB>::T* __restrict__ Nc,
                                              const PhiEntry3D* __restrict__ tab, float D, float et,
                                              float rf0, float rf1, float rb0, float rb1,
                                              const RapEta* __restrict__ rp, float jw,
                                              float2* __restrict__ sl) {
-  using NodeT = typename Node3D<kB>::T;
+  using NodeT = typename NodeC<kB>::T;
   constexpr int K = kCellsPerThread;
   constexpr int kS = slots3d<kB>();
   const int NX = ev.NX, NY = ev.NY, NP = ev.NPHI;
@@ -1028,14 +1053,10 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
     a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
     a3[k] = a4[k] = a5[k] = 0.0f;
   }
-  // eta interpolation with the rapidity weights in one pair per field:
-  // (1 - et) rf(slice) and et rf(slice + 1)
-  const float omet = 1.0f - et;
-  const float2 wE = make_float2(omet * rf0, et * rf1), wB = make_float2(omet * rb0, et * rb1);
-  // float2 nodes of the last offset stay in registers; float4 nodes (with
-  // baryons) are reloaded for every phi_p (kept, they would not fit the
-  // registers of two CTAs per SM)
-  constexpr bool kCache = !kB;
+  // the nodes of the pair's combined plane (eta interpolation and rapidity
+  // weights applied once per node by the prep kernel): (E, B) float2 with
+  // baryons, E float without; those of the last offset stay in registers
+  constexpr bool kCache = true;
   NodeT n0[K + 1], n1[K + 1];
   int pox = INT_MIN, poy = INT_MIN;  // no nodes held yet
   // phi_p in blocks of 32: the warp's lanes test the 32 phi_p at once (does
@@ -1088,8 +1109,8 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
               const int q0 = i0 * NY + j;
 #pragma unroll
               for (int r = 0; r <= K; ++r) {
-                n0[r] = __ldg(N + (q0 + r * NY));
-                n1[r] = __ldg(N + (q0 + r * NY + 1));
+                n0[r] = __ldg(Nc + (q0 + r * NY));
+                n1[r] = __ldg(Nc + (q0 + r * NY + 1));
               }
             } else {
               // clamped indices keep the loads of edge lanes inside the arrays
@@ -1098,7 +1119,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
 #pragma unroll
               for (int r = 0; r <= K; ++r) {
                 const int i = min(max(i0 + r, 0), NX - 1);
-                const NodeT* q = N + (size_t)i * NY + jj;
+                const NodeT* q = Nc + (size_t)i * NY + jj;
                 n0[r] = __ldg(q);
                 n1[r] = __ldg(q + 1);
               }
@@ -1107,30 +1128,20 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
             poy = oy;
           }
           const float uc = e.u + ey;
-          const float2 uc2 = make_float2(uc, uc);
           float v[K], vb[K];
-          float2 Bp = make_float2(0.f, 0.f), Cp = make_float2(0.f, 0.f);
+          NodeT Bp = NodeT();
 #pragma unroll
           for (int r = 0; r <= K; ++r) {
-            // y interpolation of the row on both eta slices (packed pairs)
-            const float2 B = lerp2(uc2, node_e(n0[r]), node_e(n1[r]));
-            float2 C = make_float2(0.f, 0.f);
-            if (kB) C = lerp2(uc2, node_b(n0[r]), node_b(n1[r]));
+            // y interpolation of the row (energy and charge as one packed pair)
+            const NodeT B = lerpc(uc, n0[r], n1[r]);
             if (r > 0) {
               const int q = r - 1;
-              const float tk = e.t + ex[q];
-              const float2 tk2 = make_float2(tk, tk);
-              // x interpolation, then the eta interpolation with the rapidity weights
-              const float2 L = lerp2(tk2, Bp, B);
-              v[q] = fmaf(wE.x, L.x, wE.y * L.y);
-              vb[q] = 0.0f;
-              if (kB) {
-                const float2 M = lerp2(tk2, Cp, C);
-                vb[q] = fmaf(wB.x, M.x, wB.y * M.y);
-              }
+              // x interpolation
+              const NodeT L = lerpc(e.t + ex[q], Bp, B);
+              v[q] = comb_e(L);
+              vb[q] = comb_b(L);
             }
             Bp = B;
-            Cp = C;
           }
           const FSM_FLOAT2 cs = ev.cs[p];
           if (!inside) {
@@ -1268,7 +1279,9 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
     const size_t plane = (size_t)NX * NY;
     for (int irap = ev.r_lo; irap < ev.r_hi; ++irap) {
       const RapEta re = ev.re[ieta * NR + irap];
-      if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D)) continue;
+      // a pair without a combined plane has no sample inside the grid
+      const int pl = __ldg(ev.plane_of + ieta * NR + irap);
+      if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D) || pl < 0) continue;
       const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
       const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
       const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
@@ -1279,11 +1292,13 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
         const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
         const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
         const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
-        stream3d_rap<true>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, tab, re.D,
+        const float2* Nc = reinterpret_cast<const float2*>(ev.nodesc) + (size_t)pl * plane;
+        stream3d_rap<true>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, Nc, tab, re.D,
                            re.efrac, rf0, rf1, rb0, rb1, rp, jw, sl);
       } else {
         const float2* N = reinterpret_cast<const float2*>(ev.nodes3) + (size_t)re.efl * plane;
-        stream3d_rap<false>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, tab, re.D,
+        const float* Nc = reinterpret_cast<const float*>(ev.nodesc) + (size_t)pl * plane;
+        stream3d_rap<false>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, Nc, tab, re.D,
                             re.efrac, rf0, rf1, 0.f, 0.f, rp, jw, sl);
       }
     }

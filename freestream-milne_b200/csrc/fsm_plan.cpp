@@ -527,6 +527,32 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
       }
     }
   });
+  // combined node planes: one per sampled pair (a pair whose shift exceeds
+  // the grid's extent has no sample inside and gets none), grouped by the
+  // source eta pair they read; the weights are the float products the
+  // stream kernel applied per sample before (1 - efrac) rf(efl), efrac rf(efl+1)
+  E.plane_of.assign((size_t)NE * NR, -1);
+  E.cw_start.assign(NE, 0);
+  E.cw.clear();
+  for (int efl = 0; efl < NE - 1; ++efl) {
+    E.cw_start[efl] = (int)E.cw.size();
+    for (int ieta = 0; ieta < NE; ++ieta)
+      for (int irap = E.r_lo; irap < E.r_hi; ++irap) {
+        const size_t pr = (size_t)ieta * NR + irap;
+        const RapEta& r = E.re[pr];
+        if (!live_pair[pr] || r.efl != efl) continue;
+        const float et = r.efrac, omet = 1.0f - et;
+        CombW c;
+        c.plane = (int)E.cw.size();
+        c.w0 = omet * E.rapf[(size_t)efl * NR + irap];
+        c.w1 = et * E.rapf[(size_t)(efl + 1) * NR + irap];
+        c.b0 = omet * E.rapfB[(size_t)efl * NR + irap];
+        c.b1 = et * E.rapfB[(size_t)(efl + 1) * NR + irap];
+        E.plane_of[pr] = c.plane;
+        E.cw.push_back(c);
+      }
+  }
+  E.cw_start[NE - 1] = (int)E.cw.size();
   return FSM_OK;
 }
 

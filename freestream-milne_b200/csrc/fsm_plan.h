@@ -48,6 +48,11 @@ struct EventPlan {
   std::vector<PhiEntry3D> tab3;  // [NE*NR*NPHI]
   std::vector<int> live_eta;     // live rapidity nodes per eta slice
   std::vector<float> rapf, rapfB, jac;
+  // combined node planes (Ev3D::nodesc): plane per sampled (ieta, irap) pair,
+  // weights grouped by source eta pair
+  std::vector<int> plane_of;     // [NE*NR], -1: never sampled
+  std::vector<int> cw_start;     // [NE]
+  std::vector<CombW> cw;         // [nplanes]
   int r_lo = 0, r_hi = 0;
   float norm = 0, normB = 0;
   // 2D with BARYON: fallback and output scales of the charge pass (Ev2D)

@@ -177,8 +177,8 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
   // ---- layout
   Layout L;
   struct EvOffs {
-    size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac, tab3;
-    size_t fa, sy, nodes, nodes3, T, J, in_e, in_nB, out;
+    size_t cs, tab2, chunks, axx, axy, re, rapf, rapfB, jac, tab3, plane_of, cw_start, cw;
+    size_t fa, sy, nodes, nodes3, nodesc, T, J, in_e, in_nB, out;
     size_t qfa, qsy, qnodes;  // charge pass scratch (2D with BARYON)
   };
   std::vector<EvOffs> eo(n);
@@ -218,6 +218,9 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       o.rapfB = L.take(P.rapfB.size() * 4);
       o.jac = L.take(P.jac.size() * 4);
       o.tab3 = L.take(P.tab3.size() * sizeof(PhiEntry3D));
+      o.plane_of = L.take(P.plane_of.size() * 4);
+      o.cw_start = L.take(P.cw_start.size() * 4);
+      o.cw = L.take(std::max<size_t>(P.cw.size(), 1) * sizeof(CombW));
     }
   }
   // work lists (host side first, to know their sizes)
@@ -357,6 +360,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       o.nodes = L.take((size_t)P.DIM * 16);
     } else {
       o.nodes3 = L.take((size_t)(P.p.DIM_ETA - 1) * P.p.DIM_X * P.p.DIM_Y * (P.baryon ? 16 : 8));
+      o.nodesc = L.take(std::max<size_t>(P.cw.size(), 1) * P.p.DIM_X * P.p.DIM_Y * (P.baryon ? 8 : 4));
     }
     if (!b->own_io) {
       o.T = L.take((size_t)P.DIM * 10 * 4);
@@ -443,6 +447,9 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       std::memcpy(H + o.rapfB, P.rapfB.data(), P.rapfB.size() * 4);
       std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
       parallel_copy(H + o.tab3, P.tab3.data(), P.tab3.size() * sizeof(PhiEntry3D));
+      std::memcpy(H + o.plane_of, P.plane_of.data(), P.plane_of.size() * 4);
+      std::memcpy(H + o.cw_start, P.cw_start.data(), P.cw_start.size() * 4);
+      std::memcpy(H + o.cw, P.cw.data(), P.cw.size() * sizeof(CombW));
     }
   });
   // ---- output slab layout: per event (default) or group by group
@@ -605,6 +612,10 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       e.jac = reinterpret_cast<const float*>(D + o.jac);
       e.e_gev = b->d_in_e[i];
       e.nodes3 = D + o.nodes3;
+      e.nodesc = D + o.nodesc;
+      e.plane_of = reinterpret_cast<const int*>(D + o.plane_of);
+      e.cw_start = reinterpret_cast<const int*>(D + o.cw_start);
+      e.cw = reinterpret_cast<const CombW*>(D + o.cw);
       e.tab3 = reinterpret_cast<const PhiEntry3D*>(D + o.tab3);
       e.nB = b->d_in_nB[i];
       e.T = b->d_T[i];

@@ -49,6 +49,7 @@ using fsm::LineBlock;
 using fsm::Tile2D;
 using fsm::Tile3D;
 using fsm::PhiEntry3D;
+using fsm::CombW;
 
 namespace fsm {
 namespace rt {
