@@ -37,7 +37,13 @@ sys.path.insert(0, str(ROOT / "freestream-milne_b200"))
 
 METRIC = "events/s & p99 latency, batched/served vs plain GPU path at ≤1e-5 Tμν rel err"
 FLOPS_PER_SAMPLE_2D = 55  # shift 4 + bicubic 30 + bilinear 9 + 6 moments 12
-FLOPS_PER_SAMPLE_3D_BARYON = 75  # shift 5 + 2 trilinear x 21 + 14 moments x 2
+# 3D with baryons, per in-grid sample: the reference's trilinear form counts
+# shift 5 + 2 trilinear x 21 + 14 moments x 2 = 75; the kernel interpolates
+# combined node planes (eta interpolation and rapidity weights applied once
+# per node and (slice, rapidity) pair by the prep kernel), executing shift 5
+# + 2 bilinear x 9 + 14 moments x 2 = 51 per sample
+FLOPS_PER_SAMPLE_3D_BARYON = 51
+FLOPS_PER_SAMPLE_3D_BARYON_REF = 75
 # algorithmic DRAM bytes per cell of the 2D prep and Landau kernels: prep reads
 # the profile (4 B), writes and re-reads F and its y-slopes (8 + 8 B) and
 # writes the node array (16 B); Landau reads the 6 non-zero T components of a
@@ -314,7 +320,9 @@ def event_3d(F, W, local, sp, stream, args):
            "live_samples": live, "reference_samples": ref,
            "live_samples_per_s": live / (stream_ms * 1e-3),
            "stream_tflops": live * FLOPS_PER_SAMPLE_3D_BARYON / (stream_ms * 1e-3) / 1e12,
-           "flops_per_sample": FLOPS_PER_SAMPLE_3D_BARYON}
+           "flops_per_sample": FLOPS_PER_SAMPLE_3D_BARYON,
+           "reference_form_tflops": live * FLOPS_PER_SAMPLE_3D_BARYON_REF / (stream_ms * 1e-3) / 1e12,
+           "reference_form_flops_per_sample": FLOPS_PER_SAMPLE_3D_BARYON_REF}
     b.close()
     ctx.close()
     return out
@@ -578,7 +586,9 @@ def main():
                             "achieved": ev3d["stream_tflops"], "peak": peak, "unit": "TFLOP/s",
                             "frac": ev3d["stream_tflops"] / peak,
                             "peak_source": "measured FP32 FMA probe on this GPU",
-                            "frac_of_issue_peak": ev3d["stream_tflops"] / issue_peak(torch, local, clocks)}
+                            "frac_of_issue_peak": ev3d["stream_tflops"] / issue_peak(torch, local, clocks),
+                            "flops_per_sample": FLOPS_PER_SAMPLE_3D_BARYON,
+                            "reference_form_frac": ev3d["reference_form_tflops"] / peak}
 
     files = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -63,7 +63,7 @@ extern "C" int fsm_hosttest_plan_digest(const fsm_params* p, int serial, unsigne
   mix(E.re.data(), E.re.size() * sizeof(E.re[0]));
   mix(E.rapf.data(), E.rapf.size() * 4);
   mix(E.rapfB.data(), E.rapfB.size() * 4);
-  mix(E.tab3.data(), E.tab3.size() * sizeof(E.tab3[0]));
+  if (E.tab3) mix(E.tab3->data(), E.tab3->size() * sizeof(fsm::PhiEntry3D));
   mix(E.live_eta.data(), E.live_eta.size() * sizeof(E.live_eta[0]));
   mix(&E.r_lo, sizeof(E.r_lo));
   mix(&E.r_hi, sizeof(E.r_hi));

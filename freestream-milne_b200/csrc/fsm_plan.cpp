@@ -112,7 +112,7 @@ void run_parallel(int n, int threads, const std::function<void(int)>& f) {
 void parallel_copy(void* dst, const void* src, size_t bytes) {
   constexpr size_t kPiece = (size_t)1 << 20;
   const int pieces = (int)((bytes + kPiece - 1) / kPiece);
-  parallel_for(pieces, bytes >= 4 * kPiece ? host_threads() : 1, [&](int k) {
+  parallel_for(pieces, bytes >= 2 * kPiece ? host_threads() : 1, [&](int k) {
     const size_t o = (size_t)k * kPiece;
     std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o,
                 std::min(kPiece, bytes - o));
@@ -500,7 +500,8 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
   E.ref_samples = (double)p.DIM * NR * NP;
   // 3D stream table: integer offsets and fractions of the shifted points
   // (src/FreeStream.cpp:193-212) for every live (ieta, irap) and phi_p
-  E.tab3.assign((size_t)NE * NR * NP, PhiEntry3D{0.0f, 0.0f, 0, 0});
+  E.tab3 = std::make_shared<std::vector<PhiEntry3D>>((size_t)NE * NR * NP, PhiEntry3D{0.0f, 0.0f, 0, 0});
+  std::vector<PhiEntry3D>& tab3 = *E.tab3;
   E.live_eta.assign(NE, 0);
   parallel_for(NE, plan_threads, [&](int ieta) {
     for (int irap = E.r_lo; irap < E.r_hi; ++irap) {
@@ -511,7 +512,7 @@ fsm_status plan_event(const fsm_params& in, const float* host_e_gev, EventPlan* 
         const float shx = E.cs[k].x * r.D, shy = E.cs[k].y * r.D;  // reference float products
         const double sx = -(double)shx / (double)p.DX, sy = -(double)shy / (double)p.DY;
         const double ox = std::floor(sx), oy = std::floor(sy);
-        PhiEntry3D& w = E.tab3[((size_t)ieta * NR + irap) * NP + k];
+        PhiEntry3D& w = tab3[((size_t)ieta * NR + irap) * NP + k];
         const double t = sx - ox, u = sy - oy;
         w.t = (float)t;
         w.u = (float)u;

@@ -4,6 +4,7 @@
 // table entry is rounded exactly as the reference computes it.
 #pragma once
 #include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -45,7 +46,8 @@ struct EventPlan {
   std::vector<AxisNode> axx, axy;
   // 3D tables
   std::vector<RapEta> re;
-  std::vector<PhiEntry3D> tab3;  // [NE*NR*NPHI]
+  // [NE*NR*NPHI]; shared, so that copies of a cached plan do not copy it
+  std::shared_ptr<std::vector<PhiEntry3D>> tab3;
   std::vector<int> live_eta;     // live rapidity nodes per eta slice
   std::vector<float> rapf, rapfB, jac;
   // combined node planes (Ev3D::nodesc): plane per sampled (ieta, irap) pair,

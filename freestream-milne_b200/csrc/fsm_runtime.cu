@@ -160,13 +160,40 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     std::vector<fsm_status> st(n, FSM_OK);
     std::vector<std::string> why(n);
     // (many small events also pay: ~35 us of host planning each)
+    const bool fm4 = mem && mem->input_fm4;
     parallel_for(n, (work > 2.0e5 || n >= 16) ? host_threads() : 1, [&](int i) {
       int window = 0, chunk = 0;
       bool tail = true;
       event_tuning(ctx, params[i], &window, &chunk, &tail);
-      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window,
-                         mem && mem->input_fm4, tail);
+      // a 3D plan depends on nothing but the parameters and the tuning
+      // (E_DEP_FS: also on the profile, so never cached)
+      const bool cacheable = params[i].DIM_ETA > 1 && params[i].E_DEP_FS != 1;
+      std::string key;
+      if (cacheable) {
+        const int extra[4] = {window, chunk, tail ? 1 : 0, fm4 ? 1 : 0};
+        key.assign(reinterpret_cast<const char*>(&params[i]), sizeof(fsm_params));
+        key.append(reinterpret_cast<const char*>(extra), sizeof(extra));
+        std::lock_guard<std::mutex> g(ctx->plan_mu);
+        auto it = ctx->plan_cache.find(key);
+        if (it != ctx->plan_cache.end()) {
+          b->plans[i] = *it->second;
+          return;
+        }
+      }
+      st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window, fm4,
+                         tail);
       b->plans[i].phi_chunk = chunk;
+      if (cacheable && st[i] == FSM_OK) {
+        auto cached = std::make_shared<const EventPlan>(b->plans[i]);
+        std::lock_guard<std::mutex> g(ctx->plan_mu);
+        if (ctx->plan_cache.emplace(key, std::move(cached)).second) {
+          ctx->plan_order.push_back(key);
+          if (ctx->plan_order.size() > kPlanCacheEntries) {
+            ctx->plan_cache.erase(ctx->plan_order.front());
+            ctx->plan_order.erase(ctx->plan_order.begin());
+          }
+        }
+      }
     });
     for (int i = 0; i < n; ++i)
       if (st[i] != FSM_OK) {  // the first failing event, as a serial loop would report
@@ -217,7 +244,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       o.rapf = L.take(P.rapf.size() * 4);
       o.rapfB = L.take(P.rapfB.size() * 4);
       o.jac = L.take(P.jac.size() * 4);
-      o.tab3 = L.take(P.tab3.size() * sizeof(PhiEntry3D));
+      o.tab3 = L.take(P.tab3->size() * sizeof(PhiEntry3D));
       o.plane_of = L.take(P.plane_of.size() * 4);
       o.cw_start = L.take(P.cw_start.size() * 4);
       o.cw = L.take(std::max<size_t>(P.cw.size(), 1) * sizeof(CombW));
@@ -446,7 +473,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       std::memcpy(H + o.rapf, P.rapf.data(), P.rapf.size() * 4);
       std::memcpy(H + o.rapfB, P.rapfB.data(), P.rapfB.size() * 4);
       std::memcpy(H + o.jac, P.jac.data(), P.jac.size() * 4);
-      parallel_copy(H + o.tab3, P.tab3.data(), P.tab3.size() * sizeof(PhiEntry3D));
+      parallel_copy(H + o.tab3, P.tab3->data(), P.tab3->size() * sizeof(PhiEntry3D));
       std::memcpy(H + o.plane_of, P.plane_of.data(), P.plane_of.size() * 4);
       std::memcpy(H + o.cw_start, P.cw_start.data(), P.cw_start.size() * 4);
       std::memcpy(H + o.cw, P.cw.data(), P.cw.size() * sizeof(CombW));

@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <thread>
 #include <string>
 #include <vector>
@@ -94,7 +96,14 @@ struct fsm_ctx {
   // of one chunk overlapping the device copy of the next
   char* pin_stage = nullptr;
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+  // plans of 3D events by their parameters and tuning (a 3D plan takes
+  // milliseconds of host work; its shift table is shared, not copied, by the
+  // batches that use it); at most kPlanCacheEntries, oldest dropped first
+  std::mutex plan_mu;
+  std::unordered_map<std::string, std::shared_ptr<const EventPlan>> plan_cache;
+  std::vector<std::string> plan_order;
 };
+constexpr size_t kPlanCacheEntries = 32;
 
 struct fsm_batch {
   fsm_ctx* ctx = nullptr;

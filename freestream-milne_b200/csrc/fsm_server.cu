@@ -393,11 +393,32 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
       // wave's, the requests' inputs are read-only after submit), large ones
       // on several threads; then the stream work of the wave
       lk.unlock();
-      for (size_t i = 0; i < take.size(); ++i) {
-        float* dst = reinterpret_cast<float*>(w->hin) + b->in_off[i];
-        const size_t n = take[i]->e.size();
-        parallel_copy(dst, take[i]->e.data(), n * 4);
-        if (b->plans[i].baryon) parallel_copy(dst + n, take[i]->nB.data(), n * 4);
+      {
+        // all inputs of the wave in 1 MiB pieces, spread over the worker
+        // pool in one job once the wave holds 2 MiB or more
+        struct Piece {
+          char* dst;
+          const char* src;
+          size_t bytes;
+        };
+        constexpr size_t kPiece = (size_t)1 << 20;
+        std::vector<Piece> pieces;
+        size_t total = 0;
+        auto add = [&](float* dst, const float* src, size_t n) {
+          for (size_t o = 0; o < n * 4; o += kPiece)
+            pieces.push_back(Piece{reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o,
+                                   std::min(kPiece, n * 4 - o)});
+          total += n * 4;
+        };
+        for (size_t i = 0; i < take.size(); ++i) {
+          float* dst = reinterpret_cast<float*>(w->hin) + b->in_off[i];
+          const size_t n = take[i]->e.size();
+          add(dst, take[i]->e.data(), n);
+          if (b->plans[i].baryon) add(dst + n, take[i]->nB.data(), n);
+        }
+        parallel_for((int)pieces.size(), total >= 2 * kPiece ? host_threads() : 1, [&](int k) {
+          std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+        });
       }
       w->stage_ms = std::chrono::duration<double, std::milli>(Clock::now() - t_planned).count();
       lk.lock();
