@@ -1047,11 +1047,13 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
   // moment partial sums: (energy, baryon) pairs of the weights 1, cos, sin
   // and the energy-only cos^2, cos sin, sin^2
   float2 a01[K], a1c[K], a1s[K];
-  float a3[K], a4[K], a5[K];
+  float2 a34[K];  // (cos^2, cos sin) moments of the energy
+  float a5[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
-    a3[k] = a4[k] = a5[k] = 0.0f;
+    a34[k] = make_float2(0.f, 0.f);
+    a5[k] = 0.0f;
   }
   // the nodes of the pair's combined plane (eta interpolation and rapidity
   // weights applied once per node by the prep kernel): (E, B) float2 with
@@ -1173,7 +1175,8 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
               }
             }
           }
-          const float cc = cs.x * cs.x, csn = cs.x * cs.y, ss = cs.y * cs.y;
+          const float csn = cs.x * cs.y, ss = cs.y * cs.y;
+          const float2 ccs = make_float2(cs.x * cs.x, csn);
           const float2 c2 = make_float2(cs.x, cs.x), s2 = make_float2(cs.y, cs.y);
 #pragma unroll
           for (int k = 0; k < K; ++k) {
@@ -1181,8 +1184,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
             a01[k] = __fadd2_rn(a01[k], w);
             a1c[k] = __ffma2_rn(w, c2, a1c[k]);
             a1s[k] = __ffma2_rn(w, s2, a1s[k]);
-            a3[k] = fmaf(v[k], cc, a3[k]);
-            a4[k] = fmaf(v[k], csn, a4[k]);
+            a34[k] = __ffma2_rn(make_float2(v[k], v[k]), ccs, a34[k]);
             a5[k] = fmaf(v[k], ss, a5[k]);
           }
         }
@@ -1205,7 +1207,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
           auto acc = [&](int j, float2 a, float2 c) { q[j * kThreads3D] = __ffma2_rn(a, c, q[j * kThreads3D]); };
           acc(0, make_float2(a01[k].x, a01[k].x), make_float2(jw, cD));
           acc(1, make_float2(a1c[k].x, a1s[k].x), make_float2(cA, cA));
-          acc(2, make_float2(a3[k], a4[k]), make_float2(cB, cB));
+          acc(2, a34[k], make_float2(cB, cB));
           acc(3, make_float2(a1c[k].x, a1s[k].x), make_float2(cC, cC));
           acc(4, make_float2(a5[k], a01[k].x), make_float2(cB, cE));
           if (kB) {
@@ -1214,7 +1216,8 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
             acc(6, make_float2(a1c[k].y, a1s[k].y), make_float2(bA, bA));
           }
           a01[k] = a1c[k] = a1s[k] = make_float2(0.f, 0.f);
-          a3[k] = a4[k] = a5[k] = 0.0f;
+          a34[k] = make_float2(0.f, 0.f);
+          a5[k] = 0.0f;
         }
       }
     }
