@@ -6,7 +6,10 @@
 //       of F = e/(2 pi), 16 B/cell, read by the stream kernel through staged
 //       shared-memory windows of each output tile.
 //   3D: nodes3[e][ix][iy] eta-pair nodes (e in fm^-4 of slices e and e+1, and
-//       n_B of both with BARYON), float2 / float4, read through L1.
+//       n_B of both with BARYON), float2 / float4, read by the exact boundary
+//       samples; nodesc[plane][ix][iy] combined planes (one per sampled eta
+//       slice x rapidity pair: both source slices eta-interpolated with the
+//       pair's rapidity weights), float / float2 (e, n_B), read through L1.
 //   T[10][DIM], J[4][DIM]: moments written by the stream kernels, read by the
 //   Landau kernel.  Outputs e,P,Pi,u[4],pi[10],nB,V[4] are [comp][DIM] floats.
 #pragma once
@@ -32,7 +35,11 @@ constexpr int kTileX = kWarps2D * kCellsPerThread;  // 2D output tile: x extent 
 constexpr int kThreads2D = kWarps2D * 32;
 constexpr int kPhiTab2D = 6;         // float4 per phi_p entry of the 2D table
 constexpr int kMaxRunPhi2D = 64;     // phi_p per staged run (the run's table slice is staged with it)
-constexpr int kThreads3D = 256;
+// 3D stream CTAs of 4 warps, each taking one part (warps 0-3 or 4-7 of the
+// 8-warp tile layout) of an output tile: the CTA's end-of-tile barrier then
+// waits for 4 warps of unequal work instead of 8
+constexpr int kThreads3D = 128;
+constexpr int kParts3D = kWarps2D * 32 / kThreads3D;  // work units per 3D tile
 constexpr int kThreadsLandau = 128;
 // Polls of one bounded mbarrier wait of a staged copy (a context may lower it
 // to exercise the time-out path; the drain after a time-out always uses this).

@@ -1235,16 +1235,18 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
   __shared__ int s_tile;
   constexpr int K = kCellsPerThread;
   constexpr int kS = slots3d<kB>();
-  static_assert(kThreads3D == kWarps2D * 32 && kWarps2D == 8, "the tile shapes are laid out for 8 warps");
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  static_assert(kThreads3D * kParts3D == kWarps2D * 32 && kWarps2D == 8, "the tile shapes are laid out for 8 warps");
+  const int lane = threadIdx.x & 31;
   static_assert(kSlots3D % 2 == 0 && kSlots3DBaryon % 2 == 0, "slots in pairs");
   float2* const sl = reinterpret_cast<float2*>(slots3) + threadIdx.x;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
-    const int tix = s_tile;
-    if (tix >= ntiles) return;
-    const Tile3D tl = tiles[tix];
+    const int unit = s_tile;  // part unit % kParts3D of tile unit / kParts3D
+    if (unit >= ntiles * kParts3D) return;
+    const Tile3D tl = tiles[unit / kParts3D];
+    // this warp's place in the 8-warp layout of the tile
+    const int warp = (unit % kParts3D) * (kThreads3D / 32) + (threadIdx.x >> 5);
     const Ev3D& ev = evs[tl.ev];
     const int NX = ev.NX, NY = ev.NY, NE = ev.NE, NR = ev.NR, NP = ev.NPHI;
     const int ieta = tl.ieta;
@@ -1328,14 +1330,14 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
 }
 
 // 3D events without baryon charge (float2 eta-pair nodes).
-__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
+__global__ void __launch_bounds__(kThreads3D, 2 * kParts3D) fsm_stream3d_kernel(const Ev3D* __restrict__ evs,
                                                                      const Tile3D* __restrict__ tiles,
                                                                      int ntiles, Counters* ctr) {
   stream3d_tiles<false>(evs, tiles, ntiles, &ctr->block3d);
 }
 
 // 3D events with baryon charge (float4 eta-pair nodes of energy and charge).
-__global__ void __launch_bounds__(kThreads3D, 2) fsm_stream3d_baryon_kernel(
+__global__ void __launch_bounds__(kThreads3D, 2 * kParts3D) fsm_stream3d_baryon_kernel(
     const Ev3D* __restrict__ evs, const Tile3D* __restrict__ tiles, int ntiles, Counters* ctr) {
   stream3d_tiles<true>(evs, tiles, ntiles, &ctr->block3d_b);
 }

@@ -748,7 +748,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_kernel, kThreads3D,
                                                                b->smem3));
-    b->grid3 = std::max(1, std::min(b->ntiles3 - b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
+    b->grid3 = std::max(1, std::min((b->ntiles3 - b->ntiles3b) * kParts3D, ctx->num_sms * std::max(occ, 1)));
   }
   if (b->ntiles3b) {
     fsm_status ss = ensure_dyn_smem((const void*)fsm_stream3d_baryon_kernel, ctx->device, b->smem3b,
@@ -757,7 +757,7 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
     int occ = 0;
     FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fsm_stream3d_baryon_kernel,
                                                                kThreads3D, b->smem3b));
-    b->grid3b = std::max(1, std::min(b->ntiles3b, ctx->num_sms * std::max(occ, 1)));
+    b->grid3b = std::max(1, std::min(b->ntiles3b * kParts3D, ctx->num_sms * std::max(occ, 1)));
   }
   if (mem && mem->dev)
     FSM_CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int) * 4, mem->stream));
