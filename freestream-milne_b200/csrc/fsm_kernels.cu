@@ -995,6 +995,24 @@ __device__ __forceinline__ bool exact_sample3d(const Ev3D& ev, const typename No
   return true;
 }
 
+// exact_sample3d for (eta slice, rapidity) pair rp / irap: its eta pair, eta
+// fraction and rapidity weights are read here, on the rare exact path, rather
+// than held in registers through the phi_p loop.
+template <bool kB>
+__device__ __forceinline__ bool exact_sample3d_pair(const Ev3D& ev, const RapEta* __restrict__ rp, int irap,
+                                                    float x, float y, float c, float s, float& v, float& vb) {
+  const RapEta r = *rp;
+  const int NR = ev.NR;
+  const float rf0 = __ldg(ev.rapf + r.efl * NR + irap), rf1 = __ldg(ev.rapf + (r.efl + 1) * NR + irap);
+  float rb0 = 0.0f, rb1 = 0.0f;
+  if (kB) {
+    rb0 = __ldg(ev.rapfB + r.efl * NR + irap);
+    rb1 = __ldg(ev.rapfB + (r.efl + 1) * NR + irap);
+  }
+  const auto* N = reinterpret_cast<const typename Node3D<kB>::T*>(ev.nodes3) + (size_t)r.efl * ev.NX * ev.NY;
+  return exact_sample3d<kB>(ev, N, x, y, c, s, r.D, r.efrac, rf0, rf1, rb0, rb1, v, vb);
+}
+
 // Persistent kernel over 32 x 32 output tiles of one eta slice (largest
 // rapidity count first).  For a fixed slice and rapidity node the shift length
 // D is the same for every cell, so for each phi_p the whole tile shifts by one
@@ -1034,10 +1052,8 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
                                              int wxn, int wya, int wyb, int wyn, float y, float ey,
                                              const float (&ex)[kCellsPerThread],
                                              const bool (&act)[kCellsPerThread],
-                                             const typename Node3D<kB>::T* __restrict__ N,
                                              const typename NodeC<kB>::T* __restrict__ Nc,
-                                             const PhiEntry3D* __restrict__ tab, float D, float et,
-                                             float rf0, float rf1, float rb0, float rb1,
+                                             const PhiEntry3D* __restrict__ tab, int irap,
                                              const RapEta* __restrict__ rp, float jw,
                                              float2* __restrict__ sl) {
   using NodeT = typename NodeC<kB>::T;
@@ -1166,7 +1182,7 @@ __device__ __forceinline__ void stream3d_rap(const Ev3D& ev, int ixb, int iy, in
                 if (act[k] && (ux || uy)) {
                   // the in-grid decision depends on the rounding: reference arithmetic
                   const float x = __fadd_rn(__fmul_rn((float)(ixb + k), ev.DX), ev.xmin);
-                  in = exact_sample3d<kB>(ev, N, x, y, cs.x, cs.y, D, et, rf0, rf1, rb0, rb1, v[k], vb[k]);
+                  in = exact_sample3d_pair<kB>(ev, rp, irap, x, y, cs.x, cs.y, v[k], vb[k]);
                 }
                 if (!in) {
                   v[k] = 0.0f;
@@ -1287,24 +1303,16 @@ __device__ __forceinline__ void stream3d_tiles(const Ev3D* __restrict__ evs,
       // a pair without a combined plane has no sample inside the grid
       const int pl = __ldg(ev.plane_of + ieta * NR + irap);
       if (!(re.efl >= 1 && re.efl < NE - 1) || !isfinite(re.D) || pl < 0) continue;
-      const float rf0 = __ldg(ev.rapf + re.efl * NR + irap);
-      const float rf1 = __ldg(ev.rapf + (re.efl + 1) * NR + irap);
       const PhiEntry3D* tab = ev.tab3 + ((size_t)ieta * NR + irap) * NP;
       // rapidity Jacobian (src/LandauMatch.cpp:101) times the profile norm
       const float jw = ev.jac[irap] * ev.norm;
       const RapEta* rp = ev.re + ieta * NR + irap;
       if constexpr (kB) {
-        const float rb0 = __ldg(ev.rapfB + re.efl * NR + irap);
-        const float rb1 = __ldg(ev.rapfB + (re.efl + 1) * NR + irap);
-        const float4* N = reinterpret_cast<const float4*>(ev.nodes3) + (size_t)re.efl * plane;
         const float2* Nc = reinterpret_cast<const float2*>(ev.nodesc) + (size_t)pl * plane;
-        stream3d_rap<true>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, Nc, tab, re.D,
-                           re.efrac, rf0, rf1, rb0, rb1, rp, jw, sl);
+        stream3d_rap<true>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, Nc, tab, irap, rp, jw, sl);
       } else {
-        const float2* N = reinterpret_cast<const float2*>(ev.nodes3) + (size_t)re.efl * plane;
         const float* Nc = reinterpret_cast<const float*>(ev.nodesc) + (size_t)pl * plane;
-        stream3d_rap<false>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, N, Nc, tab, re.D,
-                            re.efrac, rf0, rf1, 0.f, 0.f, rp, jw, sl);
+        stream3d_rap<false>(ev, ixb, iy, wxa, wxb, wxn, wya, wyb, ly, y, ey, ex, act, Nc, tab, irap, rp, jw, sl);
       }
     }
     const float dphi = ev.d_phip;
