@@ -65,6 +65,9 @@ extern "C" int fsm_hosttest_plan_digest(const fsm_params* p, int serial, unsigne
   mix(E.rapfB.data(), E.rapfB.size() * 4);
   if (E.tab3) mix(E.tab3->data(), E.tab3->size() * sizeof(fsm::PhiEntry3D));
   mix(E.live_eta.data(), E.live_eta.size() * sizeof(E.live_eta[0]));
+  mix(E.plane_of.data(), E.plane_of.size() * sizeof(int));
+  mix(E.cw_start.data(), E.cw_start.size() * sizeof(int));
+  mix(E.cw.data(), E.cw.size() * sizeof(fsm::CombW));
   mix(&E.r_lo, sizeof(E.r_lo));
   mix(&E.r_hi, sizeof(E.r_hi));
   *digest = h;
@@ -91,4 +94,35 @@ extern "C" int fsm_hosttest_tiles(const fsm_params* p, int tail_tiles, int windo
   for (int s = 0; s < fsm::kShapes2D; ++s) nch[s] = E.nch[s];
   *box_elems = E.box_elems;
   return (int)t.size();
+}
+
+// The combined-plane tables of a 3D event: plane_of[NE*NR], cw_start[NE],
+// cw as (plane, w0, w1, b0, b1) float rows [cap], and per (ieta, irap) pair
+// (efl, efrac, D) [NE*NR] and the rapidity weights rapf, rapfB [NE*NR], with
+// r_lo, r_hi.  Returns the number of planes (at most cap written) or -1.
+extern "C" int fsm_hosttest_comb_planes(const fsm_params* p, int* plane_of, int* cw_start, float* cw,
+                                        int cap, float* pair3, float* rapf, float* rapfB, int* r_lohi) {
+  fsm::EventPlan E;
+  std::string why;
+  if (fsm::plan_event(*p, nullptr, &E, &why) != FSM_OK || !E.is3d) return -1;
+  const size_t np = E.re.size();
+  for (size_t i = 0; i < np; ++i) {
+    plane_of[i] = E.plane_of[i];
+    pair3[3 * i + 0] = (float)E.re[i].efl;
+    pair3[3 * i + 1] = E.re[i].efrac;
+    pair3[3 * i + 2] = E.re[i].D;
+    rapf[i] = E.rapf[i];
+    rapfB[i] = E.rapfB[i];
+  }
+  for (size_t e = 0; e < E.cw_start.size(); ++e) cw_start[e] = E.cw_start[e];
+  for (int k = 0; k < (int)E.cw.size() && k < cap; ++k) {
+    cw[5 * k + 0] = (float)E.cw[k].plane;
+    cw[5 * k + 1] = E.cw[k].w0;
+    cw[5 * k + 2] = E.cw[k].w1;
+    cw[5 * k + 3] = E.cw[k].b0;
+    cw[5 * k + 4] = E.cw[k].b1;
+  }
+  r_lohi[0] = E.r_lo;
+  r_lohi[1] = E.r_hi;
+  return (int)E.cw.size();
 }

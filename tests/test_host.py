@@ -414,3 +414,61 @@ def test_initial_conditions_match_reference(tmp_path, case):
     with pytest.raises(F.FsmError) as ei:
         F.initial_profile(q, "energy", d)
     assert ei.value.status == 3
+
+
+def test_combined_planes_cover_sampled_pairs_with_reference_weights():
+    """Every sampled (eta slice, rapidity) pair of a 3D plan has its own
+    combined plane, listed under the source eta pair it reads, with the
+    weights (1 - eta_frac) rf(efl) and eta_frac rf(efl + 1) of the reference's
+    eta interpolation and rapidity factors (src/FreeStream.cpp:264-266, 345,
+    381-382); pairs that cannot sample the grid have none."""
+    import workloads as W
+    L = ctypes.CDLL(str(ROOT / "freestream-milne_b200" / "_build" / "libfsm_hosttest.so"))
+    ip, fp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
+    L.fsm_hosttest_comb_planes.argtypes = [ctypes.POINTER(F.Params), ip, ip, fp, ctypes.c_int,
+                                           fp, fp, fp, ip]
+    for p in (W.baryon3d(seed=1, side=41, neta=51, nrap=41)[0],
+              W.baryon3d(seed=2, side=31, neta=25, nrap=21, nphip=40)[0]):
+        NE, NR = p.DIM_ETA, p.DIM_RAP
+        plane_of = np.zeros(NE * NR, np.int32)
+        cw_start = np.zeros(NE, np.int32)
+        cap = NE * NR
+        cw = np.zeros((cap, 5), np.float32)
+        pair3 = np.zeros((NE * NR, 3), np.float32)
+        rapf = np.zeros(NE * NR, np.float32)
+        rapfB = np.zeros(NE * NR, np.float32)
+        lohi = np.zeros(2, np.int32)
+        c = lambda a, t: a.ctypes.data_as(t)
+        n = L.fsm_hosttest_comb_planes(ctypes.byref(p), c(plane_of, ip), c(cw_start, ip), c(cw, fp), cap,
+                                       c(pair3, fp), c(rapf, fp), c(rapfB, fp), c(lohi, ip))
+        assert 0 < n <= cap
+        efl, efrac, D = pair3[:, 0].astype(int), pair3[:, 1], pair3[:, 2]
+        irap = np.tile(np.arange(NR), NE)
+        bound = np.float32((p.DIM_X + p.DIM_Y) * max(p.DX, p.DY))
+        sampled = ((irap >= lohi[0]) & (irap < lohi[1]) & (efl >= 1) & (efl < NE - 1) &
+                   np.isfinite(D) & (np.abs(D) <= bound))
+        assert np.array_equal(plane_of >= 0, sampled)
+        assert sorted(plane_of[sampled].tolist()) == list(range(n))
+        assert cw_start[-1] == n and np.all(np.diff(cw_start) >= 0)
+        pair_of_plane = np.full(n, -1)
+        pair_of_plane[plane_of[sampled]] = np.nonzero(sampled)[0]
+        for e in range(NE - 1):
+            for k in range(cw_start[e], cw_start[e + 1]):
+                pr = pair_of_plane[int(cw[k, 0])]
+                assert efl[pr] == e
+                r = irap[pr]
+                om = np.float32(1.0) - efrac[pr]
+                assert cw[k, 1] == np.float32(om * rapf[e * NR + r])
+                assert cw[k, 2] == np.float32(efrac[pr] * rapf[(e + 1) * NR + r])
+                assert cw[k, 3] == np.float32(om * rapfB[e * NR + r])
+                assert cw[k, 4] == np.float32(efrac[pr] * rapfB[(e + 1) * NR + r])
+        # the combined value is the reference's eta interpolation of the
+        # rapidity-weighted slices to float rounding
+        rng = np.random.default_rng(0)
+        e0, e1 = rng.uniform(0, 50, n).astype(np.float32), rng.uniform(0, 50, n).astype(np.float32)
+        k = np.argsort(cw[:n, 0])
+        pr = pair_of_plane[np.arange(n)]
+        got = cw[k, 1] * e0 + cw[k, 2] * e1
+        f, r0 = efrac[pr].astype(np.float64), efl[pr]
+        ref = ((1 - f) * e0 * rapf[r0 * NR + irap[pr]] + f * e1 * rapf[(r0 + 1) * NR + irap[pr]])
+        assert np.allclose(got, ref, rtol=1e-6, atol=1e-30 + 1e-6 * np.abs(ref).max())
