@@ -183,13 +183,18 @@ fsm_status batch_build(fsm_ctx* ctx, int n, const fsm_params* params, const floa
       st[i] = plan_event(params[i], host_e ? host_e[i] : nullptr, &b->plans[i], &why[i], window, fm4,
                          tail);
       b->plans[i].phi_chunk = chunk;
-      if (cacheable && st[i] == FSM_OK) {
+      const size_t tab_bytes = b->plans[i].tab3 ? b->plans[i].tab3->size() * sizeof(PhiEntry3D) : 0;
+      if (cacheable && st[i] == FSM_OK && tab_bytes <= kPlanCacheMaxPlan) {
         auto cached = std::make_shared<const EventPlan>(b->plans[i]);
         std::lock_guard<std::mutex> g(ctx->plan_mu);
         if (ctx->plan_cache.emplace(key, std::move(cached)).second) {
           ctx->plan_order.push_back(key);
-          if (ctx->plan_order.size() > kPlanCacheEntries) {
-            ctx->plan_cache.erase(ctx->plan_order.front());
+          ctx->plan_bytes += tab_bytes;
+          while (ctx->plan_order.size() > kPlanCacheEntries || ctx->plan_bytes > kPlanCacheBytes) {
+            auto old = ctx->plan_cache.find(ctx->plan_order.front());
+            const auto& t = old->second->tab3;
+            ctx->plan_bytes -= t ? t->size() * sizeof(PhiEntry3D) : 0;
+            ctx->plan_cache.erase(old);
             ctx->plan_order.erase(ctx->plan_order.begin());
           }
         }

@@ -98,12 +98,17 @@ struct fsm_ctx {
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   // plans of 3D events by their parameters and tuning (a 3D plan takes
   // milliseconds of host work; its shift table is shared, not copied, by the
-  // batches that use it); at most kPlanCacheEntries, oldest dropped first
+  // batches that use it); at most kPlanCacheEntries holding at most
+  // kPlanCacheBytes of shift tables, oldest dropped first; a plan whose table
+  // alone exceeds kPlanCacheMaxPlan is not kept
   std::mutex plan_mu;
   std::unordered_map<std::string, std::shared_ptr<const EventPlan>> plan_cache;
   std::vector<std::string> plan_order;
+  size_t plan_bytes = 0;
 };
 constexpr size_t kPlanCacheEntries = 32;
+constexpr size_t kPlanCacheBytes = (size_t)512 << 20;
+constexpr size_t kPlanCacheMaxPlan = (size_t)64 << 20;
 
 struct fsm_batch {
   fsm_ctx* ctx = nullptr;
