@@ -191,11 +191,11 @@ def serve_stream(args, F, W, local, rank, ctx, reps, frac3d=0.2, opts=None):
     gaps = [reqs[0][0]] + [reqs[k][0] - reqs[k - 1][0] for k in range(1, len(reqs))]
     events = [ev for _, ev in reqs]
     hydro = ["e", "P", "Pi", "u", "pi", "nB", "V"]  # the fields the reference hands to hydro
-    # 8 streams (waves overlap host planning, copies and kernels; measured
-    # burst capacity 916 / 1180 / ~1550-1680 events/s with 2 / 3 / 4-12, p99
-    # at 70 % load 23 ms with 4, 15-17 ms with 8) and one more reserved for
-    # boost-invariant waves
-    budget = dict(hbm_budget=48 << 30, host_budget=8 << 30, streams=8, stream_2d=True, outputs=hydro)
+    # 12 streams (waves overlap host planning, copies and kernels; measured
+    # burst capacity on one box with the current kernels 1705 / ~1770 / 1885
+    # events/s with 4 / 8 / 12, p99 at 70 % load 16.9 / 11.2-13.0 / 11.5 ms)
+    # and one more reserved for boost-invariant waves
+    budget = dict(hbm_budget=48 << 30, host_budget=8 << 30, streams=12, stream_2d=True, outputs=hydro)
     budget.update(opts or {})
 
     def run(rate_hz):

@@ -431,12 +431,24 @@ bool wave_launch(fsm_server* S, std::unique_lock<std::mutex>& lk, int slot) {
       else st = FSM_ERR_CUDA;
       if (w->ev[2]) cudaEventRecord(w->ev[2], s);
       if (st == FSM_OK) {
-        // only the output groups the server keeps, one copy per group
+        // only the output groups the server keeps: one copy per run of kept
+        // groups that lie back to back in the slab and in the pinned buffer
         ce = cudaSuccess;
-        for (int g = 0; g < kOutGroups && ce == cudaSuccess; ++g) {
-          if (w->hgrp[g] == (size_t)-1) continue;
+        for (int g = 0; g < kOutGroups && ce == cudaSuccess;) {
+          if (w->hgrp[g] == (size_t)-1) {
+            ++g;
+            continue;
+          }
+          size_t elems = b->group_elems[g];
+          int h = g + 1;
+          while (h < kOutGroups && w->hgrp[h] == w->hgrp[g] + elems &&
+                 b->group_off[h] == b->group_off[g] + elems) {
+            elems += b->group_elems[h];
+            ++h;
+          }
           ce = cudaMemcpyAsync(w->hout + w->hgrp[g] * 4, b->d_mem + b->out_slab_off + b->group_off[g] * 4,
-                               b->group_elems[g] * 4, cudaMemcpyDeviceToHost, s);
+                               elems * 4, cudaMemcpyDeviceToHost, s);
+          g = h;
         }
         if (ce == cudaSuccess)
           ce = cudaMemcpyAsync(w->hout + w->houtbytes - 16, b->d_err, 16, cudaMemcpyDeviceToHost, s);
