@@ -18,6 +18,11 @@ Printed JSON line (rank 0):
   roofline     fused stream kernel, FP32 pipe: algorithmic FLOPs / measured
                launch time vs the measured FP32 FMA peak of the same GPU
   cpu_baseline the reference's own sources (or the oracle port) on host cores
+  served       Poisson streams of mixed 2D/3D requests (and 2D only) through
+               the continuous-batching server: burst capacity, p50/p99 at 70 %
+               load, per-wave breakdown, against the one-event host path
+  event_3d     one 131^2 x 51 baryon event (21 rapidities, 100 phi_p) with the
+               3D stream kernel's roofline
 
 `--impl reference` times the reference's CPU implementation on the same
 workload and prints the same metric.
